@@ -1,0 +1,220 @@
+// cg.cu -- congrad: CGNE on M^dagger M (rhmc/cheisdwf.f:1064-1157).
+//
+// Vectors are FP64 as in the reference; the scalars alpha, beta, alphad,
+// alphan, betad, betan and resid are REAL*4 there (implicit typing), so they
+// are REAL*4 here too.  The reference accumulates alphad and betan
+// element by element in REAL*4 (:1105-1108, :1133-1136), an order no parallel
+// reduction can follow; here each sum is formed in FP64 with a fixed tree and
+// rounded to REAL*4 once.
+#include <cstring>
+
+#include "cg.h"
+#include "dwf_stencil.cuh"
+
+namespace chdwf {
+
+struct LdCg {
+    const double2* __restrict__ p;
+    __device__ __forceinline__ double2 operator()(int64_t j) const { return __ldg(p + j); }
+};
+
+__device__ __forceinline__ bool cg_last_block(double v, double* part, unsigned* count,
+                                              double* total) {
+    __shared__ double sh[kThreads / 32];
+    __shared__ bool is_last;
+    v = block_sum<kThreads>(v, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = v;
+        __threadfence();
+        is_last = (atomicAdd(count, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += ((volatile double*)part)[i];
+    s = block_sum<kThreads>(s, sh);
+    if (threadIdx.x == 0) {
+        *total = s;
+        *count = 0;
+    }
+    return true;
+}
+
+// x1 = M p ; alphad = |x1|^2 ; alpha = alphan/alphad   (:1093-1117)
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_cg1(CgArgs a) {
+    CgCtl* c = a.ctl;
+    if (c->done) return;
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double loc = 0.0;
+    if (p < a.g.npts) {
+        const PointIdx q = point_of(a.g, p);
+        double2 acc[2][4];
+        dwf_apply_point<false, IMASS>(acc, LdCg{a.p}, a.g, q, a.chif, a.diag, a.hpin, a.apbc != 0);
+#pragma unroll
+        for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                a.x1[p + a.g.cs * (d + 4 * f)] = acc[f][d];
+                loc += acc[f][d].x * acc[f][d].x + acc[f][d].y * acc[f][d].y;
+            }
+    }
+    double tot;
+    if (!cg_last_block(loc, a.part, &c->count1, &tot)) return;
+    if (threadIdx.x == 0 && c->nx > 1) {
+        const float alphad = (float)tot;
+        c->alpha = c->alphan / alphad;
+    }
+}
+
+// x2 = M^dagger x1 ; x += alpha p (nx>1) ; r -= alpha x2 ; betan = |r|^2 (:1119-1141)
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_cg2(CgArgs a) {
+    CgCtl* c = a.ctl;
+    if (c->done) return;
+    const int nx = c->nx;
+    const double alpha = (double)c->alpha;
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double loc = 0.0;
+    if (p < a.g.npts) {
+        const PointIdx q = point_of(a.g, p);
+        double2 acc[2][4];
+        dwf_apply_point<true, IMASS>(acc, LdCg{a.x1}, a.g, q, a.chif, a.diag, a.hpin, a.apbc != 0);
+#pragma unroll
+        for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const int64_t e = p + a.g.cs * (d + 4 * f);
+                if (nx > 1) a.x[e] = zadd(a.x[e], zscal(alpha, a.p[e]));
+                const double2 r = zsub(a.r[e], zscal(alpha, acc[f][d]));
+                a.r[e] = r;
+                loc += r.x * r.x + r.y * r.y;
+            }
+    }
+    double tot;
+    if (!cg_last_block(loc, a.part, &c->count2, &tot)) return;
+    if (threadIdx.x == 0) {
+        const float betan = (float)tot;
+        float beta = betan / c->betad;
+        c->betad = betan;
+        c->alphan = betan;
+        if (nx == 1) beta = 0.0f;
+        c->beta = beta;
+        if (betan < c->resid) {
+            c->done = 1;
+            c->iters = nx;
+        } else if (nx >= c->niterc) {
+            c->done = 2;
+            c->iters = nx;
+        }
+        if (!(betan == betan)) { c->done = 3; c->iters = nx; }
+        if (c->done && a.hflag) {
+            *(volatile int*)a.hflag = c->done;
+            __threadfence_system();
+        }
+        // all other blocks finished (they were counted), so the iteration
+        // index can advance for the next launches
+        if (!c->done) c->nx = nx + 1;
+    }
+}
+
+// p = r + beta p ; next iteration  (:1147-1150)
+__global__ void __launch_bounds__(kThreads) k_cg3(CgArgs a) {
+    CgCtl* c = a.ctl;
+    if (c->done) return;
+    const double beta = (double)c->beta;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < a.g.kferm) a.p[i] = zadd(a.r[i], zscal(beta, a.p[i]));
+}
+
+CgWork::~CgWork() { release(); }
+
+void CgWork::release() {
+    if (ctl) cudaFree(ctl);
+    if (part) cudaFree(part);
+    if (hflag_host) cudaFreeHost(hflag_host);
+    if (x1) cudaFree(x1);
+    if (p) cudaFree(p);
+    if (r) cudaFree(r);
+    ctl = nullptr; part = nullptr; hflag_host = nullptr; x1 = p = r = nullptr;
+}
+
+cudaError_t CgWork::ensure(const Geom& g) {
+    if (ctl && g.kferm == geom.kferm && g.L == geom.L && g.Lt == geom.Lt) return cudaSuccess;
+    release();
+    geom = g;
+    cudaError_t e;
+    if ((e = cudaMalloc(&ctl, sizeof(CgCtl)))) return e;
+    const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+    if ((e = cudaMalloc(&part, sizeof(double) * (nb + 64)))) return e;
+    if ((e = cudaMalloc(&x1, sizeof(double2) * g.kferm))) return e;
+    if ((e = cudaMalloc(&p, sizeof(double2) * g.kferm))) return e;
+    if ((e = cudaMalloc(&r, sizeof(double2) * g.kferm))) return e;
+    if ((e = cudaHostAlloc(&hflag_host, sizeof(int), cudaHostAllocMapped))) return e;
+    if ((e = cudaHostGetDevicePointer((void**)&hflag_dev, hflag_host, 0))) return e;
+    return cudaSuccess;
+}
+
+cudaError_t cg_solve(CgWork& w, const Geom& g, const double2* phi, float res, const float* chif,
+                     float am3, float hpin, int imass, int ibound, double2* x, int* itercg,
+                     int* status, cudaStream_t st) {
+    cudaError_t e = w.ensure(g);
+    if (e) return e;
+    CgCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.nx = 1;
+    hc.alpha = 1.0f;                                  // :1090-1091
+    hc.betad = 1.0f;
+    hc.resid = (float)g.kferm * res * res;            // :1076
+    hc.niterc = (int)(g.Ls * (int64_t)g.kvol);        // niterc = kthird*kvol
+    if ((e = cudaMemcpyAsync(w.ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st))) return e;
+    *w.hflag_host = 0;
+    // p = x ; r = Phi (:1086-1089)
+    cudaMemcpyAsync(w.p, x, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(w.r, phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+    CgArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = g;
+    a.x = x; a.p = w.p; a.r = w.r; a.x1 = w.x1;
+    a.chif = chif;
+    a.diag = (double)(2.0f * ((3.0f - am3) + 1.0f));
+    a.hpin = (double)hpin;
+    a.apbc = ibound == -1;
+    a.ctl = w.ctl;
+    a.part = w.part;
+    a.hflag = w.hflag_dev;
+    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const unsigned nbf = (unsigned)((g.kferm + kThreads - 1) / kThreads);
+    const int chunk = 16;
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    int64_t launched = 0;
+    int nchunk = 0;
+    const int64_t cap = hc.niterc;
+    while (launched < cap) {
+        for (int c = 0; c < chunk && launched < cap; c++, launched++) {
+            if (imass == 3) { k_cg1<3><<<nb, kThreads, 0, st>>>(a); k_cg2<3><<<nb, kThreads, 0, st>>>(a); }
+            else { k_cg1<1><<<nb, kThreads, 0, st>>>(a); k_cg2<1><<<nb, kThreads, 0, st>>>(a); }
+            k_cg3<<<nbf, kThreads, 0, st>>>(a);
+        }
+        cudaEventRecord(ev[nchunk & 1], st);
+        if (nchunk >= 1) {
+            cudaEventSynchronize(ev[(nchunk - 1) & 1]);
+            if (*(volatile int*)w.hflag_host) break;
+        }
+        nchunk++;
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if ((e = cudaGetLastError())) return e;
+    CgCtl hr;
+    if ((e = cudaMemcpyAsync(&hr, w.ctl, sizeof(hr), cudaMemcpyDeviceToHost, st))) return e;
+    if ((e = cudaStreamSynchronize(st))) return e;
+    *itercg = hr.iters;
+    *status = hr.done == 1 ? 0 : (hr.done == 2 ? 1 : 2);
+    return cudaSuccess;
+}
+
+}  // namespace chdwf

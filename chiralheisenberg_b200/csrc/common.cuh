@@ -1,0 +1,104 @@
+// common.cuh -- shared device helpers for the chiral-Heisenberg domain-wall
+// fermion kernels (sm_100a).
+//
+// Field layout in HBM is the reference's own Fortran layout
+// (rhmc/cheisdwf.f:50-54, :2644-2645), 0-based:
+//   spinor element (s, x, y, t, dirac d, flavour f) at
+//     s + Ls*(x + L*(y + L*t)) + cs*(d + 4*f),   cs = Ls*kvol,
+// i.e. eight component planes ("SoA over the 8 complex components"), each
+// point-fastest with the fifth dimension s innermost.  One thread owns one
+// lattice point (s, site) and all eight components, so every plane access of
+// a warp is a contiguous, coalesced run of 16-byte (FP64) elements and the
+// host<->device copies at the drop-in boundary are plain memcpys.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace chdwf {
+
+struct Geom {
+    int L, Lt, Ls;
+    int kvol;         // L*L*Lt
+    int64_t npts;     // kvol*Ls
+    int64_t cs;       // component-plane stride = npts
+    int64_t kferm;    // 8*npts complex numbers
+};
+
+inline Geom make_geom(int L, int Lt, int Ls) {
+    Geom g;
+    g.L = L; g.Lt = Lt; g.Ls = Ls;
+    g.kvol = L * L * Lt;
+    g.npts = (int64_t)g.kvol * Ls;
+    g.cs = g.npts;
+    g.kferm = 8 * g.npts;
+    return g;
+}
+
+// ---- exact (non-contracted) double-complex arithmetic ---------------------
+// The FP64 operator reproduces the reference's per-element operation order
+// without fused multiply-add, so it agrees bit for bit with the CPU oracle.
+__device__ __forceinline__ double2 zadd(double2 a, double2 b) {
+    return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) {
+    return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 zmuli(double2 a) { return make_double2(-a.y, a.x); }
+__device__ __forceinline__ double2 zscal(double s, double2 a) {
+    return make_double2(__dmul_rn(s, a.x), __dmul_rn(s, a.y));
+}
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+    return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                        __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+// x + (i? i*y : y) or x - (...)
+__device__ __forceinline__ double2 zcomb(double2 x, double2 y, bool use_i, int sgn) {
+    double2 t = use_i ? zmuli(y) : y;
+    return sgn > 0 ? zadd(x, t) : zsub(x, t);
+}
+
+// ---- single-precision complex (mixed-precision path; contraction allowed) --
+__device__ __forceinline__ float2 zadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 zsub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 zmuli(float2 a) { return make_float2(-a.y, a.x); }
+__device__ __forceinline__ float2 zscal(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+__device__ __forceinline__ float2 zmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 zconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 zcomb(float2 x, float2 y, bool use_i, int sgn) {
+    float2 t = use_i ? zmuli(y) : y;
+    return sgn > 0 ? zadd(x, t) : zsub(x, t);
+}
+
+template <class T> struct real_of;
+template <> struct real_of<double2> { typedef double type; };
+template <> struct real_of<float2> { typedef float type; };
+template <class T> __device__ __forceinline__ T zmake(typename real_of<T>::type re,
+                                                      typename real_of<T>::type im);
+template <> __device__ __forceinline__ double2 zmake<double2>(double re, double im) {
+    return make_double2(re, im);
+}
+template <> __device__ __forceinline__ float2 zmake<float2>(float re, float im) {
+    return make_float2(re, im);
+}
+
+// ---- block reductions (deterministic order) -------------------------------
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NT / 32; i++) r += sh[i];
+    }
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+
+}  // namespace chdwf

@@ -1,0 +1,173 @@
+// dslash.cu -- FP64 domain-wall operator kernels (rhmc/cheisdwf.f:2634-3501)
+// and the chi-force contraction derivs (rhmc/cheisdwf.f:747-849).
+#include "dwf_stencil.cuh"
+#include "internal.h"
+
+namespace chdwf {
+
+struct LdF64 {
+    const double2* __restrict__ p;
+    __device__ __forceinline__ double2 operator()(int64_t j) const { return __ldg(p + j); }
+};
+
+template <bool DAG, int IMASS>
+__global__ void __launch_bounds__(kThreads) k_dslash64(double2* __restrict__ out,
+                                                      const double2* __restrict__ in,
+                                                      const float* __restrict__ chif, Geom g,
+                                                      double diag, double hpin, int apbc) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= g.npts) return;
+    const PointIdx q = point_of(g, p);
+    double2 acc[2][4];
+    dwf_apply_point<DAG, IMASS>(acc, LdF64{in}, g, q, chif, diag, hpin, apbc != 0);
+#pragma unroll
+    for (int f = 0; f < 2; f++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) out[p + g.cs * (d + 4 * f)] = acc[f][d];
+}
+
+static inline float diag_of(float am3) { return 2.0f * ((3.0f - am3) + 1.0f); }  // :2652
+
+void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
+                     const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
+    const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+    const double diag = (double)diag_of(am3), hp = (double)hpin;
+    const int apbc = ibound == -1;
+#define LAUNCH(D, I) k_dslash64<D, I><<<(unsigned)nb, kThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc)
+    if (!dag) {
+        if (imass == 1) LAUNCH(false, 1); else if (imass == 3) LAUNCH(false, 3); else LAUNCH(false, 0);
+    } else {
+        if (imass == 1) LAUNCH(true, 1); else if (imass == 3) LAUNCH(true, 3); else LAUNCH(true, 0);
+    }
+#undef LAUNCH
+}
+
+// M on npole stacked two-slice lattices: blockIdx.y = pole.
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_wall_dslash64(double2* __restrict__ out,
+                                                           const double2* __restrict__ in,
+                                                           const float* __restrict__ chif,
+                                                           Geom g2, double diag, double hpin,
+                                                           int apbc) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= g2.npts) return;
+    const int64_t off = (int64_t)blockIdx.y * g2.kferm;
+    const PointIdx q = point_of(g2, p);
+    double2 acc[2][4];
+    dwf_apply_point<false, IMASS>(acc, LdF64{in + off}, g2, q, chif, diag, hpin, apbc != 0);
+#pragma unroll
+    for (int f = 0; f < 2; f++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) out[off + p + g2.cs * (d + 4 * f)] = acc[f][d];
+}
+
+void launch_wall_dslash64(int npole, double2* out, const double2* in, const float* chif,
+                          const Geom& g, float am3, float hpin, int ibound, int imass,
+                          cudaStream_t st) {
+    const Geom g2 = make_geom(g.L, g.Lt, 2);
+    const unsigned nb = (unsigned)((g2.npts + kThreads - 1) / kThreads);
+    const dim3 grid(nb, npole);
+    const double diag = (double)diag_of(am3), hp = (double)hpin;
+    const int apbc = ibound == -1;
+    if (imass == 1) k_wall_dslash64<1><<<grid, kThreads, 0, st>>>(out, in, chif, g2, diag, hp, apbc);
+    else if (imass == 3) k_wall_dslash64<3><<<grid, kThreads, 0, st>>>(out, in, chif, g2, diag, hp, apbc);
+    else k_wall_dslash64<0><<<grid, kThreads, 0, st>>>(out, in, chif, g2, diag, hp, apbc);
+}
+
+// ---- derivs ---------------------------------------------------------------
+// One term of derivs for one site and one Dirac index: R and X2 of both
+// flavours; REAL*8 products, REAL*4 accumulation (cheisdwf.f:762-845).
+template <int IMASS>
+__device__ __forceinline__ void derivs_term(float* f, double2 r1, double2 r2, double2 y1,
+                                            double2 y2, double tzi, bool lower) {
+    r1 = zconj(r1);
+    r2 = zconj(r2);
+    const double2 c1 = zscal(tzi, zadd(zmul(r1, y2), zmul(r2, y1)));
+    const double2 c2 = zscal(tzi, zsub(zmul(r1, y2), zmul(r2, y1)));
+    const double2 c3 = zscal(tzi, zsub(zmul(r1, y1), zmul(r2, y2)));
+    if (IMASS == 1) {
+        f[0] = (float)__dsub_rn((double)f[0], c1.x);
+        f[1] = (float)__dsub_rn((double)f[1], c2.y);
+        f[2] = (float)__dsub_rn((double)f[2], c3.x);
+    } else if (IMASS == 3) {
+        if (lower) {   // Dirac 1,2 (:806-823)
+            f[0] = (float)__dsub_rn((double)f[0], c1.y);
+            f[1] = (float)__dadd_rn((double)f[1], c2.x);
+            f[2] = (float)__dsub_rn((double)f[2], c3.y);
+        } else {       // Dirac 3,4 (:825-843)
+            f[0] = (float)__dadd_rn((double)f[0], c1.y);
+            f[1] = (float)__dsub_rn((double)f[1], c2.x);
+            f[2] = (float)__dadd_rn((double)f[2], c3.y);
+        }
+    }
+}
+
+// Per site, poles in order k=1..npole, Dirac 1,2 (R at s=Ls, X2 at s=1)
+// then Dirac 3,4 (R at s=1, X2 at s=Ls) -- the accumulation order of
+// qmrherm's force branch (cheisdwf.f:733-740) calling derivs.
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_derivs_walls(int npole,
+                                                          const double2* __restrict__ xw,
+                                                          const double2* __restrict__ x2w,
+                                                          const double* __restrict__ anum1,
+                                                          float* __restrict__ dS, Geom g2) {
+    const int site = blockIdx.x * blockDim.x + threadIdx.x;
+    if (site >= g2.kvol) return;
+    float f[3] = {dS[site], dS[site + g2.kvol], dS[site + 2 * g2.kvol]};
+    for (int k = 0; k < npole; k++) {
+        const double tzi = -2 * anum1[k];
+        const int64_t off = (int64_t)k * g2.kferm;
+        const int64_t pL = 1 + 2 * (int64_t)site, p0 = 2 * (int64_t)site;
+#pragma unroll
+        for (int d = 0; d < 2; d++)
+            derivs_term<IMASS>(f, xw[off + pL + g2.cs * d], xw[off + pL + g2.cs * (d + 4)],
+                               x2w[off + p0 + g2.cs * d], x2w[off + p0 + g2.cs * (d + 4)], tzi, true);
+#pragma unroll
+        for (int d = 2; d < 4; d++)
+            derivs_term<IMASS>(f, xw[off + p0 + g2.cs * d], xw[off + p0 + g2.cs * (d + 4)],
+                               x2w[off + pL + g2.cs * d], x2w[off + pL + g2.cs * (d + 4)], tzi, false);
+    }
+    dS[site] = f[0];
+    dS[site + g2.kvol] = f[1];
+    dS[site + 2 * g2.kvol] = f[2];
+}
+
+void launch_derivs_walls(int npole, const double2* xw, const double2* x2w, const double* anum1,
+                         int imass, float* dSdchi, const Geom& g, cudaStream_t st) {
+    const Geom g2 = make_geom(g.L, g.Lt, 2);
+    const unsigned nb = (unsigned)((g.kvol + kThreads - 1) / kThreads);
+    if (imass == 1) k_derivs_walls<1><<<nb, kThreads, 0, st>>>(npole, xw, x2w, anum1, dSdchi, g2);
+    else if (imass == 3) k_derivs_walls<3><<<nb, kThreads, 0, st>>>(npole, xw, x2w, anum1, dSdchi, g2);
+}
+
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_derivs_full(const double2* __restrict__ R,
+                                                         const double2* __restrict__ X2,
+                                                         double tzi, float* __restrict__ dS,
+                                                         Geom g) {
+    const int site = blockIdx.x * blockDim.x + threadIdx.x;
+    if (site >= g.kvol) return;
+    float f[3] = {dS[site], dS[site + g.kvol], dS[site + 2 * g.kvol]};
+    const int64_t pL = (int64_t)g.Ls * site + g.Ls - 1, p0 = (int64_t)g.Ls * site;
+#pragma unroll
+    for (int d = 0; d < 2; d++)
+        derivs_term<IMASS>(f, R[pL + g.cs * d], R[pL + g.cs * (d + 4)], X2[p0 + g.cs * d],
+                           X2[p0 + g.cs * (d + 4)], tzi, true);
+#pragma unroll
+    for (int d = 2; d < 4; d++)
+        derivs_term<IMASS>(f, R[p0 + g.cs * d], R[p0 + g.cs * (d + 4)], X2[pL + g.cs * d],
+                           X2[pL + g.cs * (d + 4)], tzi, false);
+    dS[site] = f[0];
+    dS[site + g.kvol] = f[1];
+    dS[site + 2 * g.kvol] = f[2];
+}
+
+void launch_derivs_full(const double2* R, const double2* X2, double anum, int imass,
+                        float* dSdchi, const Geom& g, cudaStream_t st) {
+    const unsigned nb = (unsigned)((g.kvol + kThreads - 1) / kThreads);
+    const double tzi = -2 * anum;
+    if (imass == 1) k_derivs_full<1><<<nb, kThreads, 0, st>>>(R, X2, tzi, dSdchi, g);
+    else if (imass == 3) k_derivs_full<3><<<nb, kThreads, 0, st>>>(R, X2, tzi, dSdchi, g);
+}
+
+}  // namespace chdwf

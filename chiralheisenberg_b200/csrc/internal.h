@@ -1,0 +1,77 @@
+// internal.h -- host-side declarations shared by the CUDA translation units of
+// libchdwf (not part of the public C ABI, which is include/chdwf.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace chdwf {
+
+constexpr int kMaxPoles = 32;
+constexpr int kMaxIter = 5000;     // niterc of qmrherm (rhmc/cheisdwf.f:603)
+constexpr int kThreads = 256;
+
+// Device-resident control block of one multi-shift solve.  Written by the
+// last block of each reduction kernel; the iteration index and the buffer
+// rotation are read from here so every launch of the loop is identical
+// (and therefore capturable in a CUDA graph).
+struct LzCtl {
+    int iter;          // current Lanczos iteration j (1-based)
+    int done;          // 0 running, 1 converged, 2 iteration cap
+    int m;             // iteration at which the loop ended
+    int npole;
+    int niter_cap;
+    int pad_;
+    double phimod;     // |Phi|
+    double thresh;     // arelax*resid, REAL*4 product promoted (cheisdwf.f:711-712)
+    double sigma[kMaxPoles];
+    double d[kMaxPoles];
+    double rho[kMaxPoles];
+    double anum[kMaxPoles];    // a_1..a_n (force weights / solution weights)
+    unsigned count1, count2;   // last-block counters of the two reductions
+};
+
+// Per-iteration scalar history (device), sized for kMaxIter iterations.
+struct LzHist {
+    double* alphat;    // [kMaxIter+2]  alpha~_j
+    double* beta;      // [kMaxIter+2]  beta_j (beta_1 = |Phi|)
+    double* invbeta;   // [kMaxIter+2]
+    double* rho;       // [kMaxPoles][kMaxIter+2]
+    double* mu;        // [kMaxPoles][kMaxIter+2]
+    double* y;         // [kMaxPoles][kMaxIter+2]  coefficients of q_j in x_k
+    double* c;         // [kMaxIter+2]             sum_k a_k y_kj
+};
+
+// Operator launchers (FP64, exact evaluation order).
+void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
+                     const Geom& g, float am3, float hpin, int ibound, cudaStream_t st);
+
+// Wall-slice operator for npole stacked two-slice fields (s'=0 <-> s=1,
+// s'=1 <-> s=Ls): computes M on the Ls=2 lattice of each pole.
+void launch_wall_dslash64(int npole, double2* out, const double2* in, const float* chif,
+                          const Geom& g, float am3, float hpin, int ibound, int imass,
+                          cudaStream_t st);
+
+// derivs over npole wall fields in pole order into REAL*4 dSdchi.
+void launch_derivs_walls(int npole, const double2* xw, const double2* x2w, const double* anum1,
+                         int imass, float* dSdchi, const Geom& g, cudaStream_t st);
+// derivs of one pole on full fields (the reference routine itself).
+void launch_derivs_full(const double2* R, const double2* X2, double anum, int imass,
+                        float* dSdchi, const Geom& g, cudaStream_t st);
+
+// small utilities (blas.cu)
+void launch_round_chi(const double* chi, float* chif, int kvol, cudaStream_t st);
+void launch_dsdchi_init(const double* chi, float twobeta, float* dS, int kvol, cudaStream_t st);
+void launch_scale(double2* out, const double2* in, double a, int64_t n, cudaStream_t st);
+// sum |v|^2 into *out (device), deterministic
+void launch_norm2(const double2* v, int64_t n, double* partials, double* out, cudaStream_t st);
+// Re <a, b> into *out
+void launch_redot(const double2* a, const double2* b, int64_t n, double* partials, double* out,
+                  cudaStream_t st);
+int reduce_blocks(int64_t n);
+
+}  // namespace chdwf

@@ -1,0 +1,447 @@
+// lanczos.cu -- multi-shift solver for (M^dagger M + sigma_k) x_k = Phi over
+// the Remez poles: the reference's qmrherm (rhmc/cheisdwf.f:599-745).
+//
+// The reference runs the Lanczos-based multi-shift recurrence and keeps two
+// ndiag x kferm arrays (p_k, x_k), so every iteration streams (10 + 4n)
+// spinors.  This implementation runs the SAME Lanczos process and the SAME
+// scalar recurrences (d_k, mu_k, rho_k and the stopping rule, :670-715) but
+// in two passes:
+//   pass 1  Lanczos vectors + scalar recurrences only; 6 spinor streams per
+//           iteration (M with a fused |Mq|^2, M^dagger with the fused
+//           three-term update and |r|^2);
+//   pass 2  regenerate the identical Lanczos vectors (same kernels, same
+//           stored scalars, bit-identical) and accumulate the solution
+//           x = a0 Phi + sum_j c_j q_j, where c_j = sum_k a_k y_kj and y_kj is
+//           the coefficient of q_j in x_k, obtained from rho and mu by the
+//           backward recurrence y_km = rho_km, y_ki = rho_ki - mu_k,i+1 y_k,i+1
+//           (x_k = sum_j rho_kj p_kj, p_kj = q_j - mu_kj p_k,j-1).
+// For iflag=1 only the two wall slices of each x_k are accumulated: the force
+// (derivs) reads x_k and M x_k on s=1 and s=Ls only, and M x_k there depends
+// on x_k on those two slices alone.
+// alpha~_j = q_j^dagger M^dagger M q_j is evaluated as |M q_j|^2, which lets
+// the three-term update be fused into the M^dagger kernel.
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+
+#include "dwf_stencil.cuh"
+#include "lanczos.h"
+
+namespace chdwf {
+
+struct LdScaled {
+    const double2* __restrict__ p;
+    double s;
+    __device__ __forceinline__ double2 operator()(int64_t j) const {
+        const double2 v = __ldg(p + j);
+        return make_double2(__dmul_rn(v.x, s), __dmul_rn(v.y, s));
+    }
+};
+
+struct LdF64b {
+    const double2* __restrict__ p;
+    __device__ __forceinline__ double2 operator()(int64_t j) const { return __ldg(p + j); }
+};
+
+__device__ __forceinline__ double2* ring(const LzArgs& a, int j) {
+    const int r = j % 3;
+    return r == 0 ? a.rb0 : (r == 1 ? a.rb1 : a.rb2);
+}
+
+// Deterministic last-block reduction of the per-block partial sums.
+__device__ __forceinline__ bool last_block_sum(double v, double* part, unsigned* count,
+                                               double* total) {
+    __shared__ double sh[kThreads / 32];
+    __shared__ bool is_last;
+    v = block_sum<kThreads>(v, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = v;
+        __threadfence();
+        const unsigned t = atomicAdd(count, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += ((volatile double*)part)[i];
+    s = block_sum<kThreads>(s, sh);
+    if (threadIdx.x == 0) {
+        *total = s;
+        *count = 0;
+    }
+    return true;
+}
+
+// ---- pass 1, kernel 1: vt = M q_j, alpha~_j = |vt|^2, pole recurrences -----
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgs a) {
+    LzCtl* ctl = a.ctl;
+    if (ctl->done) return;
+    const int j = ctl->iter;
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double loc = 0.0;
+    if (p < a.g.npts) {
+        const PointIdx q = point_of(a.g, p);
+        double2 acc[2][4];
+        dwf_apply_point<false, IMASS>(acc, LdScaled{ring(a, j), a.h.invbeta[j]}, a.g, q, a.chif,
+                                      a.diag, a.hpin, a.apbc != 0);
+#pragma unroll
+        for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                a.vt[p + a.g.cs * (d + 4 * f)] = acc[f][d];
+                loc += acc[f][d].x * acc[f][d].x + acc[f][d].y * acc[f][d].y;
+            }
+    }
+    double tot;
+    if (!last_block_sum(loc, a.part, &ctl->count1, &tot)) return;
+    if (threadIdx.x != 0) return;
+    // scalar recurrences of qmrherm (cheisdwf.f:666-715), one pole at a time
+    const double at = tot;
+    const double beta0 = a.h.beta[j];
+    a.h.alphat[j] = at;
+    const int n = ctl->npole;
+    const int64_t H = kMaxIter + 2;
+    double rhomax = 0.0;
+    for (int k = 0; k < n; k++) {
+        const double alpha = __dadd_rn(at, ctl->sigma[k]);
+        double rho, mu = 0.0;
+        if (j == 1) {
+            ctl->d[k] = alpha;
+            rho = __ddiv_rn(beta0, alpha);
+        } else {
+            mu = __ddiv_rn(beta0, ctl->d[k]);
+            const double dm1 = ctl->d[k];
+            const double dn = __dsub_rn(alpha, __dmul_rn(beta0, mu));
+            ctl->d[k] = dn;
+            rho = -__ddiv_rn(__dmul_rn(__dmul_rn(mu, dm1), ctl->rho[k]), dn);
+        }
+        ctl->rho[k] = rho;
+        a.h.rho[k * H + j] = rho;
+        a.h.mu[k * H + j] = mu;
+        const double v = fabs(__dmul_rn(ctl->phimod, rho));
+        if (k == 0 || v > rhomax) rhomax = v;
+    }
+    int done = 0;
+    if (j >= 2 && rhomax < ctl->thresh) done = 1;
+    else if (j >= ctl->niter_cap) done = 2;
+    if (!(rhomax == rhomax)) done = 3;   // NaN: stop, reported as non-finite
+    if (done) {
+        ctl->done = done;
+        ctl->m = j;
+        if (a.hflag) {
+            *(volatile int*)a.hflag = done;
+            __threadfence_system();
+        }
+    }
+}
+
+// ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgs a) {
+    LzCtl* ctl = a.ctl;
+    if (ctl->done) return;
+    const int j = ctl->iter;
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double loc = 0.0;
+    if (p < a.g.npts) {
+        const PointIdx q = point_of(a.g, p);
+        double2 acc[2][4];
+        dwf_apply_point<true, IMASS>(acc, LdF64b{a.vt}, a.g, q, a.chif, a.diag, a.hpin,
+                                     a.apbc != 0);
+        const double2* rj = ring(a, j);
+        const double2* rjm = ring(a, j - 1);
+        double2* rn = ring(a, j + 1);
+        const double ib = a.h.invbeta[j], at = a.h.alphat[j], bj = a.h.beta[j];
+        const double ibm = j > 1 ? a.h.invbeta[j - 1] : 0.0;
+#pragma unroll
+        for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const int64_t e = p + a.g.cs * (d + 4 * f);
+                const double2 qj = zscal(ib, rj[e]);
+                double2 v = zsub(acc[f][d], zscal(at, qj));
+                if (j > 1) v = zsub(v, zscal(bj, zscal(ibm, rjm[e])));
+                rn[e] = v;
+                loc += v.x * v.x + v.y * v.y;
+            }
+    }
+    double tot;
+    if (!last_block_sum(loc, a.part, &ctl->count2, &tot)) return;
+    if (threadIdx.x == 0) {
+        const double b = sqrt(tot);
+        a.h.beta[j + 1] = b;
+        a.h.invbeta[j + 1] = 1.0 / b;
+        ctl->iter = j + 1;
+    }
+}
+
+// ---- pass 2: regenerate q_j and accumulate --------------------------------
+template <int IMASS, int IFLAG>
+__global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgs a, int j, int apply) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= a.g.npts) return;
+    const PointIdx q = point_of(a.g, p);
+    const double ib = a.h.invbeta[j];
+    const double2* rj = ring(a, j);
+    if (apply) {
+        double2 acc[2][4];
+        dwf_apply_point<false, IMASS>(acc, LdScaled{rj, ib}, a.g, q, a.chif, a.diag, a.hpin,
+                                      a.apbc != 0);
+#pragma unroll
+        for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int d = 0; d < 4; d++) a.vt[p + a.g.cs * (d + 4 * f)] = acc[f][d];
+    }
+    if (IFLAG == 0) {
+        const double cj = a.h.c[j];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int64_t e = p + a.g.cs * c;
+            const double2 qj = zscal(ib, __ldg(rj + e));
+            double2 xv = a.x[e];
+            xv.x += cj * qj.x;
+            xv.y += cj * qj.y;
+            a.x[e] = xv;
+        }
+    } else {
+        const int Ls = a.g.Ls;
+        if (q.s != 0 && q.s != Ls - 1) return;
+        const int sw = (q.s == 0) ? 0 : 1;
+        const int64_t cs2 = 2 * (int64_t)a.g.kvol, kf2 = 8 * cs2;
+        const int64_t H = kMaxIter + 2;
+        const int n = a.npole;
+        double2 qv[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) qv[c] = zscal(ib, __ldg(rj + p + a.g.cs * c));
+        const int64_t base = sw + 2 * (int64_t)q.site;
+        for (int k = 0; k < n; k++) {
+            const double y = a.h.y[k * H + j];
+            double2* xk = a.xw + k * kf2 + base;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                double2 xv = xk[cs2 * c];
+                xv.x += y * qv[c].x;
+                xv.y += y * qv[c].y;
+                xk[cs2 * c] = xv;
+            }
+        }
+    }
+}
+
+template <int IMASS>
+__global__ void __launch_bounds__(kThreads) k_lz2_Md(LzArgs a, int j) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= a.g.npts) return;
+    const PointIdx q = point_of(a.g, p);
+    double2 acc[2][4];
+    dwf_apply_point<true, IMASS>(acc, LdF64b{a.vt}, a.g, q, a.chif, a.diag, a.hpin, a.apbc != 0);
+    const double2* rj = ring(a, j);
+    const double2* rjm = ring(a, j - 1);
+    double2* rn = ring(a, j + 1);
+    const double ib = a.h.invbeta[j], at = a.h.alphat[j], bj = a.h.beta[j];
+    const double ibm = j > 1 ? a.h.invbeta[j - 1] : 0.0;
+#pragma unroll
+    for (int f = 0; f < 2; f++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int64_t e = p + a.g.cs * (d + 4 * f);
+            const double2 qj = zscal(ib, rj[e]);
+            double2 v = zsub(acc[f][d], zscal(at, qj));
+            if (j > 1) v = zsub(v, zscal(bj, zscal(ibm, rjm[e])));
+            rn[e] = v;
+        }
+}
+
+// ---- between the passes: y_kj and c_j -------------------------------------
+__global__ void k_lz_coeffs(LzCtl* ctl, LzHist h, int iflag) {
+    const int m = ctl->m, n = ctl->npole;
+    const int64_t H = kMaxIter + 2;
+    const int k = threadIdx.x;
+    if (k < n) {
+        double y = h.rho[k * H + m];
+        h.y[k * H + m] = y;
+        for (int i = m - 1; i >= 1; i--) {
+            y = __dsub_rn(h.rho[k * H + i], __dmul_rn(h.mu[k * H + i + 1], y));
+            h.y[k * H + i] = y;
+        }
+    }
+    __syncthreads();
+    if (iflag == 0) {
+        for (int i = 1 + threadIdx.x; i <= m; i += blockDim.x) {
+            double c = 0.0;
+            for (int kk = 0; kk < n; kk++) c = __dadd_rn(c, __dmul_rn(ctl->anum[kk], h.y[kk * H + i]));
+            h.c[i] = c;
+        }
+    }
+}
+
+__global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* nrm2) {
+    const double b = sqrt(*nrm2);
+    h.beta[1] = b;
+    h.invbeta[1] = 1.0 / b;
+    ctl->phimod = b;
+}
+
+template <int IMASS>
+static void launch_pass1(const LzArgs& a, unsigned nb, cudaStream_t st) {
+    k_lz1_M<IMASS><<<nb, kThreads, 0, st>>>(a);
+    k_lz1_Md<IMASS><<<nb, kThreads, 0, st>>>(a);
+}
+
+template <int IMASS>
+static void launch_pass2(const LzArgs& a, unsigned nb, int j, int m, int iflag, cudaStream_t st) {
+    const int apply = j < m;
+    if (iflag == 0) k_lz2_M<IMASS, 0><<<nb, kThreads, 0, st>>>(a, j, apply);
+    else k_lz2_M<IMASS, 1><<<nb, kThreads, 0, st>>>(a, j, apply);
+    if (apply) k_lz2_Md<IMASS><<<nb, kThreads, 0, st>>>(a, j);
+}
+
+LzWork::~LzWork() { release(); }
+
+void LzWork::release() {
+    if (ctl) cudaFree(ctl);
+    if (hist_mem) cudaFree(hist_mem);
+    if (part) cudaFree(part);
+    if (hflag_host) cudaFreeHost(hflag_host);
+    for (int i = 0; i < 3; i++)
+        if (rb[i]) cudaFree(rb[i]);
+    if (vt) cudaFree(vt);
+    if (xw) cudaFree(xw);
+    if (x2w) cudaFree(x2w);
+    ctl = nullptr; hist_mem = nullptr; part = nullptr; hflag_host = nullptr;
+    rb[0] = rb[1] = rb[2] = vt = xw = x2w = nullptr;
+}
+
+cudaError_t LzWork::ensure(const Geom& g, int npole_max) {
+    if (ctl && g.kferm == geom.kferm && g.L == geom.L && g.Lt == geom.Lt && npole_max <= xw_poles)
+        return cudaSuccess;
+    release();
+    geom = g;
+    cudaError_t e;
+    if ((e = cudaMalloc(&ctl, sizeof(LzCtl)))) return e;
+    const int64_t H = kMaxIter + 2;
+    const size_t nh = 4 * H + 3 * (size_t)kMaxPoles * H;
+    if ((e = cudaMalloc(&hist_mem, nh * sizeof(double)))) return e;
+    hist.alphat = hist_mem;
+    hist.beta = hist_mem + H;
+    hist.invbeta = hist_mem + 2 * H;
+    hist.c = hist_mem + 3 * H;
+    hist.rho = hist_mem + 4 * H;
+    hist.mu = hist.rho + kMaxPoles * H;
+    hist.y = hist.mu + kMaxPoles * H;
+    const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+    if ((e = cudaMalloc(&part, sizeof(double) * (nb + 2048)))) return e;
+    for (int i = 0; i < 3; i++)
+        if ((e = cudaMalloc(&rb[i], sizeof(double2) * g.kferm))) return e;
+    if ((e = cudaMalloc(&vt, sizeof(double2) * g.kferm))) return e;
+    xw_poles = npole_max < 1 ? 1 : npole_max;
+    const size_t nw = (size_t)xw_poles * 16 * g.kvol;
+    if ((e = cudaMalloc(&xw, sizeof(double2) * nw))) return e;
+    if ((e = cudaMalloc(&x2w, sizeof(double2) * nw))) return e;
+    if ((e = cudaHostAlloc(&hflag_host, sizeof(int), cudaHostAllocMapped))) return e;
+    if ((e = cudaHostGetDevicePointer((void**)&hflag_dev, hflag_host, 0))) return e;
+    return cudaSuccess;
+}
+
+// Multi-shift solve.  anum[0..n], aden[0..n-1] as in the reference.
+// iflag 0: x = a0 Phi + sum_k a_k x_k.  iflag 1: x = a0 Phi and the force
+// contribution of every pole is accumulated into dSdchi (device, REAL*4).
+cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
+                     const double* anum, const double* aden, int iflag, const float* chif,
+                     float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
+                     int* itercg, int* status, LzStats* stats, cudaStream_t st) {
+    cudaError_t e = w.ensure(g, iflag ? ndiag : 1);
+    if (e) return e;
+    if (ndiag < 1 || ndiag > kMaxPoles) return cudaErrorInvalidValue;
+    LzCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.iter = 1;
+    hc.npole = ndiag;
+    hc.niter_cap = kMaxIter;
+    const float resid = sqrtf((float)g.kferm * res * res);   // :621
+    const float arelax = 2.0f;                                // :711
+    hc.thresh = (double)(arelax * resid);
+    for (int k = 0; k < ndiag; k++) {
+        hc.sigma[k] = aden[k];
+        hc.anum[k] = anum[k + 1];
+    }
+    if ((e = cudaMemcpyAsync(w.ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st))) return e;
+    *w.hflag_host = 0;
+
+    LzArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = g;
+    a.rb0 = w.rb[0]; a.rb1 = w.rb[1]; a.rb2 = w.rb[2];
+    a.vt = w.vt;
+    a.chif = chif;
+    a.diag = (double)(2.0f * ((3.0f - am3) + 1.0f));
+    a.hpin = (double)hpin;
+    a.apbc = ibound == -1;
+    a.ctl = w.ctl;
+    a.h = w.hist;
+    a.part = w.part;
+    a.hflag = w.hflag_dev;
+    a.x = x;
+    a.xw = w.xw;
+    a.npole = ndiag;
+    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+
+    // beta_1 = |Phi|, r_1 = Phi
+    launch_norm2(phi, g.kferm, w.part + nb + 8, w.part + nb, st);
+    k_lz_init<<<1, 1, 0, st>>>(w.ctl, w.hist, w.part + nb);
+    cudaMemcpyAsync(w.rb[1], phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+
+    // pass 1: launch chunks of iterations, poll the mapped flag with one
+    // chunk in flight ahead of the one being checked
+    const int chunk = 16;
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    int launched = 0, nchunk = 0;
+    while (launched < kMaxIter) {
+        for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
+            if (imass == 3) launch_pass1<3>(a, nb, st);
+            else launch_pass1<1>(a, nb, st);
+        }
+        cudaEventRecord(ev[nchunk & 1], st);
+        if (nchunk >= 1) {
+            cudaEventSynchronize(ev[(nchunk - 1) & 1]);
+            if (*(volatile int*)w.hflag_host) break;
+        }
+        nchunk++;
+    }
+    cudaEventSynchronize(ev[nchunk & 1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if ((e = cudaGetLastError())) return e;
+    LzCtl hr;
+    if ((e = cudaMemcpyAsync(&hr, w.ctl, sizeof(hr), cudaMemcpyDeviceToHost, st))) return e;
+    if ((e = cudaStreamSynchronize(st))) return e;
+    const int m = hr.m;
+    *itercg = m;
+    *status = hr.done == 1 ? 0 : (hr.done == 2 ? 1 : 2);
+    if (stats) { stats->iters = m; stats->pass1_launches = 2 * launched; }
+    if (m < 1) return cudaErrorUnknown;
+
+    // coefficients, then pass 2
+    k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag);
+    launch_scale(x, phi, anum[0], g.kferm, st);                       // x = a0 Phi (:628)
+    if (iflag) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
+    cudaMemcpyAsync(w.rb[1], phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+    for (int j = 1; j <= m; j++) {
+        if (imass == 3) launch_pass2<3>(a, nb, j, m, iflag, st);
+        else launch_pass2<1>(a, nb, j, m, iflag, st);
+    }
+    if (iflag) {
+        // X2 = M x_k on the walls, then derivs pole by pole (:733-740)
+        launch_wall_dslash64(ndiag, w.x2w, w.xw, chif, g, am3, hpin, ibound, imass, st);
+        const double* anum_dev = reinterpret_cast<const double*>(
+            reinterpret_cast<const char*>(w.ctl) + offsetof(LzCtl, anum));
+        launch_derivs_walls(ndiag, w.xw, w.x2w, anum_dev, imass, dSdchi, g, st);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace chdwf

@@ -1,0 +1,51 @@
+// lanczos.h -- two-pass multi-shift Lanczos solver (qmrherm replacement).
+#pragma once
+#include "internal.h"
+
+namespace chdwf {
+
+struct LzArgs {
+    Geom g;
+    double2 *rb0, *rb1, *rb2;   // Lanczos residual ring: r_j lives in rb[j % 3]
+    double2* vt;                // M q_j
+    const float* chif;          // chi rounded to REAL*4 (wall coupling)
+    double diag, hpin;
+    int apbc;
+    LzCtl* ctl;
+    LzHist h;
+    double* part;               // per-block partial sums
+    int* hflag;                 // device view of the mapped host stop flag
+    double2* x;                 // solution (iflag 0)
+    double2* xw;                // two-slice x_k per pole (iflag 1)
+    int npole;
+};
+
+struct LzStats {
+    int iters;
+    int pass1_launches;
+};
+
+struct LzWork {
+    Geom geom{};
+    LzCtl* ctl = nullptr;
+    double* hist_mem = nullptr;
+    LzHist hist{};
+    double* part = nullptr;
+    double2* rb[3] = {nullptr, nullptr, nullptr};
+    double2* vt = nullptr;
+    double2* xw = nullptr;
+    double2* x2w = nullptr;
+    int xw_poles = 0;
+    int* hflag_host = nullptr;
+    int* hflag_dev = nullptr;
+    ~LzWork();
+    void release();
+    cudaError_t ensure(const Geom& g, int npole_max);
+};
+
+cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
+                     const double* anum, const double* aden, int iflag, const float* chif,
+                     float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
+                     int* itercg, int* status, LzStats* stats, cudaStream_t st);
+
+}  // namespace chdwf

@@ -1,0 +1,115 @@
+/*
+ * chdwf.h -- C ABI of libchdwf: the RHMC fermion hot path of the 2+1D chiral
+ * Heisenberg domain-wall code (j-ostmeyer/chiralHeisenberg, rhmc/cheisdwf.f)
+ * on NVIDIA B200 (sm_100a).
+ *
+ * Two levels:
+ *  1. Routine level: one entry point per reference subroutine on the path,
+ *     same arguments, same meaning, host arrays in the reference layout and
+ *     types.  The reference's subroutines take implicit-interface, by-reference
+ *     arguments and read/write COMMON blocks; here the COMMON inputs
+ *     (/para/ beta, am3, ibound) are set once per context
+ *     (chdwf_set_para) and the COMMON outputs (/vector/ x, /sforce/ dSdchi)
+ *     are explicit output arrays.  Each call copies its inputs to HBM and its
+ *     outputs back.
+ *  2. Resident level (chdwf_traj_*): the blocks of the trajectory that call
+ *     those subroutines (heatbath, hamilton, force, leapfrog updates,
+ *     Metropolis bookkeeping) with every field kept in HBM; only REAL*4
+ *     momenta/forces or scalars cross when the caller asks for them.
+ *
+ * Layouts (reference, Fortran column-major, shown 0-based):
+ *   spinor   complex*16 R(kthird, ksize, ksize, ksizet, 4, 2): s fastest.
+ *            Passed as double* pointing at (re, im) pairs.
+ *   chi      real*8 chi(ksize*ksize*ksizet, 3)
+ *   pp, dSdchi  REAL*4 (kvol, 3)
+ *
+ * Every function returns a status: CHDWF_OK, CHDWF_ITER_CAP (solver hit its
+ * iteration cap: the reference's qmrherm stops silently at 5000, congrad
+ * prints "# iterations of congrad exceeds niterc"), CHDWF_NONFINITE,
+ * CHDWF_CUDA_ERROR, CHDWF_BAD_ARG.  chdwf_last_error() describes the last
+ * failure of a context.  A context is single-threaded: one CUDA stream,
+ * calls must not overlap.
+ */
+#ifndef CHDWF_H
+#define CHDWF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHDWF_OK 0
+#define CHDWF_ITER_CAP 1
+#define CHDWF_NONFINITE 2
+#define CHDWF_CUDA_ERROR 3
+#define CHDWF_BAD_ARG 4
+
+typedef struct chdwf_ctx chdwf_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+/* Lattice sizes are the reference's compile-time parameters ksize, ksizet,
+ * kthird (rhmc/cheisdwf.f:31).  device: CUDA ordinal. */
+int chdwf_create(chdwf_ctx** ctx, int ksize, int ksizet, int kthird, int device);
+void chdwf_destroy(chdwf_ctx* ctx);
+/* /para/ beta, am3, ibound (rhmc/cheisdwf.f:40, :85) */
+int chdwf_set_para(chdwf_ctx* ctx, float beta, float am3, int ibound);
+const char* chdwf_last_error(const chdwf_ctx* ctx);
+/* version string of the library build */
+const char* chdwf_version(void);
+
+/* ---- routine level (host arrays) -------------------------------------- */
+/* Phi = M R.  Replaces dslash(Phi,R,chi,am,hpin,imass), rhmc/cheisdwf.f:2634.
+ * am is accepted and unused, as in the reference (":26 not currently
+ * implemented"). */
+int chdwf_dslash(chdwf_ctx* ctx, double* Phi, const double* R, const double* chi, float am,
+                 float hpin, int imass);
+/* Phi = M^dagger R.  Replaces dslashd(...), rhmc/cheisdwf.f:3071. */
+int chdwf_dslashd(chdwf_ctx* ctx, double* Phi, const double* R, const double* chi, float am,
+                  float hpin, int imass);
+/* Multi-shift solve over ndiag poles.  Replaces
+ * qmrherm(Phi,res,itercg,am,hpin,imass,anum,aden,ndiag,iflag),
+ * rhmc/cheisdwf.f:599.  anum[0..ndiag], aden[0..ndiag-1].  x receives
+ * /vector/x: iflag 0: a0*Phi + sum_k a_k (M^dagger M + aden_k)^-1 Phi;
+ * iflag 1: a0*Phi, and the force of every pole is added to dSdchi (in/out,
+ * the /sforce/ block) exactly as the reference's derivs calls do.
+ * chi is the /trial/ field the operator reads. */
+int chdwf_qmrherm(chdwf_ctx* ctx, const double* Phi, float res, int* itercg, float am,
+                  float hpin, int imass, const double* anum, const double* aden, int ndiag,
+                  int iflag, const double* chi, double* x, float* dSdchi);
+/* dSdchi += force term of one pole.  Replaces derivs(R,X2,anum,imass),
+ * rhmc/cheisdwf.f:747. */
+int chdwf_derivs(chdwf_ctx* ctx, const double* R, const double* X2, double anum, int imass,
+                 float* dSdchi);
+/* CGNE on M^dagger M with x as initial guess (in/out, the /vector/ block).
+ * Replaces congrad(Phi,res,itercg,am,hpin,imass), rhmc/cheisdwf.f:1064. */
+int chdwf_congrad(chdwf_ctx* ctx, const double* Phi, float res, int* itercg, float am,
+                  float hpin, int imass, const double* chi, double* x);
+/* dSdchi = 2 beta chi + fermion force via two solves over the guidance set
+ * (b then a coefficients).  Replaces force(Phi,res1,am,hpin,imass),
+ * rhmc/cheisdwf.f:470, with the remez2g common block passed explicitly. */
+int chdwf_force(chdwf_ctx* ctx, const double* Phi, float res1, float am, float hpin, int imass,
+                const double* chi, const double* anum, const double* aden, const double* bnum,
+                const double* bden, int ndiag, float* dSdchi, double* x, int* itg, int* itf);
+/* h = hg + hp + hf, s = hg + hf.  Replaces
+ * hamilton(Phi,h,hg,hp,s,res2,isweep,am,hpin,imass), rhmc/cheisdwf.f:522,
+ * with /trial/ (chi, pp) and the remez2 b-coefficients passed explicitly.
+ * out[0..4] = h, hg, hp, s, hf. */
+int chdwf_hamilton(chdwf_ctx* ctx, const double* Phi, float res2, float am, float hpin, int imass,
+                   const double* chi, const float* pp, const double* bnum, const double* bden,
+                   int ndiag, double* out, double* x, int* itercg);
+
+/* ---- device-pointer variants (arrays already in HBM, same layouts) ------ */
+/* stream: a cudaStream_t or NULL for the context's own stream. */
+int chdwf_dslash_dev(chdwf_ctx* ctx, void* Phi, const void* R, const void* chi, float hpin,
+                     int imass, int dagger, void* stream);
+int chdwf_qmrherm_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, float hpin,
+                      int imass, const double* anum, const double* aden, int ndiag, int iflag,
+                      const void* chi, void* x, void* dSdchi);
+int chdwf_congrad_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, float hpin,
+                      int imass, const void* chi, void* x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,247 @@
+"""ctypes bindings to the CPU oracle (oracle/_build/liboracle.so).
+
+Test infrastructure only: imported by tests/, by ``__graft_entry__.smoke`` and
+by the CPU-baseline legs of ``bench.py``.  The product package never imports
+this module.  Array layouts are those of the reference (rhmc/cheisdwf.f):
+spinors complex128 of shape (2, 4, Lt, L, L, Ls) in C order == Fortran
+R(Ls, L, L, Lt, 4, 2); chi float64 (3, Lt, L, L) == chi(kvol, 3).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, no fused multiply-add)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+class Lat(C.Structure):
+    _fields_ = [("L", C.c_int), ("Lt", C.c_int), ("Ls", C.c_int),
+                ("beta", C.c_float), ("am3", C.c_float), ("ibound", C.c_int),
+                ("threads", C.c_int)]
+
+
+class Rng(C.Structure):
+    _fields_ = [("ds", C.c_double * 2), ("v", C.c_float * 97), ("yran", C.c_float),
+                ("yrun", C.c_float), ("idum", C.c_int)]
+
+
+class Remez(C.Structure):
+    _fields_ = [("n", C.c_int), ("anum", C.c_double * 32), ("aden", C.c_double * 32),
+                ("bnum", C.c_double * 32), ("bden", C.c_double * 32)]
+
+
+class TrajRec(C.Structure):
+    _fields_ = [("H0", C.c_double), ("H1", C.c_double), ("dH", C.c_double), ("dS", C.c_double),
+                ("S0", C.c_double), ("S1", C.c_double), ("hg", C.c_double), ("hp", C.c_double),
+                ("y", C.c_float), ("x", C.c_float), ("accepted", C.c_int), ("nsteps", C.c_int),
+                ("it_pf", C.c_int), ("it_h0", C.c_int), ("it_h1", C.c_int),
+                ("it_guid", C.c_double), ("it_force", C.c_double), ("nforce", C.c_int),
+                ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
+                ("vel2", C.c_float), ("measured", C.c_int), ("cond", C.c_float * 3),
+                ("susc", C.c_float * 3), ("condmod", C.c_float), ("susctot", C.c_float),
+                ("ancgm", C.c_float)]
+
+
+class State(C.Structure):
+    _fields_ = [("lat", Lat), ("rng", Rng), ("r2", Remez), ("r4", Remez), ("r2g", Remez),
+                ("dt", C.c_float), ("am", C.c_float), ("hpin", C.c_float),
+                ("imass", C.c_int), ("iterl", C.c_int), ("iprint", C.c_int), ("measure", C.c_int),
+                ("rescga", C.c_float), ("rescgg", C.c_float), ("rescgm", C.c_float),
+                ("chi", C.POINTER(C.c_double)), ("chit", C.POINTER(C.c_double)),
+                ("pp", C.POINTER(C.c_float)), ("dSdchi", C.POINTER(C.c_float)),
+                ("Phi", C.POINTER(C.c_double)), ("X1", C.POINTER(C.c_double)),
+                ("R", C.POINTER(C.c_double)), ("ps", C.POINTER(C.c_float)),
+                ("cferm", C.POINTER(C.c_float)), ("isweep", C.c_int)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or (
+                os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "chdwf_oracle.c"))):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        P = C.c_void_p
+        L.orc_rranf.restype = C.c_float
+        L.orc_rano.restype = C.c_float
+        L.orc_rranget.restype = C.c_double
+        L.orc_rranset.argtypes = [P, C.c_double]
+        L.orc_rng_startup.argtypes = [P, C.c_double]
+        L.orc_gauss0.argtypes = [P, C.c_int64, P]
+        L.orc_gaussp.argtypes = [P, C.c_int64, P]
+        for f in (L.orc_dslash, L.orc_dslashd):
+            f.argtypes = [P, P, P, P, C.c_float, C.c_float, C.c_int]
+        L.orc_qmrherm.argtypes = [P, P, C.c_float, P, C.c_float, C.c_float, C.c_int, P, P,
+                                  C.c_int, C.c_int, P, P, P, C.c_int]
+        L.orc_derivs.argtypes = [P, P, P, C.c_double, C.c_int, P]
+        L.orc_congrad.argtypes = [P, P, C.c_float, P, C.c_float, C.c_float, C.c_int, P, P]
+        L.orc_force.argtypes = [P, P, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P, P, P, P]
+        L.orc_hamilton.argtypes = [P, P, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P, P,
+                                   P, P]
+        L.orc_fermion.argtypes = [P, P, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P, P]
+        L.orc_fermion.restype = C.c_float
+        L.orc_state_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                    C.c_float, C.c_float, C.c_int, C.c_int]
+        L.orc_state_new.restype = C.POINTER(State)
+        L.orc_state_free.argtypes = [C.POINTER(State)]
+        L.orc_state_set_remez.argtypes = [C.POINTER(State), C.c_int, P]
+        L.orc_sweep.argtypes = [C.POINTER(State), P]
+        L.orc_read_remez.argtypes = [C.c_char_p, C.c_int, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def make_lat(L, Lt, Ls, beta=0.475, am3=1.0, ibound=-1, threads=1) -> Lat:
+    return Lat(L, Lt, Ls, beta, am3, ibound, threads)
+
+
+def spinor_shape(lat: Lat):
+    return (2, 4, lat.Lt, lat.L, lat.L, lat.Ls)
+
+
+def kvol(lat: Lat) -> int:
+    return lat.L * lat.L * lat.Lt
+
+
+def dslash(lat, R, chi, hpin=0.0, imass=1, dag=False, am=0.0):
+    R = np.ascontiguousarray(R, dtype=np.complex128)
+    chi = np.ascontiguousarray(chi, dtype=np.float64)
+    out = np.empty_like(R)
+    f = lib().orc_dslashd if dag else lib().orc_dslash
+    f(C.byref(lat), _p(out), _p(R), _p(chi), am, hpin, imass)
+    return out
+
+
+def qmrherm(lat, Phi, chi, anum, aden, res, iflag=0, hpin=0.0, imass=1, dSdchi=None,
+            niterc=5000, am=0.0):
+    Phi = np.ascontiguousarray(Phi, dtype=np.complex128)
+    chi = np.ascontiguousarray(chi, dtype=np.float64)
+    anum = np.ascontiguousarray(anum, dtype=np.float64)
+    aden = np.ascontiguousarray(aden, dtype=np.float64)
+    x = np.empty_like(Phi)
+    if dSdchi is None:
+        dSdchi = np.zeros((3, kvol(lat)), dtype=np.float32)
+    it = C.c_int(0)
+    st = lib().orc_qmrherm(C.byref(lat), _p(Phi), res, C.byref(it), am, hpin, imass, _p(anum),
+                           _p(aden), len(aden), iflag, _p(chi), _p(x), _p(dSdchi), niterc)
+    return x, it.value, st, dSdchi
+
+
+def derivs(lat, R, X2, anum, imass, dSdchi):
+    lib().orc_derivs(C.byref(lat), _p(np.ascontiguousarray(R)), _p(np.ascontiguousarray(X2)),
+                     float(anum), imass, _p(dSdchi))
+    return dSdchi
+
+
+def congrad(lat, Phi, chi, x0, res, hpin=0.0, imass=1, am=0.0):
+    x = np.ascontiguousarray(x0, dtype=np.complex128).copy()
+    it = C.c_int(0)
+    capped = lib().orc_congrad(C.byref(lat), _p(np.ascontiguousarray(Phi)), res, C.byref(it), am,
+                               hpin, imass, _p(np.ascontiguousarray(chi)), _p(x))
+    return x, it.value, capped
+
+
+def remez_struct(a0, anum, aden, b0, bnum, bden) -> Remez:
+    r = Remez()
+    r.n = len(aden)
+    r.anum[0] = a0
+    r.bnum[0] = b0
+    for k in range(r.n):
+        r.anum[k + 1] = anum[k]
+        r.aden[k] = aden[k]
+        r.bnum[k + 1] = bnum[k]
+        r.bden[k] = bden[k]
+    return r
+
+
+def read_remez(path, n) -> Remez:
+    r = Remez()
+    rc = lib().orc_read_remez(path.encode(), n, C.byref(r))
+    if rc != 0:
+        raise IOError(f"cannot read remez file {path}: {rc}")
+    return r
+
+
+class Sweeper:
+    """The main loop of program dwf3d (cheisdwf.f:207-399) over the oracle."""
+
+    def __init__(self, L, Lt, Ls, beta, am3, dt, am, hpin, imass, iterl, remez2, remez4,
+                 remez2g, chi=None, seed=None, measure=True, threads=1):
+        self.lib = lib()
+        self.st = self.lib.orc_state_new(L, Lt, Ls, beta, am3, dt, am, hpin, imass, iterl)
+        self.st.contents.lat.threads = threads
+        self.st.contents.measure = 1 if measure else 0
+        for which, r in ((2, remez2), (4, remez4), (22, remez2g)):
+            self.lib.orc_state_set_remez(self.st, which, C.byref(r))
+        self.kvol = L * L * Lt
+        if chi is not None:
+            self.chi[:] = np.asarray(chi, dtype=np.float64).reshape(-1)
+        if seed is not None:
+            self.lib.orc_rng_startup(C.byref(self.st.contents.rng), float(seed))
+
+    @property
+    def chi(self):
+        return np.ctypeslib.as_array(self.st.contents.chi, shape=(3 * self.kvol,))
+
+    @property
+    def cferm(self):
+        Lt = self.st.contents.lat.Lt
+        return np.ctypeslib.as_array(self.st.contents.cferm, shape=(2, 2, Lt, 2)).copy()
+
+    def sweep(self) -> TrajRec:
+        rec = TrajRec()
+        self.lib.orc_sweep(self.st, C.byref(rec))
+        return rec
+
+    def close(self):
+        if self.st:
+            self.lib.orc_state_free(self.st)
+            self.st = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Rand:
+    """The reference RNG (RRANF + rano) on the oracle."""
+
+    def __init__(self, seed):
+        self.g = Rng()
+        lib().orc_rng_startup(C.byref(self.g), float(seed))
+
+    def seed(self) -> float:
+        return lib().orc_rranget(C.byref(self.g))
+
+    def rano(self, which="yran") -> float:
+        y = C.c_float(getattr(self.g, which))
+        v = lib().orc_rano(C.byref(self.g), C.byref(y))
+        setattr(self.g, which, y.value)
+        return v
+
+    def gauss0(self, kvol):
+        ps = np.empty((2, kvol), dtype=np.float32)
+        lib().orc_gauss0(C.byref(self.g), kvol, _p(ps))
+        return ps
+
+    def gaussp(self, kvol):
+        ps = np.empty((2, kvol), dtype=np.float32)
+        lib().orc_gaussp(C.byref(self.g), kvol, _p(ps))
+        return ps

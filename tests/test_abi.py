@@ -1,0 +1,48 @@
+"""CPU checks of the C-ABI library: it builds, loads without a GPU, and
+exports every function include/chdwf.h declares (no compute calls here)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import chiralheisenberg_b200 as chb
+from chiralheisenberg_b200 import build as chbuild
+from conftest import ROOT
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "chdwf.h")).read()
+    return sorted(set(re.findall(r"\b(chdwf_\w+)\s*\(", text)))
+
+
+def test_header_matches_python_export_list():
+    assert set(declared_symbols()) == set(chb.EXPORTS)
+
+
+def test_library_builds_and_exports_all_symbols():
+    lib_path = chbuild.build()
+    assert os.path.exists(lib_path)
+    lib = C.CDLL(lib_path)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version_string():
+    chbuild.build()
+    assert "sm_100a" in chb.version()
+
+
+def test_create_rejects_bad_sizes():
+    chbuild.build()
+    lib = chb.load_library()
+    h = C.c_void_p()
+    assert lib.chdwf_create(C.byref(h), 1, 4, 4, 0) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_create(None, 4, 4, 4, 0) == chb.CHDWF_BAD_ARG
+
+
+def test_null_context_is_rejected():
+    chbuild.build()
+    lib = chb.load_library()
+    assert lib.chdwf_set_para(None, 0.5, 1.0, -1) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_dslash(None, None, None, None, 0.0, 0.0, 1) == chb.CHDWF_BAD_ARG

@@ -1,0 +1,118 @@
+"""GPU parity of the solvers, the force and the Hamiltonian against the
+oracle, through the C ABI.
+
+The GPU multi-shift solver runs the reference's Lanczos recurrence and
+stopping rule in two passes (see chiralheisenberg_b200/csrc/lanczos.cu), the
+oracle the reference's one-pass form; both make the same iterations, and the
+solutions agree to rounding amplified by the Krylov process.  Tolerances:
+  qmrherm x        relative L2 1e-10
+  force dSdchi     |diff| <= 2 REAL*4 ulps of max|dSdchi| (REAL*4 result)
+  hamilton h       relative 1e-12
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import chiralheisenberg_b200 as chb
+from conftest import random_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b))
+
+
+@pytest.mark.parametrize("L,Lt,Ls", [(4, 4, 4), (8, 8, 8)])
+@pytest.mark.parametrize("which,res", [("remez4", 1e-9), ("remez2", 1e-9), ("remez2g", 1e-6)])
+def test_qmrherm_iflag0(remez, L, Lt, Ls, which, res):
+    r = remez[which]
+    Phi, chi = random_fields(L, Lt, Ls, seed=21, chi_scale=0.4)
+    lat = po.make_lat(L, Lt, Ls, beta=0.475)
+    xr, itr, st, _ = po.qmrherm(lat, Phi, chi, r["anum"], r["aden"], res)
+    gl = chb.Lattice(L, Lt, Ls, beta=0.475)
+    xg, itg, _ = gl.qmrherm(Phi, res, r["anum"], r["aden"], 0, chi)
+    assert st == 0
+    assert itg == itr
+    assert rel(xg, xr) < 1e-10
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_qmrherm_iflag1_force(remez, imass):
+    L, Lt, Ls = 6, 6, 6
+    r = remez["remez2g"]
+    Phi, chi = random_fields(L, Lt, Ls, seed=22, chi_scale=0.4)
+    lat = po.make_lat(L, Lt, Ls, beta=0.475)
+    dS0 = (np.random.default_rng(1).standard_normal((3, L * L * Lt))).astype(np.float32)
+    xr, itr, st, dSr = po.qmrherm(lat, Phi, chi, r["anum"], r["aden"], 1e-6, iflag=1,
+                                  imass=imass, hpin=0.0, dSdchi=dS0.copy())
+    gl = chb.Lattice(L, Lt, Ls, beta=0.475)
+    xg, itg, dSg = gl.qmrherm(Phi, 1e-6, r["anum"], r["aden"], 1, chi, imass=imass,
+                              dSdchi=dS0.copy())
+    assert itg == itr
+    assert np.array_equal(xg, xr)  # x = a0*Phi exactly
+    tol = 2 * np.spacing(np.float32(np.abs(dSr).max()))
+    assert np.abs(dSg - dSr).max() <= tol
+
+
+def test_derivs_bit_exact():
+    L, Lt, Ls = 4, 4, 6
+    R, chi = random_fields(L, Lt, Ls, seed=23)
+    X2, _ = random_fields(L, Lt, Ls, seed=24)
+    lat = po.make_lat(L, Lt, Ls)
+    dS = np.random.default_rng(2).standard_normal((3, L * L * Lt)).astype(np.float32)
+    for imass in (1, 3):
+        ref = po.derivs(lat, R, X2, -0.731, imass, dS.copy())
+        gl = chb.Lattice(L, Lt, Ls)
+        out = gl.derivs(R, X2, -0.731, imass, dS.copy())
+        assert np.array_equal(out, ref)
+
+
+def test_force_and_hamilton(remez, con12):
+    """force and hamilton on the reference's 12^3 configuration, Ls=8."""
+    chi, _ = con12
+    L, Lt, Ls = 12, 12, 8
+    Phi, _ = random_fields(L, Lt, Ls, seed=25)
+    kvol = L * L * Lt
+    pp = np.random.default_rng(3).standard_normal((3, kvol)).astype(np.float32)
+    lat = po.make_lat(L, Lt, Ls, beta=0.45)
+    r2g, r2 = remez["remez2g"], remez["remez2"]
+    import ctypes as C
+    lib = po.lib()
+    R2G = po.remez_struct(r2g["anum"][0], r2g["anum"][1:], r2g["aden"], r2g["bnum"][0],
+                          r2g["bnum"][1:], r2g["bden"])
+    R2 = po.remez_struct(r2["anum"][0], r2["anum"][1:], r2["aden"], r2["bnum"][0],
+                         r2["bnum"][1:], r2["bden"])
+    dSr = np.zeros((3, kvol), np.float32)
+    xr = np.empty_like(Phi)
+    itg, itf = C.c_int(), C.c_int()
+    lib.orc_force(C.byref(lat), po._p(Phi), 1e-6, 0.0, 0.5, 1, po._p(chi), C.byref(R2G),
+                  po._p(dSr), po._p(xr), C.byref(itg), C.byref(itf))
+    hr = np.zeros(5)
+    xh = np.empty_like(Phi)
+    ith = C.c_int()
+    lib.orc_hamilton(C.byref(lat), po._p(Phi), 1e-9, 0.0, 0.5, 1, po._p(chi), po._p(pp),
+                     C.byref(R2), po._p(hr), po._p(xh), C.byref(ith))
+    gl = chb.Lattice(L, Lt, Ls, beta=0.45)
+    dSg, xg, g1, g2 = gl.force(Phi, 1e-6, chi, (r2g["anum"], r2g["aden"], r2g["bnum"], r2g["bden"]),
+                               hpin=0.5)
+    assert (g1, g2) == (itg.value, itf.value)
+    tol = 2 * np.spacing(np.float32(np.abs(dSr).max()))
+    assert np.abs(dSg - dSr).max() <= tol
+    hg, xhg, itg_h = gl.hamilton(Phi, 1e-9, chi, pp, r2["bnum"], r2["bden"], hpin=0.5)
+    assert itg_h == ith.value
+    assert abs(hg[0] - hr[0]) <= 1e-12 * abs(hr[0])
+    assert hg[1] == hr[1] and hg[2] == hr[2]
+
+
+def test_congrad(remez):
+    L, Lt, Ls = 6, 6, 6
+    Phi, chi = random_fields(L, Lt, Ls, seed=26, chi_scale=0.4)
+    lat = po.make_lat(L, Lt, Ls)
+    xr, itr, capped = po.congrad(lat, Phi, chi, Phi, 1e-9)
+    gl = chb.Lattice(L, Lt, Ls)
+    xg, itg = gl.congrad(Phi, 1e-9, chi, Phi)
+    # REAL*4 scalars: the reference sums in REAL*4 sequentially, the GPU in
+    # FP64 then rounds; the iteration paths agree to the solver tolerance
+    assert abs(itg - itr) <= 2
+    assert rel(xg, xr) < 1e-6

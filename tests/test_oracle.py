@@ -1,0 +1,195 @@
+"""CPU tests of the oracle against the reference's golden data and against
+mathematical identities of the operator and solvers.
+
+Golden data (tests/golden/, made by make_golden.py from the reference tree):
+  * seed_pins.json: (seed read from 'con', seed printed after start-up) pairs
+    from rhmc/Ls_8/<run>/out_1 -- exactly 196 RRANF draws apart
+    (rhmc/cheisdwf.f:125-130 with the table fill of rano, :1725-1737);
+  * remez2/remez4/remez2g: rational approximations of x^(+-1/2), x^(+-1/4)
+    (read at rhmc/cheisdwf.f:140-159);
+  * con_12x12x12.bin: rhmc/_con, an FP64 12^3 chi configuration.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import random_fields
+
+
+def test_rng_seed_pins(seed_pins):
+    """RRANF/G900ST/G900GT and the start-up draw count reproduce every seed
+    pair the reference printed."""
+    assert seed_pins["draws_between"] == 196
+    assert len(seed_pins["pins"]) >= 10
+    for p in seed_pins["pins"]:
+        r = po.Rand(p["seed_in"])
+        assert r.seed() == p["seed_after_startup"], p["source"]
+
+
+def test_rng_lcg_arithmetic():
+    """48-bit LCG: the state after n draws is seed * a^n mod 2^48."""
+    a = 2651554 * 2 ** 24 + 15184245
+    seed = 693764523745.0
+    r = po.Rand(seed)
+    s0 = int(r.seed())
+    for n in range(1, 50):
+        r.rano("yran")
+        assert int(r.seed()) == s0 * pow(a, n, 2 ** 48) % 2 ** 48
+
+
+def test_rng_streams_share_table():
+    """rano(yran) and rano(yrun) share v(97) and the LCG (cheisdwf.f:298,:329)."""
+    r1, r2 = po.Rand(1234567.0), po.Rand(1234567.0)
+    a = [r1.rano("yran") for _ in range(5)]
+    b = [r2.rano("yran") for _ in range(2)] + [r2.rano("yrun")] + \
+        [r2.rano("yran") for _ in range(2)]
+    assert a[:2] == b[:2]
+    assert a[2:] != b[3:]  # the yrun draw moved the shared state
+
+
+def test_gauss_moments():
+    """gauss0: variance 1/2 per component (sqrt(-ln u)); gaussp: variance 1."""
+    r = po.Rand(693764523745.0)
+    g0 = r.gauss0(200000)
+    gp = r.gaussp(200000)
+    assert abs(g0.var() - 0.5) < 0.01
+    assert abs(gp.var() - 1.0) < 0.02
+    assert g0.dtype == np.float32
+
+
+@pytest.mark.parametrize("name,n,power", [("remez4", 25, 0.25), ("remez2", 25, 0.5),
+                                          ("remez2g", 12, 0.5)])
+def test_remez_accuracy(remez, name, n, power):
+    """a-coefficients approximate x^p and b-coefficients x^-p on the
+    spectral range the reference uses."""
+    r = remez[name]
+    lo, hi = (2e-5, 2e2) if n == 25 else (7.5e-5, 67.0)
+    x = np.logspace(np.log10(lo), np.log10(hi), 400)
+    fa = r["anum"][0] + sum(r["anum"][k + 1] / (x + r["aden"][k]) for k in range(n))
+    fb = r["bnum"][0] + sum(r["bnum"][k + 1] / (x + r["bden"][k]) for k in range(n))
+    assert np.max(np.abs(fa / x ** power - 1)) < 1e-3
+    assert np.max(np.abs(fb * x ** power - 1)) < 1e-3
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_operator_adjoint(imass):
+    """<y, M x> == <M^dagger y, x>: dslashd is the adjoint of dslash."""
+    lat = po.make_lat(4, 6, 5)
+    x, chi = random_fields(4, 6, 5, seed=1)
+    y, _ = random_fields(4, 6, 5, seed=2)
+    Mx = po.dslash(lat, x, chi, hpin=0.37, imass=imass)
+    Mdy = po.dslash(lat, y, chi, hpin=0.37, imass=imass, dag=True)
+    a, b = np.vdot(y, Mx), np.vdot(Mdy, x)
+    assert abs(a - b) <= 1e-13 * abs(a)
+
+
+def test_operator_free_field_structure():
+    """chi=0: flavours decouple and M acts identically on both."""
+    lat = po.make_lat(4, 4, 4)
+    x, _ = random_fields(4, 4, 4, seed=3)
+    x[1] = x[0]
+    out = po.dslash(lat, x, np.zeros((3, 64)), imass=1)
+    assert np.array_equal(out[0], out[1])
+
+
+def test_operator_apbc_sign():
+    """Antiperiodic t: a field constant in t picks up the opposite sign on
+    the wrapped hop; ibound=+1 makes the operator translation invariant."""
+    lat = po.make_lat(3, 4, 2, ibound=1)
+    x, chi = random_fields(3, 4, 2, seed=4)
+    chi[:] = 0.3
+    out = po.dslash(lat, x, chi, imass=1)
+    xs = np.roll(x, 1, axis=2)
+    outs = po.dslash(lat, xs, chi, imass=1)
+    assert np.allclose(np.roll(out, 1, axis=2), outs, rtol=0, atol=1e-13)
+
+
+def _dense(lat, chi, imass=1, hpin=0.0):
+    sh = po.spinor_shape(lat)
+    n = int(np.prod(sh))
+    M = np.zeros((n, n), complex)
+    e = np.zeros(n, complex)
+    for i in range(n):
+        e[:] = 0
+        e[i] = 1
+        M[:, i] = po.dslash(lat, e.reshape(sh), chi, imass=imass, hpin=hpin).reshape(-1)
+    return M
+
+
+def test_qmrherm_matches_dense_rational(remez):
+    """x = a0 Phi + sum_k a_k (M^dag M + sigma_k)^-1 Phi against a dense
+    evaluation; converges to the requested residual."""
+    lat = po.make_lat(2, 4, 4)
+    Phi, chi = random_fields(2, 4, 4, seed=5, chi_scale=0.5)
+    M = _dense(lat, chi)
+    A = M.conj().T @ M
+    r = remez["remez4"]
+    x, it, st, _ = po.qmrherm(lat, Phi, chi, r["anum"], r["aden"], 1e-9)
+    assert st == 0 and 2 <= it < 5000
+    w, V = np.linalg.eigh(A)
+    f = r["anum"][0] + sum(r["anum"][k + 1] / (w + r["aden"][k]) for k in range(25))
+    exact = V @ (f * (V.conj().T @ Phi.reshape(-1)))
+    assert np.linalg.norm(x.reshape(-1) - exact) <= 1e-9 * np.linalg.norm(exact)
+
+
+def test_qmrherm_iteration_cap(remez):
+    """The cap is reported (the reference stops silently at niterc)."""
+    lat = po.make_lat(4, 4, 4)
+    Phi, chi = random_fields(4, 4, 4, seed=6)
+    r = remez["remez4"]
+    _, it, st, _ = po.qmrherm(lat, Phi, chi, r["anum"], r["aden"], 1e-12, niterc=3)
+    assert it == 3 and st == 1
+
+
+def test_congrad_solves_normal_equations():
+    lat = po.make_lat(4, 4, 4)
+    Phi, chi = random_fields(4, 4, 4, seed=7)
+    x, it, capped = po.congrad(lat, Phi, chi, Phi, 1e-9)
+    assert not capped
+    r = Phi - po.dslash(lat, po.dslash(lat, x, chi), chi, dag=True)
+    # stopping rule |r|^2 < kferm res^2 on the recursive residual
+    assert np.vdot(r, r).real < 10 * Phi.size * 1e-18
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_force_is_gradient_of_action(remez, imass):
+    """dS/dchi from force (derivs over the guidance poles) against a central
+    finite difference of the action hg + hf evaluated by hamilton, on a
+    small lattice.  Agreement is limited by the two rational approximations
+    (remez2g for the force, remez2 for the action), ~1e-4 relative each."""
+    L, Lt, Ls = 2, 4, 4
+    lat = po.make_lat(L, Lt, Ls, beta=0.475)
+    Phi, chi = random_fields(L, Lt, Ls, seed=8, chi_scale=0.3)
+    kvol = L * L * Lt
+    r2g = remez["remez2g"]
+    r2 = remez["remez2"]
+    R2G = po.remez_struct(r2g["anum"][0], r2g["anum"][1:], r2g["aden"], r2g["bnum"][0],
+                          r2g["bnum"][1:], r2g["bden"])
+    R2 = po.remez_struct(r2["anum"][0], r2["anum"][1:], r2["aden"], r2["bnum"][0],
+                         r2["bnum"][1:], r2["bden"])
+    import ctypes as C
+    lib = po.lib()
+
+    def action(ch):
+        out = np.zeros(5)
+        x = np.empty_like(Phi)
+        it = C.c_int()
+        pp = np.zeros((3, kvol), np.float32)
+        lib.orc_hamilton(C.byref(lat), po._p(Phi), 1e-12, 0.0, 0.0, imass, po._p(ch), po._p(pp),
+                         C.byref(R2), po._p(out), po._p(x), C.byref(it))
+        return out[3]  # s = hg + hf
+
+    dS = np.zeros((3, kvol), np.float32)
+    x = np.empty_like(Phi)
+    itg, itf = C.c_int(), C.c_int()
+    lib.orc_force(C.byref(lat), po._p(Phi), 1e-12, 0.0, 0.0, imass, po._p(chi), C.byref(R2G),
+                  po._p(dS), po._p(x), C.byref(itg), C.byref(itf))
+    rng = np.random.default_rng(0)
+    for _ in range(4):
+        a, i = int(rng.integers(3)), int(rng.integers(kvol))
+        h = 1e-4
+        cp, cm = chi.copy(), chi.copy()
+        cp[a, i] += h
+        cm[a, i] -= h
+        fd = (action(cp) - action(cm)) / (2 * h)
+        assert abs(dS[a, i] - fd) <= 2e-3 * max(1.0, abs(fd)), (a, i, dS[a, i], fd)
