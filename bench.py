@@ -1,0 +1,338 @@
+"""bench.py -- RHMC trajectory throughput of the chiral-Heisenberg domain-wall
+path on B200, in the reference's own algorithm (1 pseudofermion, the shipped
+25/25/12-pole Remez sets, leapfrog with random trajectory length).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--L 24] [--Ls 24]
+
+A step is one RHMC trajectory (heatbath, H0, molecular dynamics with a force
+evaluation per step, H1, Metropolis) at L=Lt=24, Ls=24 on synthetic fields:
+chi drawn from a seeded N(0, 1/beta), the reference's random-number generator
+from its default seed.  Measurements (fermion()) are off.  Printed metric:
+seconds per trajectory (lower is better).
+
+  value     trajectories whose random inputs were staged in HBM before the
+            timed region (chdwf_prog_stage); CUDA events on the library's
+            stream, max over ranks.
+  e2e       the same trajectories through the host-facing driver API with the
+            random numbers drawn on the host and copied in every step.
+  roofline  the dominant solver kernel, timed with CUDA events inside the
+            timed region, against algorithmic bytes per launch.
+  cpu_baseline / --impl reference
+            the CPU oracle (a C restatement of rhmc/cheisdwf.f; the Fortran
+            reference cannot be built here) on the host cores: per-iteration
+            cost of each solve type sampled at the same lattice, times the
+            trajectory's iteration profile.
+
+Multi-GPU: independent Markov chains, one per rank ("replicas only"); value
+is trajectories of all ranks per unit time expressed as seconds per
+trajectory of the whole job.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Workload (the configuration the metric is quoted on): L=Lt=24, Ls=24,
+# beta=0.475, m=0.01 (accepted and unused, as in the reference), am3=1,
+# imass=1, hpin=0; dt=0.1 with mean trajectory length dt*iterl = 1.
+CFG = dict(beta=0.475, am3=1.0, am=0.01, hpin=0.0, imass=1, dt=0.1, iterl=10,
+           seed=693764523745.0, chi_seed=12345)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--L", type=int, default=24)
+    ap.add_argument("--Ls", type=int, default=24)
+    ap.add_argument("--cpu-sample-iters", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        loaded = [s for s in sm if s > 0.5 * mx] if mx else sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def synthetic_chi(L, Lt, beta, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((3, L * L * Lt)) / np.sqrt(beta)
+
+
+# algorithmic bytes per launch of the four solver kernel classes (16 B per
+# complex128 component, V = 8*kvol*Ls components, chi read as REAL*4 planes)
+def kernel_bytes(L, Ls):
+    kvol = L * L * L
+    V = 8 * kvol * Ls
+    chi = 12 * kvol
+    return {0: ("pass-1 M q (+|Mq|^2)", 2 * 16 * V + chi),
+            1: ("pass-1 M^dag + 3-term update (+|r|^2)", 4 * 16 * V + chi),
+            2: ("pass-2 M q + solution accumulate", 4 * 16 * V + chi),
+            3: ("pass-2 M^dag + 3-term update", 4 * 16 * V + chi)}
+
+
+KERNEL_NAMES = {0: "k_lz1_M", 1: "k_lz1_Md", 2: "k_lz2_M", 3: "k_lz2_Md"}
+
+
+def cpu_sample(L, Ls, threads, iters, profile):
+    """Oracle cost per solver iteration for each solve type at this lattice,
+    combined with a trajectory's iteration profile into seconds/trajectory."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    import chiralheisenberg_b200 as chb
+    rz = chb.reference_remez()
+    lat = po.make_lat(L, L, Ls, beta=CFG["beta"], am3=CFG["am3"], threads=threads)
+    rng = np.random.default_rng(7)
+    shape = (2, 4, L, L, L, Ls)
+    Phi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    chi = synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"])
+    t_iter = {}
+    t0all = time.perf_counter()
+    for name, n in (("remez2", 25), ("remez2g", 12)):
+        r = rz[name]
+        t0 = time.perf_counter()
+        po.qmrherm(lat, Phi, chi, r["bnum"], r["bden"], 1e-30, niterc=iters)
+        t_iter[n] = (time.perf_counter() - t0) / iters
+    # force tail: one M apply + derivs per guidance pole (rhmc/cheisdwf.f:733-740)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        po.dslash(lat, Phi, chi)
+    t_apply = (time.perf_counter() - t0) / 2
+    sampled = time.perf_counter() - t0all
+    it25 = profile["it_pf"] + profile["it_h0"] + profile["it_h1"]
+    it12 = profile["it_guid"] + profile["it_force"]
+    s_traj = it25 * t_iter[25] + it12 * t_iter[12] + profile["nforce"] * 12 * t_apply
+    sample = (f"oracle qmrherm at {L}^3x{Ls}: {iters} iterations each of the 25- and 12-pole "
+              f"solves + 2 operator applies ({sampled:.1f} s), scaled by the iteration profile "
+              f"of one trajectory ({it25:.0f} 25-pole + {it12:.0f} 12-pole iterations, "
+              f"{profile['nforce']:.1f} force calls)")
+    return s_traj, sample, {"t_iter_25": t_iter[25], "t_iter_12": t_iter[12], "t_apply": t_apply}
+
+
+def default_profile():
+    p = os.path.join(ROOT, "profiles", "iteration_profile_24x24.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    # iteration counts of a trajectory at 24^3x24 on this workload, from the
+    # GPU arm (same algorithm and stopping rule)
+    return {"it_pf": 530, "it_h0": 530, "it_h1": 530, "it_guid": 5000.0, "it_force": 5000.0,
+            "nforce": 11.0}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    profile = default_profile()
+    vals = []
+    sample = ""
+    for step in range(args.warmup + args.steps):
+        s_traj, sample, _ = cpu_sample(args.L, args.Ls, threads, args.cpu_sample_iters, profile)
+        if step >= args.warmup:
+            vals.append(s_traj)
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "s/trajectory", "value": v, "unit": "s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"RHMC trajectory L=Lt={args.L} Ls={args.Ls}", **CFG},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import chiralheisenberg_b200 as chb
+    torch.cuda.set_device(local_rank)
+    L, Ls = args.L, args.Ls
+    rz = chb.reference_remez()
+    prog = chb.Program(L, L, Ls, CFG["dt"], CFG["beta"], CFG["am3"], CFG["am"], CFG["hpin"],
+                       CFG["imass"], CFG["iterl"], rz["remez2"], rz["remez4"], rz["remez2g"],
+                       device=local_rank)
+    prog.set_chi(synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"] + rank))
+    prog.startup(CFG["seed"] + 1000.0 * rank)
+    prog.set_measure(5, False)
+    stream = torch.cuda.ExternalStream(prog.stream, device=local_rank)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        prog.sweep()
+
+    def timed(staged):
+        if staged:
+            prog.stage(args.steps)
+        recs = []
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            recs.append(prog.sweep())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()), recs
+
+    prog.timing(True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    n0 = chb.kernel_launches()
+    ms_value, recs = timed(staged=True)
+    launches = chb.kernel_launches() - n0
+    clk = clocks.stop()
+    kms, ktimed, klaunched = prog.timing_read()
+    prog.timing(False)
+    ms_e2e, recs_e2e = timed(staged=False)
+
+    # whole job: steps*world trajectories in the slowest rank's time
+    ntraj = args.steps * world
+    value = (ms_value / 1e3) / ntraj
+    e2e = (ms_e2e / 1e3) / ntraj
+    kvol = L * L * L
+    h2d = 64 * kvol * Ls + 12 * kvol          # heatbath Gaussians + momenta
+    d2h = 12 * kvol + 64                      # momenta for vel2 + scalars
+    kb = kernel_bytes(L, Ls)
+    dom = int(np.argmax(kms))
+    avg_ms = kms[dom] / max(ktimed[dom], 1)
+    achieved = kb[dom][1] / (avg_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_24x24.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(KERNEL_NAMES[dom])
+    prof = {"it_pf": float(np.mean([r.it_pf for r in recs])),
+            "it_h0": float(np.mean([r.it_h0 for r in recs])),
+            "it_h1": float(np.mean([r.it_h1 for r in recs])),
+            "it_guid": float(np.mean([r.it_guid for r in recs])),
+            "it_force": float(np.mean([r.it_force for r in recs])),
+            "nforce": float(np.mean([r.nforce for r in recs]))}
+    line = {"metric": "s/trajectory", "value": value, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_value / args.steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"RHMC trajectory L=Lt={L} Ls={Ls}", "precision": "fp64",
+                       "parallelism": f"replicas{world}", "l2": "fields larger than L2 "
+                       "(solver working set > 126 MB)", **CFG},
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "what": kb[dom][0],
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "bytes_per_launch": kb[dom][1], "avg_launch_us": avg_ms * 1e3},
+            "kernel_avg_us": {KERNEL_NAMES[k]: kms[k] / max(ktimed[k], 1) * 1e3 for k in range(4)},
+            "gpu_launches": launches,
+            "iteration_profile": prof,
+            "trajectories": [{"dH": r.dH, "accepted": r.accepted, "nsteps": r.nsteps}
+                             for r in recs],
+            "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        s_cpu, sample, _ = cpu_sample(L, Ls, threads, args.cpu_sample_iters, prof)
+        line["cpu_baseline"] = {"value": s_cpu, "unit": "s", "cores": threads, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    prog.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -31,12 +31,23 @@ LIB_PATH = os.path.join(_HERE, "libchdwf.so")
 
 CHDWF_OK, CHDWF_ITER_CAP, CHDWF_NONFINITE, CHDWF_CUDA_ERROR, CHDWF_BAD_ARG = 0, 1, 2, 3, 4
 
-# every symbol include/chdwf.h declares (checked by the CPU test suite)
+# every symbol include/*.h declares (checked by the CPU test suite)
 EXPORTS = (
     "chdwf_create", "chdwf_destroy", "chdwf_set_para", "chdwf_last_error", "chdwf_version",
     "chdwf_dslash", "chdwf_dslashd", "chdwf_qmrherm", "chdwf_derivs", "chdwf_congrad",
     "chdwf_force", "chdwf_hamilton", "chdwf_dslash_dev", "chdwf_qmrherm_dev",
     "chdwf_congrad_dev",
+    "chdwf_traj_set_remez", "chdwf_traj_set_chi", "chdwf_traj_get_chi", "chdwf_traj_begin",
+    "chdwf_traj_heatbath", "chdwf_traj_heatbath_dev", "chdwf_traj_set_momenta",
+    "chdwf_traj_get_momenta", "chdwf_traj_hamilton", "chdwf_traj_force", "chdwf_traj_get_force",
+    "chdwf_traj_get_phi", "chdwf_traj_update_momenta", "chdwf_traj_update_chi",
+    "chdwf_traj_accept", "chdwf_traj_sync", "chdwf_traj_propagator",
+    "chdwf_traj_set_momenta_dev", "chdwf_timing", "chdwf_timing_read", "chdwf_prog_stage",
+    "chdwf_get_stream", "chdwf_kernel_launches",
+    "chdwf_prog_create", "chdwf_prog_destroy", "chdwf_prog_context", "chdwf_prog_set_remez",
+    "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
+    "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
+    "chdwf_prog_correlators", "chdwf_prog_last_error",
 )
 
 _lib = None
@@ -79,8 +90,164 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_dslash_dev.argtypes = [P, P, P, P, F, I, I, P]
     L.chdwf_qmrherm_dev.argtypes = [P, P, F, PI, F, I, P, P, I, I, P, P, P]
     L.chdwf_congrad_dev.argtypes = [P, P, F, PI, F, I, P, P]
+    L.chdwf_traj_set_remez.argtypes = [P, I, P, P, P, P, I]
+    L.chdwf_traj_set_chi.argtypes = [P, P]
+    L.chdwf_traj_get_chi.argtypes = [P, P, I]
+    L.chdwf_traj_begin.argtypes = [P]
+    L.chdwf_traj_heatbath.argtypes = [P, P, F, F, F, I, PI]
+    L.chdwf_traj_heatbath_dev.argtypes = [P, P, F, F, F, I, PI]
+    L.chdwf_traj_set_momenta.argtypes = [P, P]
+    L.chdwf_traj_get_momenta.argtypes = [P, P]
+    L.chdwf_traj_hamilton.argtypes = [P, F, F, F, I, P, PI]
+    L.chdwf_traj_force.argtypes = [P, F, F, F, I, PI, PI]
+    L.chdwf_traj_get_force.argtypes = [P, P]
+    L.chdwf_traj_get_phi.argtypes = [P, P]
+    L.chdwf_traj_update_momenta.argtypes = [P, F]
+    L.chdwf_traj_update_chi.argtypes = [P, F]
+    L.chdwf_traj_accept.argtypes = [P]
+    L.chdwf_traj_sync.argtypes = [P]
+    L.chdwf_traj_propagator.argtypes = [P, I, I, F, F, F, I, P, PI]
+    L.chdwf_prog_create.argtypes = [C.POINTER(P), I, I, I, F, F, F, F, F, I, I, I]
+    L.chdwf_prog_destroy.argtypes = [P]
+    L.chdwf_prog_destroy.restype = None
+    L.chdwf_prog_context.argtypes = [P]
+    L.chdwf_prog_context.restype = P
+    L.chdwf_prog_set_remez.argtypes = [P, I, P, P, P, P, I]
+    L.chdwf_prog_set_chi.argtypes = [P, P]
+    L.chdwf_prog_get_chi.argtypes = [P, P]
+    L.chdwf_prog_startup.argtypes = [P, D]
+    L.chdwf_prog_seed.argtypes = [P]
+    L.chdwf_prog_seed.restype = D
+    L.chdwf_prog_set_measure.argtypes = [P, I, I]
+    L.chdwf_prog_set_residuals.argtypes = [P, F, F, F]
+    L.chdwf_prog_sweep.argtypes = [P, P]
+    L.chdwf_prog_correlators.argtypes = [P, P]
+    L.chdwf_prog_last_error.argtypes = [P]
+    L.chdwf_prog_last_error.restype = C.c_char_p
+    L.chdwf_prog_stage.argtypes = [P, I]
+    L.chdwf_traj_set_momenta_dev.argtypes = [P, P]
+    L.chdwf_timing.argtypes = [P, I]
+    L.chdwf_timing_read.argtypes = [P, P, P, P]
+    L.chdwf_get_stream.argtypes = [P]
+    L.chdwf_get_stream.restype = P
+    L.chdwf_kernel_launches.restype = C.c_longlong
     _lib = L
     return L
+
+
+class SweepRecord(C.Structure):
+    """chdwf_sweep_record (include/chdwf_program.h)."""
+    _fields_ = [("H0", C.c_double), ("H1", C.c_double), ("dH", C.c_double), ("dS", C.c_double),
+                ("S0", C.c_double), ("S1", C.c_double), ("hg", C.c_double), ("hp", C.c_double),
+                ("y", C.c_float), ("x", C.c_float), ("accepted", C.c_int), ("nsteps", C.c_int),
+                ("it_pf", C.c_int), ("it_h0", C.c_int), ("it_h1", C.c_int),
+                ("it_guid", C.c_double), ("it_force", C.c_double), ("nforce", C.c_int),
+                ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
+                ("vel2", C.c_float), ("measured", C.c_int), ("cond", C.c_float * 3),
+                ("susc", C.c_float * 3), ("condmod", C.c_float), ("susctot", C.c_float),
+                ("ancgm", C.c_float)]
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class Program:
+    """The main loop of program dwf3d (rhmc/cheisdwf.f:207-399) on the GPU:
+    host random numbers and control flow, resident fields (see
+    include/chdwf_program.h).  Parameters are those of the 'midout' file."""
+
+    def __init__(self, ksize, ksizet, kthird, dt, beta, am3, am, hpin, imass, iterl, remez2,
+                 remez4, remez2g, device=0):
+        self.lib = load_library()
+        self.kvol = ksize * ksize * ksizet
+        self.Lt = ksizet
+        h = C.c_void_p()
+        rc = self.lib.chdwf_prog_create(C.byref(h), ksize, ksizet, kthird, dt, beta, am3, am,
+                                        hpin, imass, iterl, device)
+        if rc != CHDWF_OK:
+            raise ChdwfError(rc, self.lib.chdwf_last_error(None).decode())
+        self.h = h
+        for which, r in ((2, remez2), (4, remez4), (22, remez2g)):
+            arrs = [np.ascontiguousarray(r[k], dtype=np.float64)
+                    for k in ("anum", "aden", "bnum", "bden")]
+            self._check(self.lib.chdwf_prog_set_remez(self.h, which, *[_ptr(a) for a in arrs],
+                                                      len(arrs[1])))
+            setattr(self, f"_keep{which}", arrs)
+
+    def _check(self, rc):
+        if rc != CHDWF_OK:
+            msg = self.lib.chdwf_prog_last_error(self.h).decode()
+            raise (IterationCapError if rc == CHDWF_ITER_CAP else ChdwfError)(rc, msg)
+
+    def startup(self, seed):
+        self._check(self.lib.chdwf_prog_startup(self.h, float(seed)))
+
+    def seed(self):
+        return self.lib.chdwf_prog_seed(self.h)
+
+    def set_chi(self, chi):
+        chi = np.ascontiguousarray(chi, dtype=np.float64)
+        self._check(self.lib.chdwf_prog_set_chi(self.h, _ptr(chi)))
+
+    def get_chi(self):
+        chi = np.empty((3, self.kvol), dtype=np.float64)
+        self._check(self.lib.chdwf_prog_get_chi(self.h, _ptr(chi)))
+        return chi
+
+    def set_measure(self, iprint=5, measure=True):
+        self._check(self.lib.chdwf_prog_set_measure(self.h, iprint, 1 if measure else 0))
+
+    def set_residuals(self, rescga, rescgg, rescgm):
+        self._check(self.lib.chdwf_prog_set_residuals(self.h, rescga, rescgg, rescgm))
+
+    def sweep(self) -> SweepRecord:
+        rec = SweepRecord()
+        self._check(self.lib.chdwf_prog_sweep(self.h, C.byref(rec)))
+        return rec
+
+    def correlators(self):
+        cf = np.empty((2, 2, self.Lt, 2), dtype=np.float32)
+        self._check(self.lib.chdwf_prog_correlators(self.h, _ptr(cf)))
+        return cf
+
+    def stage(self, ntraj):
+        """Draw the next ntraj trajectories' random inputs and place them in HBM."""
+        self._check(self.lib.chdwf_prog_stage(self.h, ntraj))
+
+    @property
+    def context(self):
+        return self.lib.chdwf_prog_context(self.h)
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the program's context, as an integer handle."""
+        return self.lib.chdwf_get_stream(self.context) or 0
+
+    def timing(self, enable=True):
+        self._check(self.lib.chdwf_timing(self.context, 1 if enable else 0))
+
+    def timing_read(self):
+        ms = np.zeros(4, dtype=np.float64)
+        timed = np.zeros(4, dtype=np.int64)
+        launched = np.zeros(4, dtype=np.int64)
+        self._check(self.lib.chdwf_timing_read(self.context, _ptr(ms), _ptr(timed),
+                                               _ptr(launched)))
+        return ms, timed, launched
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chdwf_prog_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _ptr(a):
@@ -218,3 +385,37 @@ class Lattice:
 
 def version() -> str:
     return load_library().chdwf_version().decode()
+
+
+def kernel_launches() -> int:
+    """Kernels libchdwf has launched in this process."""
+    return int(load_library().chdwf_kernel_launches())
+
+
+DATA_DIR = os.path.join(_HERE, "data")
+
+
+def read_remez(name: str, n: int, path: str = None) -> dict:
+    """Read a Remez data file in the reference's format (rhmc/remez*, read at
+    rhmc/cheisdwf.f:140-159): a0; n lines "a_k, sigma_k"; b0; n lines
+    "b_k, sigma_k".  Returns anum (a0..a_n), aden, bnum (b0..b_n), bden."""
+    vals = []
+    for line in open(path or os.path.join(DATA_DIR, name)):
+        line = line.replace(",", " ").replace("d", "e").replace("D", "e").strip()
+        if line:
+            vals.append([float(t) for t in line.split()])
+    if len(vals) < 2 * n + 2:
+        raise ValueError(f"{name}: expected {2 * n + 2} lines, found {len(vals)}")
+    a0 = vals[0][0]
+    b0 = vals[n + 1][0]
+    return {"anum": np.array([a0] + [v[0] for v in vals[1:n + 1]]),
+            "aden": np.array([v[1] for v in vals[1:n + 1]]),
+            "bnum": np.array([b0] + [v[0] for v in vals[n + 2:2 * n + 2]]),
+            "bden": np.array([v[1] for v in vals[n + 2:2 * n + 2]])}
+
+
+def reference_remez() -> dict:
+    """The three rational approximations the reference ships: remez2 and
+    remez4 (25 poles), remez2g (12 poles)."""
+    return {"remez2": read_remez("remez2", 25), "remez4": read_remez("remez4", 25),
+            "remez2g": read_remez("remez2g", 12)}

@@ -21,8 +21,11 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libchdwf.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# host code is compiled without fused multiply-add so the REAL*4/REAL*8
+# host arithmetic (Gaussians, correlators, Hamiltonian sums) is reproducible
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-              "--expt-relaxed-constexpr", "-I", CSRC, "-I", os.path.join(ROOT, "include")]
+              "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr",
+              "-I", CSRC, "-I", os.path.join(ROOT, "include")]
 
 
 def _nvcc() -> str:
@@ -63,7 +66,11 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
             continue
         cmd = [nvcc] + _host_cxx() + ARCH + NVCC_FLAGS + ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [nvcc] + _host_cxx() + NVCC_FLAGS + ["-x", "c++", "-c", src, "-o", obj]
+            cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+            cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc)), "include")
+            cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall",
+                   "-I", CSRC, "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                   "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
@@ -72,7 +79,8 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     _wait(procs)
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [nvcc] + _host_cxx() + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [nvcc] + _host_cxx() + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart",
+                                                                             "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -47,6 +47,11 @@ Ctx::~Ctx() {
     if (chif) cudaFree(chif);
     if (dS) cudaFree(dS);
     if (red) cudaFree(red);
+    if (chit) cudaFree(chit);
+    if (pp) cudaFree(pp);
+    if (phi) cudaFree(phi);
+    if (gauss) cudaFree(gauss);
+    if (walls) cudaFree(walls);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -66,6 +71,37 @@ static thread_local std::string g_create_err;
 extern "C" {
 
 const char* chdwf_version(void) { return "chdwf-b200 0.1 (sm_100a)"; }
+
+int chdwf_timing(chdwf_ctx* ctx, int enable) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return CHDWF_BAD_ARG;
+    cudaSetDevice(c->device);
+    if (enable) {
+        c->lz.timer.enable();
+        c->lz.timer.reset();
+    } else {
+        c->lz.timer.release();
+    }
+    return c->status_of(cudaGetLastError(), "timing");
+}
+
+long long chdwf_kernel_launches(void) { return launches_total(); }
+
+void* chdwf_get_stream(chdwf_ctx* ctx) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    return c ? (void*)c->stream : nullptr;
+}
+
+int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !ms || !timed || !launched) return CHDWF_BAD_ARG;
+    for (int k = 0; k < KernelTimer::kClasses; k++) {
+        ms[k] = c->lz.timer.total_ms[k];
+        timed[k] = c->lz.timer.count[k];
+        launched[k] = c->lz.timer.launches[k];
+    }
+    return CHDWF_OK;
+}
 
 int chdwf_create(chdwf_ctx** out, int ksize, int ksizet, int kthird, int device) {
     if (!out) return CHDWF_BAD_ARG;

@@ -1,8 +1,14 @@
 // blas.cu -- small field utilities: chi rounding, force initialisation,
 // scaling and deterministic reductions.
+#include <atomic>
+
 #include "internal.h"
 
 namespace chdwf {
+
+static std::atomic<long long> g_launches{0};
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 __global__ void k_round_chi(const double* __restrict__ chi, float* __restrict__ chif, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -11,7 +17,7 @@ __global__ void k_round_chi(const double* __restrict__ chi, float* __restrict__ 
 
 void launch_round_chi(const double* chi, float* chif, int kvol, cudaStream_t st) {
     const int n = 3 * kvol;
-    k_round_chi<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(chi, chif, n);
+    k_round_chi<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(chi, chif, n); count_launches(1);
 }
 
 // dSdchi = 2*beta*chi with 2*beta a REAL*4 product (cheisdwf.f:494-498)
@@ -23,7 +29,7 @@ __global__ void k_dsdchi_init(const double* __restrict__ chi, float twob, float*
 
 void launch_dsdchi_init(const double* chi, float twobeta, float* dS, int kvol, cudaStream_t st) {
     const int n = 3 * kvol;
-    k_dsdchi_init<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(chi, twobeta, dS, n);
+    k_dsdchi_init<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(chi, twobeta, dS, n); count_launches(1);
 }
 
 __global__ void k_scale(double2* __restrict__ out, const double2* __restrict__ in, double a,
@@ -33,7 +39,7 @@ __global__ void k_scale(double2* __restrict__ out, const double2* __restrict__ i
 }
 
 void launch_scale(double2* out, const double2* in, double a, int64_t n, cudaStream_t st) {
-    k_scale<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(out, in, a, n);
+    k_scale<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(out, in, a, n); count_launches(1);
 }
 
 int reduce_blocks(int64_t n) {
@@ -79,15 +85,15 @@ __global__ void k_final_sum(const double* __restrict__ part, int nb, double* __r
 
 void launch_norm2(const double2* v, int64_t n, double* partials, double* out, cudaStream_t st) {
     const int nb = reduce_blocks(n);
-    k_norm2_part<<<nb, kThreads, 0, st>>>(v, n, partials);
-    k_final_sum<<<1, kThreads, 0, st>>>(partials, nb, out);
+    k_norm2_part<<<nb, kThreads, 0, st>>>(v, n, partials); count_launches(1);
+    k_final_sum<<<1, kThreads, 0, st>>>(partials, nb, out); count_launches(1);
 }
 
 void launch_redot(const double2* a, const double2* b, int64_t n, double* partials, double* out,
                   cudaStream_t st) {
     const int nb = reduce_blocks(n);
-    k_redot_part<<<nb, kThreads, 0, st>>>(a, b, n, partials);
-    k_final_sum<<<1, kThreads, 0, st>>>(partials, nb, out);
+    k_redot_part<<<nb, kThreads, 0, st>>>(a, b, n, partials); count_launches(1);
+    k_final_sum<<<1, kThreads, 0, st>>>(partials, nb, out); count_launches(1);
 }
 
 }  // namespace chdwf

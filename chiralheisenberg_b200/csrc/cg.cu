@@ -195,9 +195,9 @@ cudaError_t cg_solve(CgWork& w, const Geom& g, const double2* phi, float res, co
     const int64_t cap = hc.niterc;
     while (launched < cap) {
         for (int c = 0; c < chunk && launched < cap; c++, launched++) {
-            if (imass == 3) { k_cg1<3><<<nb, kThreads, 0, st>>>(a); k_cg2<3><<<nb, kThreads, 0, st>>>(a); }
-            else { k_cg1<1><<<nb, kThreads, 0, st>>>(a); k_cg2<1><<<nb, kThreads, 0, st>>>(a); }
-            k_cg3<<<nbf, kThreads, 0, st>>>(a);
+            if (imass == 3) { k_cg1<3><<<nb, kThreads, 0, st>>>(a); count_launches(1); k_cg2<3><<<nb, kThreads, 0, st>>>(a); count_launches(1); }
+            else { k_cg1<1><<<nb, kThreads, 0, st>>>(a); count_launches(1); k_cg2<1><<<nb, kThreads, 0, st>>>(a); count_launches(1); }
+            k_cg3<<<nbf, kThreads, 0, st>>>(a); count_launches(1);
         }
         cudaEventRecord(ev[nchunk & 1], st);
         if (nchunk >= 1) {

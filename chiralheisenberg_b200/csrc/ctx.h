@@ -8,6 +8,13 @@
 
 namespace chdwf {
 
+// One rational approximation as the reference reads it (rhmc/cheisdwf.f:
+// 140-159): anum[0] = a0, anum[1..n], aden = sigma_1..n; same for b.
+struct RemezSet {
+    int n = 0;
+    std::vector<double> anum, aden, bnum, bden;
+};
+
 struct Ctx {
     static constexpr int kSpin = 4;
     int device = 0;
@@ -24,11 +31,19 @@ struct Ctx {
     CgWork cg;
     LzStats last_lz{};
     std::string err;
+    // resident trajectory state (traj.cu)
+    double* chit = nullptr;             // /trial/ chit
+    float* pp = nullptr;                // /trial/ pp (REAL*4)
+    double2* phi = nullptr;             // pseudofermion field
+    float* gauss = nullptr;             // staging of the heatbath Gaussians
+    double2* walls = nullptr;           // propagator wall slices
+    RemezSet rz2, rz4, rz2g;
 
     ~Ctx();
     bool fail(cudaError_t e, const char* where);
     int status_of(cudaError_t e, const char* where);
     cudaError_t ensure_fields();
+    cudaError_t ensure_traj();
     cudaError_t upload_chi(const double* chi_host);
 };
 

@@ -39,6 +39,7 @@ void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const
     } else {
         if (imass == 1) LAUNCH(true, 1); else if (imass == 3) LAUNCH(true, 3); else LAUNCH(true, 0);
     }
+    count_launches(1);
 #undef LAUNCH
 }
 
@@ -72,6 +73,7 @@ void launch_wall_dslash64(int npole, double2* out, const double2* in, const floa
     if (imass == 1) k_wall_dslash64<1><<<grid, kThreads, 0, st>>>(out, in, chif, g2, diag, hp, apbc);
     else if (imass == 3) k_wall_dslash64<3><<<grid, kThreads, 0, st>>>(out, in, chif, g2, diag, hp, apbc);
     else k_wall_dslash64<0><<<grid, kThreads, 0, st>>>(out, in, chif, g2, diag, hp, apbc);
+    count_launches(1);
 }
 
 // ---- derivs ---------------------------------------------------------------
@@ -138,6 +140,7 @@ void launch_derivs_walls(int npole, const double2* xw, const double2* x2w, const
     const unsigned nb = (unsigned)((g.kvol + kThreads - 1) / kThreads);
     if (imass == 1) k_derivs_walls<1><<<nb, kThreads, 0, st>>>(npole, xw, x2w, anum1, dSdchi, g2);
     else if (imass == 3) k_derivs_walls<3><<<nb, kThreads, 0, st>>>(npole, xw, x2w, anum1, dSdchi, g2);
+    count_launches(1);
 }
 
 template <int IMASS>
@@ -168,6 +171,7 @@ void launch_derivs_full(const double2* R, const double2* X2, double anum, int im
     const double tzi = -2 * anum;
     if (imass == 1) k_derivs_full<1><<<nb, kThreads, 0, st>>>(R, X2, tzi, dSdchi, g);
     else if (imass == 3) k_derivs_full<3><<<nb, kThreads, 0, st>>>(R, X2, tzi, dSdchi, g);
+    count_launches(1);
 }
 
 }  // namespace chdwf

@@ -11,6 +11,11 @@
 
 namespace chdwf {
 
+// Number of kernels this library has launched (all contexts); read through
+// chdwf_kernel_launches().
+void count_launches(long long n);
+long long launches_total();
+
 constexpr int kMaxPoles = 32;
 constexpr int kMaxIter = 5000;     // niterc of qmrherm (rhmc/cheisdwf.f:603)
 constexpr int kThreads = 256;

@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <utility>
 
 #include "dwf_stencil.cuh"
 #include "lanczos.h"
@@ -285,20 +286,80 @@ __global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* nrm2) {
 }
 
 template <int IMASS>
-static void launch_pass1(const LzArgs& a, unsigned nb, cudaStream_t st) {
-    k_lz1_M<IMASS><<<nb, kThreads, 0, st>>>(a);
-    k_lz1_Md<IMASS><<<nb, kThreads, 0, st>>>(a);
+static void launch_pass1(const LzArgs& a, unsigned nb, cudaStream_t st, KernelTimer& tm) {
+    tm.begin(0, st);
+    k_lz1_M<IMASS><<<nb, kThreads, 0, st>>>(a); count_launches(1);
+    tm.end(st);
+    tm.begin(1, st);
+    k_lz1_Md<IMASS><<<nb, kThreads, 0, st>>>(a); count_launches(1);
+    tm.end(st);
 }
 
 template <int IMASS>
-static void launch_pass2(const LzArgs& a, unsigned nb, int j, int m, int iflag, cudaStream_t st) {
+static void launch_pass2(const LzArgs& a, unsigned nb, int j, int m, int iflag, cudaStream_t st,
+                         KernelTimer& tm) {
     const int apply = j < m;
+    if (apply) tm.begin(2, st);
     if (iflag == 0) k_lz2_M<IMASS, 0><<<nb, kThreads, 0, st>>>(a, j, apply);
     else k_lz2_M<IMASS, 1><<<nb, kThreads, 0, st>>>(a, j, apply);
-    if (apply) k_lz2_Md<IMASS><<<nb, kThreads, 0, st>>>(a, j);
+    count_launches(1);
+    if (apply) {
+        tm.end(st);
+        tm.begin(3, st);
+        k_lz2_Md<IMASS><<<nb, kThreads, 0, st>>>(a, j); count_launches(1);
+        tm.end(st);
+    }
 }
 
-LzWork::~LzWork() { release(); }
+// ---- kernel timer ----------------------------------------------------------
+void KernelTimer::enable() {
+    if (enabled) return;
+    for (int i = 0; i < 2 * kPool; i++) cudaEventCreate(&ev[i]);
+    enabled = true;
+    reset();
+}
+
+void KernelTimer::release() {
+    if (!enabled) return;
+    for (int i = 0; i < 2 * kPool; i++) cudaEventDestroy(ev[i]);
+    enabled = false;
+}
+
+void KernelTimer::reset() {
+    used = 0;
+    for (int c = 0; c < kClasses; c++) { total_ms[c] = 0; count[c] = 0; launches[c] = 0; }
+}
+
+void KernelTimer::begin(int c, cudaStream_t st) {
+    if (!enabled) return;
+    launches[c]++;
+    if (used >= kPool) return;          // pool full: the launch is counted, not timed
+    cls[used] = c;
+    cudaEventRecord(ev[2 * used], st);
+}
+
+void KernelTimer::end(cudaStream_t st) {
+    if (!enabled || used >= kPool) return;
+    cudaEventRecord(ev[2 * used + 1], st);
+    used++;
+}
+
+void KernelTimer::collect() {
+    if (!enabled) return;
+    for (int i = 0; i < used; i++) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) {
+            total_ms[cls[i]] += ms;
+            count[cls[i]]++;
+        }
+    }
+    used = 0;
+}
+
+LzWork::~LzWork() {
+    release();
+    timer.release();
+}
 
 void LzWork::release() {
     if (ctl) cudaFree(ctl);
@@ -390,7 +451,7 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
 
     // beta_1 = |Phi|, r_1 = Phi
     launch_norm2(phi, g.kferm, w.part + nb + 8, w.part + nb, st);
-    k_lz_init<<<1, 1, 0, st>>>(w.ctl, w.hist, w.part + nb);
+    k_lz_init<<<1, 1, 0, st>>>(w.ctl, w.hist, w.part + nb); count_launches(1);
     cudaMemcpyAsync(w.rb[1], phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
 
     // pass 1: launch chunks of iterations, poll the mapped flag with one
@@ -402,8 +463,8 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
     int launched = 0, nchunk = 0;
     while (launched < kMaxIter) {
         for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
-            if (imass == 3) launch_pass1<3>(a, nb, st);
-            else launch_pass1<1>(a, nb, st);
+            if (imass == 3) launch_pass1<3>(a, nb, st, w.timer);
+            else launch_pass1<1>(a, nb, st, w.timer);
         }
         cudaEventRecord(ev[nchunk & 1], st);
         if (nchunk >= 1) {
@@ -411,6 +472,28 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
             if (*(volatile int*)w.hflag_host) break;
         }
         nchunk++;
+    }
+    // no-op launches after convergence are not timed as work
+    if (w.timer.enabled) {
+        cudaStreamSynchronize(st);
+        LzCtl hm;
+        cudaMemcpy(&hm, w.ctl, sizeof(hm), cudaMemcpyDeviceToHost);
+        // pairs beyond the converged iteration ran as immediate returns
+        int keep = 0;
+        for (int i = 0, it = 0; i < w.timer.used; i++) {
+            if (w.timer.cls[i] == 0) it++;
+            const bool real = it <= hm.m && !(w.timer.cls[i] == 1 && it >= hm.m);
+            if (real) {
+                w.timer.cls[keep] = w.timer.cls[i];
+                std::swap(w.timer.ev[2 * keep], w.timer.ev[2 * i]);
+                std::swap(w.timer.ev[2 * keep + 1], w.timer.ev[2 * i + 1]);
+                keep++;
+            }
+        }
+        w.timer.launches[0] -= launched - hm.m;
+        w.timer.launches[1] -= launched - hm.m + 1;
+        w.timer.used = keep;
+        w.timer.collect();
     }
     cudaEventSynchronize(ev[nchunk & 1]);
     cudaEventDestroy(ev[0]);
@@ -426,13 +509,21 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
     if (m < 1) return cudaErrorUnknown;
 
     // coefficients, then pass 2
-    k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag);
+    k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag); count_launches(1);
     launch_scale(x, phi, anum[0], g.kferm, st);                       // x = a0 Phi (:628)
     if (iflag) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
     cudaMemcpyAsync(w.rb[1], phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
     for (int j = 1; j <= m; j++) {
-        if (imass == 3) launch_pass2<3>(a, nb, j, m, iflag, st);
-        else launch_pass2<1>(a, nb, j, m, iflag, st);
+        if (imass == 3) launch_pass2<3>(a, nb, j, m, iflag, st, w.timer);
+        else launch_pass2<1>(a, nb, j, m, iflag, st, w.timer);
+        if (w.timer.enabled && w.timer.used >= KernelTimer::kPool - 2) {
+            cudaStreamSynchronize(st);
+            w.timer.collect();
+        }
+    }
+    if (w.timer.enabled) {
+        cudaStreamSynchronize(st);
+        w.timer.collect();
     }
     if (iflag) {
         // X2 = M x_k on the walls, then derivs pole by pole (:733-740)

@@ -25,6 +25,28 @@ struct LzStats {
     int pass1_launches;
 };
 
+// Optional CUDA-event timing of the four stencil kernels of the solver
+// (0: pass-1 M, 1: pass-1 M^dagger + update, 2: pass-2 M + accumulate,
+// 3: pass-2 M^dagger + update).  Events bracket each launch on the solver's
+// stream; durations are summed when the solve synchronises.
+struct KernelTimer {
+    static constexpr int kClasses = 4;
+    static constexpr int kPool = 2 * kMaxIter + 256;
+    bool enabled = false;
+    cudaEvent_t ev[2 * kPool] = {};
+    int cls[kPool] = {};
+    int used = 0;
+    double total_ms[kClasses] = {0, 0, 0, 0};
+    long long count[kClasses] = {0, 0, 0, 0};
+    long long launches[kClasses] = {0, 0, 0, 0};
+    void enable();
+    void release();
+    void begin(int c, cudaStream_t st);   // records the start event of one launch
+    void end(cudaStream_t st);
+    void collect();                       // after a synchronisation
+    void reset();
+};
+
 struct LzWork {
     Geom geom{};
     LzCtl* ctl = nullptr;
@@ -38,6 +60,7 @@ struct LzWork {
     int xw_poles = 0;
     int* hflag_host = nullptr;
     int* hflag_dev = nullptr;
+    KernelTimer timer;
     ~LzWork();
     void release();
     cudaError_t ensure(const Geom& g, int npole_max);

@@ -1,0 +1,372 @@
+// program.cpp -- host driver mirroring program dwf3d (rhmc/cheisdwf.f:1-466)
+// over the resident C ABI: random numbers and control flow on the host, every
+// field operation on the GPU.
+//
+// The random stream of a trajectory does not depend on the fields: the
+// heatbath Gaussians, the momenta, the trajectory-end draws and the
+// Metropolis draw are fixed by the generator state alone.  The driver
+// therefore generates trajectory n+1's heatbath Gaussians on a host thread
+// while trajectory n runs on the GPU.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <future>
+#include <string>
+#include <vector>
+
+#include "../../include/chdwf.h"
+#include "../../include/chdwf_program.h"
+#include "rng.h"
+
+namespace {
+
+struct Draws {                       // the random numbers of one trajectory
+    std::vector<float> gauss;        // 2*4*kthird gauss0 calls, (kvol,2) each
+    std::vector<float> pp;           // pp(kvol,3) from two gaussp calls
+    std::vector<float> ytest;        // trajectory-end draws, one per MD step
+    float x = 0.0f;                  // Metropolis draw
+    float yferm = 0.0f;              // fermion()'s draw (measurement sweeps)
+    bool measured = false;
+    double seed_after = 0.0;
+};
+
+}  // namespace
+
+struct Staged {                      // a trajectory's random inputs already in HBM
+    Draws d;
+    float* gauss_dev = nullptr;
+    float* pp_dev = nullptr;
+};
+
+struct chdwf_prog {
+    chdwf_ctx* ctx = nullptr;
+    std::deque<Staged> staged;
+    int L = 0, Lt = 0, Ls = 0, kvol = 0;
+    float dt = 0.1f, beta = 0.5f, am3 = 1.0f, am = 0.0f, hpin = 0.0f;
+    int imass = 1, iterl = 1, iprint = 5, measure = 1, isweep = 0;
+    float rescga = 0.000000001f, rescgg = 0.000001f, rescgm = 0.000000001f;   // :32-33
+    chdwf::Rng rng;
+    bool have_next = false;
+    std::future<Draws> next;
+    std::vector<float> cferm;        // cferm1(0:Lt-1,2), cferm2 as complex64 pairs
+    std::string err;
+
+    // All random numbers of the next trajectory, in the reference's order.
+    Draws draw(int sweep_index) {
+        Draws d;
+        const int64_t kv = kvol;
+        d.gauss.resize(16 * (size_t)kv * Ls);
+        for (int c = 0; c < 8 * Ls; c++) rng.gauss0(kv, d.gauss.data() + (size_t)c * 2 * kv);  // :221-230
+        std::vector<float> ps(2 * kv);
+        d.pp.resize(3 * kv);
+        rng.gaussp(kv, ps.data());                                                          // :249-253
+        std::memcpy(d.pp.data(), ps.data(), sizeof(float) * 2 * kv);
+        rng.gaussp(kv, ps.data());                                                          // :254-257
+        std::memcpy(d.pp.data() + 2 * kv, ps.data(), sizeof(float) * kv);
+        const float proby = 1.0f / (float)iterl;                                            // :164
+        for (int iter = 1; iter <= 1000; iter++) {                                          // :281
+            const float y = rng.rano_yrun();                                                // :298
+            d.ytest.push_back(y);
+            if (y < proby) break;
+        }
+        d.x = rng.rano_yrun();                                                              // :329
+        d.measured = measure && (sweep_index / iprint) * iprint == sweep_index;
+        if (d.measured) d.yferm = rng.rano_yran();                                          // :929
+        d.seed_after = rng.seed();
+        return d;
+    }
+
+    void prefetch(int sweep_index) {
+        next = std::async(std::launch::async, [this, sweep_index] { return draw(sweep_index); });
+        have_next = true;
+    }
+};
+
+namespace {
+
+int fermion(chdwf_prog* p, float yferm, float* aviter) {
+    // fermion(res, aviter, am, hpin, imass), rhmc/cheisdwf.f:897-1058
+    const int L = p->L, Lt = p->Lt, kvol = p->kvol;
+    const int ksize2 = L * L, nsource = 5;
+    const float akappa = 0.5f;
+    std::vector<float> cf1(4 * Lt, 0.0f), cf2(4 * Lt, 0.0f);
+    std::vector<double> walls(2 * 8 * (size_t)kvol);
+    // prop00(kvol,3:4,1:2,2), prop0L(kvol,3:4,3:4,2) complex64
+    std::vector<float> prop00(2 * 8 * (size_t)kvol), prop0L(2 * 8 * (size_t)kvol);
+    auto PI = [kvol](int64_t i, int a, int b, int f) { return 2 * (i + kvol * (a + 2 * (b + 2 * (int64_t)f))); };
+    int iter = 0;
+    const int ittt0 = (int)((float)Lt * yferm) + 1;                              // :929
+    int ittt = 0;
+    for (int ksource = 1; ksource <= nsource; ksource++) {
+        ittt = (ittt0 + ksource * (Lt / nsource)) % Lt + 1;                        // :937
+        for (int idsource = 3; idsource <= 4; idsource++) {
+            int it = 0;
+            const int rc = chdwf_traj_propagator(p->ctx, ittt, idsource, p->rescgm, p->am, p->hpin,
+                                                 p->imass, walls.data(), &it);
+            if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+            iter += it;
+            // walls[(w*2 + dd)*2 + f][kvol]: w=0 s=1 Dirac 1,2; w=1 s=Ls Dirac 3,4
+            for (int f = 0; f < 2; f++)
+                for (int dd = 0; dd < 2; dd++)
+                    for (int64_t i = 0; i < kvol; i++) {
+                        const double* a = &walls[2 * (((0 * 2 + dd) * 2 + f) * (int64_t)kvol + i)];
+                        const double* b = &walls[2 * (((1 * 2 + dd) * 2 + f) * (int64_t)kvol + i)];
+                        const int64_t pa = PI(i, idsource - 3, dd, f), pb = PI(i, idsource - 3, dd, f);
+                        prop00[pa] = (float)a[0];
+                        prop00[pa + 1] = (float)a[1];
+                        prop0L[pb] = (float)b[0];
+                        prop0L[pb + 1] = (float)b[1];
+                    }
+        }
+        // correlators (:1014-1034); gamval(3,3..4)*akappa = (0,+-0.5), gamin = 1,2
+        for (int idd = 3; idd <= 4; idd++)
+            for (int it = 0; it < Lt; it++) {
+                const int itt = (ittt + it - 1) % Lt + 1;
+                const int isign = itt >= ittt ? 1 : -1;   // ibound = -1 (:85)
+                const int64_t ioff = (int64_t)(itt - 1) * ksize2;
+                const double gim = idd == 3 ? 0.5 : -0.5;
+                for (int f = 0; f < 2; f++)
+                    for (int64_t i = 0; i < ksize2; i++) {
+                        const float sk = (float)isign * akappa;
+                        const int64_t pl = PI(i + ioff, idd - 3, idd - 3, f);
+                        float* c1 = &cf1[2 * (it + Lt * f)];
+                        c1[0] = c1[0] + sk * prop0L[pl];
+                        c1[1] = c1[1] + sk * prop0L[pl + 1];
+                        // (isign*gamval) * prop00, gamval = (0, gim)
+                        const double gre = (double)isign * 0.0, gimv = (double)isign * gim;
+                        const int64_t p0 = PI(i + ioff, idd - 3, idd - 3, f);
+                        const double pr = prop00[p0], pim = prop00[p0 + 1];
+                        const double tre = gre * pr - gimv * pim, tim = gre * pim + gimv * pr;
+                        float* c2 = &cf2[2 * (it + Lt * f)];
+                        c2[0] = (float)((double)c2[0] + tre);
+                        c2[1] = (float)((double)c2[1] + tim);
+                    }
+            }
+    }
+    for (int i = 0; i < 4 * Lt; i++) {
+        cf1[i] = cf1[i] / (float)nsource;
+        cf2[i] = cf2[i] / (float)nsource;
+    }
+    p->cferm.assign(cf1.begin(), cf1.end());
+    p->cferm.insert(p->cferm.end(), cf2.begin(), cf2.end());
+    *aviter = (float)iter / (float)(2 * nsource);
+    return CHDWF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chdwf_prog_create(chdwf_prog** out, int ksize, int ksizet, int kthird, float dt, float beta,
+                      float am3, float am, float hpin, int imass, int iterl, int device) {
+    if (!out || iterl < 1 || (imass != 1 && imass != 3)) return CHDWF_BAD_ARG;
+    chdwf_prog* p = new chdwf_prog();
+    int rc = chdwf_create(&p->ctx, ksize, ksizet, kthird, device);
+    if (rc != CHDWF_OK) { delete p; return rc; }
+    chdwf_set_para(p->ctx, beta, am3, -1);
+    p->L = ksize; p->Lt = ksizet; p->Ls = kthird; p->kvol = ksize * ksize * ksizet;
+    p->dt = dt; p->beta = beta; p->am3 = am3; p->am = am; p->hpin = hpin;
+    p->imass = imass; p->iterl = iterl;
+    // sread without a 'con' file (:1467-1468): chi = 0.1/beta, default seed
+    std::vector<double> chi(3 * (size_t)p->kvol, (double)(0.1f / beta));
+    chdwf_traj_set_chi(p->ctx, chi.data());
+    p->rng.startup((double)693764523745.0f);
+    *out = p;
+    return CHDWF_OK;
+}
+
+void chdwf_prog_destroy(chdwf_prog* p) {
+    if (!p) return;
+    if (p->have_next) p->next.wait();
+    for (Staged& s : p->staged) {
+        cudaFree(s.gauss_dev);
+        cudaFree(s.pp_dev);
+    }
+    chdwf_destroy(p->ctx);
+    delete p;
+}
+
+// Draw the random inputs of the next ntraj sweeps now and copy them to HBM,
+// so those sweeps start with every input resident.
+int chdwf_prog_stage(chdwf_prog* p, int ntraj) {
+    if (!p || ntraj < 0) return CHDWF_BAD_ARG;
+    if (p->have_next) {                  // a prefetched trajectory comes first
+        Staged s;
+        s.d = p->next.get();
+        p->have_next = false;
+        p->staged.push_back(std::move(s));
+        ntraj--;
+    }
+    const int base = p->isweep + (int)p->staged.size();
+    for (int k = 0; k < ntraj; k++) {
+        Staged s;
+        s.d = p->draw(base + 1 + k);
+        p->staged.push_back(std::move(s));
+    }
+    for (Staged& s : p->staged) {
+        if (s.gauss_dev) continue;
+        if (cudaMalloc(&s.gauss_dev, sizeof(float) * s.d.gauss.size()) ||
+            cudaMalloc(&s.pp_dev, sizeof(float) * s.d.pp.size()))
+            return CHDWF_CUDA_ERROR;
+        cudaMemcpy(s.gauss_dev, s.d.gauss.data(), sizeof(float) * s.d.gauss.size(),
+                   cudaMemcpyHostToDevice);
+        cudaMemcpy(s.pp_dev, s.d.pp.data(), sizeof(float) * s.d.pp.size(), cudaMemcpyHostToDevice);
+    }
+    return cudaDeviceSynchronize() == cudaSuccess ? CHDWF_OK : CHDWF_CUDA_ERROR;
+}
+
+chdwf_ctx* chdwf_prog_context(chdwf_prog* p) { return p ? p->ctx : nullptr; }
+
+int chdwf_prog_set_remez(chdwf_prog* p, int which, const double* anum, const double* aden,
+                         const double* bnum, const double* bden, int ndiag) {
+    if (!p) return CHDWF_BAD_ARG;
+    return chdwf_traj_set_remez(p->ctx, which, anum, aden, bnum, bden, ndiag);
+}
+
+int chdwf_prog_set_chi(chdwf_prog* p, const double* chi) {
+    if (!p) return CHDWF_BAD_ARG;
+    return chdwf_traj_set_chi(p->ctx, chi);
+}
+
+int chdwf_prog_get_chi(chdwf_prog* p, double* chi) {
+    if (!p) return CHDWF_BAD_ARG;
+    return chdwf_traj_get_chi(p->ctx, chi, 0);
+}
+
+int chdwf_prog_startup(chdwf_prog* p, double seed) {
+    if (!p) return CHDWF_BAD_ARG;
+    if (p->have_next) { p->next.wait(); p->have_next = false; }
+    p->rng.startup(seed);
+    return CHDWF_OK;
+}
+
+double chdwf_prog_seed(chdwf_prog* p) { return p ? p->rng.seed() : 0.0; }
+
+int chdwf_prog_set_measure(chdwf_prog* p, int iprint, int measure) {
+    if (!p || iprint < 1) return CHDWF_BAD_ARG;
+    if (p->have_next) { p->next.wait(); p->have_next = false; }
+    p->iprint = iprint;
+    p->measure = measure;
+    return CHDWF_OK;
+}
+
+int chdwf_prog_set_residuals(chdwf_prog* p, float rescga, float rescgg, float rescgm) {
+    if (!p) return CHDWF_BAD_ARG;
+    p->rescga = rescga; p->rescgg = rescgg; p->rescgm = rescgm;
+    return CHDWF_OK;
+}
+
+int chdwf_prog_correlators(chdwf_prog* p, float* cferm) {
+    if (!p || !cferm) return CHDWF_BAD_ARG;
+    if (p->cferm.empty()) return CHDWF_BAD_ARG;
+    std::memcpy(cferm, p->cferm.data(), sizeof(float) * p->cferm.size());
+    return CHDWF_OK;
+}
+
+// One sweep of the main loop (rhmc/cheisdwf.f:207-399).
+int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
+    if (!p || !rec) return CHDWF_BAD_ARG;
+    std::memset(rec, 0, sizeof(*rec));
+    chdwf_ctx* c = p->ctx;
+    const int kvol = p->kvol;
+    p->isweep++;
+    Staged stg;
+    const bool from_stage = !p->staged.empty();
+    if (from_stage) {
+        stg = std::move(p->staged.front());
+        p->staged.pop_front();
+    } else {
+        stg.d = p->have_next ? p->next.get() : p->draw(p->isweep);
+        p->have_next = false;
+    }
+    Draws& d = stg.d;
+    struct Free {
+        Staged& s;
+        ~Free() { if (s.gauss_dev) { cudaFree(s.gauss_dev); cudaFree(s.pp_dev); } }
+    } free_guard{stg};
+    int rc;
+#define CK(x) do { rc = (x); if (rc != CHDWF_OK) { p->err = chdwf_last_error(c); return rc; } } while (0)
+    CK(chdwf_traj_begin(c));                                                        // :213-216
+    if (from_stage)
+        CK(chdwf_traj_heatbath_dev(c, stg.gauss_dev, p->rescga, p->am, p->hpin, p->imass,
+                                   &rec->it_pf));                                   // :218-245
+    else
+        CK(chdwf_traj_heatbath(c, d.gauss.data(), p->rescga, p->am, p->hpin, p->imass,
+                               &rec->it_pf));
+    if (p->staged.empty()) p->prefetch(p->isweep + 1);   // next trajectory's draws, overlapped
+    if (from_stage) CK(chdwf_traj_set_momenta_dev(c, stg.pp_dev));                 // :249-257
+    else CK(chdwf_traj_set_momenta(c, d.pp.data()));
+    double h[5];
+    CK(chdwf_traj_hamilton(c, p->rescga, p->am, p->hpin, p->imass, h, &rec->it_h0));  // :261
+    rec->H0 = h[0];
+    rec->S0 = h[3];
+    if (p->isweep == 1) rec->gaction = (float)(h[1] / (double)kvol);
+    rec->action = (float)(h[3] / (double)kvol);
+    rec->paction = (float)(h[2] / (double)kvol);
+    int itg = 0, itf = 0;
+    CK(chdwf_traj_force(c, p->rescgg, p->am, p->hpin, p->imass, &itg, &itf));       // :272
+    rec->it_guid += itg; rec->it_force += itf; rec->nforce++;
+    CK(chdwf_traj_update_momenta(c, p->dt * 0.5f));                                 // :273-277
+    const int nsteps = (int)d.ytest.size();
+    const float proby = 1.0f / (float)p->iterl;
+    for (int iter = 1; iter <= nsteps; iter++) {                                    // :281-315
+        CK(chdwf_traj_update_chi(c, p->dt));
+        CK(chdwf_traj_force(c, p->rescgg, p->am, p->hpin, p->imass, &itg, &itf));
+        rec->it_guid += itg; rec->it_force += itf; rec->nforce++;
+        rec->nsteps = iter;
+        if (d.ytest[iter - 1] < proby) {
+            CK(chdwf_traj_update_momenta(c, p->dt * 0.5f));
+            break;
+        }
+        CK(chdwf_traj_update_momenta(c, p->dt));
+    }
+    CK(chdwf_traj_hamilton(c, p->rescga, p->am, p->hpin, p->imass, h, &rec->it_h1));  // :321
+    rec->H1 = h[0]; rec->S1 = h[3]; rec->hg = h[1]; rec->hp = h[2];
+    rec->dH = rec->H0 - rec->H1;
+    rec->dS = rec->S0 - rec->S1;
+    rec->y = (float)std::exp(rec->dH);
+    rec->x = d.x;
+    rec->accepted = 0;
+    if (rec->x < rec->y) {                                                          // :331-344
+        rec->accepted = 1;
+        CK(chdwf_traj_accept(c));
+        rec->action = (float)(h[3] / (double)kvol);
+        rec->gaction = (float)(h[1] / (double)kvol);
+        rec->paction = (float)(h[2] / (double)kvol);
+    }
+    std::vector<float> pp(3 * (size_t)kvol);
+    CK(chdwf_traj_get_momenta(c, pp.data()));
+    float vel2 = 0.0f;                                                              // :349-355
+    for (size_t i = 0; i < pp.size(); i++) vel2 = vel2 + pp[i] * pp[i];
+    rec->vel2 = vel2 / (float)kvol;
+    if (d.measured) {                                                               // :359-399
+        rec->measured = 1;
+        CK(chdwf_traj_begin(c));                                                    // chit = chi
+        std::vector<double> chi(3 * (size_t)kvol);
+        CK(chdwf_traj_get_chi(c, chi.data(), 0));
+        float susctot = 0.0f, condmod = 0.0f;
+        for (int a = 0; a < 3; a++) {
+            float cnd = 0.0f;
+            for (int i = 0; i < kvol; i++) cnd = (float)((double)cnd + chi[i + (size_t)kvol * a]);
+            float su = cnd * cnd;
+            cnd = cnd / (float)kvol;
+            condmod = condmod + cnd * cnd;
+            su = su / (float)kvol;
+            susctot = susctot + su;
+            rec->cond[a] = cnd;
+            rec->susc[a] = su;
+        }
+        rec->condmod = std::sqrt(condmod);
+        rec->susctot = susctot;
+        CK(fermion(p, d.yferm, &rec->ancgm));
+    }
+#undef CK
+    return CHDWF_OK;
+}
+
+const char* chdwf_prog_last_error(chdwf_prog* p) { return p ? p->err.c_str() : ""; }
+
+}  // extern "C"

@@ -57,6 +57,19 @@ int chdwf_set_para(chdwf_ctx* ctx, float beta, float am3, int ibound);
 const char* chdwf_last_error(const chdwf_ctx* ctx);
 /* version string of the library build */
 const char* chdwf_version(void);
+/* CUDA-event timing of the multi-shift solver's stencil kernels (no
+ * reference counterpart; instrumentation).  enable=1 turns it on and resets
+ * the totals.  chdwf_timing_read fills, per kernel class (0: pass-1 M,
+ * 1: pass-1 M^dagger + update, 2: pass-2 M + accumulate, 3: pass-2
+ * M^dagger + update), the summed milliseconds, the number of timed launches
+ * and the number of launches. */
+int chdwf_timing(chdwf_ctx* ctx, int enable);
+/* the context's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against the library's */
+void* chdwf_get_stream(chdwf_ctx* ctx);
+/* number of CUDA kernels the library has launched in this process */
+long long chdwf_kernel_launches(void);
+int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched);
 
 /* ---- routine level (host arrays) -------------------------------------- */
 /* Phi = M R.  Replaces dslash(Phi,R,chi,am,hpin,imass), rhmc/cheisdwf.f:2634.
@@ -108,6 +121,57 @@ int chdwf_qmrherm_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, f
                       const void* chi, void* x, void* dSdchi);
 int chdwf_congrad_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, float hpin,
                       int imass, const void* chi, void* x);
+
+/* ---- resident trajectory level ------------------------------------------
+ * The blocks of the main loop of program dwf3d (rhmc/cheisdwf.f:207-399)
+ * that call the routines above, with chi, chit, pp, dSdchi and Phi resident
+ * in HBM.  The caller keeps the control flow and the random numbers. */
+/* Remez set: which = 2 (remez2, hamilton), 4 (remez4, heatbath),
+ * 22 (remez2g, force); the common blocks /remez2/, /remez4/, /remez2g/
+ * filled at rhmc/cheisdwf.f:140-159. */
+int chdwf_traj_set_remez(chdwf_ctx* ctx, int which, const double* anum, const double* aden,
+                         const double* bnum, const double* bden, int ndiag);
+/* /chi/ chi(kvol,3) in and out; trial=1 reads /trial/ chit instead. */
+int chdwf_traj_set_chi(chdwf_ctx* ctx, const double* chi);
+int chdwf_traj_get_chi(chdwf_ctx* ctx, double* chi, int trial);
+/* chit = chi (rhmc/cheisdwf.f:213-216) */
+int chdwf_traj_begin(chdwf_ctx* ctx);
+/* Pseudofermion heatbath (rhmc/cheisdwf.f:218-245): ps holds the outputs of
+ * the 2*4*kthird gauss0 calls in call order (flavour, Dirac, s; s fastest),
+ * each ps(kvol,2) REAL*4; R = cmplx(ps(:,1), ps(:,2)); Phi = (M^dag M)^(1/4) R
+ * with the remez4 a-coefficients, kept resident. */
+int chdwf_traj_heatbath(chdwf_ctx* ctx, const float* ps, float res, float am, float hpin,
+                        int imass, int* itercg);
+int chdwf_traj_heatbath_dev(chdwf_ctx* ctx, const void* ps_dev, float res, float am, float hpin,
+                            int imass, int* itercg);
+/* /trial/ pp(kvol,3) REAL*4 in and out */
+int chdwf_traj_set_momenta(chdwf_ctx* ctx, const float* pp);
+int chdwf_traj_set_momenta_dev(chdwf_ctx* ctx, const void* pp_dev);
+int chdwf_traj_get_momenta(chdwf_ctx* ctx, float* pp);
+/* hamilton on the resident fields (rhmc/cheisdwf.f:522-589):
+ * out[0..4] = h, hg, hp, s, hf */
+int chdwf_traj_hamilton(chdwf_ctx* ctx, float res2, float am, float hpin, int imass, double* out,
+                        int* itercg);
+/* force on the resident fields (rhmc/cheisdwf.f:470-518) into a resident
+ * dSdchi; chdwf_traj_get_force copies it out. */
+int chdwf_traj_force(chdwf_ctx* ctx, float res1, float am, float hpin, int imass, int* itg,
+                     int* itf);
+int chdwf_traj_get_force(chdwf_ctx* ctx, float* dSdchi);
+int chdwf_traj_get_phi(chdwf_ctx* ctx, double* Phi);
+/* pp = pp - dSdchi*d (REAL*4; rhmc/cheisdwf.f:273-277, :300-311) */
+int chdwf_traj_update_momenta(chdwf_ctx* ctx, float d);
+/* chit = chit + d*pp (rhmc/cheisdwf.f:285-289) */
+int chdwf_traj_update_chi(chdwf_ctx* ctx, float d);
+/* chi = chit (rhmc/cheisdwf.f:337-341) */
+int chdwf_traj_accept(chdwf_ctx* ctx);
+int chdwf_traj_sync(chdwf_ctx* ctx);
+/* One wall-source propagator of fermion() (rhmc/cheisdwf.f:937-1012):
+ * source 1/ksize^2 on timeslice ittt (1-based), s=1, Dirac idsource,
+ * flavour 1; Phi = M^dag xi; CGNE from x0 = Phi.  walls receives the
+ * solution on s=1 Dirac 1,2 and s=kthird Dirac 3,4, both flavours, as
+ * complex128 [(w*2 + dd)*2 + f][kvol] (w=0: s=1, dd: Dirac pair index). */
+int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, float am, float hpin,
+                          int imass, double* walls, int* itercg);
 
 #ifdef __cplusplus
 }

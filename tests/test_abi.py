@@ -12,8 +12,13 @@ from conftest import ROOT
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "chdwf.h")).read()
-    return sorted(set(re.findall(r"\b(chdwf_\w+)\s*\(", text)))
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for h in sorted(os.listdir(inc)):
+        if h.endswith(".h"):
+            text = open(os.path.join(inc, h)).read()
+            names |= set(re.findall(r"\b(chdwf_\w+)\s*\(", text))
+    return sorted(names)
 
 
 def test_header_matches_python_export_list():

@@ -1,0 +1,106 @@
+"""Trajectory-level parity: the GPU driver (host random numbers and control
+flow, resident fields, include/chdwf_program.h) against the oracle's restatement
+of program dwf3d on the same seeds.
+
+Workload: L=Lt=8, Ls=8, beta=0.475, am3=1, am=0.01 (unused, as in the
+reference), hpin=0, imass=1, dt=0.1, iterl=10 (mean trajectory length 1);
+chi from a seeded N(0, 1/beta); the reference's default seed; the shipped
+remez2/remez4/remez2g sets.
+
+Tolerances (FP64 path):
+  H0, H1, S0, S1       relative 1e-10
+  dH                   |dH_gpu - dH_oracle| <= 1e-10 * |H0|
+  accept/reject, MD step count, Metropolis draw   identical
+  solver iterations    within the reference's own +-3 envelope
+  REAL*4 outputs (action, vel2, condmod, correlators) relative 1e-5 / 1e-4
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import chiralheisenberg_b200 as chb
+
+pytestmark = pytest.mark.gpu
+
+CFG = dict(L=8, Lt=8, Ls=8, beta=0.475, am3=1.0, dt=0.1, am=0.01, hpin=0.0, imass=1, iterl=10)
+SEED = 693764523745.0
+ITER_ENVELOPE = 3
+
+
+def _oracle_remez(r):
+    return po.remez_struct(r["anum"][0], r["anum"][1:], r["aden"], r["bnum"][0], r["bnum"][1:],
+                           r["bden"])
+
+
+@pytest.fixture(scope="module")
+def runs(remez):
+    c = CFG
+    chi = np.random.default_rng(12345).standard_normal((3, c["L"] ** 2 * c["Lt"])) / np.sqrt(c["beta"])
+    sw = po.Sweeper(c["L"], c["Lt"], c["Ls"], c["beta"], c["am3"], c["dt"], c["am"], c["hpin"],
+                    c["imass"], c["iterl"], _oracle_remez(remez["remez2"]),
+                    _oracle_remez(remez["remez4"]), _oracle_remez(remez["remez2g"]), chi=chi,
+                    seed=SEED, measure=True)
+    sw.st.contents.iprint = 2
+    prog = chb.Program(c["L"], c["Lt"], c["Ls"], c["dt"], c["beta"], c["am3"], c["am"], c["hpin"],
+                       c["imass"], c["iterl"], remez["remez2"], remez["remez4"], remez["remez2g"])
+    prog.set_chi(chi)
+    prog.startup(SEED)
+    prog.set_measure(2, True)
+    out = []
+    for k in range(2):
+        ro = sw.sweep()
+        rg = prog.sweep()
+        cf_o = sw.cferm if ro.measured else None
+        cf_g = prog.correlators() if rg.measured else None
+        out.append((ro, rg, cf_o, cf_g))
+    chi_o, chi_g = sw.chi.copy().reshape(3, -1), prog.get_chi()
+    seed_o = po.lib().orc_rranget(po.C.byref(sw.st.contents.rng))
+    seed_g = prog.seed()
+    prog.close()
+    sw.close()
+    return out, (chi_o, chi_g), (seed_o, seed_g)
+
+
+def test_random_stream_and_decisions(runs):
+    out, _, (seed_o, seed_g) = runs
+    for ro, rg, _, _ in out:
+        assert rg.nsteps == ro.nsteps
+        assert rg.x == ro.x
+        assert rg.accepted == ro.accepted
+        assert rg.measured == ro.measured
+    assert seed_g == seed_o
+
+
+def test_hamiltonian_and_dH(runs):
+    out, _, _ = runs
+    for ro, rg, _, _ in out:
+        for f in ("H0", "H1", "S0", "S1"):
+            a, b = getattr(rg, f), getattr(ro, f)
+            assert abs(a - b) <= 1e-10 * abs(b), (f, a, b)
+        assert abs(rg.dH - ro.dH) <= 1e-10 * abs(ro.H0), (rg.dH, ro.dH)
+        assert abs(rg.hg - ro.hg) <= 1e-12 * abs(ro.hg)
+
+
+def test_iterations_within_envelope(runs):
+    out, _, _ = runs
+    for ro, rg, _, _ in out:
+        assert abs(rg.it_pf - ro.it_pf) <= ITER_ENVELOPE
+        assert abs(rg.it_h0 - ro.it_h0) <= ITER_ENVELOPE
+        assert abs(rg.it_h1 - ro.it_h1) <= ITER_ENVELOPE
+        assert rg.nforce == ro.nforce
+        assert abs(rg.it_guid - ro.it_guid) <= ITER_ENVELOPE * ro.nforce
+        assert abs(rg.it_force - ro.it_force) <= ITER_ENVELOPE * ro.nforce
+
+
+def test_single_precision_outputs(runs):
+    out, (chi_o, chi_g), _ = runs
+    for ro, rg, cf_o, cf_g in out:
+        for f in ("action", "paction", "vel2"):
+            a, b = getattr(rg, f), getattr(ro, f)
+            assert abs(a - b) <= 1e-5 * abs(b), (f, a, b)
+        if ro.measured:
+            assert abs(rg.condmod - ro.condmod) <= 1e-5 * abs(ro.condmod)
+            assert abs(rg.ancgm - ro.ancgm) <= ITER_ENVELOPE
+            scale = np.abs(cf_o).max()
+            assert np.abs(cf_g - cf_o).max() <= 1e-4 * scale
+    assert np.abs(chi_g - chi_o).max() <= 1e-6 * np.abs(chi_o).max()
