@@ -251,6 +251,11 @@ def run_b200(args, rank, world, local_rank):
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item()), recs
 
+    # value and e2e run the SAME trajectories: the chain state (chi and the
+    # complete generator state) is saved before the first and restored
+    # before the second
+    chi0 = prog.get_chi()
+    state0 = prog.get_state()
     prog.timing(True)
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -260,7 +265,11 @@ def run_b200(args, rank, world, local_rank):
     clk = clocks.stop()
     kms, ktimed, klaunched = prog.timing_read()
     prog.timing(False)
+    prog.set_chi(chi0)
+    prog.set_state(state0)
     ms_e2e, recs_e2e = timed(staged=False)
+    same = all(a.nsteps == b.nsteps and a.accepted == b.accepted and a.dH == b.dH
+               for a, b in zip(recs, recs_e2e))
 
     # whole job: steps*world trajectories in the slowest rank's time
     ntraj = args.steps * world
@@ -292,7 +301,7 @@ def run_b200(args, rank, world, local_rank):
                        "parallelism": f"replicas{world}", "l2": "fields larger than L2 "
                        "(solver working set > 126 MB)", **CFG},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "same_trajectories_as_value": same},
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "what": kb[dom][0],
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

@@ -43,7 +43,8 @@ EXPORTS = (
     "chdwf_traj_get_phi", "chdwf_traj_update_momenta", "chdwf_traj_update_chi",
     "chdwf_traj_accept", "chdwf_traj_sync", "chdwf_traj_propagator",
     "chdwf_traj_set_momenta_dev", "chdwf_timing", "chdwf_timing_read", "chdwf_prog_stage",
-    "chdwf_get_stream", "chdwf_kernel_launches",
+    "chdwf_get_stream", "chdwf_kernel_launches", "chdwf_set_precision", "chdwf_dslash_dev_lp",
+    "chdwf_prog_state_size", "chdwf_prog_get_state", "chdwf_prog_set_state",
     "chdwf_prog_create", "chdwf_prog_destroy", "chdwf_prog_context", "chdwf_prog_set_remez",
     "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
@@ -131,6 +132,10 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_get_stream.argtypes = [P]
     L.chdwf_get_stream.restype = P
     L.chdwf_kernel_launches.restype = C.c_longlong
+    L.chdwf_set_precision.argtypes = [P, I, I]
+    L.chdwf_dslash_dev_lp.argtypes = [P, P, P, P, F, I, I, I, P]
+    L.chdwf_prog_get_state.argtypes = [P, P, I]
+    L.chdwf_prog_set_state.argtypes = [P, P, I]
     _lib = L
     return L
 
@@ -214,6 +219,17 @@ class Program:
         self._check(self.lib.chdwf_prog_correlators(self.h, _ptr(cf)))
         return cf
 
+    def get_state(self) -> bytes:
+        """Generator state + sweep counter (exact resume; see chdwf_prog_get_state)."""
+        n = self.lib.chdwf_prog_state_size()
+        buf = C.create_string_buffer(n)
+        self._check(self.lib.chdwf_prog_get_state(self.h, buf, n))
+        return buf.raw
+
+    def set_state(self, blob: bytes):
+        buf = C.create_string_buffer(blob, len(blob))
+        self._check(self.lib.chdwf_prog_set_state(self.h, buf, len(blob)))
+
     def stage(self, ntraj):
         """Draw the next ntraj trajectories' random inputs and place them in HBM."""
         self._check(self.lib.chdwf_prog_stage(self.h, ntraj))
@@ -229,6 +245,12 @@ class Program:
 
     def timing(self, enable=True):
         self._check(self.lib.chdwf_timing(self.context, 1 if enable else 0))
+
+    def set_precision(self, md="f64", accept="f64"):
+        """Krylov-vector precision of the force solves (md) and of the
+        heatbath/hamilton solves (accept): "f64" (drop-in) or "f32"."""
+        code = {"f64": 0, "f32": 1}
+        self._check(self.lib.chdwf_set_precision(self.context, code[md], code[accept]))
 
     def timing_read(self):
         ms = np.zeros(4, dtype=np.float64)

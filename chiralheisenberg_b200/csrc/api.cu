@@ -87,6 +87,14 @@ int chdwf_timing(chdwf_ctx* ctx, int enable) {
 
 long long chdwf_kernel_launches(void) { return launches_total(); }
 
+int chdwf_set_precision(chdwf_ctx* ctx, int md, int accept) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || md < 0 || md > 1 || accept < 0 || accept > 1) return CHDWF_BAD_ARG;
+    c->prec_md = md;
+    c->prec_accept = accept;
+    return CHDWF_OK;
+}
+
 void* chdwf_get_stream(chdwf_ctx* ctx) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     return c ? (void*)c->stream : nullptr;
@@ -181,6 +189,18 @@ int chdwf_dslash_dev(chdwf_ctx* ctx, void* Phi, const void* R, const void* chi, 
     launch_dslash64(dagger != 0, imass, (double2*)Phi, (const double2*)R, c->chif, c->g, c->am3,
                     hpin, c->ibound, st);
     return c->status_of(cudaGetLastError(), "dslash_dev");
+}
+
+int chdwf_dslash_dev_lp(chdwf_ctx* ctx, void* Phi, const void* R, const void* chi, float hpin,
+                        int imass, int dagger, int prec, void* stream) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !Phi || !R || !chi || (prec != 1 && prec != 2)) return CHDWF_BAD_ARG;
+    cudaSetDevice(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    launch_round_chi((const double*)chi, c->chif, c->g.kvol, st);
+    launch_dslash_lp(dagger != 0, imass, prec == 2, Phi, R, c->chif, c->g, c->am3, hpin, c->ibound,
+                     st);
+    return c->status_of(cudaGetLastError(), "dslash_dev_lp");
 }
 
 static int solver_status(Ctx* c, cudaError_t e, int st, const char* where) {

@@ -38,6 +38,7 @@ struct Ctx {
     float* gauss = nullptr;             // staging of the heatbath Gaussians
     double2* walls = nullptr;           // propagator wall slices
     RemezSet rz2, rz4, rz2g;
+    int prec_md = 0, prec_accept = 0;   // vector precision of the resident solves
 
     ~Ctx();
     bool fail(cudaError_t e, const char* where);

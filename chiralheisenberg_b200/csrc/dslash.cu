@@ -1,5 +1,7 @@
 // dslash.cu -- FP64 domain-wall operator kernels (rhmc/cheisdwf.f:2634-3501)
 // and the chi-force contraction derivs (rhmc/cheisdwf.f:747-849).
+#include <cuda_fp16.h>
+
 #include "dwf_stencil.cuh"
 #include "internal.h"
 
@@ -41,6 +43,55 @@ void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const
     }
     count_launches(1);
 #undef LAUNCH
+}
+
+// ---- reduced-precision storage: FP32 spinors (complex64) and FP16 spinors
+// (two halves per complex), FP32 arithmetic ----------------------------------
+struct LdF32 {
+    const float2* __restrict__ p;
+    __device__ __forceinline__ float2 operator()(int64_t j) const { return __ldg(p + j); }
+};
+struct LdF16 {
+    const __half2* __restrict__ p;
+    __device__ __forceinline__ float2 operator()(int64_t j) const { return __half22float2(__ldg(p + j)); }
+};
+
+template <bool DAG, int IMASS, int HALF>
+__global__ void __launch_bounds__(kThreads) k_dslash_lp(void* __restrict__ out,
+                                                       const void* __restrict__ in,
+                                                       const float* __restrict__ chif, Geom g,
+                                                       float diag, float hpin, int apbc) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= g.npts) return;
+    const PointIdx q = point_of(g, p);
+    float2 acc[2][4];
+    if (HALF) dwf_apply_point<DAG, IMASS>(acc, LdF16{(const __half2*)in}, g, q, chif, diag, hpin, apbc != 0);
+    else dwf_apply_point<DAG, IMASS>(acc, LdF32{(const float2*)in}, g, q, chif, diag, hpin, apbc != 0);
+#pragma unroll
+    for (int f = 0; f < 2; f++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int64_t e = p + g.cs * (d + 4 * f);
+            if (HALF) ((__half2*)out)[e] = __float22half2_rn(acc[f][d]);
+            else ((float2*)out)[e] = acc[f][d];
+        }
+}
+
+void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
+                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
+    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const float diag = diag_of(am3);
+    const int apbc = ibound == -1;
+#define LP(D, I, H) k_dslash_lp<D, I, H><<<nb, kThreads, 0, st>>>(out, in, chif, g, diag, hpin, apbc)
+    if (half) {
+        if (!dag) { if (imass == 3) LP(false, 3, 1); else LP(false, 1, 1); }
+        else { if (imass == 3) LP(true, 3, 1); else LP(true, 1, 1); }
+    } else {
+        if (!dag) { if (imass == 3) LP(false, 3, 0); else LP(false, 1, 0); }
+        else { if (imass == 3) LP(true, 3, 0); else LP(true, 1, 0); }
+    }
+#undef LP
+    count_launches(1);
 }
 
 // M on npole stacked two-slice lattices: blockIdx.y = pole.

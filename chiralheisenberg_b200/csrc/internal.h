@@ -55,6 +55,11 @@ struct LzHist {
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st);
 
+// Operator on FP32 (half=0, complex64) or FP16 (half=1, two halves per
+// complex) storage with FP32 arithmetic.
+void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
+                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st);
+
 // Wall-slice operator for npole stacked two-slice fields (s'=0 <-> s=1,
 // s'=1 <-> s=Ls): computes M on the Ls=2 lattice of each pole.
 void launch_wall_dslash64(int npole, double2* out, const double2* in, const float* chif,

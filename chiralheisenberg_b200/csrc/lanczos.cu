@@ -30,7 +30,8 @@
 
 namespace chdwf {
 
-struct LdScaled {
+template <class T> struct LdScaledT;
+template <> struct LdScaledT<double2> {
     const double2* __restrict__ p;
     double s;
     __device__ __forceinline__ double2 operator()(int64_t j) const {
@@ -38,13 +39,25 @@ struct LdScaled {
         return make_double2(__dmul_rn(v.x, s), __dmul_rn(v.y, s));
     }
 };
-
-struct LdF64b {
-    const double2* __restrict__ p;
-    __device__ __forceinline__ double2 operator()(int64_t j) const { return __ldg(p + j); }
+template <> struct LdScaledT<float2> {
+    const float2* __restrict__ p;
+    float s;
+    __device__ __forceinline__ float2 operator()(int64_t j) const {
+        const float2 v = __ldg(p + j);
+        return make_float2(v.x * s, v.y * s);
+    }
+};
+template <class T> struct LdPlainT {
+    const T* __restrict__ p;
+    __device__ __forceinline__ T operator()(int64_t j) const { return __ldg(p + j); }
 };
 
-__device__ __forceinline__ double2* ring(const LzArgs& a, int j) {
+__device__ __forceinline__ double2 widen(double2 v) { return v; }
+__device__ __forceinline__ double2 widen(float2 v) { return make_double2((double)v.x, (double)v.y); }
+
+template <class T>
+__device__ __forceinline__ T* ring(const LzArgsT<T>& a, int j) {
+    if (j < a.hcap) return a.basis + (int64_t)j * a.g.kferm;
     const int r = j % 3;
     return r == 0 ? a.rb0 : (r == 1 ? a.rb1 : a.rb2);
 }
@@ -75,8 +88,9 @@ __device__ __forceinline__ bool last_block_sum(double v, double* part, unsigned*
 }
 
 // ---- pass 1, kernel 1: vt = M q_j, alpha~_j = |vt|^2, pole recurrences -----
-template <int IMASS>
-__global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgs a) {
+template <class T, int IMASS>
+__global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgsT<T> a) {
+    typedef typename real_of<T>::type Real;
     LzCtl* ctl = a.ctl;
     if (ctl->done) return;
     const int j = ctl->iter;
@@ -84,15 +98,16 @@ __global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgs a) {
     double loc = 0.0;
     if (p < a.g.npts) {
         const PointIdx q = point_of(a.g, p);
-        double2 acc[2][4];
-        dwf_apply_point<false, IMASS>(acc, LdScaled{ring(a, j), a.h.invbeta[j]}, a.g, q, a.chif,
-                                      a.diag, a.hpin, a.apbc != 0);
+        T acc[2][4];
+        dwf_apply_point<false, IMASS>(acc, LdScaledT<T>{ring(a, j), (Real)a.h.invbeta[j]}, a.g, q,
+                                      a.chif, a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
         for (int f = 0; f < 2; f++)
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 a.vt[p + a.g.cs * (d + 4 * f)] = acc[f][d];
-                loc += acc[f][d].x * acc[f][d].x + acc[f][d].y * acc[f][d].y;
+                const double2 w = widen(acc[f][d]);
+                loc += w.x * w.x + w.y * w.y;
             }
     }
     double tot;
@@ -138,9 +153,22 @@ __global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgs a) {
     }
 }
 
+// r_{j+1} = x3 - alpha~ q_j - beta_j q_{j-1} at one point (cheisdwf.f:655)
+template <class T>
+__device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, int j) {
+    typedef typename real_of<T>::type Real;
+    const T* rj = ring(a, j);
+    const T* rjm = ring(a, j - 1);
+    const Real ib = (Real)a.h.invbeta[j], at = (Real)a.h.alphat[j], bj = (Real)a.h.beta[j];
+    const T qj = zscal(ib, rj[e]);
+    T v = zsub(x3, zscal(at, qj));
+    if (j > 1) v = zsub(v, zscal(bj, zscal((Real)a.h.invbeta[j - 1], rjm[e])));
+    return v;
+}
+
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
-template <int IMASS>
-__global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgs a) {
+template <class T, int IMASS>
+__global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgsT<T> a) {
     LzCtl* ctl = a.ctl;
     if (ctl->done) return;
     const int j = ctl->iter;
@@ -148,24 +176,19 @@ __global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgs a) {
     double loc = 0.0;
     if (p < a.g.npts) {
         const PointIdx q = point_of(a.g, p);
-        double2 acc[2][4];
-        dwf_apply_point<true, IMASS>(acc, LdF64b{a.vt}, a.g, q, a.chif, a.diag, a.hpin,
+        T acc[2][4];
+        dwf_apply_point<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, a.chif, a.diag, a.hpin,
                                      a.apbc != 0);
-        const double2* rj = ring(a, j);
-        const double2* rjm = ring(a, j - 1);
-        double2* rn = ring(a, j + 1);
-        const double ib = a.h.invbeta[j], at = a.h.alphat[j], bj = a.h.beta[j];
-        const double ibm = j > 1 ? a.h.invbeta[j - 1] : 0.0;
+        T* rn = ring(a, j + 1);
 #pragma unroll
         for (int f = 0; f < 2; f++)
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const int64_t e = p + a.g.cs * (d + 4 * f);
-                const double2 qj = zscal(ib, rj[e]);
-                double2 v = zsub(acc[f][d], zscal(at, qj));
-                if (j > 1) v = zsub(v, zscal(bj, zscal(ibm, rjm[e])));
+                const T v = three_term(a, acc[f][d], e, j);
                 rn[e] = v;
-                loc += v.x * v.x + v.y * v.y;
+                const double2 w = widen(v);
+                loc += w.x * w.x + w.y * w.y;
             }
     }
     double tot;
@@ -179,16 +202,17 @@ __global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgs a) {
 }
 
 // ---- pass 2: regenerate q_j and accumulate --------------------------------
-template <int IMASS, int IFLAG>
-__global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgs a, int j, int apply) {
+template <class T, int IMASS, int IFLAG>
+__global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgsT<T> a, int j, int apply) {
+    typedef typename real_of<T>::type Real;
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= a.g.npts) return;
     const PointIdx q = point_of(a.g, p);
-    const double ib = a.h.invbeta[j];
-    const double2* rj = ring(a, j);
+    const Real ib = (Real)a.h.invbeta[j];
+    const T* rj = ring(a, j);
     if (apply) {
-        double2 acc[2][4];
-        dwf_apply_point<false, IMASS>(acc, LdScaled{rj, ib}, a.g, q, a.chif, a.diag, a.hpin,
+        T acc[2][4];
+        dwf_apply_point<false, IMASS>(acc, LdScaledT<T>{rj, ib}, a.g, q, a.chif, a.diag, a.hpin,
                                       a.apbc != 0);
 #pragma unroll
         for (int f = 0; f < 2; f++)
@@ -200,7 +224,7 @@ __global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgs a, int j, int apply) 
 #pragma unroll
         for (int c = 0; c < 8; c++) {
             const int64_t e = p + a.g.cs * c;
-            const double2 qj = zscal(ib, __ldg(rj + e));
+            const double2 qj = widen(zscal(ib, __ldg(rj + e)));
             double2 xv = a.x[e];
             xv.x += cj * qj.x;
             xv.y += cj * qj.y;
@@ -215,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgs a, int j, int apply) 
         const int n = a.npole;
         double2 qv[8];
 #pragma unroll
-        for (int c = 0; c < 8; c++) qv[c] = zscal(ib, __ldg(rj + p + a.g.cs * c));
+        for (int c = 0; c < 8; c++) qv[c] = widen(zscal(ib, __ldg(rj + p + a.g.cs * c)));
         const int64_t base = sw + 2 * (int64_t)q.site;
         for (int k = 0; k < n; k++) {
             const double y = a.h.y[k * H + j];
@@ -231,27 +255,21 @@ __global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgs a, int j, int apply) 
     }
 }
 
-template <int IMASS>
-__global__ void __launch_bounds__(kThreads) k_lz2_Md(LzArgs a, int j) {
+template <class T, int IMASS>
+__global__ void __launch_bounds__(kThreads) k_lz2_Md(LzArgsT<T> a, int j) {
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= a.g.npts) return;
     const PointIdx q = point_of(a.g, p);
-    double2 acc[2][4];
-    dwf_apply_point<true, IMASS>(acc, LdF64b{a.vt}, a.g, q, a.chif, a.diag, a.hpin, a.apbc != 0);
-    const double2* rj = ring(a, j);
-    const double2* rjm = ring(a, j - 1);
-    double2* rn = ring(a, j + 1);
-    const double ib = a.h.invbeta[j], at = a.h.alphat[j], bj = a.h.beta[j];
-    const double ibm = j > 1 ? a.h.invbeta[j - 1] : 0.0;
+    T acc[2][4];
+    dwf_apply_point<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, a.chif, a.diag, a.hpin,
+                                 a.apbc != 0);
+    T* rn = ring(a, j + 1);
 #pragma unroll
     for (int f = 0; f < 2; f++)
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             const int64_t e = p + a.g.cs * (d + 4 * f);
-            const double2 qj = zscal(ib, rj[e]);
-            double2 v = zsub(acc[f][d], zscal(at, qj));
-            if (j > 1) v = zsub(v, zscal(bj, zscal(ibm, rjm[e])));
-            rn[e] = v;
+            rn[e] = three_term(a, acc[f][d], e, j);
         }
 }
 
@@ -278,36 +296,64 @@ __global__ void k_lz_coeffs(LzCtl* ctl, LzHist h, int iflag) {
     }
 }
 
-__global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* nrm2) {
-    const double b = sqrt(*nrm2);
-    h.beta[1] = b;
-    h.invbeta[1] = 1.0 / b;
-    ctl->phimod = b;
+// r_1 = Phi in the vector precision; partial sums of |r_1|^2
+template <class T>
+__global__ void k_lz_source(T* __restrict__ r1, const double2* __restrict__ phi, int64_t n,
+                            double* __restrict__ part) {
+    __shared__ double sh[kThreads / 32];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = phi[i];
+        T t;
+        t.x = (typename real_of<T>::type)v.x;
+        t.y = (typename real_of<T>::type)v.y;
+        r1[i] = t;
+        const double2 w = widen(t);
+        s += w.x * w.x + w.y * w.y;
+    }
+    s = block_sum<kThreads>(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-template <int IMASS>
-static void launch_pass1(const LzArgs& a, unsigned nb, cudaStream_t st, KernelTimer& tm) {
+__global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* part, int nb) {
+    __shared__ double sh[kThreads / 32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) s += part[i];
+    s = block_sum<kThreads>(s, sh);
+    if (threadIdx.x == 0) {
+        const double b = sqrt(s);
+        h.beta[1] = b;
+        h.invbeta[1] = 1.0 / b;
+        ctl->phimod = b;
+    }
+}
+
+template <class T, int IMASS>
+static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, KernelTimer& tm) {
     tm.begin(0, st);
-    k_lz1_M<IMASS><<<nb, kThreads, 0, st>>>(a); count_launches(1);
+    k_lz1_M<T, IMASS><<<nb, kThreads, 0, st>>>(a);
     tm.end(st);
     tm.begin(1, st);
-    k_lz1_Md<IMASS><<<nb, kThreads, 0, st>>>(a); count_launches(1);
+    k_lz1_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a);
     tm.end(st);
+    count_launches(2);
 }
 
-template <int IMASS>
-static void launch_pass2(const LzArgs& a, unsigned nb, int j, int m, int iflag, cudaStream_t st,
-                         KernelTimer& tm) {
+template <class T, int IMASS>
+static void launch_pass2(const LzArgsT<T>& a, unsigned nb, int j, int m, int iflag,
+                         cudaStream_t st, KernelTimer& tm) {
     const int apply = j < m;
     if (apply) tm.begin(2, st);
-    if (iflag == 0) k_lz2_M<IMASS, 0><<<nb, kThreads, 0, st>>>(a, j, apply);
-    else k_lz2_M<IMASS, 1><<<nb, kThreads, 0, st>>>(a, j, apply);
+    if (iflag == 0) k_lz2_M<T, IMASS, 0><<<nb, kThreads, 0, st>>>(a, j, apply);
+    else k_lz2_M<T, IMASS, 1><<<nb, kThreads, 0, st>>>(a, j, apply);
     count_launches(1);
     if (apply) {
         tm.end(st);
         tm.begin(3, st);
-        k_lz2_Md<IMASS><<<nb, kThreads, 0, st>>>(a, j); count_launches(1);
+        k_lz2_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a, j);
         tm.end(st);
+        count_launches(1);
     }
 }
 
@@ -366,56 +412,167 @@ void LzWork::release() {
     if (hist_mem) cudaFree(hist_mem);
     if (part) cudaFree(part);
     if (hflag_host) cudaFreeHost(hflag_host);
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 3; i++) {
         if (rb[i]) cudaFree(rb[i]);
+        if (rb32[i]) cudaFree(rb32[i]);
+    }
     if (vt) cudaFree(vt);
+    if (vt32) cudaFree(vt32);
+    if (basis) cudaFree(basis);
+    if (basis32) cudaFree(basis32);
+    basis = nullptr;
+    basis32 = nullptr;
+    hcap = hcap32 = 0;
     if (xw) cudaFree(xw);
     if (x2w) cudaFree(x2w);
     ctl = nullptr; hist_mem = nullptr; part = nullptr; hflag_host = nullptr;
     rb[0] = rb[1] = rb[2] = vt = xw = x2w = nullptr;
+    rb32[0] = rb32[1] = rb32[2] = vt32 = nullptr;
+    xw_poles = 0;
 }
 
-cudaError_t LzWork::ensure(const Geom& g, int npole_max) {
-    if (ctl && g.kferm == geom.kferm && g.L == geom.L && g.Lt == geom.Lt && npole_max <= xw_poles)
-        return cudaSuccess;
-    release();
-    geom = g;
+cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec) {
     cudaError_t e;
-    if ((e = cudaMalloc(&ctl, sizeof(LzCtl)))) return e;
-    const int64_t H = kMaxIter + 2;
-    const size_t nh = 4 * H + 3 * (size_t)kMaxPoles * H;
-    if ((e = cudaMalloc(&hist_mem, nh * sizeof(double)))) return e;
-    hist.alphat = hist_mem;
-    hist.beta = hist_mem + H;
-    hist.invbeta = hist_mem + 2 * H;
-    hist.c = hist_mem + 3 * H;
-    hist.rho = hist_mem + 4 * H;
-    hist.mu = hist.rho + kMaxPoles * H;
-    hist.y = hist.mu + kMaxPoles * H;
-    const int64_t nb = (g.npts + kThreads - 1) / kThreads;
-    if ((e = cudaMalloc(&part, sizeof(double) * (nb + 2048)))) return e;
-    for (int i = 0; i < 3; i++)
-        if ((e = cudaMalloc(&rb[i], sizeof(double2) * g.kferm))) return e;
-    if ((e = cudaMalloc(&vt, sizeof(double2) * g.kferm))) return e;
-    xw_poles = npole_max < 1 ? 1 : npole_max;
-    const size_t nw = (size_t)xw_poles * 16 * g.kvol;
-    if ((e = cudaMalloc(&xw, sizeof(double2) * nw))) return e;
-    if ((e = cudaMalloc(&x2w, sizeof(double2) * nw))) return e;
-    if ((e = cudaHostAlloc(&hflag_host, sizeof(int), cudaHostAllocMapped))) return e;
-    if ((e = cudaHostGetDevicePointer((void**)&hflag_dev, hflag_host, 0))) return e;
+    const bool same = ctl && g.kferm == geom.kferm && g.L == geom.L && g.Lt == geom.Lt;
+    if (!same) {
+        release();
+        geom = g;
+        if ((e = cudaMalloc(&ctl, sizeof(LzCtl)))) return e;
+        const int64_t H = kMaxIter + 2;
+        const size_t nh = 4 * H + 3 * (size_t)kMaxPoles * H;
+        if ((e = cudaMalloc(&hist_mem, nh * sizeof(double)))) return e;
+        hist.alphat = hist_mem;
+        hist.beta = hist_mem + H;
+        hist.invbeta = hist_mem + 2 * H;
+        hist.c = hist_mem + 3 * H;
+        hist.rho = hist_mem + 4 * H;
+        hist.mu = hist.rho + kMaxPoles * H;
+        hist.y = hist.mu + kMaxPoles * H;
+        const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+        if ((e = cudaMalloc(&part, sizeof(double) * (nb + 2048)))) return e;
+        if ((e = cudaHostAlloc(&hflag_host, sizeof(int), cudaHostAllocMapped))) return e;
+        if ((e = cudaHostGetDevicePointer((void**)&hflag_dev, hflag_host, 0))) return e;
+    }
+    if (prec == kPrecF64 && !rb[0]) {
+        for (int i = 0; i < 3; i++)
+            if ((e = cudaMalloc(&rb[i], sizeof(double2) * g.kferm))) return e;
+        if ((e = cudaMalloc(&vt, sizeof(double2) * g.kferm))) return e;
+    }
+    if (prec == kPrecF32 && !rb32[0]) {
+        for (int i = 0; i < 3; i++)
+            if ((e = cudaMalloc(&rb32[i], sizeof(float2) * g.kferm))) return e;
+        if ((e = cudaMalloc(&vt32, sizeof(float2) * g.kferm))) return e;
+    }
+    // Basis store: up to kMaxIter+2 vectors, at most 40% of the free HBM per
+    // precision.  Solves longer than the store regenerate their vectors.
+    if (basis_enabled && ((prec == kPrecF64 && !basis) || (prec == kPrecF32 && !basis32))) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        const size_t vb = (prec == kPrecF64 ? sizeof(double2) : sizeof(float2)) * (size_t)g.kferm;
+        int64_t cap = (int64_t)(0.4 * (double)fr / (double)vb);
+        if (cap > kMaxIter + 2) cap = kMaxIter + 2;
+        if (cap >= 8) {
+            void* ptr = nullptr;
+            if (cudaMalloc(&ptr, vb * (size_t)cap) == cudaSuccess) {
+                if (prec == kPrecF64) { basis = (double2*)ptr; hcap = (int)cap; }
+                else { basis32 = (float2*)ptr; hcap32 = (int)cap; }
+            } else {
+                cudaGetLastError();   // not enough memory: regenerate instead
+            }
+        }
+    }
+    if (npole_max > xw_poles) {
+        if (xw) cudaFree(xw);
+        if (x2w) cudaFree(x2w);
+        xw_poles = npole_max;
+        const size_t nw = (size_t)xw_poles * 16 * g.kvol;
+        if ((e = cudaMalloc(&xw, sizeof(double2) * nw))) return e;
+        if ((e = cudaMalloc(&x2w, sizeof(double2) * nw))) return e;
+    }
     return cudaSuccess;
 }
 
-// Multi-shift solve.  anum[0..n], aden[0..n-1] as in the reference.
-// iflag 0: x = a0 Phi + sum_k a_k x_k.  iflag 1: x = a0 Phi and the force
-// contribution of every pole is accumulated into dSdchi (device, REAL*4).
-cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
-                     const double* anum, const double* aden, int iflag, const float* chif,
-                     float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
-                     int* itercg, int* status, LzStats* stats, cudaStream_t st) {
-    cudaError_t e = w.ensure(g, iflag ? ndiag : 1);
-    if (e) return e;
-    if (ndiag < 1 || ndiag > kMaxPoles) return cudaErrorInvalidValue;
+template <class T>
+static void set_ring(LzArgsT<T>& a, LzWork& w);
+template <>
+void set_ring<double2>(LzArgsT<double2>& a, LzWork& w) {
+    a.rb0 = w.rb[0]; a.rb1 = w.rb[1]; a.rb2 = w.rb[2]; a.vt = w.vt;
+    a.basis = w.basis_enabled ? w.basis : nullptr;
+    a.hcap = a.basis ? w.hcap : 0;
+}
+template <>
+void set_ring<float2>(LzArgsT<float2>& a, LzWork& w) {
+    a.rb0 = w.rb32[0]; a.rb1 = w.rb32[1]; a.rb2 = w.rb32[2]; a.vt = w.vt32;
+    a.basis = w.basis_enabled ? w.basis32 : nullptr;
+    a.hcap = a.basis ? w.hcap32 : 0;
+}
+
+// ---- pass 2 from the stored basis ---------------------------------------
+// x += sum_j c_j q_j, q_j = r_j / beta_j, j = 1..m, in j order per element
+// (the same sequence of operations as the regenerating pass 2).
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int m) {
+    typedef typename real_of<T>::type Real;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= a.g.kferm) return;
+    double2 xv = a.x[e];
+    const T* b = a.basis + e;
+    const int64_t stride = a.g.kferm;
+#pragma unroll 4
+    for (int j = 1; j <= m; j++) {
+        const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(b + j * stride)));
+        const double cj = a.h.c[j];
+        xv.x += cj * qj.x;
+        xv.y += cj * qj.y;
+    }
+    a.x[e] = xv;
+}
+
+// Two-slice x_k of every pole from the stored basis (force solves):
+// thread per wall element (slice, component, site), poles in chunks of 8.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_lz_accum_walls(LzArgsT<T> a, int m) {
+    typedef typename real_of<T>::type Real;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t cs2 = 2 * (int64_t)a.g.kvol;
+    if (t >= 8 * cs2) return;
+    const int c = (int)(t / cs2);                     // component
+    const int64_t r = t - c * cs2;                    // s' + 2 site
+    const int sw = (int)(r & 1);
+    const int64_t site = r >> 1;
+    const int64_t e = (sw ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * site + a.g.cs * c;
+    const int64_t H = kMaxIter + 2, kf2 = 8 * cs2;
+    const int n = a.npole;
+    const int64_t stride = a.g.kferm;
+    for (int k0 = 0; k0 < n; k0 += 8) {
+        double2 acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = make_double2(0.0, 0.0);
+        for (int j = 1; j <= m; j++) {
+            const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(a.basis + j * stride + e)));
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (k0 + k < n) {
+                    const double y = a.h.y[(k0 + k) * H + j];
+                    acc[k].x += y * qj.x;
+                    acc[k].y += y * qj.y;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (k0 + k < n) a.xw[(k0 + k) * kf2 + r + cs2 * c] = acc[k];
+    }
+}
+
+template <class T>
+static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
+                              const double* anum, const double* aden, int iflag,
+                              const float* chif, float am3, float hpin, int imass, int ibound,
+                              double2* x, float* dSdchi, int* itercg, int* status,
+                              LzStats* stats, cudaStream_t st) {
+    typedef typename real_of<T>::type Real;
+    cudaError_t e;
     LzCtl hc;
     memset(&hc, 0, sizeof(hc));
     hc.iter = 1;
@@ -431,14 +588,13 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
     if ((e = cudaMemcpyAsync(w.ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st))) return e;
     *w.hflag_host = 0;
 
-    LzArgs a;
+    LzArgsT<T> a;
     memset(&a, 0, sizeof(a));
     a.g = g;
-    a.rb0 = w.rb[0]; a.rb1 = w.rb[1]; a.rb2 = w.rb[2];
-    a.vt = w.vt;
+    set_ring(a, w);
     a.chif = chif;
-    a.diag = (double)(2.0f * ((3.0f - am3) + 1.0f));
-    a.hpin = (double)hpin;
+    a.diag = (Real)(2.0f * ((3.0f - am3) + 1.0f));
+    a.hpin = (Real)hpin;
     a.apbc = ibound == -1;
     a.ctl = w.ctl;
     a.h = w.hist;
@@ -448,11 +604,13 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
     a.xw = w.xw;
     a.npole = ndiag;
     const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const int nbr = reduce_blocks(g.kferm);
+    T* r1 = a.rb1;
 
-    // beta_1 = |Phi|, r_1 = Phi
-    launch_norm2(phi, g.kferm, w.part + nb + 8, w.part + nb, st);
-    k_lz_init<<<1, 1, 0, st>>>(w.ctl, w.hist, w.part + nb); count_launches(1);
-    cudaMemcpyAsync(w.rb[1], phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+    // r_1 = Phi, beta_1 = |r_1|
+    k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);
+    k_lz_init<<<1, kThreads, 0, st>>>(w.ctl, w.hist, w.part, nbr);
+    count_launches(2);
 
     // pass 1: launch chunks of iterations, poll the mapped flag with one
     // chunk in flight ahead of the one being checked
@@ -463,8 +621,8 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
     int launched = 0, nchunk = 0;
     while (launched < kMaxIter) {
         for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
-            if (imass == 3) launch_pass1<3>(a, nb, st, w.timer);
-            else launch_pass1<1>(a, nb, st, w.timer);
+            if (imass == 3) launch_pass1<T, 3>(a, nb, st, w.timer);
+            else launch_pass1<T, 1>(a, nb, st, w.timer);
         }
         cudaEventRecord(ev[nchunk & 1], st);
         if (nchunk >= 1) {
@@ -473,12 +631,11 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
         }
         nchunk++;
     }
-    // no-op launches after convergence are not timed as work
     if (w.timer.enabled) {
+        // launches after convergence returned at once: drop them
         cudaStreamSynchronize(st);
         LzCtl hm;
         cudaMemcpy(&hm, w.ctl, sizeof(hm), cudaMemcpyDeviceToHost);
-        // pairs beyond the converged iteration ran as immediate returns
         int keep = 0;
         for (int i = 0, it = 0; i < w.timer.used; i++) {
             if (w.timer.cls[i] == 0) it++;
@@ -508,17 +665,30 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
     if (stats) { stats->iters = m; stats->pass1_launches = 2 * launched; }
     if (m < 1) return cudaErrorUnknown;
 
-    // coefficients, then pass 2
-    k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag); count_launches(1);
+    // coefficients, then pass 2 over the regenerated vectors
+    k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag);
+    k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);
+    count_launches(2);
     launch_scale(x, phi, anum[0], g.kferm, st);                       // x = a0 Phi (:628)
     if (iflag) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
-    cudaMemcpyAsync(w.rb[1], phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
-    for (int j = 1; j <= m; j++) {
-        if (imass == 3) launch_pass2<3>(a, nb, j, m, iflag, st, w.timer);
-        else launch_pass2<1>(a, nb, j, m, iflag, st, w.timer);
-        if (w.timer.enabled && w.timer.used >= KernelTimer::kPool - 2) {
-            cudaStreamSynchronize(st);
-            w.timer.collect();
+    if (m < a.hcap) {
+        // every q_j is still in HBM: one streaming pass over the basis
+        w.timer.begin(2, st);
+        if (iflag == 0)
+            k_lz_accum_x<T><<<(unsigned)((g.kferm + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, m);
+        else
+            k_lz_accum_walls<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads),
+                                  kThreads, 0, st>>>(a, m);
+        w.timer.end(st);
+        count_launches(1);
+    } else {
+        for (int j = 1; j <= m; j++) {
+            if (imass == 3) launch_pass2<T, 3>(a, nb, j, m, iflag, st, w.timer);
+            else launch_pass2<T, 1>(a, nb, j, m, iflag, st, w.timer);
+            if (w.timer.enabled && w.timer.used >= KernelTimer::kPool - 2) {
+                cudaStreamSynchronize(st);
+                w.timer.collect();
+            }
         }
     }
     if (w.timer.enabled) {
@@ -533,6 +703,23 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
         launch_derivs_walls(ndiag, w.xw, w.x2w, anum_dev, imass, dSdchi, g, st);
     }
     return cudaGetLastError();
+}
+
+// Multi-shift solve.  anum[0..n], aden[0..n-1] as in the reference.
+// iflag 0: x = a0 Phi + sum_k a_k x_k.  iflag 1: x = a0 Phi and the force
+// contribution of every pole is accumulated into dSdchi (device, REAL*4).
+cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
+                     const double* anum, const double* aden, int iflag, const float* chif,
+                     float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
+                     int* itercg, int* status, LzStats* stats, cudaStream_t st, int prec) {
+    if (ndiag < 1 || ndiag > kMaxPoles) return cudaErrorInvalidValue;
+    cudaError_t e = w.ensure(g, iflag ? ndiag : 1, prec);
+    if (e) return e;
+    if (prec == kPrecF32)
+        return lz_solve_t<float2>(w, g, phi, res, ndiag, anum, aden, iflag, chif, am3, hpin,
+                                  imass, ibound, x, dSdchi, itercg, status, stats, st);
+    return lz_solve_t<double2>(w, g, phi, res, ndiag, anum, aden, iflag, chif, am3, hpin, imass,
+                               ibound, x, dSdchi, itercg, status, stats, st);
 }
 
 }  // namespace chdwf

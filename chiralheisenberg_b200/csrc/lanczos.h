@@ -4,19 +4,26 @@
 
 namespace chdwf {
 
-struct LzArgs {
+// Kernel arguments; T is the complex type of the Krylov vectors: double2
+// (the FP64 drop-in path) or float2 (mixed precision: FP32 vectors and
+// stencil arithmetic, FP64 reductions, scalars and solution accumulation).
+template <class T>
+struct LzArgsT {
+    typedef typename real_of<T>::type Real;
     Geom g;
-    double2 *rb0, *rb1, *rb2;   // Lanczos residual ring: r_j lives in rb[j % 3]
-    double2* vt;                // M q_j
+    T *rb0, *rb1, *rb2;         // Lanczos residual ring: r_j lives in rb[j % 3] ...
+    T* basis;                   // ... unless j < hcap: then in basis + j*kferm
+    int hcap;
+    T* vt;                      // M q_j
     const float* chif;          // chi rounded to REAL*4 (wall coupling)
-    double diag, hpin;
+    Real diag, hpin;
     int apbc;
     LzCtl* ctl;
     LzHist h;
     double* part;               // per-block partial sums
     int* hflag;                 // device view of the mapped host stop flag
-    double2* x;                 // solution (iflag 0)
-    double2* xw;                // two-slice x_k per pole (iflag 1)
+    double2* x;                 // solution (iflag 0), FP64
+    double2* xw;                // two-slice x_k per pole (iflag 1), FP64
     int npole;
 };
 
@@ -55,6 +62,14 @@ struct LzWork {
     double* part = nullptr;
     double2* rb[3] = {nullptr, nullptr, nullptr};
     double2* vt = nullptr;
+    float2* rb32[3] = {nullptr, nullptr, nullptr};
+    float2* vt32 = nullptr;
+    // Lanczos basis kept in HBM: pass 2 then reads the stored vectors once
+    // instead of regenerating them (2 operator applies per vector)
+    double2* basis = nullptr;
+    float2* basis32 = nullptr;
+    int hcap = 0, hcap32 = 0;
+    int basis_enabled = 1;
     double2* xw = nullptr;
     double2* x2w = nullptr;
     int xw_poles = 0;
@@ -63,12 +78,16 @@ struct LzWork {
     KernelTimer timer;
     ~LzWork();
     void release();
-    cudaError_t ensure(const Geom& g, int npole_max);
+    cudaError_t ensure(const Geom& g, int npole_max, int prec);
 };
+
+// Precision of the Krylov vectors.
+enum { kPrecF64 = 0, kPrecF32 = 1 };
 
 cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
                      const double* anum, const double* aden, int iflag, const float* chif,
                      float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
-                     int* itercg, int* status, LzStats* stats, cudaStream_t st);
+                     int* itercg, int* status, LzStats* stats, cudaStream_t st,
+                     int prec = kPrecF64);
 
 }  // namespace chdwf

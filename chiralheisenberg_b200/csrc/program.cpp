@@ -30,7 +30,7 @@ struct Draws {                       // the random numbers of one trajectory
     float x = 0.0f;                  // Metropolis draw
     float yferm = 0.0f;              // fermion()'s draw (measurement sweeps)
     bool measured = false;
-    double seed_after = 0.0;
+    chdwf::Rng::State state_after{};  // generator state after these draws
 };
 
 }  // namespace
@@ -53,6 +53,22 @@ struct chdwf_prog {
     std::future<Draws> next;
     std::vector<float> cferm;        // cferm1(0:Lt-1,2), cferm2 as complex64 pairs
     std::string err;
+    chdwf::Rng::State last_state{};  // generator after the last completed sweep
+
+    // Drop prefetched or staged draws and rewind the generator to the end
+    // of the last completed sweep, so the stream continues exactly there.
+    void discard_pending() {
+        if (have_next) {
+            next.wait();
+            have_next = false;
+        }
+        for (Staged& s : staged) {
+            cudaFree(s.gauss_dev);
+            cudaFree(s.pp_dev);
+        }
+        staged.clear();
+        rng.set_state(last_state);
+    }
 
     // All random numbers of the next trajectory, in the reference's order.
     Draws draw(int sweep_index) {
@@ -75,7 +91,7 @@ struct chdwf_prog {
         d.x = rng.rano_yrun();                                                              // :329
         d.measured = measure && (sweep_index / iprint) * iprint == sweep_index;
         if (d.measured) d.yferm = rng.rano_yran();                                          // :929
-        d.seed_after = rng.seed();
+        d.state_after = rng.state();
         return d;
     }
 
@@ -174,6 +190,7 @@ int chdwf_prog_create(chdwf_prog** out, int ksize, int ksizet, int kthird, float
     std::vector<double> chi(3 * (size_t)p->kvol, (double)(0.1f / beta));
     chdwf_traj_set_chi(p->ctx, chi.data());
     p->rng.startup((double)693764523745.0f);
+    p->last_state = p->rng.state();
     *out = p;
     return CHDWF_OK;
 }
@@ -238,16 +255,49 @@ int chdwf_prog_get_chi(chdwf_prog* p, double* chi) {
 
 int chdwf_prog_startup(chdwf_prog* p, double seed) {
     if (!p) return CHDWF_BAD_ARG;
-    if (p->have_next) { p->next.wait(); p->have_next = false; }
+    p->discard_pending();
     p->rng.startup(seed);
+    p->last_state = p->rng.state();
     return CHDWF_OK;
 }
 
-double chdwf_prog_seed(chdwf_prog* p) { return p ? p->rng.seed() : 0.0; }
+// rranget after the last completed sweep (the value the reference would
+// checkpoint there)
+double chdwf_prog_seed(chdwf_prog* p) {
+    if (!p) return 0.0;
+    return p->last_state.ds[1] * 16777216.0 + p->last_state.ds[0];
+}
+
+struct ProgState {
+    chdwf::Rng::State rng;
+    int isweep;
+};
+
+int chdwf_prog_state_size(void) { return (int)sizeof(ProgState); }
+
+int chdwf_prog_get_state(chdwf_prog* p, void* buf, int nbytes) {
+    if (!p || !buf || nbytes < (int)sizeof(ProgState)) return CHDWF_BAD_ARG;
+    ProgState s;
+    s.rng = p->last_state;
+    s.isweep = p->isweep;
+    std::memcpy(buf, &s, sizeof(s));
+    return CHDWF_OK;
+}
+
+int chdwf_prog_set_state(chdwf_prog* p, const void* buf, int nbytes) {
+    if (!p || !buf || nbytes < (int)sizeof(ProgState)) return CHDWF_BAD_ARG;
+    ProgState s;
+    std::memcpy(&s, buf, sizeof(s));
+    p->discard_pending();
+    p->rng.set_state(s.rng);
+    p->last_state = s.rng;
+    p->isweep = s.isweep;
+    return CHDWF_OK;
+}
 
 int chdwf_prog_set_measure(chdwf_prog* p, int iprint, int measure) {
     if (!p || iprint < 1) return CHDWF_BAD_ARG;
-    if (p->have_next) { p->next.wait(); p->have_next = false; }
+    p->discard_pending();
     p->iprint = iprint;
     p->measure = measure;
     return CHDWF_OK;
@@ -283,6 +333,7 @@ int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
         p->have_next = false;
     }
     Draws& d = stg.d;
+    p->last_state = d.state_after;
     struct Free {
         Staged& s;
         ~Free() { if (s.gauss_dev) { cudaFree(s.gauss_dev); cudaFree(s.pp_dev); } }

@@ -47,6 +47,26 @@ float Rng::rano(float& y) {
     return out;
 }
 
+Rng::State Rng::state() const {
+    State s;
+    s.ds[0] = ds_[0];
+    s.ds[1] = ds_[1];
+    for (int j = 0; j < 97; j++) s.v[j] = v_[j];
+    s.yran = yran_;
+    s.yrun = yrun_;
+    s.idum = idum_;
+    return s;
+}
+
+void Rng::set_state(const State& s) {
+    ds_[0] = s.ds[0];
+    ds_[1] = s.ds[1];
+    for (int j = 0; j < 97; j++) v_[j] = s.v[j];
+    yran_ = s.yran;
+    yrun_ = s.yrun;
+    idum_ = s.idum;
+}
+
 void Rng::startup(double seed) {
     set_seed(seed);
     idum_ = -1;

@@ -27,6 +27,19 @@ public:
     void gauss0(int64_t kvol, float* ps);
     void gaussp(int64_t kvol, float* ps);
 
+    // Complete generator state: the LCG halves, the shuffle table and both
+    // "last output" variables.  The reference checkpoints only the LCG seed
+    // (rhmc/cheisdwf.f:401-411), so its resumed runs differ from
+    // uninterrupted ones; restoring this state resumes exactly.
+    struct State {
+        double ds[2];
+        float v[97];
+        float yran, yrun;
+        int idum;
+    };
+    State state() const;
+    void set_state(const State& s);
+
 private:
     float rano(float& y);
     double ds_[2] = {0.0, 0.0};

@@ -166,7 +166,7 @@ int chdwf_traj_heatbath_dev(chdwf_ctx* ctx, const void* ps_dev, float res, float
     // Phi = (M^dagger M)^(1/4) R with the remez4 a-coefficients (:233), Phi <- X1 (:237-245)
     cudaError_t e = lz_solve(c->lz, c->g, c->spin[0], res, c->rz4.n, c->rz4.anum.data(),
                              c->rz4.aden.data(), 0, c->chif, c->am3, hpin, imass, c->ibound,
-                             c->phi, c->dS, itercg, &st, &c->last_lz, c->stream);
+                             c->phi, c->dS, itercg, &st, &c->last_lz, c->stream, c->prec_accept);
     return traj_solver_status(c, e, st, "heatbath");
 }
 
@@ -216,7 +216,7 @@ int chdwf_traj_hamilton(chdwf_ctx* ctx, float res2, float am, float hpin, int im
     int st = 0;
     cudaError_t e = lz_solve(c->lz, c->g, c->phi, res2, c->rz2.n, c->rz2.bnum.data(),
                              c->rz2.bden.data(), 0, c->chif, c->am3, hpin, imass, c->ibound,
-                             c->spin[1], c->dS, itercg, &st, &c->last_lz, c->stream);   // :572
+                             c->spin[1], c->dS, itercg, &st, &c->last_lz, c->stream, c->prec_accept);   // :572
     if (e) return traj_solver_status(c, e, st, "hamilton");
     launch_redot(c->phi, c->spin[1], c->g.kferm, c->red + 32, c->red, c->stream);          // :578-580
     double h[3];
@@ -242,11 +242,11 @@ int chdwf_traj_force(chdwf_ctx* ctx, float res1, float am, float hpin, int imass
     int st1 = 0, st2 = 0;
     cudaError_t e = lz_solve(c->lz, c->g, c->phi, res1, c->rz2g.n, c->rz2g.bnum.data(),
                              c->rz2g.bden.data(), 0, c->chif, c->am3, hpin, imass, c->ibound,
-                             c->spin[1], c->dS, itg, &st1, &c->last_lz, c->stream);   // :505
+                             c->spin[1], c->dS, itg, &st1, &c->last_lz, c->stream, c->prec_md);   // :505
     if (e || st1) return traj_solver_status(c, e, st1, "force (guidance solve)");
     e = lz_solve(c->lz, c->g, c->spin[1], res1, c->rz2g.n, c->rz2g.anum.data(),
                  c->rz2g.aden.data(), 1, c->chif, c->am3, hpin, imass, c->ibound, c->spin[2],
-                 c->dS, itf, &st2, &c->last_lz, c->stream);                           // :513
+                 c->dS, itf, &st2, &c->last_lz, c->stream, c->prec_md);                           // :513
     return traj_solver_status(c, e, st2, "force (force solve)");
 }
 

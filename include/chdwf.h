@@ -64,6 +64,15 @@ const char* chdwf_version(void);
  * M^dagger + update), the summed milliseconds, the number of timed launches
  * and the number of launches. */
 int chdwf_timing(chdwf_ctx* ctx, int enable);
+/* Precision of the Krylov vectors in the resident trajectory solves (no
+ * reference counterpart: the reference is FP64 throughout).  md: the two
+ * multi-shift solves of every force evaluation; accept: the heatbath and
+ * hamilton solves that enter the Metropolis test.  CHDWF_PREC_F64 (default,
+ * the drop-in) or CHDWF_PREC_F32 (FP32 vectors and stencil, FP64
+ * reductions, recurrences and solution accumulation). */
+#define CHDWF_PREC_F64 0
+#define CHDWF_PREC_F32 1
+int chdwf_set_precision(chdwf_ctx* ctx, int md, int accept);
 /* the context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's */
 void* chdwf_get_stream(chdwf_ctx* ctx);
@@ -116,6 +125,12 @@ int chdwf_hamilton(chdwf_ctx* ctx, const double* Phi, float res2, float am, floa
 /* stream: a cudaStream_t or NULL for the context's own stream. */
 int chdwf_dslash_dev(chdwf_ctx* ctx, void* Phi, const void* R, const void* chi, float hpin,
                      int imass, int dagger, void* stream);
+/* The operator on reduced-precision storage (no reference counterpart; the
+ * reference is FP64): prec = CHDWF_PREC_F32 (complex64 spinors) or
+ * CHDWF_PREC_F16 (two IEEE halves per complex); arithmetic in FP32. */
+#define CHDWF_PREC_F16 2
+int chdwf_dslash_dev_lp(chdwf_ctx* ctx, void* Phi, const void* R, const void* chi, float hpin,
+                        int imass, int dagger, int prec, void* stream);
 int chdwf_qmrherm_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, float hpin,
                       int imass, const double* anum, const double* aden, int ndiag, int iflag,
                       const void* chi, void* x, void* dSdchi);

@@ -48,8 +48,15 @@ int chdwf_prog_set_chi(chdwf_prog* p, const double* chi);
 int chdwf_prog_get_chi(chdwf_prog* p, double* chi);
 /* rranset(seed); idum=-1; rano(yran) (rhmc/cheisdwf.f:125-130) */
 int chdwf_prog_startup(chdwf_prog* p, double seed);
-/* rranget (rhmc/cheisdwf.f:1755) */
+/* rranget (rhmc/cheisdwf.f:1755) as of the end of the last completed sweep */
 double chdwf_prog_seed(chdwf_prog* p);
+/* Full generator state (LCG, shuffle table, yran, yrun) and sweep counter as
+ * an opaque blob of chdwf_prog_state_size() bytes.  The reference's 'con'
+ * keeps only the LCG seed, so its resumed runs re-shuffle (rhmc/cheisdwf.f:
+ * 129-130); restoring this blob (with chi) resumes the Markov chain exactly. */
+int chdwf_prog_state_size(void);
+int chdwf_prog_get_state(chdwf_prog* p, void* buf, int nbytes);
+int chdwf_prog_set_state(chdwf_prog* p, const void* buf, int nbytes);
 /* measurement every iprint sweeps (default 5); measure=0 disables it */
 int chdwf_prog_set_measure(chdwf_prog* p, int iprint, int measure);
 /* stopping residuals rescga, rescgg, rescgm (default 1e-9, 1e-6, 1e-9, :32-33) */

@@ -1,0 +1,71 @@
+"""Reduced-precision paths (no reference counterpart: the reference is FP64
+throughout), checked against the FP64 oracle and the FP64 GPU path.
+
+  operator, FP32 storage + arithmetic      relative L2 error <= 1e-6
+  operator, FP16 storage, FP32 arithmetic  relative L2 error <= 2e-3
+  mixed trajectory (FP32 force solves)     same accept/reject decisions and
+                                           MD steps; |dH_mixed - dH_fp64| <= 1e-8 * |H0|
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+import chiralheisenberg_b200 as chb
+from conftest import random_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _lp_apply(gl, R, chi, prec, dag, hpin=0.3):
+    import torch
+    dt = torch.complex64 if prec == 1 else torch.float16
+    Rt = torch.from_numpy(R.astype(np.complex64)).cuda()
+    if prec == 2:
+        Rt = torch.view_as_real(Rt).to(torch.float16).contiguous()
+    out = torch.empty_like(Rt)
+    chit = torch.from_numpy(np.ascontiguousarray(chi)).cuda()
+    rc = gl.lib.chdwf_dslash_dev_lp(gl.h, C.c_void_p(out.data_ptr()), C.c_void_p(Rt.data_ptr()),
+                                    C.c_void_p(chit.data_ptr()), hpin, 1, int(dag), prec, None)
+    assert rc == 0
+    gl.lib.chdwf_traj_sync(gl.h)
+    torch.cuda.synchronize()
+    if prec == 2:
+        o = out.float().cpu().numpy()
+        return o[..., 0] + 1j * o[..., 1]
+    return out.cpu().numpy().astype(np.complex128)
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 1e-6), (2, 2e-3)])
+@pytest.mark.parametrize("dag", [False, True])
+def test_operator_reduced_precision(prec, tol, dag):
+    L, Lt, Ls = 8, 8, 8
+    R, chi = random_fields(L, Lt, Ls, seed=31)
+    lat = po.make_lat(L, Lt, Ls)
+    ref = po.dslash(lat, R, chi, hpin=0.3, imass=1, dag=dag)
+    gl = chb.Lattice(L, Lt, Ls)
+    out = _lp_apply(gl, R, chi, prec, dag)
+    err = np.linalg.norm(out.reshape(-1) - ref.reshape(-1)) / np.linalg.norm(ref)
+    assert err <= tol, err
+
+
+def test_mixed_precision_trajectory(remez):
+    """FP32 Krylov vectors in the force solves, FP64 heatbath/hamilton: the
+    same Markov chain decisions and dH within 1e-8 of H."""
+    L, Lt, Ls = 8, 8, 8
+    beta = 0.475
+    chi = np.random.default_rng(12345).standard_normal((3, L * L * Lt)) / np.sqrt(beta)
+    recs = {}
+    for mode in ("f64", "f32"):
+        prog = chb.Program(L, Lt, Ls, 0.1, beta, 1.0, 0.01, 0.0, 1, 10, remez["remez2"],
+                           remez["remez4"], remez["remez2g"])
+        prog.set_chi(chi)
+        prog.startup(693764523745.0)
+        prog.set_measure(5, False)
+        prog.set_precision(md=mode, accept="f64")
+        recs[mode] = [prog.sweep() for _ in range(2)]
+        prog.close()
+    for a, b in zip(recs["f64"], recs["f32"]):
+        assert a.nsteps == b.nsteps and a.accepted == b.accepted
+        assert abs(a.dH - b.dH) <= 1e-8 * abs(a.H0), (a.dH, b.dH)

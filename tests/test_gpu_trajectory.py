@@ -68,7 +68,31 @@ def test_random_stream_and_decisions(runs):
         assert rg.x == ro.x
         assert rg.accepted == ro.accepted
         assert rg.measured == ro.measured
+    # the driver prefetches the next trajectory's draws; its seed() reports the
+    # generator as of the end of the last completed sweep, like rranget there
     assert seed_g == seed_o
+
+
+def test_exact_resume(remez):
+    """Saving chi and the full generator state and restoring them replays
+    the same trajectory bit for bit (the reference's 'con' keeps only the
+    LCG seed, so its resume re-shuffles)."""
+    c = CFG
+    chi = np.random.default_rng(7).standard_normal((3, c["L"] ** 2 * c["Lt"])) / np.sqrt(c["beta"])
+    prog = chb.Program(c["L"], c["Lt"], c["Ls"], c["dt"], c["beta"], c["am3"], c["am"], c["hpin"],
+                       c["imass"], c["iterl"], remez["remez2"], remez["remez4"], remez["remez2g"])
+    prog.set_chi(chi)
+    prog.startup(SEED)
+    prog.set_measure(5, False)
+    prog.sweep()
+    chi1, st1 = prog.get_chi(), prog.get_state()
+    a = prog.sweep()
+    prog.set_chi(chi1)
+    prog.set_state(st1)
+    b = prog.sweep()
+    prog.close()
+    assert (a.dH, a.H0, a.H1, a.nsteps, a.accepted, a.x) == (b.dH, b.H0, b.H1, b.nsteps,
+                                                              b.accepted, b.x)
 
 
 def test_hamiltonian_and_dH(runs):
