@@ -54,7 +54,8 @@ CFG = dict(beta=0.475, am3=1.0, am=0.01, hpin=0.0, imass=1, dt=0.1, iterl=10,
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--L", type=int, default=24)
@@ -270,6 +271,22 @@ def run_b200(args, rank, world, local_rank):
     ms_e2e, recs_e2e = timed(staged=False)
     same = all(a.nsteps == b.nsteps and a.accepted == b.accepted and a.dH == b.dH
                for a, b in zip(recs, recs_e2e))
+    mixed = None
+    if not args.no_mixed:
+        # the same trajectories with FP32 Krylov vectors in the force solves
+        prog.set_chi(chi0)
+        prog.set_state(state0)
+        prog.set_precision(md="f32", accept="f64")
+        ms_mix, recs_mix = timed(staged=True)
+        prog.set_precision(md="f64", accept="f64")
+        dh = [abs(a.dH - b.dH) for a, b in zip(recs, recs_mix)]
+        dh_rel = [abs(a.dH - b.dH) / abs(a.H0) for a, b in zip(recs, recs_mix)]
+        mixed = {"value": (ms_mix / 1e3) / (args.steps * world), "unit": "s",
+                 "precision": "FP32 Krylov vectors in the force solves, FP64 heatbath/hamilton",
+                 "speedup_vs_fp64": ms_value / ms_mix,
+                 "dH_max_abs_diff_vs_fp64": max(dh), "dH_max_diff_rel_H": max(dh_rel),
+                 "same_decisions": all(a.accepted == b.accepted and a.nsteps == b.nsteps
+                                       for a, b in zip(recs, recs_mix))}
 
     # whole job: steps*world trajectories in the slowest rank's time
     ntraj = args.steps * world
@@ -308,6 +325,7 @@ def run_b200(args, rank, world, local_rank):
                          "bytes_per_launch": kb[dom][1], "avg_launch_us": avg_ms * 1e3},
             "kernel_avg_us": {KERNEL_NAMES[k]: kms[k] / max(ktimed[k], 1) * 1e3 for k in range(4)},
             "gpu_launches": launches,
+            "mixed": mixed,
             "iteration_profile": prof,
             "trajectories": [{"dH": r.dH, "accepted": r.accepted, "nsteps": r.nsteps}
                              for r in recs],
