@@ -6,8 +6,8 @@ stopping rule in two passes (see chiralheisenberg_b200/csrc/lanczos.cu), the
 oracle the reference's one-pass form; both make the same iterations, and the
 solutions agree to rounding amplified by the Krylov process.  Iteration
 counts agree to within the reference's own reproducibility envelope: the
-reference's OpenMP reductions make its count move by up to 2 with the thread
-count (tests/test_oracle.py::test_oracle_thread_envelope), so +-3 is allowed.
+reference's OpenMP reductions make its count move by 2-3 with the thread
+count (tests/test_oracle.py::test_oracle_thread_envelope), so +-5 is allowed.
 Tolerances:
   qmrherm x        relative L2 1e-10
   force dSdchi     |diff| <= 2 REAL*4 ulps of max|dSdchi| (REAL*4 result)
@@ -22,7 +22,7 @@ from conftest import random_fields
 
 pytestmark = pytest.mark.gpu
 
-ITER_ENVELOPE = 3
+ITER_ENVELOPE = 5
 
 
 def rel(a, b):

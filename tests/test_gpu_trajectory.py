@@ -11,7 +11,7 @@ Tolerances (FP64 path):
   H0, H1, S0, S1       relative 1e-10
   dH                   |dH_gpu - dH_oracle| <= 1e-10 * |H0|
   accept/reject, MD step count, Metropolis draw   identical
-  solver iterations    within the reference's own +-3 envelope
+  solver iterations    within the reference's own envelope (+-5)
   REAL*4 outputs (action, vel2, condmod, correlators) relative 1e-5 / 1e-4
 """
 import numpy as np
@@ -24,7 +24,7 @@ pytestmark = pytest.mark.gpu
 
 CFG = dict(L=8, Lt=8, Ls=8, beta=0.475, am3=1.0, dt=0.1, am=0.01, hpin=0.0, imass=1, iterl=10)
 SEED = 693764523745.0
-ITER_ENVELOPE = 3
+ITER_ENVELOPE = 5
 
 
 def _oracle_remez(r):
