@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-propagators", action="store_true")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--L", type=int, default=24)
@@ -187,6 +188,61 @@ def default_profile():
     # GPU arm (same algorithm and stopping rule)
     return {"it_pf": 530, "it_h0": 530, "it_h1": 530, "it_guid": 5000.0, "it_force": 5000.0,
             "nforce": 11.0}
+
+
+def bench_propagators(local_rank, seed=2024, nens=24, nsrc=4, res=1e-8):
+    """Config of the batched-solve case: 24 ensembles of uneven size
+    (L=Lt in {8,12,16}, Ls in {8,16,24}, seeded), chi ~ N(0,1), 4 point
+    sources each (flavour 1,2 x Dirac 3,4 at a seeded site on s=1),
+    Phi = M^dag xi, x0 = Phi as in fermion(); CGNE to residual 1e-8.
+    Returns solves/s one at a time and batched (one set of launches)."""
+    import ctypes as C
+    import torch
+    import chiralheisenberg_b200 as chb
+    rng = np.random.default_rng(seed)
+    ens = [(int(rng.choice([8, 12, 16])), int(rng.choice([8, 16, 24]))) for _ in range(nens)]
+    lats, keep, systems = [], [], []
+    for e, (L, Ls) in enumerate(ens):
+        gl = chb.Lattice(L, L, Ls, am3=1.0, device=local_rank)
+        chi = torch.from_numpy(rng.standard_normal((3, L ** 3))).cuda()
+        site = int(rng.integers(L ** 3))
+        for src in range(nsrc):
+            f, d = src // 2, 2 + src % 2
+            xi = torch.zeros((2, 4, L, L, L, Ls), dtype=torch.complex128, device="cuda")
+            xi.view(2, 4, -1, Ls)[f, d, site, 0] = 1.0
+            Phi = torch.empty_like(xi)
+            gl.lib.chdwf_dslash_dev(gl.h, C.c_void_p(Phi.data_ptr()), C.c_void_p(xi.data_ptr()),
+                                    C.c_void_p(chi.data_ptr()), 0.0, 1, 1, None)
+            gl.lib.chdwf_traj_sync(gl.h)
+            x = Phi.clone()
+            keep += [Phi, x, chi]
+            systems.append((gl, chb.CgSystem(L, L, Ls, 1, 0.0, 1.0, -1, Phi.data_ptr(),
+                                             x.data_ptr(), chi.data_ptr()), Phi, x, chi))
+        lats.append(gl)
+    torch.cuda.synchronize()
+    # one at a time (the reference's sequence of congrad calls)
+    t0 = time.perf_counter()
+    its1 = []
+    for gl, s, Phi, x, chi in systems:
+        xx = Phi.clone()
+        it = C.c_int()
+        gl.lib.chdwf_congrad_dev(gl.h, C.c_void_p(Phi.data_ptr()), res, C.byref(it), 0.0, 1,
+                                 C.c_void_p(chi.data_ptr()), C.c_void_p(xx.data_ptr()))
+        its1.append(it.value)
+    torch.cuda.synchronize()
+    t_one = time.perf_counter() - t0
+    # batched
+    t0 = time.perf_counter()
+    its2, sts = chb.congrad_batch(lats[0], [s for _, s, _, _, _ in systems], res)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    for gl in lats:
+        gl.close()
+    n = len(systems)
+    return {"solves": n, "ensembles": nens, "residual": res,
+            "one_at_a_time_solves_per_s": n / t_one, "batched_solves_per_s": n / t_batch,
+            "speedup": t_one / t_batch, "mean_iterations": float(np.mean(its2)),
+            "same_iterations": bool(list(its1) == list(its2)), "all_converged": bool((sts == 0).all())}
 
 
 def run_reference(args, rank, world):
@@ -330,6 +386,8 @@ def run_b200(args, rank, world, local_rank):
             "trajectories": [{"dH": r.dH, "accepted": r.accepted, "nsteps": r.nsteps}
                              for r in recs],
             "clocks": clk}
+    if rank == 0 and not args.no_propagators:
+        line["propagators"] = bench_propagators(local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         s_cpu, sample, _ = cpu_sample(L, Ls, threads, args.cpu_sample_iters, prof)

@@ -45,6 +45,7 @@ EXPORTS = (
     "chdwf_traj_set_momenta_dev", "chdwf_timing", "chdwf_timing_read", "chdwf_prog_stage",
     "chdwf_get_stream", "chdwf_kernel_launches", "chdwf_set_precision", "chdwf_dslash_dev_lp",
     "chdwf_prog_state_size", "chdwf_prog_get_state", "chdwf_prog_set_state",
+    "chdwf_congrad_batch",
     "chdwf_prog_create", "chdwf_prog_destroy", "chdwf_prog_context", "chdwf_prog_set_remez",
     "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
@@ -134,10 +135,33 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_kernel_launches.restype = C.c_longlong
     L.chdwf_set_precision.argtypes = [P, I, I]
     L.chdwf_dslash_dev_lp.argtypes = [P, P, P, P, F, I, I, I, P]
+    L.chdwf_congrad_batch.argtypes = [P, P, I, F, P, P]
     L.chdwf_prog_get_state.argtypes = [P, P, I]
     L.chdwf_prog_set_state.argtypes = [P, P, I]
     _lib = L
     return L
+
+
+class CgSystem(C.Structure):
+    """chdwf_cg_system (include/chdwf.h): one propagator solve of a batch."""
+    _fields_ = [("ksize", C.c_int), ("ksizet", C.c_int), ("kthird", C.c_int),
+                ("imass", C.c_int), ("hpin", C.c_float), ("am3", C.c_float),
+                ("ibound", C.c_int), ("Phi", C.c_void_p), ("x", C.c_void_p), ("chi", C.c_void_p)]
+
+
+def congrad_batch(lattice, systems, res):
+    """Solve every CgSystem of the list in one set of launches (device
+    pointers inside); returns (itercg, status) arrays.  lattice: any Lattice
+    (its context supplies the stream and the workspace)."""
+    n = len(systems)
+    arr = (CgSystem * n)(*systems)
+    it = np.zeros(n, dtype=np.int32)
+    st = np.zeros(n, dtype=np.int32)
+    rc = lattice.lib.chdwf_congrad_batch(lattice.h, C.cast(arr, C.c_void_p), n, res, _ptr(it),
+                                         _ptr(st))
+    if rc not in (CHDWF_OK, CHDWF_ITER_CAP, CHDWF_NONFINITE):
+        raise ChdwfError(rc, lattice.lib.chdwf_last_error(lattice.h).decode())
+    return it, st
 
 
 class SweepRecord(C.Structure):

@@ -41,6 +41,7 @@ Ctx::~Ctx() {
     cudaSetDevice(device);
     lz.release();
     cg.release();
+    free_batch(batch);
     for (int i = 0; i < kSpin; i++)
         if (spin[i]) cudaFree(spin[i]);
     if (chid) cudaFree(chid);

@@ -8,6 +8,9 @@
 
 namespace chdwf {
 
+struct BatchWork;                       // batch.cu
+void free_batch(BatchWork* w);
+
 // One rational approximation as the reference reads it (rhmc/cheisdwf.f:
 // 140-159): anum[0] = a0, anum[1..n], aden = sigma_1..n; same for b.
 struct RemezSet {
@@ -39,6 +42,7 @@ struct Ctx {
     double2* walls = nullptr;           // propagator wall slices
     RemezSet rz2, rz4, rz2g;
     int prec_md = 0, prec_accept = 0;   // vector precision of the resident solves
+    BatchWork* batch = nullptr;         // workspace of chdwf_congrad_batch
 
     ~Ctx();
     bool fail(cudaError_t e, const char* where);

@@ -605,7 +605,8 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.npole = ndiag;
     const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
     const int nbr = reduce_blocks(g.kferm);
-    T* r1 = a.rb1;
+    // r_1 lives where ring(a, 1) looks for it: the basis store when present
+    T* r1 = a.hcap > 1 ? a.basis + g.kferm : a.rb1;
 
     // r_1 = Phi, beta_1 = |r_1|
     k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);

@@ -137,6 +137,26 @@ int chdwf_qmrherm_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, f
 int chdwf_congrad_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, float hpin,
                       int imass, const void* chi, void* x);
 
+/* ---- batched propagator solves ------------------------------------------
+ * fermion() (rhmc/cheisdwf.f:897-1058) runs congrad once per source.  This
+ * solves nsys independent CGNE systems M^dag M x = Phi in one set of
+ * launches per CG stage; every system has its own lattice size, chi, imass,
+ * hpin, am3, ibound, REAL*4 scalars and stopping test (congrad's rule with
+ * residual res).  Pointers are device memory; x is the initial guess on
+ * input.  itercg[i], status[i] per system; the return value is the worst
+ * status. */
+typedef struct {
+    int ksize, ksizet, kthird;
+    int imass;
+    float hpin, am3;
+    int ibound;
+    const void* Phi;   /* complex128, reference layout */
+    void* x;           /* complex128, in: initial guess, out: solution */
+    const void* chi;   /* real*8 chi(kvol,3) */
+} chdwf_cg_system;
+int chdwf_congrad_batch(chdwf_ctx* ctx, const chdwf_cg_system* sys, int nsys, float res,
+                        int* itercg, int* status);
+
 /* ---- resident trajectory level ------------------------------------------
  * The blocks of the main loop of program dwf3d (rhmc/cheisdwf.f:207-399)
  * that call the routines above, with chi, chit, pp, dSdchi and Phi resident
