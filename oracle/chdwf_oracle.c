@@ -187,6 +187,9 @@ static void hop_sweep(const orc_lat* lat, double* Phi, const double* R, int f,
             }
 }
 
+static void s_and_walls(const orc_lat* lat, double* Phi, const double* R, const double* chi,
+                        float hpin, int imass, int dag);
+
 static void dslash_common(const orc_lat* lat, double* Phi, const double* R,
                           const double* chi, float hpin, int imass, int dag) {
     const int L = lat->L, Lt = lat->Lt;
@@ -229,6 +232,12 @@ static void dslash_common(const orc_lat* lat, double* Phi, const double* R,
                 }
         }
     }
+    s_and_walls(lat, Phi, R, chi, hpin, imass, dag);
+}
+
+static void s_and_walls(const orc_lat* lat, double* Phi, const double* R, const double* chi,
+                        float hpin, int imass, int dag) {
+    const int64_t Ls = lat->Ls, kvol = orc_kvol(lat);
     /* s hops exploiting the chiral projection (:2879-2908 / :3313-3342).
      * M: Dirac 3,4 from s+1 then Dirac 1,2 from s-1; M^dagger the reverse roles. */
     const int up0 = dag ? 0 : 2;   /* Dirac pair taking s+1 */
@@ -347,6 +356,102 @@ void orc_dslashd(const orc_lat* lat, double* Phi, const double* R, const double*
                  float am, float hpin, int imass) {
     (void)am;
     dslash_common(lat, Phi, R, chi, hpin, imass, 1);
+}
+
+/* ======================================================================
+ * The dead "v1" operator (cheisdwf.f:1804-2217): separate Wilson and Dirac
+ * sweeps driven by the gamma tables of init (:1521-1597).  Restated only
+ * as a second, independent formulation of M to check the v2 restatement.
+ * ==================================================================== */
+void orc_dslash_v1(const orc_lat* lat, double* Phi, const double* R, const double* chi,
+                   float am, float hpin, int imass) {
+    (void)am;
+    const int L = lat->L, Lt = lat->Lt;
+    const int64_t Ls = lat->Ls, kvol = orc_kvol(lat), kferm = orc_kferm(lat);
+    const double ak = 0.5;
+    /* gamval(mu,idirac)*akappa and gamin(mu,idirac), mu = 1,2,3 (:1524-1561) */
+    const cx gv[3][4] = {{{0, -ak}, {0, -ak}, {0, ak}, {0, ak}},
+                         {{-ak, 0}, {ak, 0}, {ak, 0}, {-ak, 0}},
+                         {{0, -ak}, {0, ak}, {0, ak}, {0, -ak}}};
+    const int gi[3][4] = {{3, 2, 1, 0}, {3, 2, 1, 0}, {2, 3, 0, 1}};
+    const float diag = (3.0f - lat->am3) + 1.0f;                      /* :1823 */
+    for (int64_t j = 0; j < kferm; j++) st(Phi, j, cscal((double)diag, ld(R, j)));
+#define NB(ix, iy, it) ((int64_t)(ix) + (int64_t)L * ((iy) + (int64_t)L * (it)))
+    /* Wilson term (:1841-1888) */
+    for (int f = 0; f < 2; f++)
+        for (int d = 0; d < 4; d++)
+            for (int mu = 0; mu < 3; mu++)
+                for (int it = 0; it < Lt; it++)
+                    for (int iy = 0; iy < L; iy++)
+                        for (int ix = 0; ix < L; ix++) {
+                            int xp = ix, xm = ix, yp = iy, ym = iy, tp = it, tm = it;
+                            if (mu == 0) { xp = (ix + 1) % L; xm = (ix + L - 1) % L; }
+                            if (mu == 1) { yp = (iy + 1) % L; ym = (iy + L - 1) % L; }
+                            if (mu == 2) { tp = (it + 1) % Lt; tm = (it + Lt - 1) % Lt; }
+                            for (int64_t s = 0; s < Ls; s++) {
+                                int64_t o = SIDX(s, NB(ix, iy, it), d, f);
+                                cx sum = cadd(ld(R, SIDX(s, NB(xp, yp, tp), d, f)),
+                                              ld(R, SIDX(s, NB(xm, ym, tm), d, f)));
+                                st(Phi, o, csub(ld(Phi, o), cscal(ak, sum)));
+                            }
+                        }
+    if (lat->ibound == -1)                                            /* :1891-1919 */
+        for (int f = 0; f < 2; f++)
+            for (int d = 0; d < 4; d++) {
+                for (int iy = 0; iy < L; iy++)
+                    for (int ix = 0; ix < L; ix++)
+                        for (int64_t s = 0; s < Ls; s++) {
+                            int64_t o = SIDX(s, NB(ix, iy, Lt - 1), d, f);
+                            st(Phi, o, cadd(ld(Phi, o), ld(R, SIDX(s, NB(ix, iy, 0), d, f))));
+                        }
+                for (int iy = 0; iy < L; iy++)
+                    for (int ix = 0; ix < L; ix++)
+                        for (int64_t s = 0; s < Ls; s++) {
+                            int64_t o = SIDX(s, NB(ix, iy, 0), d, f);
+                            st(Phi, o, cadd(ld(Phi, o), ld(R, SIDX(s, NB(ix, iy, Lt - 1), d, f))));
+                        }
+            }
+    /* Dirac term (:1921-1979) */
+    for (int f = 0; f < 2; f++)
+        for (int d = 0; d < 4; d++)
+            for (int mu = 0; mu < 3; mu++) {
+                const int ig = gi[mu][d];
+                for (int it = 0; it < Lt; it++)
+                    for (int iy = 0; iy < L; iy++)
+                        for (int ix = 0; ix < L; ix++) {
+                            int xp = ix, xm = ix, yp = iy, ym = iy, tp = it, tm = it;
+                            if (mu == 0) { xp = (ix + 1) % L; xm = (ix + L - 1) % L; }
+                            if (mu == 1) { yp = (iy + 1) % L; ym = (iy + L - 1) % L; }
+                            if (mu == 2) { tp = (it + 1) % Lt; tm = (it + Lt - 1) % Lt; }
+                            for (int64_t s = 0; s < Ls; s++) {
+                                int64_t o = SIDX(s, NB(ix, iy, it), d, f);
+                                cx dif = csub(ld(R, SIDX(s, NB(xp, yp, tp), ig, f)),
+                                              ld(R, SIDX(s, NB(xm, ym, tm), ig, f)));
+                                st(Phi, o, cadd(ld(Phi, o), cmul(gv[mu][d], dif)));
+                            }
+                        }
+            }
+    if (lat->ibound == -1)                                            /* :1981-2011 */
+        for (int f = 0; f < 2; f++)
+            for (int d = 0; d < 4; d++) {
+                const int ig = gi[2][d];
+                const cx g2 = cscal(2.0, gv[2][d]);
+                for (int iy = 0; iy < L; iy++)
+                    for (int ix = 0; ix < L; ix++)
+                        for (int64_t s = 0; s < Ls; s++) {
+                            int64_t o = SIDX(s, NB(ix, iy, Lt - 1), d, f);
+                            st(Phi, o, csub(ld(Phi, o), cmul(g2, ld(R, SIDX(s, NB(ix, iy, 0), ig, f)))));
+                        }
+                for (int iy = 0; iy < L; iy++)
+                    for (int ix = 0; ix < L; ix++)
+                        for (int64_t s = 0; s < Ls; s++) {
+                            int64_t o = SIDX(s, NB(ix, iy, 0), d, f);
+                            st(Phi, o, cadd(ld(Phi, o), cmul(g2, ld(R, SIDX(s, NB(ix, iy, Lt - 1), ig, f)))));
+                        }
+            }
+#undef NB
+    /* s hops and wall coupling: the same statements as v2 (:2013-2217) */
+    s_and_walls(lat, Phi, R, chi, hpin, imass, 0);
 }
 
 /* ======================================================================

@@ -71,6 +71,9 @@ void orc_dslash (const orc_lat* lat, double* Phi, const double* R,
                  const double* chi, float am, float hpin, int imass);
 void orc_dslashd(const orc_lat* lat, double* Phi, const double* R,
                  const double* chi, float am, float hpin, int imass);
+/* The dead table-driven "v1" M (cheisdwf.f:1804-2217), a second formulation. */
+void orc_dslash_v1(const orc_lat* lat, double* Phi, const double* R,
+                   const double* chi, float am, float hpin, int imass);
 
 /* --- solvers ------------------------------------------------------------- */
 /* qmrherm (cheisdwf.f:599-745).  x: /vector/x output (kferm complex).

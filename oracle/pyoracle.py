@@ -80,7 +80,7 @@ def lib():
         L.orc_rng_startup.argtypes = [P, C.c_double]
         L.orc_gauss0.argtypes = [P, C.c_int64, P]
         L.orc_gaussp.argtypes = [P, C.c_int64, P]
-        for f in (L.orc_dslash, L.orc_dslashd):
+        for f in (L.orc_dslash, L.orc_dslashd, L.orc_dslash_v1):
             f.argtypes = [P, P, P, P, C.c_float, C.c_float, C.c_int]
         L.orc_qmrherm.argtypes = [P, P, C.c_float, P, C.c_float, C.c_float, C.c_int, P, P,
                                   C.c_int, C.c_int, P, P, P, C.c_int]
@@ -118,11 +118,11 @@ def kvol(lat: Lat) -> int:
     return lat.L * lat.L * lat.Lt
 
 
-def dslash(lat, R, chi, hpin=0.0, imass=1, dag=False, am=0.0):
+def dslash(lat, R, chi, hpin=0.0, imass=1, dag=False, am=0.0, v1=False):
     R = np.ascontiguousarray(R, dtype=np.complex128)
     chi = np.ascontiguousarray(chi, dtype=np.float64)
     out = np.empty_like(R)
-    f = lib().orc_dslashd if dag else lib().orc_dslash
+    f = lib().orc_dslashd if dag else (lib().orc_dslash_v1 if v1 else lib().orc_dslash)
     f(C.byref(lat), _p(out), _p(R), _p(chi), am, hpin, imass)
     return out
 
