@@ -45,7 +45,7 @@ EXPORTS = (
     "chdwf_traj_set_momenta_dev", "chdwf_timing", "chdwf_timing_read", "chdwf_prog_stage",
     "chdwf_get_stream", "chdwf_kernel_launches", "chdwf_set_precision", "chdwf_dslash_dev_lp",
     "chdwf_prog_state_size", "chdwf_prog_get_state", "chdwf_prog_set_state",
-    "chdwf_congrad_batch",
+    "chdwf_congrad_static", "chdwf_congrad_batch",
     "chdwf_prog_create", "chdwf_prog_destroy", "chdwf_prog_context", "chdwf_prog_set_remez",
     "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
@@ -135,6 +135,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_kernel_launches.restype = C.c_longlong
     L.chdwf_set_precision.argtypes = [P, I, I]
     L.chdwf_dslash_dev_lp.argtypes = [P, P, P, P, F, I, I, I, P]
+    L.chdwf_congrad_static.argtypes = [P, P, P, I, I, I, F, I, F, F, I, PI, P]
     L.chdwf_congrad_batch.argtypes = [P, P, I, F, P, P]
     L.chdwf_prog_get_state.argtypes = [P, P, I]
     L.chdwf_prog_set_state.argtypes = [P, P, I]

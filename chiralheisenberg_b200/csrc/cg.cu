@@ -217,4 +217,101 @@ cudaError_t cg_solve(CgWork& w, const Geom& g, const double2* phi, float res, co
     return cudaSuccess;
 }
 
+// ---- congrad without any allocation ---------------------------------------
+// For callers that cannot allocate device memory: a host program whose device
+// memory is owned by another runtime's pool or reserved in full up front, or
+// code that must not allocate (a real-time or otherwise allocation-free
+// section).  The solver's scratch -- the REAL*4 copy of chi, the CG vectors
+// x1, p, r, the per-block partial sums and the control block -- lives in one
+// file-scope device array sized for kferm <= kStaticMaxFerm.  The array is
+// shared by every call: calls whose GPU work overlaps (other streams, other
+// host threads) race on it.  Each call clears the part that must start at
+// zero (the control block) before its first kernel.
+constexpr int64_t kStaticMaxFerm = 262144;            // 8*kvol*kthird, e.g. 16^3 x 8
+constexpr int64_t kStaticMaxKvol = kStaticMaxFerm / 16;   // kthird >= 2
+constexpr size_t kStaticBytes = 256 + 64 * 1024 +          // control block, partials
+                                3 * kStaticMaxKvol * sizeof(float) +
+                                3 * kStaticMaxFerm * sizeof(double2);
+static __device__ __align__(256) unsigned char g_cg_scratch[kStaticBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+unsigned char* g_scratch_addr[kMaxDevices] = {};   // device address per device ordinal
+}  // namespace
+
 }  // namespace chdwf
+
+extern "C" int chdwf_congrad_static(const void* Phi, void* x, const void* chi, int ksize,
+                                    int ksizet, int kthird, float am3, int ibound, float res,
+                                    float hpin, int imass, int* itercg, void* stream) {
+    using namespace chdwf;
+    if (!Phi || !x || !chi || !itercg || ksize < 2 || ksizet < 2 || kthird < 2) return 4;
+    if (imass != 1 && imass != 3) return 4;
+    const Geom g = make_geom(ksize, ksizet, kthird);
+    if (g.kferm > kStaticMaxFerm) return 4;          // beyond the static scratch
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 3;
+    // once per device: the device address of the array (its host-side name
+    // is only a stand-in and must never be passed to a kernel)
+    if (!g_scratch_addr[dev]) {
+        void* ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_cg_scratch) != cudaSuccess || !ptr) return 3;
+        g_scratch_addr[dev] = (unsigned char*)ptr;
+    }
+    unsigned char* base = g_scratch_addr[dev];
+    CgCtl* ctl = reinterpret_cast<CgCtl*>(base);
+    double* part = reinterpret_cast<double*>(base + 256);
+    float* chif = reinterpret_cast<float*>(base + 256 + 64 * 1024);
+    double2* x1 = reinterpret_cast<double2*>(base + 256 + 64 * 1024 +
+                                             3 * kStaticMaxKvol * sizeof(float));
+    double2* p = x1 + kStaticMaxFerm;
+    double2* r = p + kStaticMaxFerm;
+    cudaStream_t st = (cudaStream_t)stream;
+    CgCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.nx = 1;
+    hc.alpha = 1.0f;                                  // rhmc/cheisdwf.f:1090-1091
+    hc.betad = 1.0f;
+    hc.resid = (float)g.kferm * res * res;            // :1076
+    hc.niterc = (int)(g.Ls * (int64_t)g.kvol);
+    if (cudaMemcpyAsync(ctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st) != cudaSuccess) return 3;
+    launch_round_chi((const double*)chi, chif, g.kvol, st);
+    cudaMemcpyAsync(p, x, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(r, Phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, st);
+    CgArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = g;
+    a.x = (double2*)x; a.p = p; a.r = r; a.x1 = x1;
+    a.chif = chif;
+    a.diag = (double)(2.0f * ((3.0f - am3) + 1.0f));
+    a.hpin = (double)hpin;
+    a.apbc = ibound == -1;
+    a.ctl = ctl;
+    a.part = part;
+    a.hflag = nullptr;
+    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const unsigned nbf = (unsigned)((g.kferm + kThreads - 1) / kThreads);
+    // chunks of 16 iterations; the done flag is copied into a host stack
+    // variable after each chunk (launches after convergence return at once)
+    const int64_t cap = hc.niterc;
+    int64_t launched = 0;
+    CgCtl hr;
+    memset(&hr, 0, sizeof(hr));
+    while (launched < cap) {
+        for (int c = 0; c < 16 && launched < cap; c++, launched++) {
+            if (imass == 3) { k_cg1<3><<<nb, kThreads, 0, st>>>(a); k_cg2<3><<<nb, kThreads, 0, st>>>(a); }
+            else { k_cg1<1><<<nb, kThreads, 0, st>>>(a); k_cg2<1><<<nb, kThreads, 0, st>>>(a); }
+            k_cg3<<<nbf, kThreads, 0, st>>>(a);
+            count_launches(3);
+        }
+        if (cudaMemcpyAsync(&hr, ctl, sizeof(hr), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return 3;
+        if (hr.done) break;
+    }
+    if (cudaGetLastError() != cudaSuccess) return 3;
+    *itercg = hr.iters;
+    if (hr.done == 2) return 1;
+    if (hr.done == 3) return 2;
+    return 0;
+}

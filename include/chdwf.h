@@ -136,6 +136,22 @@ int chdwf_qmrherm_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, f
                       const void* chi, void* x, void* dSdchi);
 int chdwf_congrad_dev(chdwf_ctx* ctx, const void* Phi, float res, int* itercg, float hpin,
                       int imass, const void* chi, void* x);
+/* congrad that allocates nothing (no counterpart in the reference).  For
+ * callers that cannot allocate device memory -- e.g. a host program whose GPU
+ * memory belongs to another runtime's pool or is reserved in full up front,
+ * or a code path where allocating is not allowed -- and so cannot create a
+ * context either.  Same solve as chdwf_congrad_dev; every argument is
+ * explicit and Phi, x (initial guess in, solution out) and chi (real*8
+ * (kvol,3)) are device pointers on the current device; stream may be NULL.
+ * Scratch lives in one static device array of the library, sized for
+ * 8*ksize^2*ksizet*kthird <= 262144 (about 13 MB, held by every GPU that
+ * loads the library until the process exits); larger lattices return
+ * CHDWF_BAD_ARG.  The first call on a device looks up the array's device
+ * address (make it before any stream capture).  All calls share the array:
+ * calls whose GPU work overlaps race.  Returns the CHDWF_* statuses. */
+int chdwf_congrad_static(const void* Phi, void* x, const void* chi, int ksize, int ksizet,
+                         int kthird, float am3, int ibound, float res, float hpin, int imass,
+                         int* itercg, void* stream);
 
 /* ---- batched propagator solves ------------------------------------------
  * fermion() (rhmc/cheisdwf.f:897-1058) runs congrad once per source.  This
