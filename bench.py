@@ -16,8 +16,10 @@ seconds per trajectory (lower is better).
             stream, max over ranks.
   e2e       the same trajectories through the host-facing driver API with the
             random numbers drawn on the host and copied in every step.
-  roofline  the dominant solver kernel, timed with CUDA events inside the
-            timed region, against algorithmic bytes per launch.
+  roofline  the dominant solver kernel class, timed with CUDA events around
+            every solver launch in an instrumented replay of the first timed
+            trajectory, against the algorithmic bytes the library reports for
+            each launch.
   cpu_baseline / --impl reference
             the CPU oracle (a C restatement of rhmc/cheisdwf.f; the Fortran
             reference cannot be built here) on the host cores: per-iteration
@@ -63,6 +65,10 @@ def parse():
     ap.add_argument("--Ls", type=int, default=24)
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="bounded work for profilers: one heatbath and one force evaluation")
+    ap.add_argument("--basis-gb", type=float, default=-1.0,
+                    help="HBM budget of the stored Lanczos basis (GB; <0 library default)")
     return ap.parse_args()
 
 
@@ -130,19 +136,12 @@ def synthetic_chi(L, Lt, beta, seed):
     return rng.standard_normal((3, L * L * Lt)) / np.sqrt(beta)
 
 
-# algorithmic bytes per launch of the four solver kernel classes (16 B per
-# complex128 component, V = 8*kvol*Ls components, chi read as REAL*4 planes)
-def kernel_bytes(L, Ls):
-    kvol = L * L * L
-    V = 8 * kvol * Ls
-    chi = 12 * kvol
-    return {0: ("pass-1 M q (+|Mq|^2)", 2 * 16 * V + chi),
-            1: ("pass-1 M^dag + 3-term update (+|r|^2)", 4 * 16 * V + chi),
-            2: ("pass-2 M q + solution accumulate", 4 * 16 * V + chi),
-            3: ("pass-2 M^dag + 3-term update", 4 * 16 * V + chi)}
-
-
-KERNEL_NAMES = {0: "k_lz1_M", 1: "k_lz1_Md", 2: "k_lz2_M", 3: "k_lz2_Md"}
+# solver kernel classes reported by chdwf_timing_read
+KERNEL_NAMES = {0: "k_lz1_M", 1: "k_lz1_Md", 2: "k_lz_accum", 3: "k_lz2_M/k_lz2_Md"}
+KERNEL_WHAT = {0: "pass-1 M q_j with |M q_j|^2",
+               1: "pass-1 M^dag + three-term update with |r|^2",
+               2: "pass-2 solution accumulation from the stored Lanczos basis",
+               3: "pass-2 regeneration (solves longer than the basis store)"}
 
 
 def cpu_sample(L, Ls, threads, iters, profile):
@@ -268,6 +267,40 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_solve(args, local_rank):
+    """One pseudofermion heatbath and one force evaluation at the bench
+    lattice: a bounded launch sequence for profilers."""
+    import torch
+    import chiralheisenberg_b200 as chb
+    torch.cuda.set_device(local_rank)
+    L, Ls = args.L, args.Ls
+    rz = chb.reference_remez()
+    prog = chb.Program(L, L, Ls, CFG["dt"], CFG["beta"], CFG["am3"], CFG["am"], CFG["hpin"],
+                       CFG["imass"], CFG["iterl"], rz["remez2"], rz["remez4"], rz["remez2g"],
+                       device=local_rank)
+    if args.basis_gb >= 0:
+        prog.set_basis_store(args.basis_gb * 1e9)
+    prog.set_chi(synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"]))
+    prog.startup(CFG["seed"])
+    lib, ctx = prog.lib, prog.context
+    import ctypes as C
+    kvol = L ** 3
+    rng = np.random.default_rng(3)
+    ps = (rng.standard_normal(16 * kvol * Ls) * np.sqrt(0.5)).astype(np.float32)
+    it = C.c_int()
+    t0 = time.perf_counter()
+    lib.chdwf_traj_begin(ctx)
+    rc1 = lib.chdwf_traj_heatbath(ctx, ps.ctypes.data_as(C.c_void_p), 1e-9, 0.0, 0.0, 1,
+                                  C.byref(it))
+    itg, itf = C.c_int(), C.c_int()
+    rc2 = lib.chdwf_traj_force(ctx, 1e-6, 0.0, 0.0, 1, C.byref(itg), C.byref(itf))
+    lib.chdwf_traj_sync(ctx)
+    dt = time.perf_counter() - t0
+    print(json.dumps({"profile_solve": f"L=Lt={L} Ls={Ls}", "rc": [rc1, rc2],
+                      "iterations": [it.value, itg.value, itf.value], "seconds": dt}), flush=True)
+    prog.close()
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import chiralheisenberg_b200 as chb
@@ -313,15 +346,12 @@ def run_b200(args, rank, world, local_rank):
     # before the second
     chi0 = prog.get_chi()
     state0 = prog.get_state()
-    prog.timing(True)
     clocks = ClockSampler(local_rank)
     clocks.start()
     n0 = chb.kernel_launches()
     ms_value, recs = timed(staged=True)
     launches = chb.kernel_launches() - n0
     clk = clocks.stop()
-    kms, ktimed, klaunched = prog.timing_read()
-    prog.timing(False)
     prog.set_chi(chi0)
     prog.set_state(state0)
     ms_e2e, recs_e2e = timed(staged=False)
@@ -344,6 +374,17 @@ def run_b200(args, rank, world, local_rank):
                  "same_decisions": all(a.accepted == b.accepted and a.nsteps == b.nsteps
                                        for a, b in zip(recs, recs_mix))}
 
+    # Per-kernel timing: the first timed trajectory again, instrumented --
+    # CUDA events around every solver launch on the library's stream (the
+    # instrumented replay issues launches one by one, so it is not part of
+    # the timed value above)
+    prog.set_chi(chi0)
+    prog.set_state(state0)
+    prog.timing(True)
+    prog.sweep()
+    kms, ktimed, klaunched, kbytes = prog.timing_read()
+    prog.timing(False)
+
     # whole job: steps*world trajectories in the slowest rank's time
     ntraj = args.steps * world
     value = (ms_value / 1e3) / ntraj
@@ -351,10 +392,10 @@ def run_b200(args, rank, world, local_rank):
     kvol = L * L * L
     h2d = 64 * kvol * Ls + 12 * kvol          # heatbath Gaussians + momenta
     d2h = 12 * kvol + 64                      # momenta for vel2 + scalars
-    kb = kernel_bytes(L, Ls)
     dom = int(np.argmax(kms))
     avg_ms = kms[dom] / max(ktimed[dom], 1)
-    achieved = kb[dom][1] / (avg_ms * 1e-3) / 1e9
+    achieved = kbytes[dom] / (kms[dom] * 1e-3) / 1e9
+    bytes_per_launch = kbytes[dom] / max(ktimed[dom], 1)
     peak, peak_kind = peaks()
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic_24x24.json")
@@ -375,11 +416,17 @@ def run_b200(args, rank, world, local_rank):
                        "(solver working set > 126 MB)", **CFG},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "same_trajectories_as_value": same},
-            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "what": kb[dom][0],
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "what": KERNEL_WHAT[dom],
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "bytes_per_launch": kb[dom][1], "avg_launch_us": avg_ms * 1e3},
-            "kernel_avg_us": {KERNEL_NAMES[k]: kms[k] / max(ktimed[k], 1) * 1e3 for k in range(4)},
+                         "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_ms * 1e3,
+                         "measured_in": "instrumented replay of the first timed trajectory, "
+                                        "CUDA events around every solver launch"},
+            "solver_kernels": {KERNEL_NAMES[k]: {
+                "launches": int(klaunched[k]), "avg_us": kms[k] / max(ktimed[k], 1) * 1e3,
+                "share_of_solver_time": kms[k] / max(sum(kms), 1e-30),
+                "GBps": (kbytes[k] / (kms[k] * 1e-3) / 1e9) if kms[k] > 0 else None}
+                for k in range(4)},
             "gpu_launches": launches,
             "mixed": mixed,
             "iteration_profile": prof,
@@ -405,6 +452,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile_solve:
+        run_profile_solve(args, local_rank)
         return
     if world > 1:
         import datetime

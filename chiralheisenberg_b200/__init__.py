@@ -45,7 +45,7 @@ EXPORTS = (
     "chdwf_traj_set_momenta_dev", "chdwf_timing", "chdwf_timing_read", "chdwf_prog_stage",
     "chdwf_get_stream", "chdwf_kernel_launches", "chdwf_set_precision", "chdwf_dslash_dev_lp",
     "chdwf_prog_state_size", "chdwf_prog_get_state", "chdwf_prog_set_state",
-    "chdwf_congrad_static", "chdwf_congrad_batch",
+    "chdwf_congrad_static", "chdwf_congrad_batch", "chdwf_set_basis_store",
     "chdwf_prog_create", "chdwf_prog_destroy", "chdwf_prog_context", "chdwf_prog_set_remez",
     "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
@@ -129,7 +129,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_prog_stage.argtypes = [P, I]
     L.chdwf_traj_set_momenta_dev.argtypes = [P, P]
     L.chdwf_timing.argtypes = [P, I]
-    L.chdwf_timing_read.argtypes = [P, P, P, P]
+    L.chdwf_timing_read.argtypes = [P, P, P, P, P]
     L.chdwf_get_stream.argtypes = [P]
     L.chdwf_get_stream.restype = P
     L.chdwf_kernel_launches.restype = C.c_longlong
@@ -137,6 +137,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_dslash_dev_lp.argtypes = [P, P, P, P, F, I, I, I, P]
     L.chdwf_congrad_static.argtypes = [P, P, P, I, I, I, F, I, F, F, I, PI, P]
     L.chdwf_congrad_batch.argtypes = [P, P, I, F, P, P]
+    L.chdwf_set_basis_store.argtypes = [P, D]
     L.chdwf_prog_get_state.argtypes = [P, P, I]
     L.chdwf_prog_set_state.argtypes = [P, P, I]
     _lib = L
@@ -271,6 +272,10 @@ class Program:
     def timing(self, enable=True):
         self._check(self.lib.chdwf_timing(self.context, 1 if enable else 0))
 
+    def set_basis_store(self, max_bytes):
+        """HBM budget of the stored Lanczos basis (bytes; 0 disables, <0 default)."""
+        self._check(self.lib.chdwf_set_basis_store(self.context, float(max_bytes)))
+
     def set_precision(self, md="f64", accept="f64"):
         """Krylov-vector precision of the force solves (md) and of the
         heatbath/hamilton solves (accept): "f64" (drop-in) or "f32"."""
@@ -278,12 +283,14 @@ class Program:
         self._check(self.lib.chdwf_set_precision(self.context, code[md], code[accept]))
 
     def timing_read(self):
+        """Per solver-kernel class: (ms, timed launches, launches, bytes)."""
         ms = np.zeros(4, dtype=np.float64)
         timed = np.zeros(4, dtype=np.int64)
         launched = np.zeros(4, dtype=np.int64)
+        nbytes = np.zeros(4, dtype=np.float64)
         self._check(self.lib.chdwf_timing_read(self.context, _ptr(ms), _ptr(timed),
-                                               _ptr(launched)))
-        return ms, timed, launched
+                                               _ptr(launched), _ptr(nbytes)))
+        return ms, timed, launched, nbytes
 
     def close(self):
         if getattr(self, "h", None):
@@ -347,6 +354,10 @@ class Lattice:
         if rc == CHDWF_ITER_CAP:
             raise IterationCapError(rc, msg)
         raise ChdwfError(rc, msg)
+
+    def set_basis_store(self, max_bytes):
+        """HBM budget of the stored Lanczos basis (bytes; 0 disables, <0 default)."""
+        self._check(self.lib.chdwf_set_basis_store(self.h, float(max_bytes)))
 
     def _chi(self, chi):
         chi = np.ascontiguousarray(chi, dtype=np.float64)

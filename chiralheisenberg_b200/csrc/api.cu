@@ -96,16 +96,33 @@ int chdwf_set_precision(chdwf_ctx* ctx, int md, int accept) {
     return CHDWF_OK;
 }
 
+int chdwf_set_basis_store(chdwf_ctx* ctx, double max_bytes) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return CHDWF_BAD_ARG;
+    cudaSetDevice(c->device);
+    c->lz.basis_enabled = max_bytes != 0.0;
+    c->lz.basis_max_bytes = max_bytes;
+    // drop the current store; the next solve allocates within the new limit
+    if (c->lz.basis) cudaFree(c->lz.basis);
+    if (c->lz.basis32) cudaFree(c->lz.basis32);
+    c->lz.basis = nullptr;
+    c->lz.basis32 = nullptr;
+    c->lz.hcap = c->lz.hcap32 = 0;
+    return c->status_of(cudaGetLastError(), "set_basis_store");
+}
+
 void* chdwf_get_stream(chdwf_ctx* ctx) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     return c ? (void*)c->stream : nullptr;
 }
 
-int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched) {
+int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched,
+                      double* bytes) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
-    if (!c || !ms || !timed || !launched) return CHDWF_BAD_ARG;
+    if (!c || !ms || !timed || !launched || !bytes) return CHDWF_BAD_ARG;
     for (int k = 0; k < KernelTimer::kClasses; k++) {
         ms[k] = c->lz.timer.total_ms[k];
+        bytes[k] = c->lz.timer.total_bytes[k];
         timed[k] = c->lz.timer.count[k];
         launched[k] = c->lz.timer.launches[k];
     }

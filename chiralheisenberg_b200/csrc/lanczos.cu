@@ -330,27 +330,79 @@ __global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* part, int nb) {
 }
 
 template <class T, int IMASS>
-static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, KernelTimer& tm) {
-    tm.begin(0, st);
+static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, KernelTimer* tm) {
+    // algorithmic bytes: M reads q, writes vt; M^dagger reads vt, r_j, r_{j-1}
+    // and writes r_{j+1}; both read chi as REAL*4
+    const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
+    if (tm) tm->begin(0, st, 2 * V + chi);
     k_lz1_M<T, IMASS><<<nb, kThreads, 0, st>>>(a);
-    tm.end(st);
-    tm.begin(1, st);
+    if (tm) tm->end(st);
+    if (tm) tm->begin(1, st, 4 * V + chi);
     k_lz1_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a);
-    tm.end(st);
-    count_launches(2);
+    if (tm) tm->end(st);
+}
+
+// Pass 1 is a sequence of identical launch pairs (the iteration index and the
+// residual ring live in device memory), so a chunk of them is captured once
+// as a CUDA graph and replayed; the graph is rebuilt when any argument
+// changes.
+template <class T>
+static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned nb, int imass,
+                                   int chunk, cudaStream_t st) {
+    // pass-1 kernels never touch the pass-2 fields: clear them so one graph
+    // serves every solve of this precision (heatbath, hamilton, force)
+    LzArgsT<T> a = a_in;
+    a.x = nullptr;
+    a.xw = nullptr;
+    a.npole = 0;
+    LzGraph& G = w.graph[sizeof(T) == sizeof(float2) ? 1 : 0];
+    const unsigned char* key = reinterpret_cast<const unsigned char*>(&a);
+    if (G.exec && G.nb == nb && G.imass == imass && G.chunk == chunk &&
+        G.key.size() == sizeof(a) && memcmp(G.key.data(), key, sizeof(a)) == 0)
+        return G.exec;
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G.exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    for (int c = 0; c < chunk; c++) {
+        if (imass == 3) launch_pass1<T, 3>(a, nb, st, nullptr);
+        else launch_pass1<T, 1>(a, nb, st, nullptr);
+    }
+    if (cudaStreamEndCapture(st, &graph) != cudaSuccess || !graph) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    G.exec = exec;
+    G.nb = nb;
+    G.imass = imass;
+    G.chunk = chunk;
+    G.key.assign(key, key + sizeof(a));
+    return exec;
 }
 
 template <class T, int IMASS>
 static void launch_pass2(const LzArgsT<T>& a, unsigned nb, int j, int m, int iflag,
                          cudaStream_t st, KernelTimer& tm) {
     const int apply = j < m;
-    if (apply) tm.begin(2, st);
+    const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
+    const double acc = iflag == 0 ? 2.0 * a.g.kferm * sizeof(double2) + V : 0.0;
+    if (apply) tm.begin(3, st, 2 * V + chi + acc);
     if (iflag == 0) k_lz2_M<T, IMASS, 0><<<nb, kThreads, 0, st>>>(a, j, apply);
     else k_lz2_M<T, IMASS, 1><<<nb, kThreads, 0, st>>>(a, j, apply);
     count_launches(1);
     if (apply) {
         tm.end(st);
-        tm.begin(3, st);
+        tm.begin(3, st, 4 * V + chi);
         k_lz2_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a, j);
         tm.end(st);
         count_launches(1);
@@ -373,14 +425,20 @@ void KernelTimer::release() {
 
 void KernelTimer::reset() {
     used = 0;
-    for (int c = 0; c < kClasses; c++) { total_ms[c] = 0; count[c] = 0; launches[c] = 0; }
+    for (int c = 0; c < kClasses; c++) {
+        total_ms[c] = 0;
+        total_bytes[c] = 0;
+        count[c] = 0;
+        launches[c] = 0;
+    }
 }
 
-void KernelTimer::begin(int c, cudaStream_t st) {
+void KernelTimer::begin(int c, cudaStream_t st, double nbytes) {
     if (!enabled) return;
     launches[c]++;
     if (used >= kPool) return;          // pool full: the launch is counted, not timed
     cls[used] = c;
+    bytes[used] = nbytes;
     cudaEventRecord(ev[2 * used], st);
 }
 
@@ -396,6 +454,7 @@ void KernelTimer::collect() {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) {
             total_ms[cls[i]] += ms;
+            total_bytes[cls[i]] += bytes[i];
             count[cls[i]]++;
         }
     }
@@ -408,6 +467,10 @@ LzWork::~LzWork() {
 }
 
 void LzWork::release() {
+    for (LzGraph& gr : graph) {
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
+        gr = LzGraph();
+    }
     if (ctl) cudaFree(ctl);
     if (hist_mem) cudaFree(hist_mem);
     if (part) cudaFree(part);
@@ -469,7 +532,8 @@ cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         const size_t vb = (prec == kPrecF64 ? sizeof(double2) : sizeof(float2)) * (size_t)g.kferm;
-        int64_t cap = (int64_t)(0.4 * (double)fr / (double)vb);
+        const double budget = basis_max_bytes >= 0.0 ? basis_max_bytes : 0.4 * (double)fr;
+        int64_t cap = (int64_t)(budget / (double)vb);
         if (cap > kMaxIter + 2) cap = kMaxIter + 2;
         if (cap >= 8) {
             void* ptr = nullptr;
@@ -620,10 +684,19 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
     int launched = 0, nchunk = 0;
+    // the per-launch path when kernels are being timed, else graph replays
+    cudaGraphExec_t gexec = w.timer.enabled ? nullptr : pass1_graph<T>(w, a, nb, imass, chunk, st);
     while (launched < kMaxIter) {
-        for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
-            if (imass == 3) launch_pass1<T, 3>(a, nb, st, w.timer);
-            else launch_pass1<T, 1>(a, nb, st, w.timer);
+        if (gexec) {
+            cudaGraphLaunch(gexec, st);
+            launched += chunk;
+            count_launches(2 * chunk);
+        } else {
+            for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
+                if (imass == 3) launch_pass1<T, 3>(a, nb, st, &w.timer);
+                else launch_pass1<T, 1>(a, nb, st, &w.timer);
+                count_launches(2);
+            }
         }
         cudaEventRecord(ev[nchunk & 1], st);
         if (nchunk >= 1) {
@@ -674,7 +747,13 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     if (iflag) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
     if (m < a.hcap) {
         // every q_j is still in HBM: one streaming pass over the basis
-        w.timer.begin(2, st);
+        // reads the m stored vectors (whole or their two wall slices) and
+        // the solution once
+        const double vb = (double)sizeof(T);
+        const double nbytes = iflag == 0
+            ? (double)m * g.kferm * vb + 2.0 * g.kferm * sizeof(double2)
+            : (double)m * 16.0 * g.kvol * vb + (double)ndiag * 16.0 * g.kvol * sizeof(double2);
+        w.timer.begin(2, st, nbytes);
         if (iflag == 0)
             k_lz_accum_x<T><<<(unsigned)((g.kferm + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, m);
         else

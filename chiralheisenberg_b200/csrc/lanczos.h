@@ -1,5 +1,7 @@
 // lanczos.h -- two-pass multi-shift Lanczos solver (qmrherm replacement).
 #pragma once
+#include <vector>
+
 #include "internal.h"
 
 namespace chdwf {
@@ -32,9 +34,10 @@ struct LzStats {
     int pass1_launches;
 };
 
-// Optional CUDA-event timing of the four stencil kernels of the solver
-// (0: pass-1 M, 1: pass-1 M^dagger + update, 2: pass-2 M + accumulate,
-// 3: pass-2 M^dagger + update).  Events bracket each launch on the solver's
+// Optional CUDA-event timing of the solver kernels by class (0: pass-1 M,
+// 1: pass-1 M^dagger + update, 2: pass-2 accumulation from the stored basis,
+// 3: pass-2 regeneration, M and M^dagger launches), with the algorithmic
+// bytes of every timed launch.  Events bracket each launch on the solver's
 // stream; durations are summed when the solve synchronises.
 struct KernelTimer {
     static constexpr int kClasses = 4;
@@ -42,20 +45,30 @@ struct KernelTimer {
     bool enabled = false;
     cudaEvent_t ev[2 * kPool] = {};
     int cls[kPool] = {};
+    double bytes[kPool] = {};
     int used = 0;
     double total_ms[kClasses] = {0, 0, 0, 0};
+    double total_bytes[kClasses] = {0, 0, 0, 0};   // algorithmic bytes moved
     long long count[kClasses] = {0, 0, 0, 0};
     long long launches[kClasses] = {0, 0, 0, 0};
     void enable();
     void release();
-    void begin(int c, cudaStream_t st);   // records the start event of one launch
+    void begin(int c, cudaStream_t st, double nbytes);   // start event of one launch
     void end(cudaStream_t st);
     void collect();                       // after a synchronisation
     void reset();
 };
 
+struct LzGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;   // the kernel arguments it was captured with
+    unsigned nb = 0;
+    int imass = 0, chunk = 0;
+};
+
 struct LzWork {
     Geom geom{};
+    LzGraph graph[2];                 // pass-1 chunk graph per vector precision
     LzCtl* ctl = nullptr;
     double* hist_mem = nullptr;
     LzHist hist{};
@@ -70,6 +83,7 @@ struct LzWork {
     float2* basis32 = nullptr;
     int hcap = 0, hcap32 = 0;
     int basis_enabled = 1;
+    double basis_max_bytes = -1.0;   // per precision; < 0: 40% of the free HBM
     double2* xw = nullptr;
     double2* x2w = nullptr;
     int xw_poles = 0;

@@ -57,12 +57,13 @@ int chdwf_set_para(chdwf_ctx* ctx, float beta, float am3, int ibound);
 const char* chdwf_last_error(const chdwf_ctx* ctx);
 /* version string of the library build */
 const char* chdwf_version(void);
-/* CUDA-event timing of the multi-shift solver's stencil kernels (no
- * reference counterpart; instrumentation).  enable=1 turns it on and resets
- * the totals.  chdwf_timing_read fills, per kernel class (0: pass-1 M,
- * 1: pass-1 M^dagger + update, 2: pass-2 M + accumulate, 3: pass-2
- * M^dagger + update), the summed milliseconds, the number of timed launches
- * and the number of launches. */
+/* CUDA-event timing of the multi-shift solver's kernels (no reference
+ * counterpart; instrumentation).  enable=1 turns it on (every solver launch
+ * is then bracketed by events and issued one by one) and resets the totals.
+ * chdwf_timing_read fills, per kernel class (0: pass-1 M, 1: pass-1
+ * M^dagger + update, 2: pass-2 accumulation from the stored basis, 3: pass-2
+ * regeneration), the summed milliseconds, the number of timed launches, the
+ * number of launches and the algorithmic bytes of the timed launches. */
 int chdwf_timing(chdwf_ctx* ctx, int enable);
 /* Precision of the Krylov vectors in the resident trajectory solves (no
  * reference counterpart: the reference is FP64 throughout).  md: the two
@@ -73,12 +74,20 @@ int chdwf_timing(chdwf_ctx* ctx, int enable);
 #define CHDWF_PREC_F64 0
 #define CHDWF_PREC_F32 1
 int chdwf_set_precision(chdwf_ctx* ctx, int md, int accept);
+/* HBM for the stored Lanczos basis of the multi-shift solver, per vector
+ * precision (no reference counterpart).  A solve whose iterations fit keeps
+ * every Lanczos vector and forms its solution in one pass over them; longer
+ * solves regenerate the vectors instead (same results, twice the operator
+ * applications).  max_bytes < 0: 40% of the free HBM at the first solve
+ * (default); 0: no store. */
+int chdwf_set_basis_store(chdwf_ctx* ctx, double max_bytes);
 /* the context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's */
 void* chdwf_get_stream(chdwf_ctx* ctx);
 /* number of CUDA kernels the library has launched in this process */
 long long chdwf_kernel_launches(void);
-int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched);
+int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched,
+                      double* bytes);
 
 /* ---- routine level (host arrays) -------------------------------------- */
 /* Phi = M R.  Replaces dslash(Phi,R,chi,am,hpin,imass), rhmc/cheisdwf.f:2634.

@@ -122,3 +122,24 @@ def test_congrad(remez):
     # FP64 then rounds; the iteration paths agree to the solver tolerance
     assert abs(itg - itr) <= 2
     assert rel(xg, xr) < 1e-6
+
+
+@pytest.mark.parametrize("iflag", [0, 1])
+def test_basis_store_and_regeneration_agree(remez, iflag):
+    """Pass 2 from the stored Lanczos basis and pass 2 by regenerating the
+    vectors (no store) see the same vectors and accumulate them in the same
+    order."""
+    L, Lt, Ls = 6, 6, 6
+    r = remez["remez2g"]
+    Phi, chi = random_fields(L, Lt, Ls, seed=27, chi_scale=0.4)
+    out = []
+    for store in (-1.0, 0.0):
+        gl = chb.Lattice(L, Lt, Ls, beta=0.475)
+        gl.set_basis_store(store)
+        dS0 = np.zeros((3, L * L * Lt), np.float32)
+        x, it, dS = gl.qmrherm(Phi, 1e-6, r["anum"], r["aden"], iflag, chi, dSdchi=dS0)
+        gl.close()
+        out.append((x, it, dS))
+    assert out[0][1] == out[1][1]
+    assert rel(out[0][0], out[1][0]) <= 1e-14
+    assert np.abs(out[0][2] - out[1][2]).max() <= 2 * np.spacing(np.float32(np.abs(out[1][2]).max()))

@@ -8,8 +8,15 @@ chi from a seeded N(0, 1/beta); the reference's default seed; the shipped
 remez2/remez4/remez2g sets.
 
 Tolerances (FP64 path):
-  H0, H1, S0, S1       relative 1e-10
-  dH                   |dH_gpu - dH_oracle| <= 1e-10 * |H0|
+  H0, S0               relative 1e-10 (before the molecular dynamics)
+  H1, S1               relative 1e-9 (after it)
+  dH                   |dH_gpu - dH_oracle| <= 1e-9 * |H0|
+The molecular dynamics carries REAL*4 momenta and forces (pp, dSdchi), so a
+rounding-level difference in a force solve can flip a REAL*4 last bit and
+move H1.  The reference shows the same: its own H1 changes by 6.5e-11 and
+2.7e-10 relative, and dH by 2.3e-6 and 9.7e-6, between 1 and 8 OpenMP
+threads on this workload (measured with the oracle), so 1e-9 is about 3x
+the reference's own reproducibility.
   accept/reject, MD step count, Metropolis draw   identical
   solver iterations    within the reference's own envelope (+-5)
   REAL*4 outputs (action, vel2, condmod, correlators) relative 1e-5 / 1e-4
@@ -98,10 +105,10 @@ def test_exact_resume(remez):
 def test_hamiltonian_and_dH(runs):
     out, _, _ = runs
     for ro, rg, _, _ in out:
-        for f in ("H0", "H1", "S0", "S1"):
+        for f, tol in (("H0", 1e-10), ("S0", 1e-10), ("H1", 1e-9), ("S1", 1e-9)):
             a, b = getattr(rg, f), getattr(ro, f)
-            assert abs(a - b) <= 1e-10 * abs(b), (f, a, b)
-        assert abs(rg.dH - ro.dH) <= 1e-10 * abs(ro.H0), (rg.dH, ro.dH)
+            assert abs(a - b) <= tol * abs(b), (f, a, b)
+        assert abs(rg.dH - ro.dH) <= 1e-9 * abs(ro.H0), (rg.dH, ro.dH)
         assert abs(rg.hg - ro.hg) <= 1e-12 * abs(ro.hg)
 
 
