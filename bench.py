@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-solve", action="store_true",
                     help="bounded work for profilers: one heatbath and one force evaluation")
+    ap.add_argument("--profile-res", type=float, default=0.0,
+                    help="stopping residual of both profiled solves (0: the reference's)")
     ap.add_argument("--basis-gb", type=float, default=-1.0,
                     help="HBM budget of the stored Lanczos basis (GB; <0 library default)")
     return ap.parse_args()
@@ -290,10 +292,12 @@ def run_profile_solve(args, local_rank):
     it = C.c_int()
     t0 = time.perf_counter()
     lib.chdwf_traj_begin(ctx)
-    rc1 = lib.chdwf_traj_heatbath(ctx, ps.ctypes.data_as(C.c_void_p), 1e-9, 0.0, 0.0, 1,
+    res_hb = args.profile_res or 1e-9
+    res_f = args.profile_res or 1e-6
+    rc1 = lib.chdwf_traj_heatbath(ctx, ps.ctypes.data_as(C.c_void_p), res_hb, 0.0, 0.0, 1,
                                   C.byref(it))
     itg, itf = C.c_int(), C.c_int()
-    rc2 = lib.chdwf_traj_force(ctx, 1e-6, 0.0, 0.0, 1, C.byref(itg), C.byref(itf))
+    rc2 = lib.chdwf_traj_force(ctx, res_f, 0.0, 0.0, 1, C.byref(itg), C.byref(itf))
     lib.chdwf_traj_sync(ctx)
     dt = time.perf_counter() - t0
     print(json.dumps({"profile_solve": f"L=Lt={L} Ls={Ls}", "rc": [rc1, rc2],
