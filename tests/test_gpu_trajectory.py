@@ -109,7 +109,10 @@ def test_hamiltonian_and_dH(runs):
             a, b = getattr(rg, f), getattr(ro, f)
             assert abs(a - b) <= tol * abs(b), (f, a, b)
         assert abs(rg.dH - ro.dH) <= 1e-9 * abs(ro.H0), (rg.dH, ro.dH)
-        assert abs(rg.hg - ro.hg) <= 1e-12 * abs(ro.hg)
+        # hg is the bosonic action of the chi the molecular dynamics ended on,
+        # so it carries the same REAL*4-momentum envelope as H1 (the oracle on
+        # 1 vs 8 threads moves H1 by up to 1e-5 absolute at H ~ 3.5e4).
+        assert abs(rg.hg - ro.hg) <= 1e-9 * abs(ro.H0), (rg.hg, ro.hg)
 
 
 def test_iterations_within_envelope(runs):
