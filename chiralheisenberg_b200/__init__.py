@@ -30,6 +30,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libchdwf.so")
 
 CHDWF_OK, CHDWF_ITER_CAP, CHDWF_NONFINITE, CHDWF_CUDA_ERROR, CHDWF_BAD_ARG = 0, 1, 2, 3, 4
+CHDWF_NOT_FOUND = 5
 
 # every symbol include/*.h declares (checked by the CPU test suite)
 EXPORTS = (
@@ -50,6 +51,9 @@ EXPORTS = (
     "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
     "chdwf_prog_correlators", "chdwf_prog_last_error",
+    "chdwf_prog_sums", "chdwf_prog_reset_sums", "chdwf_prog_averages", "chdwf_prog_take_cg_caps",
+    "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
+    "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
 )
 
 _lib = None
@@ -140,6 +144,17 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_set_basis_store.argtypes = [P, D]
     L.chdwf_prog_get_state.argtypes = [P, P, I]
     L.chdwf_prog_set_state.argtypes = [P, P, I]
+    L.chdwf_prog_sums.argtypes = [P, P]
+    L.chdwf_prog_reset_sums.argtypes = [P]
+    L.chdwf_prog_averages.argtypes = [P, P]
+    L.chdwf_prog_take_cg_caps.argtypes = [P]
+    L.chdwf_con_read.argtypes = [C.c_char_p, I, P, C.POINTER(D), PI]
+    L.chdwf_con_write.argtypes = [C.c_char_p, I, P, D]
+    L.chdwf_prog_read_con.argtypes = [P, C.c_char_p, C.POINTER(D)]
+    L.chdwf_prog_write_con.argtypes = [P, C.c_char_p]
+    L.chdwf_format_list.argtypes = [C.c_char_p, I, C.c_char_p, P]
+    L.chdwf_format_edit.argtypes = [C.c_char_p, I, C.c_char, I, I, D]
+    L.chdwf_run_dir.argtypes = [C.c_char_p, I, I, I, I]
     _lib = L
     return L
 
@@ -176,7 +191,7 @@ class SweepRecord(C.Structure):
                 ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
                 ("vel2", C.c_float), ("measured", C.c_int), ("cond", C.c_float * 3),
                 ("susc", C.c_float * 3), ("condmod", C.c_float), ("susctot", C.c_float),
-                ("ancgm", C.c_float)]
+                ("ancgm", C.c_float), ("ended", C.c_int)]
 
     def as_dict(self):
         out = {}
@@ -184,6 +199,80 @@ class SweepRecord(C.Structure):
             v = getattr(self, name)
             out[name] = list(v) if hasattr(v, "__len__") else v
         return out
+
+
+class RunSums(C.Structure):
+    """chdwf_run_sums (include/chdwf_program.h): the main program's running sums."""
+    _fields_ = [(n, C.c_float) for n in ("actiona", "vel2a", "condmoda", "susca")] + \
+        [("conda", C.c_float * 3), ("pbpa", C.c_float)] + \
+        [(n, C.c_float) for n in ("ancg", "ancgh", "ancgf", "ancgpf", "ancgma", "yav", "yyav")] + \
+        [(n, C.c_int) for n in ("naccp", "ipbp", "itot", "nsweep")] + [("gaction", C.c_float)]
+
+
+class RunAverages(C.Structure):
+    """chdwf_run_averages: the averages of 'output' (rhmc/cheisdwf.f:413-443)."""
+    _fields_ = [("iter2", C.c_int), ("naccp", C.c_int)] + \
+        [(n, C.c_float) for n in ("atraj", "yav", "yyav", "ancg", "ancgh", "ancgf", "ancgpf",
+                                  "ancgma", "condmoda", "susca")] + \
+        [("conda", C.c_float * 3), ("pbpa", C.c_float), ("vel2a", C.c_float),
+         ("actiona", C.c_float)]
+
+
+def con_read(path, kvol):
+    """'con' (sread): returns (chi[3, kvol] float64, seed, single), where
+    single tells that the file held a REAL*4 configuration."""
+    lib = load_library()
+    chi = np.empty((3, kvol), dtype=np.float64)
+    seed, single = C.c_double(), C.c_int()
+    rc = lib.chdwf_con_read(os.fsencode(path), kvol, _ptr(chi), C.byref(seed), C.byref(single))
+    if rc == CHDWF_NOT_FOUND:
+        raise FileNotFoundError(path)
+    if rc != CHDWF_OK:
+        raise ChdwfError(rc, f"not a {kvol}-site configuration: {path}")
+    return chi, seed.value, bool(single.value)
+
+
+def con_write(path, chi, seed):
+    """'con' as swrite writes it: one unformatted record of chi (REAL*8) and seed."""
+    lib = load_library()
+    chi = np.ascontiguousarray(chi, dtype=np.float64)
+    rc = lib.chdwf_con_write(os.fsencode(path), chi.size // 3, _ptr(chi), float(seed))
+    if rc != CHDWF_OK:
+        raise ChdwfError(rc, f"cannot write {path}")
+
+
+def format_list(kinds: str, values) -> str:
+    """One list-directed output record in gfortran's layout; kinds holds 'i'
+    (INTEGER), 'f' (REAL*4) or 'd' (REAL*8) per value."""
+    lib = load_library()
+    vals = np.ascontiguousarray(values, dtype=np.float64)
+    buf = C.create_string_buffer(64 * (len(kinds) + 1))
+    n = lib.chdwf_format_list(buf, len(buf), kinds.encode(), _ptr(vals))
+    if n < 0:
+        raise ValueError(kinds)
+    return buf.value.decode()
+
+
+def format_edit(kind: str, w: int, d: int, value) -> str:
+    """One explicit edit descriptor: 'I' (Iw), 'F' (Fw.d) or 'E' (Ew.d)."""
+    lib = load_library()
+    buf = C.create_string_buffer(w + 64)
+    n = lib.chdwf_format_edit(buf, len(buf), kind.encode(), w, d, float(value))
+    if n < 0:
+        raise ValueError(kind)
+    return buf.value.decode()
+
+
+def run_dir(path, ksize, ksizet, kthird, device=0):
+    """Run program dwf3d in directory path with the reference's input files
+    (midout, con, remez2, remez4, remez2g) and output streams."""
+    lib = load_library()
+    rc = lib.chdwf_run_dir(os.fsencode(path), ksize, ksizet, kthird, device)
+    if rc == CHDWF_NOT_FOUND:
+        raise FileNotFoundError(path)
+    if rc != CHDWF_OK:
+        raise (IterationCapError if rc == CHDWF_ITER_CAP else ChdwfError)(
+            rc, lib.chdwf_last_error(None).decode())
 
 
 class Program:
@@ -244,6 +333,29 @@ class Program:
         cf = np.empty((2, 2, self.Lt, 2), dtype=np.float32)
         self._check(self.lib.chdwf_prog_correlators(self.h, _ptr(cf)))
         return cf
+
+    def sums(self) -> RunSums:
+        out = RunSums()
+        self._check(self.lib.chdwf_prog_sums(self.h, C.byref(out)))
+        return out
+
+    def reset_sums(self):
+        self._check(self.lib.chdwf_prog_reset_sums(self.h))
+
+    def averages(self) -> RunAverages:
+        out = RunAverages()
+        self._check(self.lib.chdwf_prog_averages(self.h, C.byref(out)))
+        return out
+
+    def read_con(self, path) -> float:
+        """sread: chi from 'con' (or the cold default); returns the seed."""
+        seed = C.c_double()
+        self._check(self.lib.chdwf_prog_read_con(self.h, os.fsencode(path), C.byref(seed)))
+        return seed.value
+
+    def write_con(self, path):
+        """swrite with the generator's current seed."""
+        self._check(self.lib.chdwf_prog_write_con(self.h, os.fsencode(path)))
 
     def get_state(self) -> bytes:
         """Generator state + sweep counter (exact resume; see chdwf_prog_get_state)."""

@@ -9,6 +9,7 @@
 // while trajectory n runs on the GPU.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "../../include/chdwf.h"
 #include "../../include/chdwf_program.h"
+#include "fortio.h"
 #include "rng.h"
 
 namespace {
@@ -52,6 +54,8 @@ struct chdwf_prog {
     bool have_next = false;
     std::future<Draws> next;
     std::vector<float> cferm;        // cferm1(0:Lt-1,2), cferm2 as complex64 pairs
+    chdwf_run_sums sums{};           // running sums of the main program
+    int cg_caps = 0;                 // congrad iteration caps not yet reported
     std::string err;
     chdwf::Rng::State last_state{};  // generator after the last completed sweep
 
@@ -123,6 +127,7 @@ int fermion(chdwf_prog* p, float yferm, float* aviter) {
             const int rc = chdwf_traj_propagator(p->ctx, ittt, idsource, p->rescgm, p->am, p->hpin,
                                                  p->imass, walls.data(), &it);
             if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+            if (rc == CHDWF_ITER_CAP) p->cg_caps++;     // congrad's message (:1151-1153)
             iter += it;
             // walls[(w*2 + dd)*2 + f][kvol]: w=0 s=1 Dirac 1,2; w=1 s=Ls Dirac 3,4
             for (int f = 0; f < 2; f++)
@@ -271,6 +276,7 @@ double chdwf_prog_seed(chdwf_prog* p) {
 struct ProgState {
     chdwf::Rng::State rng;
     int isweep;
+    chdwf_run_sums sums;
 };
 
 int chdwf_prog_state_size(void) { return (int)sizeof(ProgState); }
@@ -280,6 +286,7 @@ int chdwf_prog_get_state(chdwf_prog* p, void* buf, int nbytes) {
     ProgState s;
     s.rng = p->last_state;
     s.isweep = p->isweep;
+    s.sums = p->sums;
     std::memcpy(buf, &s, sizeof(s));
     return CHDWF_OK;
 }
@@ -292,6 +299,7 @@ int chdwf_prog_set_state(chdwf_prog* p, const void* buf, int nbytes) {
     p->rng.set_state(s.rng);
     p->last_state = s.rng;
     p->isweep = s.isweep;
+    p->sums = s.sums;
     return CHDWF_OK;
 }
 
@@ -347,52 +355,69 @@ int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
     else
         CK(chdwf_traj_heatbath(c, d.gauss.data(), p->rescga, p->am, p->hpin, p->imass,
                                &rec->it_pf));
+    chdwf_run_sums& A = p->sums;
+    A.ancgpf = A.ancgpf + (float)rec->it_pf;                                       // :235
     if (p->staged.empty()) p->prefetch(p->isweep + 1);   // next trajectory's draws, overlapped
     if (from_stage) CK(chdwf_traj_set_momenta_dev(c, stg.pp_dev));                 // :249-257
     else CK(chdwf_traj_set_momenta(c, d.pp.data()));
     double h[5];
     CK(chdwf_traj_hamilton(c, p->rescga, p->am, p->hpin, p->imass, h, &rec->it_h0));  // :261
+    A.ancgh = A.ancgh + (float)rec->it_h0;                                          // :575
     rec->H0 = h[0];
     rec->S0 = h[3];
-    if (p->isweep == 1) rec->gaction = (float)(h[1] / (double)kvol);
+    if (p->isweep == 1) A.gaction = (float)(h[1] / (double)kvol);
     rec->action = (float)(h[3] / (double)kvol);
     rec->paction = (float)(h[2] / (double)kvol);
     int itg = 0, itf = 0;
+    auto force_sums = [&] {                                                         // :507, :515
+        A.ancg = A.ancg + (float)itg;
+        A.ancgf = A.ancgf + (float)itf;
+        rec->it_guid += itg; rec->it_force += itf; rec->nforce++;
+    };
     CK(chdwf_traj_force(c, p->rescgg, p->am, p->hpin, p->imass, &itg, &itf));       // :272
-    rec->it_guid += itg; rec->it_force += itf; rec->nforce++;
+    force_sums();
     CK(chdwf_traj_update_momenta(c, p->dt * 0.5f));                                 // :273-277
     const int nsteps = (int)d.ytest.size();
     const float proby = 1.0f / (float)p->iterl;
     for (int iter = 1; iter <= nsteps; iter++) {                                    // :281-315
         CK(chdwf_traj_update_chi(c, p->dt));
         CK(chdwf_traj_force(c, p->rescgg, p->am, p->hpin, p->imass, &itg, &itf));
-        rec->it_guid += itg; rec->it_force += itf; rec->nforce++;
+        force_sums();
         rec->nsteps = iter;
         if (d.ytest[iter - 1] < proby) {
             CK(chdwf_traj_update_momenta(c, p->dt * 0.5f));
+            rec->ended = 1;
+            A.itot = A.itot + iter;                                                 // :305
             break;
         }
         CK(chdwf_traj_update_momenta(c, p->dt));
     }
     CK(chdwf_traj_hamilton(c, p->rescga, p->am, p->hpin, p->imass, h, &rec->it_h1));  // :321
+    A.ancgh = A.ancgh + (float)rec->it_h1;
     rec->H1 = h[0]; rec->S1 = h[3]; rec->hg = h[1]; rec->hp = h[2];
     rec->dH = rec->H0 - rec->H1;
     rec->dS = rec->S0 - rec->S1;
     rec->y = (float)std::exp(rec->dH);
+    A.yav = A.yav + rec->y;                                                         // :326-327
+    A.yyav = A.yyav + rec->y * rec->y;
     rec->x = d.x;
     rec->accepted = 0;
     if (rec->x < rec->y) {                                                          // :331-344
         rec->accepted = 1;
         CK(chdwf_traj_accept(c));
+        A.naccp = A.naccp + 1;
         rec->action = (float)(h[3] / (double)kvol);
-        rec->gaction = (float)(h[1] / (double)kvol);
+        A.gaction = (float)(h[1] / (double)kvol);
         rec->paction = (float)(h[2] / (double)kvol);
     }
+    rec->gaction = A.gaction;           // kept from the last sweep that set it (:264, :342)
+    A.actiona = A.actiona + rec->action;                                            // :348
     std::vector<float> pp(3 * (size_t)kvol);
     CK(chdwf_traj_get_momenta(c, pp.data()));
     float vel2 = 0.0f;                                                              // :349-355
     for (size_t i = 0; i < pp.size(); i++) vel2 = vel2 + pp[i] * pp[i];
     rec->vel2 = vel2 / (float)kvol;
+    A.vel2a = A.vel2a + rec->vel2;                                                  // :356
     if (d.measured) {                                                               // :359-399
         rec->measured = 1;
         CK(chdwf_traj_begin(c));                                                    // chit = chi
@@ -412,12 +437,100 @@ int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
         }
         rec->condmod = std::sqrt(condmod);
         rec->susctot = susctot;
+        A.condmoda = A.condmoda + rec->condmod;                                     // :382-386
+        A.susca = A.susca + susctot;
+        for (int a = 0; a < 3; a++) A.conda[a] = A.conda[a] + rec->cond[a];
         CK(fermion(p, d.yferm, &rec->ancgm));
+        A.pbpa = A.pbpa + 0.0f;             // pbp: 'measure' is not called (:392-394)
+        A.ancgma = A.ancgma + rec->ancgm;                                           // :395-396
+        A.ipbp = A.ipbp + 1;
     }
+    A.nsweep = A.nsweep + 1;
 #undef CK
     return CHDWF_OK;
 }
 
 const char* chdwf_prog_last_error(chdwf_prog* p) { return p ? p->err.c_str() : ""; }
+
+int chdwf_prog_sums(chdwf_prog* p, chdwf_run_sums* out) {
+    if (!p || !out) return CHDWF_BAD_ARG;
+    *out = p->sums;
+    return CHDWF_OK;
+}
+
+int chdwf_prog_reset_sums(chdwf_prog* p) {
+    if (!p) return CHDWF_BAD_ARG;
+    const float g = p->sums.gaction;
+    p->sums = chdwf_run_sums{};
+    p->sums.gaction = g;
+    return CHDWF_OK;
+}
+
+// Averages printed at the end of a run (rhmc/cheisdwf.f:413-431), in the
+// reference's REAL*4 arithmetic and evaluation order.
+int chdwf_prog_averages(chdwf_prog* p, chdwf_run_averages* out) {
+    if (!p || !out) return CHDWF_BAD_ARG;
+    const chdwf_run_sums& A = p->sums;
+    const int iter2 = A.nsweep;
+    if (iter2 < 1) return CHDWF_BAD_ARG;
+    chdwf_run_averages v{};
+    v.iter2 = iter2;
+    v.naccp = A.naccp;
+    const float n = (float)iter2, np = (float)A.ipbp, nt = (float)A.itot;
+    v.actiona = A.actiona / n;
+    v.vel2a = A.vel2a / n;
+    v.condmoda = A.condmoda / np;
+    v.susca = A.susca / np;
+    for (int a = 0; a < 3; a++) v.conda[a] = A.conda[a] / np;
+    v.pbpa = A.pbpa / np;
+    v.ancg = A.ancg / nt;
+    v.ancgf = A.ancgf / nt;
+    v.ancgh = A.ancgh / (float)(2 * iter2);
+    v.ancgpf = A.ancgpf / n;
+    v.ancgma = A.ancgma / np;
+    v.yav = A.yav / n;
+    const float yy = A.yyav / n - v.yav * v.yav;
+    v.yyav = std::sqrt(yy / (float)(iter2 - 1));
+    v.atraj = p->dt * (float)A.itot / n;
+    *out = v;
+    return CHDWF_OK;
+}
+
+// sread (rhmc/cheisdwf.f:1455-1478)
+int chdwf_prog_read_con(chdwf_prog* p, const char* path, double* seed) {
+    if (!p || !path || !seed) return CHDWF_BAD_ARG;
+    std::vector<double> chi(3 * (size_t)p->kvol);
+    const int rc = chdwf::fio::con_read(path, p->kvol, chi.data(), seed, nullptr);
+    if (rc == 2) {
+        p->err = std::string("not a configuration of this lattice: ") + path;
+        return CHDWF_BAD_ARG;
+    }
+    if (rc == 1) {                       // no 'con': chi = 0.1/beta, default seed (:1468-1469)
+        std::fill(chi.begin(), chi.end(), (double)(0.1f / p->beta));
+        *seed = (double)693764523745.0f;
+    }
+    p->discard_pending();
+    return chdwf_traj_set_chi(p->ctx, chi.data());
+}
+
+// rranget + swrite (rhmc/cheisdwf.f:402-404, :1480-1489)
+int chdwf_prog_write_con(chdwf_prog* p, const char* path) {
+    if (!p || !path) return CHDWF_BAD_ARG;
+    std::vector<double> chi(3 * (size_t)p->kvol);
+    const int rc = chdwf_traj_get_chi(p->ctx, chi.data(), 0);
+    if (rc != CHDWF_OK) return rc;
+    if (chdwf::fio::con_write(path, p->kvol, chi.data(), chdwf_prog_seed(p)) != 0) {
+        p->err = std::string("cannot write ") + path;
+        return CHDWF_BAD_ARG;
+    }
+    return CHDWF_OK;
+}
+
+int chdwf_prog_take_cg_caps(chdwf_prog* p) {
+    if (!p) return 0;
+    const int n = p->cg_caps;
+    p->cg_caps = 0;
+    return n;
+}
 
 }  // extern "C"

@@ -26,7 +26,8 @@
  * Every function returns a status: CHDWF_OK, CHDWF_ITER_CAP (solver hit its
  * iteration cap: the reference's qmrherm stops silently at 5000, congrad
  * prints "# iterations of congrad exceeds niterc"), CHDWF_NONFINITE,
- * CHDWF_CUDA_ERROR, CHDWF_BAD_ARG.  chdwf_last_error() describes the last
+ * CHDWF_CUDA_ERROR, CHDWF_BAD_ARG, CHDWF_NOT_FOUND (a file the host driver
+ * reads is missing).  chdwf_last_error() describes the last
  * failure of a context.  A context is single-threaded: one CUDA stream,
  * calls must not overlap.
  */
@@ -44,6 +45,7 @@ extern "C" {
 #define CHDWF_NONFINITE 2
 #define CHDWF_CUDA_ERROR 3
 #define CHDWF_BAD_ARG 4
+#define CHDWF_NOT_FOUND 5
 
 typedef struct chdwf_ctx chdwf_ctx;
 

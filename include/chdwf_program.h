@@ -32,7 +32,28 @@ typedef struct {
     int measured;
     float cond[3], susc[3], condmod, susctot;
     float ancgm;                     /* fermion(): average CG iterations */
+    int ended;                       /* 1: the trajectory ended by its end-of-trajectory draw,
+                                        0: it ran the full itermax = 1000 steps */
 } chdwf_sweep_record;
+
+/* Running sums the main program keeps over a run (rhmc/cheisdwf.f:185-203,
+ * updated at :235, :264, :305, :326-348, :356, :382-396 and in force and
+ * hamilton through COMMON /param/, :507, :515, :575), in REAL*4 as there.
+ * gaction persists from the last sweep that set it (sweep 1 or an
+ * acceptance), as the reference's variable does. */
+typedef struct {
+    float actiona, vel2a, condmoda, susca, conda[3], pbpa;
+    float ancg, ancgh, ancgf, ancgpf, ancgma, yav, yyav;
+    int naccp, ipbp, itot, nsweep;
+    float gaction;
+} chdwf_run_sums;
+
+/* The averages written at the end of a run (rhmc/cheisdwf.f:413-443). */
+typedef struct {
+    int iter2, naccp;
+    float atraj, yav, yyav, ancg, ancgh, ancgf, ancgpf, ancgma;
+    float condmoda, susca, conda[3], pbpa, vel2a, actiona;
+} chdwf_run_averages;
 
 /* Create a driver for ksize^2 x ksizet x kthird with the midout parameters
  * (rhmc/cheisdwf.f:117: dt beta am3 am hpin imass iterl).  chi starts at
@@ -73,6 +94,49 @@ int chdwf_prog_stage(chdwf_prog* p, int ntraj);
  * fort.5001/5002 and 5011/5012, :1036-1047) */
 int chdwf_prog_correlators(chdwf_prog* p, float* cferm);
 const char* chdwf_prog_last_error(chdwf_prog* p);
+
+/* The running sums since creation (or the last reset); they are part of
+ * the state blob, so an exact resume continues them. */
+int chdwf_prog_sums(chdwf_prog* p, chdwf_run_sums* out);
+int chdwf_prog_reset_sums(chdwf_prog* p);
+/* Averages over the sweeps summed so far (rhmc/cheisdwf.f:413-431). */
+int chdwf_prog_averages(chdwf_prog* p, chdwf_run_averages* out);
+/* Number of congrad iteration caps met since the last call (the reference
+ * writes one line for each to units 6 and 7, :1151-1153). */
+int chdwf_prog_take_cg_caps(chdwf_prog* p);
+
+/* ---- on-disk formats of the reference program ---------------------------
+ * 'con' is one Fortran unformatted sequential record (4-byte length markers)
+ * holding chi(kvol,3) and seed, written by swrite (rhmc/cheisdwf.f:1480-1489)
+ * and read by sread (:1455-1478).  chdwf_con_read accepts a REAL*8 chi and
+ * the REAL*4 chi of the older configurations (the conversion
+ * rhmc/sp_to_dp.f makes); *single tells which it found.  Returns CHDWF_OK,
+ * CHDWF_NOT_FOUND when the file is missing, CHDWF_BAD_ARG when its record
+ * does not hold a kvol-site configuration. */
+int chdwf_con_read(const char* path, int kvol, double* chi, double* seed, int* single);
+int chdwf_con_write(const char* path, int kvol, const double* chi, double seed);
+/* sread: chi and seed from 'path', or chi = 0.1/beta and the default seed
+ * when the file is missing (:1462-1470).  Sets the driver's chi and returns
+ * the seed (not yet applied: chdwf_prog_startup does that, as :127-130). */
+int chdwf_prog_read_con(chdwf_prog* p, const char* path, double* seed);
+/* swrite with the seed rranget returns after the last completed sweep. */
+int chdwf_prog_write_con(chdwf_prog* p, const char* path);
+
+/* One record of list-directed output in gfortran's layout: kinds[i] is 'i'
+ * (INTEGER), 'f' (REAL*4) or 'd' (REAL*8) for values[i]; the line (with its
+ * newline) goes to out.  Returns its length, or -1 if cap is too small. */
+int chdwf_format_list(char* out, int cap, const char* kinds, const double* values);
+/* One explicit edit descriptor: kind 'I' (Iw), 'F' (Fw.d) or 'E' (Ew.d). */
+int chdwf_format_edit(char* out, int cap, char kind, int w, int d, double value);
+
+/* Runs program dwf3d in directory dir as the reference does in its working
+ * directory (rhmc/cheisdwf.f:1-466): reads 'midout' (dt beta am3 am hpin
+ * imass iterl iter2), 'con' (sread) and 'remez2', 'remez4', 'remez2g'
+ * (ndiag = 25, ndiagg = 12 poles); appends to 'control', fort.11-14 and
+ * fort.5001/5011/5002/5012; writes 'output' and checkpoints 'con' every
+ * iprint = 5 sweeps and at the end.  ksize, ksizet and kthird are the
+ * reference's compile-time lattice parameters. */
+int chdwf_run_dir(const char* dir, int ksize, int ksizet, int kthird, int device);
 
 #ifdef __cplusplus
 }

@@ -859,7 +859,7 @@ void orc_sweep(orc_state* st_, orc_traj_rec* rec) {
     orc_hamilton(lat, S->Phi, S->rescga, S->am, S->hpin, S->imass, S->chit, S->pp, &S->r2, h,
                  S->X1, &rec->it_h0);
     rec->H0 = h[0]; rec->S0 = h[3];
-    if (S->isweep == 1) rec->gaction = (float)(h[1] / (double)kvol);
+    if (S->isweep == 1) S->gaction = (float)(h[1] / (double)kvol);
     rec->action = (float)(h[3] / (double)kvol);
     rec->paction = (float)(h[2] / (double)kvol);
     /* half step for p (:272-277) */
@@ -900,9 +900,10 @@ void orc_sweep(orc_state* st_, orc_traj_rec* rec) {
         rec->accepted = 1;
         memcpy(S->chi, S->chit, sizeof(double) * 3 * kvol);
         rec->action = (float)(h[3] / (double)kvol);
-        rec->gaction = (float)(h[1] / (double)kvol);
+        S->gaction = (float)(h[1] / (double)kvol);
         rec->paction = (float)(h[2] / (double)kvol);
     }
+    rec->gaction = S->gaction;
     float vel2 = 0.0f;                                                           /* :349-355 */
     for (int64_t i = 0; i < 3 * kvol; i++) vel2 = vel2 + S->pp[i] * S->pp[i];
     rec->vel2 = vel2 / (float)kvol;

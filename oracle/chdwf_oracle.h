@@ -137,6 +137,7 @@ typedef struct {
     float* ps;         /* /dum1/ ps(kvol,2) */
     float* cferm;      /* 4*Lt*2 floats: cferm1, cferm2 (last measurement) */
     int isweep;
+    float gaction;     /* main-program variable, kept across sweeps (:264, :342) */
 } orc_state;
 
 orc_state* orc_state_new(int L, int Lt, int Ls, float beta, float am3,

@@ -62,7 +62,8 @@ class State(C.Structure):
                 ("pp", C.POINTER(C.c_float)), ("dSdchi", C.POINTER(C.c_float)),
                 ("Phi", C.POINTER(C.c_double)), ("X1", C.POINTER(C.c_double)),
                 ("R", C.POINTER(C.c_double)), ("ps", C.POINTER(C.c_float)),
-                ("cferm", C.POINTER(C.c_float)), ("isweep", C.c_int)]
+                ("cferm", C.POINTER(C.c_float)), ("isweep", C.c_int),
+                ("gaction", C.c_float)]
 
 
 def lib():

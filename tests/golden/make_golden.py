@@ -9,6 +9,15 @@ Writes:
                               a0, (a_k, sigma_k)*n, b0, (b_k, sigma_k)*n);
   con_12x12x12.bin         -- rhmc/_con: one Fortran unformatted record,
                               chi(1728,3) real*8 + seed real*8;
+  con_sp_12x12x12.bin      -- rhmc/Ls_8/b_0.45/_con: a configuration of the
+                              older single-precision format (chi REAL*4,
+                              seed REAL*8), the input of rhmc/sp_to_dp.f;
+  list_directed.json       -- the first 60 records of fort.11-14 (kept as
+                              action, conds, suscs, condmod) of every
+                              rhmc/Ls_8 run: list-directed output written by
+                              the reference's gfortran build;
+  out_1_b0.45.txt          -- rhmc/Ls_8/b_0.45/out_1, the 'output' file of
+                              two runs (explicit formats 9001-9024);
   seed_pins.json           -- (seed read from 'con', seed after start-up)
                               pairs printed by the reference into
                               rhmc/Ls_8/<run>/out_1.  Between the two prints
@@ -32,6 +41,24 @@ def main(ref_root: str) -> None:
     for name in ("remez2", "remez4", "remez2g"):
         shutil.copyfile(os.path.join(rhmc, name), os.path.join(HERE, name))
     shutil.copyfile(os.path.join(rhmc, "_con"), os.path.join(HERE, "con_12x12x12.bin"))
+    shutil.copyfile(os.path.join(rhmc, "Ls_8", "b_0.45", "_con"),
+                    os.path.join(HERE, "con_sp_12x12x12.bin"))
+    shutil.copyfile(os.path.join(rhmc, "Ls_8", "b_0.45", "out_1"),
+                    os.path.join(HERE, "out_1_b0.45.txt"))
+    # write(11,*) isweep,gaction,paction; write(12,*) cond; write(13,*) susc;
+    # write(14,*) condmod,susctot (cheisdwf.f:347, :387-389)
+    kinds = {"action": "iff", "conds": "fff", "suscs": "fff", "condmod": "ff"}
+    ld = []
+    for run in sorted(os.listdir(os.path.join(rhmc, "Ls_8"))):
+        for name, k in kinds.items():
+            fn = os.path.join(rhmc, "Ls_8", run, name)
+            if os.path.exists(fn):
+                with open(fn) as f:
+                    lines = [f.readline() for _ in range(60)]
+                ld.append({"source": f"rhmc/Ls_8/{run}/{name}", "kinds": k,
+                           "lines": [x for x in lines if x]})
+    with open(os.path.join(HERE, "list_directed.json"), "w") as f:
+        json.dump(ld, f, indent=0)
     pins = []
     runs_dir = os.path.join(rhmc, "Ls_8")
     for run in sorted(os.listdir(runs_dir)):

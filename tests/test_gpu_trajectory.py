@@ -129,7 +129,7 @@ def test_iterations_within_envelope(runs):
 def test_single_precision_outputs(runs):
     out, (chi_o, chi_g), _ = runs
     for ro, rg, cf_o, cf_g in out:
-        for f in ("action", "paction", "vel2"):
+        for f in ("action", "gaction", "paction", "vel2"):
             a, b = getattr(rg, f), getattr(ro, f)
             assert abs(a - b) <= 1e-5 * abs(b), (f, a, b)
         if ro.measured:
