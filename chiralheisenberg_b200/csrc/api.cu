@@ -132,7 +132,7 @@ int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* l
 int chdwf_create(chdwf_ctx** out, int ksize, int ksizet, int kthird, int device) {
     if (!out) return CHDWF_BAD_ARG;
     *out = nullptr;
-    if (ksize < 2 || ksizet < 2 || kthird < 2) return CHDWF_BAD_ARG;
+    if (!geom_ok(ksize, ksizet, kthird)) return CHDWF_BAD_ARG;
     cudaError_t e = cudaSetDevice(device);
     if (e) { g_create_err = cudaGetErrorString(e); return CHDWF_CUDA_ERROR; }
     Ctx* c = new Ctx();

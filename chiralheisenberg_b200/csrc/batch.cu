@@ -235,7 +235,7 @@ extern "C" int chdwf_congrad_batch(chdwf_ctx* ctx, const chdwf_cg_system* in, in
     int64_t elems = 0, chis = 0;
     for (int i = 0; i < nsys; i++) {
         const chdwf_cg_system& s = in[i];
-        if (s.ksize < 2 || s.ksizet < 2 || s.kthird < 2 || !s.Phi || !s.x || !s.chi ||
+        if (!geom_ok(s.ksize, s.ksizet, s.kthird) || !s.Phi || !s.x || !s.chi ||
             (s.imass != 1 && s.imass != 3))
             return CHDWF_BAD_ARG;
         BSys& b = sys[i];

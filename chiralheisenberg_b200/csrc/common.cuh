@@ -24,6 +24,14 @@ struct Geom {
     int64_t kferm;    // 8*npts complex numbers
 };
 
+// Lattices are limited to 2^31 - 1 points (kthird*ksize^2*ksizet), far
+// beyond one GPU's memory; point indices then fit 32-bit arithmetic.
+constexpr int64_t kMaxPoints = 2147483647LL;
+
+inline bool geom_ok(int L, int Lt, int Ls) {
+    return L >= 2 && Lt >= 2 && Ls >= 2 && (int64_t)L * L * Lt * Ls <= kMaxPoints;
+}
+
 inline Geom make_geom(int L, int Lt, int Ls) {
     Geom g;
     g.L = L; g.Lt = Lt; g.Ls = Ls;

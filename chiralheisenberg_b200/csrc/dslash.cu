@@ -12,30 +12,29 @@ struct LdF64 {
     __device__ __forceinline__ double2 operator()(int64_t j) const { return __ldg(p + j); }
 };
 
+// Flavour-split: two threads per point (split_point / split_flavour).
 template <bool DAG, int IMASS>
-__global__ void __launch_bounds__(kThreads) k_dslash64(double2* __restrict__ out,
-                                                      const double2* __restrict__ in,
-                                                      const float* __restrict__ chif, Geom g,
-                                                      double diag, double hpin, int apbc) {
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kSplitThreads, kSplitMinBlocks)
+    k_dslash64(double2* __restrict__ out, const double2* __restrict__ in,
+               const float* __restrict__ chif, Geom g, double diag, double hpin, int apbc) {
+    const int64_t p = split_point();
+    const int f = split_flavour();
     if (p >= g.npts) return;
     const PointIdx q = point_of(g, p);
-    double2 acc[2][4];
-    dwf_apply_point<DAG, IMASS>(acc, LdF64{in}, g, q, chif, diag, hpin, apbc != 0);
+    double2 acc[4];
+    dwf_apply_flavour<DAG, IMASS>(acc, LdF64{in}, g, q, f, chif, diag, hpin, apbc != 0);
 #pragma unroll
-    for (int f = 0; f < 2; f++)
-#pragma unroll
-        for (int d = 0; d < 4; d++) out[p + g.cs * (d + 4 * f)] = acc[f][d];
+    for (int d = 0; d < 4; d++) out[p + g.cs * (d + 4 * f)] = acc[d];
 }
 
 static inline float diag_of(float am3) { return 2.0f * ((3.0f - am3) + 1.0f); }  // :2652
 
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
-    const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+    const unsigned nb = split_blocks(g.npts);
     const double diag = (double)diag_of(am3), hp = (double)hpin;
     const int apbc = ibound == -1;
-#define LAUNCH(D, I) k_dslash64<D, I><<<(unsigned)nb, kThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc)
+#define LAUNCH(D, I) k_dslash64<D, I><<<nb, kSplitThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc)
     if (!dag) {
         if (imass == 1) LAUNCH(false, 1); else if (imass == 3) LAUNCH(false, 3); else LAUNCH(false, 0);
     } else {
@@ -56,6 +55,8 @@ struct LdF16 {
     __device__ __forceinline__ float2 operator()(int64_t j) const { return __half22float2(__ldg(p + j)); }
 };
 
+// One thread per point and both flavours: with FP32 arithmetic the registers
+// already allow full occupancy, and this shape is the faster one there.
 template <bool DAG, int IMASS, int HALF>
 __global__ void __launch_bounds__(kThreads) k_dslash_lp(void* __restrict__ out,
                                                        const void* __restrict__ in,

@@ -46,17 +46,21 @@ struct PointIdx {
     int64_t p;   // s + Ls*site
 };
 
+// Coordinates of point p (p < 2^31: see kMaxPoints), in 32-bit arithmetic.
 __device__ __forceinline__ PointIdx point_of(const Geom& g, int64_t p) {
     PointIdx q;
     q.p = p;
-    const int site = (int)(p / g.Ls);
-    q.s = (int)(p - (int64_t)site * g.Ls);
-    q.site = site;
-    const int LL = g.L * g.L;
-    q.it = site / LL;
-    const int rem = site - q.it * LL;
-    q.iy = rem / g.L;
-    q.ix = rem - q.iy * g.L;
+    const unsigned up = (unsigned)p, Ls = (unsigned)g.Ls, L = (unsigned)g.L;
+    const unsigned site = up / Ls;
+    q.s = (int)(up - site * Ls);
+    q.site = (int)site;
+    const unsigned LL = L * L;
+    const unsigned it = site / LL;
+    const unsigned rem = site - it * LL;
+    const unsigned iy = rem / L;
+    q.it = (int)it;
+    q.iy = (int)iy;
+    q.ix = (int)(rem - iy * L);
     return q;
 }
 
@@ -67,74 +71,113 @@ __device__ __forceinline__ void load4(T* r, const Ld& ld, const Geom& g, int64_t
     for (int d = 0; d < 4; d++) r[d] = ld(n + g.cs * (d + 4 * f));
 }
 
+// Wall coupling of one flavour at a wall point (s = Ls for SIDE 0, s = 1 for
+// SIDE 1): Dirac pair D0, D0+1 of flavour f takes the other wall's components
+// of both flavours.  Per element the operation sequence is that of the
+// reference's wall sweeps.
+template <bool DAG, int IMASS, int D0, int SIDE, class T, class Ld>
+__device__ __forceinline__ void wall_terms(T acc[4], const Ld& ld, int64_t cs, int64_t other,
+                                           int f, float c1f, float c2f, float c3f, bool pin,
+                                           typename real_of<T>::type hpin) {
+    typedef typename real_of<T>::type R;
+#pragma unroll
+    for (int d = D0; d < D0 + 2; d++) {
+        const T r1 = ld(other + cs * d), r2 = ld(other + cs * (d + 4));
+        if (IMASS == 1) {
+            // spm = cmplx(chi3, 0) (:2912-2946 / :3345-3379), pinning
+            // (:2948-2959 / :3381-3392), spm = cmplx(chi1, -chi2)
+            // (:2962-2995 / :3395-3428)
+            const T spm = zmake<T>((R)c3f, (R)0);
+            const T sp = zmake<T>((R)c1f, (R)(-c2f));
+            if (f == 0) {
+                acc[d] = zadd(acc[d], zmul(spm, r1));
+                if (pin) acc[d] = zadd(acc[d], zscal(hpin, r1));
+                acc[d] = zadd(acc[d], zmul(sp, r2));
+            } else {
+                acc[d] = zsub(acc[d], zmul(spm, r2));
+                if (pin) acc[d] = zsub(acc[d], zscal(hpin, r2));
+                acc[d] = zadd(acc[d], zmul(zconj(sp), r1));
+            }
+        } else if (IMASS == 3) {
+            // M: spm = cmplx(0, chi3) (:2996-3030); M^dagger cmplx(0,-chi3)
+            // (:3429-3463).  Sign of the flavour-1 term: M: -,+ at s=Ls and
+            // +,- at s=1; M^dagger: +,- at s=Ls and -,+ at s=1.
+            const T spm = zmake<T>((R)0, (R)(DAG ? -c3f : c3f));
+            constexpr bool minus_first = (!DAG && SIDE == 0) || (DAG && SIDE == 1);
+            // M: spm = cmplx(chi2, chi1) (:3032-3065); M^dagger
+            // cmplx(-chi2,-chi1) (:3465-3497)
+            const T sp = DAG ? zmake<T>((R)(-c2f), (R)(-c1f)) : zmake<T>((R)c2f, (R)c1f);
+            if (f == 0) {
+                const T t1 = zmul(spm, r1), u1 = zmul(sp, r2);
+                acc[d] = minus_first ? zsub(acc[d], t1) : zadd(acc[d], t1);
+                acc[d] = minus_first ? zsub(acc[d], u1) : zadd(acc[d], u1);
+            } else {
+                const T t2 = zmul(spm, r2), u2 = zmul(zconj(sp), r1);
+                acc[d] = minus_first ? zadd(acc[d], t2) : zsub(acc[d], t2);
+                acc[d] = minus_first ? zadd(acc[d], u2) : zsub(acc[d], u2);
+            }
+        }
+    }
+}
+
+// The four Dirac components of flavour f at one output point.  The flavours
+// couple only through the wall terms, which read both flavours' inputs on
+// the other wall, so two threads can share a point (one per flavour) and
+// each needs half the accumulator registers.
+//
 // chi is passed pre-rounded to REAL*4: the reference builds the wall
 // coupling with cmplx(chi, ...) without a KIND, i.e. in default (single)
 // precision (cheisdwf.f:2914, :2962, :2998, :3034).  chif holds (chi1, chi2,
 // chi3) as three planes of kvol floats.
 template <bool DAG, int IMASS, class T, class Ld>
-__device__ __forceinline__ void dwf_apply_point(T acc[2][4], const Ld& ld, const Geom& g,
-                                                const PointIdx& q, const float* __restrict__ chif,
-                                                typename real_of<T>::type diag,
-                                                typename real_of<T>::type hpin, bool apbc) {
+__device__ __forceinline__ void dwf_apply_flavour(T acc[4], const Ld& ld, const Geom& g,
+                                                  const PointIdx& q, int f,
+                                                  const float* __restrict__ chif,
+                                                  typename real_of<T>::type diag,
+                                                  typename real_of<T>::type hpin, bool apbc) {
     typedef typename real_of<T>::type R;
     constexpr int SF = DAG ? -1 : 1;               // pattern sign of the forward hop
     const int L = g.L, Lt = g.Lt, Ls = g.Ls;
-    const int64_t LsI = Ls;
+    const int64_t LsI = Ls, cs = g.cs, fo = g.cs * (4 * f);
     // diagonal term (:2651-2667)
 #pragma unroll
-    for (int f = 0; f < 2; f++)
-#pragma unroll
-        for (int d = 0; d < 4; d++) acc[f][d] = zscal(diag, ld(q.p + g.cs * (d + 4 * f)));
+    for (int d = 0; d < 4; d++) acc[d] = zscal(diag, ld(q.p + fo + cs * d));
     // neighbour sites
     const int xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
     const int yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
     const int tp = q.it + 1 == Lt ? 0 : q.it + 1, tm = q.it == 0 ? Lt - 1 : q.it - 1;
+    const int64_t sb = q.s + fo;
     const int64_t rowb = (int64_t)L * (q.iy + (int64_t)L * q.it);
-    const int64_t n_xp = q.s + LsI * (xp + rowb), n_xm = q.s + LsI * (xm + rowb);
+    const int64_t n_xp = sb + LsI * (xp + rowb), n_xm = sb + LsI * (xm + rowb);
     const int64_t colb = q.ix + (int64_t)L * L * q.it;
-    const int64_t n_yp = q.s + LsI * (colb + (int64_t)L * yp), n_ym = q.s + LsI * (colb + (int64_t)L * ym);
+    const int64_t n_yp = sb + LsI * (colb + (int64_t)L * yp), n_ym = sb + LsI * (colb + (int64_t)L * ym);
     const int64_t plb = q.ix + (int64_t)L * q.iy;
-    const int64_t n_tp = q.s + LsI * (plb + (int64_t)L * L * tp), n_tm = q.s + LsI * (plb + (int64_t)L * L * tm);
-#pragma unroll
-    for (int f = 0; f < 2; f++) {
-        T r[4];
-        load4(r, ld, g, n_xp, f); hop<0, SF, false>(acc[f], r);
-        load4(r, ld, g, n_xm, f); hop<0, -SF, false>(acc[f], r);
-        load4(r, ld, g, n_yp, f); hop<1, SF, false>(acc[f], r);
-        load4(r, ld, g, n_ym, f); hop<1, -SF, false>(acc[f], r);
-        load4(r, ld, g, n_tp, f); hop<2, SF, false>(acc[f], r);
-        load4(r, ld, g, n_tm, f); hop<2, -SF, false>(acc[f], r);
-    }
+    const int64_t n_tp = sb + LsI * (plb + (int64_t)L * L * tp), n_tm = sb + LsI * (plb + (int64_t)L * L * tm);
+    T r[4];
+    load4(r, ld, g, n_xp, 0); hop<0, SF, false>(acc, r);
+    load4(r, ld, g, n_xm, 0); hop<0, -SF, false>(acc, r);
+    load4(r, ld, g, n_yp, 0); hop<1, SF, false>(acc, r);
+    load4(r, ld, g, n_ym, 0); hop<1, -SF, false>(acc, r);
+    load4(r, ld, g, n_tp, 0); hop<2, SF, false>(acc, r);
+    load4(r, ld, g, n_tm, 0); hop<2, -SF, false>(acc, r);
     // kappa = 1/2 (:2815-2829)
 #pragma unroll
-    for (int f = 0; f < 2; f++)
-#pragma unroll
-        for (int d = 0; d < 4; d++) acc[f][d] = zscal((R)0.5, acc[f][d]);
+    for (int d = 0; d < 4; d++) acc[d] = zscal((R)0.5, acc[d]);
     // antiperiodic boundary in t (:2831-2876): reverse the wrapped hop
     if (apbc) {
-        if (q.it == Lt - 1) {
-#pragma unroll
-            for (int f = 0; f < 2; f++) { T r[4]; load4(r, ld, g, n_tp, f); hop<2, SF, true>(acc[f], r); }
-        }
-        if (q.it == 0) {
-#pragma unroll
-            for (int f = 0; f < 2; f++) { T r[4]; load4(r, ld, g, n_tm, f); hop<2, -SF, true>(acc[f], r); }
-        }
+        if (q.it == Lt - 1) { load4(r, ld, g, n_tp, 0); hop<2, SF, true>(acc, r); }
+        if (q.it == 0) { load4(r, ld, g, n_tm, 0); hop<2, -SF, true>(acc, r); }
     }
     // s hops with chiral projection (:2879-2908; M^dagger :3313-3342)
     constexpr int UP = DAG ? 0 : 2;    // Dirac pair fed from s+1
     constexpr int DN = DAG ? 2 : 0;    // Dirac pair fed from s-1
     if (q.s < Ls - 1) {
 #pragma unroll
-        for (int f = 0; f < 2; f++)
-#pragma unroll
-            for (int d = UP; d < UP + 2; d++) acc[f][d] = zsub(acc[f][d], ld(q.p + 1 + g.cs * (d + 4 * f)));
+        for (int d = UP; d < UP + 2; d++) acc[d] = zsub(acc[d], ld(q.p + 1 + fo + cs * d));
     }
     if (q.s > 0) {
 #pragma unroll
-        for (int f = 0; f < 2; f++)
-#pragma unroll
-            for (int d = DN; d < DN + 2; d++) acc[f][d] = zsub(acc[f][d], ld(q.p - 1 + g.cs * (d + 4 * f)));
+        for (int d = DN; d < DN + 2; d++) acc[d] = zsub(acc[d], ld(q.p - 1 + fo + cs * d));
     }
     // wall coupling: pair WA at s=Ls reads s=1, pair WB at s=1 reads s=Ls
     constexpr int WA = DAG ? 0 : 2;
@@ -143,47 +186,35 @@ __device__ __forceinline__ void dwf_apply_point(T acc[2][4], const Ld& ld, const
     if (!(atL || at0)) return;
     const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
                 c3f = __ldg(chif + 2 * g.kvol + q.site);
-    const int64_t other = atL ? (int64_t)LsI * q.site : (int64_t)LsI * q.site + Ls - 1;
+    const int64_t other = atL ? LsI * q.site : LsI * q.site + Ls - 1;
     const bool pin = (q.site == 0);
-#pragma unroll
-    for (int side = 0; side < 2; side++) {
-        const bool active = side == 0 ? atL : at0;
-        if (!active) continue;
-        const int d0 = side == 0 ? WA : WB;
-        // Sign of the terms: M/imass=1 adds on both walls; see the oracle.
-#pragma unroll
-        for (int d = d0; d < d0 + 2; d++) {
-            const T r1 = ld(other + g.cs * (d + 0)), r2 = ld(other + g.cs * (d + 4));
-            if (IMASS == 1) {
-                // spm = cmplx(chi3, 0) (:2912-2946 / :3345-3379)
-                const T spm = zmake<T>((R)c3f, (R)0);
-                acc[0][d] = zadd(acc[0][d], zmul(spm, r1));
-                acc[1][d] = zsub(acc[1][d], zmul(spm, r2));
-                if (pin) {  // (:2948-2959 / :3381-3392)
-                    acc[0][d] = zadd(acc[0][d], zscal(hpin, r1));
-                    acc[1][d] = zsub(acc[1][d], zscal(hpin, r2));
-                }
-                // spm = cmplx(chi1, -chi2) (:2962-2995 / :3395-3428)
-                const T sp = zmake<T>((R)c1f, (R)(-c2f));
-                acc[0][d] = zadd(acc[0][d], zmul(sp, r2));
-                acc[1][d] = zadd(acc[1][d], zmul(zconj(sp), r1));
-            } else if (IMASS == 3) {
-                // M: spm = cmplx(0, chi3) (:2996-3030); M^dagger cmplx(0,-chi3) (:3429-3463)
-                const T spm = zmake<T>((R)0, (R)(DAG ? -c3f : c3f));
-                const T t1 = zmul(spm, r1), t2 = zmul(spm, r2);
-                // sign of the flavour-1 term: M: -,+ at s=Ls / +,- at s=1;
-                // M^dagger: +,- at s=Ls / -,+ at s=1
-                const bool minus_first = (!DAG && side == 0) || (DAG && side == 1);
-                if (minus_first) { acc[0][d] = zsub(acc[0][d], t1); acc[1][d] = zadd(acc[1][d], t2); }
-                else             { acc[0][d] = zadd(acc[0][d], t1); acc[1][d] = zsub(acc[1][d], t2); }
-                // M: spm = cmplx(chi2, chi1) (:3032-3065); M^dagger cmplx(-chi2,-chi1) (:3465-3497)
-                const T sp = DAG ? zmake<T>((R)(-c2f), (R)(-c1f)) : zmake<T>((R)c2f, (R)c1f);
-                const T u1 = zmul(sp, r2), u2 = zmul(zconj(sp), r1);
-                if (minus_first) { acc[0][d] = zsub(acc[0][d], u1); acc[1][d] = zadd(acc[1][d], u2); }
-                else             { acc[0][d] = zadd(acc[0][d], u1); acc[1][d] = zsub(acc[1][d], u2); }
-            }
-        }
-    }
+    if (atL) wall_terms<DAG, IMASS, WA, 0>(acc, ld, cs, other, f, c1f, c2f, c3f, pin, hpin);
+    if (at0) wall_terms<DAG, IMASS, WB, 1>(acc, ld, cs, other, f, c1f, c2f, c3f, pin, hpin);
+}
+
+// All eight components of one output point (one thread per point).
+template <bool DAG, int IMASS, class T, class Ld>
+__device__ __forceinline__ void dwf_apply_point(T acc[2][4], const Ld& ld, const Geom& g,
+                                                const PointIdx& q, const float* __restrict__ chif,
+                                                typename real_of<T>::type diag,
+                                                typename real_of<T>::type hpin, bool apbc) {
+    dwf_apply_flavour<DAG, IMASS>(acc[0], ld, g, q, 0, chif, diag, hpin, apbc);
+    dwf_apply_flavour<DAG, IMASS>(acc[1], ld, g, q, 1, chif, diag, hpin, apbc);
+}
+
+// Thread -> (point, flavour) map of the flavour-split kernels: a block of
+// kSplitThreads threads covers kSplitThreads/2 consecutive points, the first
+// half of its threads flavour 0 and the second half flavour 1, so every warp
+// reads contiguous runs of one component plane.
+constexpr int kSplitThreads = 256;
+constexpr int kSplitPoints = kSplitThreads / 2;
+constexpr int kSplitMinBlocks = 4;   // 64 registers a thread: 32 warps per SM
+__device__ __forceinline__ int split_flavour() { return threadIdx.x >= kSplitPoints; }
+__device__ __forceinline__ int64_t split_point() {
+    return (int64_t)blockIdx.x * kSplitPoints + (threadIdx.x & (kSplitPoints - 1));
+}
+inline unsigned split_blocks(int64_t npts) {
+    return (unsigned)((npts + kSplitPoints - 1) / kSplitPoints);
 }
 
 }  // namespace chdwf

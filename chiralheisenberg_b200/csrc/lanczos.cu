@@ -62,6 +62,8 @@ __device__ __forceinline__ T* ring(const LzArgsT<T>& a, int j) {
     return r == 0 ? a.rb0 : (r == 1 ? a.rb1 : a.rb2);
 }
 
+static_assert(kSplitThreads == kThreads, "the reductions assume kThreads-wide blocks");
+
 // Deterministic last-block reduction of the per-block partial sums.
 __device__ __forceinline__ bool last_block_sum(double v, double* part, unsigned* count,
                                                double* total) {
@@ -87,48 +89,102 @@ __device__ __forceinline__ bool last_block_sum(double v, double* part, unsigned*
     return true;
 }
 
+// ---- thread mapping ----------------------------------------------------------
+// FP64 vectors: two threads per point, one per flavour (split_point /
+// split_flavour), which halves the accumulator registers and doubles the
+// warps in flight.  FP32 vectors: one thread per point and both flavours,
+// the faster shape when the registers already allow full occupancy.
+template <class T> struct LzShape;
+template <> struct LzShape<double2> {
+    static constexpr bool split = true;
+    static constexpr int min_blocks = 3;          // <= 85 registers: no spills
+    static constexpr int unit = kSplitPoints;     // points per block pass
+};
+template <> struct LzShape<float2> {
+    static constexpr bool split = false;
+    static constexpr int min_blocks = 3;          // <= 85 registers a thread
+    static constexpr int unit = kThreads;
+};
+
+// Pass 1 runs on a persistent grid (a whole number of blocks per SM); block b
+// owns the contiguous, warp-aligned point range below, so every SM gets the
+// same amount of work and none idles through a partial last wave.
+struct PtRange { int64_t begin, end; };
+__device__ __forceinline__ PtRange block_range(int64_t npts) {
+    const int64_t nb = gridDim.x, b = blockIdx.x;
+    PtRange r;
+    r.begin = (b * npts / nb) & ~(int64_t)31;
+    r.end = b + 1 == nb ? npts : (((b + 1) * npts / nb) & ~(int64_t)31);
+    return r;
+}
+
+// One block pass over points [base, base + unit) of flavour(s) f0..f0+NF-1.
+template <class T>
+__device__ __forceinline__ void lz_lane(int64_t base, int64_t* p, int* f0) {
+    if (LzShape<T>::split) {
+        *p = base + (threadIdx.x & (kSplitPoints - 1));
+        *f0 = split_flavour();
+    } else {
+        *p = base + threadIdx.x;
+        *f0 = 0;
+    }
+}
+
 // ---- pass 1, kernel 1: vt = M q_j, alpha~_j = |vt|^2, pole recurrences -----
 template <class T, int IMASS>
-__global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgsT<T> a) {
+__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzArgsT<T> a) {
     typedef typename real_of<T>::type Real;
+    constexpr int NF = LzShape<T>::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
     if (ctl->done) return;
     const int j = ctl->iter;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const LdScaledT<T> ld{ring(a, j), (Real)a.h.invbeta[j]};
+    const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
-    if (p < a.g.npts) {
+#pragma unroll 1
+    for (int64_t base = R.begin; base < R.end; base += LzShape<T>::unit) {
+        int64_t p;
+        int f0;
+        lz_lane<T>(base, &p, &f0);
+        if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
-        T acc[2][4];
-        dwf_apply_point<false, IMASS>(acc, LdScaledT<T>{ring(a, j), (Real)a.h.invbeta[j]}, a.g, q,
-                                      a.chif, a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
+        for (int f = f0; f < f0 + NF; f++) {
+            T acc[4];
+            dwf_apply_flavour<false, IMASS>(acc, ld, a.g, q, f, a.chif, a.diag, a.hpin,
+                                            a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
-                a.vt[p + a.g.cs * (d + 4 * f)] = acc[f][d];
-                const double2 w = widen(acc[f][d]);
+                a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
+                const double2 w = widen(acc[d]);
                 loc += w.x * w.x + w.y * w.y;
             }
+        }
     }
     double tot;
+    __shared__ double sh_tot;
     if (!last_block_sum(loc, a.part, &ctl->count1, &tot)) return;
-    if (threadIdx.x != 0) return;
-    // scalar recurrences of qmrherm (cheisdwf.f:666-715), one pole at a time
-    const double at = tot;
+    if (threadIdx.x == 0) sh_tot = tot;
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    // scalar recurrences of qmrherm (cheisdwf.f:666-715): the poles are
+    // independent, one lane each
+    const int k = threadIdx.x;
+    const double at = sh_tot;
     const double beta0 = a.h.beta[j];
-    a.h.alphat[j] = at;
+    if (k == 0) a.h.alphat[j] = at;
     const int n = ctl->npole;
     const int64_t H = kMaxIter + 2;
-    double rhomax = 0.0;
-    for (int k = 0; k < n; k++) {
+    double v = -1.0;
+    if (k < n) {
         const double alpha = __dadd_rn(at, ctl->sigma[k]);
         double rho, mu = 0.0;
         if (j == 1) {
             ctl->d[k] = alpha;
             rho = __ddiv_rn(beta0, alpha);
         } else {
-            mu = __ddiv_rn(beta0, ctl->d[k]);
             const double dm1 = ctl->d[k];
+            mu = __ddiv_rn(beta0, dm1);
             const double dn = __dsub_rn(alpha, __dmul_rn(beta0, mu));
             ctl->d[k] = dn;
             rho = -__ddiv_rn(__dmul_rn(__dmul_rn(mu, dm1), ctl->rho[k]), dn);
@@ -136,9 +192,17 @@ __global__ void __launch_bounds__(kThreads) k_lz1_M(LzArgsT<T> a) {
         ctl->rho[k] = rho;
         a.h.rho[k * H + j] = rho;
         a.h.mu[k * H + j] = mu;
-        const double v = fabs(__dmul_rn(ctl->phimod, rho));
-        if (k == 0 || v > rhomax) rhomax = v;
+        v = fabs(__dmul_rn(ctl->phimod, rho));
     }
+    // rhomax as the sequential scan over the poles forms it: start from pole
+    // 0 and take any larger value (a NaN in pole 0 stays, NaNs of the other
+    // poles are skipped)
+    const double v0 = __shfl_sync(0xffffffffu, v, 0);
+    double m1 = k >= 1 ? v : -1.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    if (k != 0) return;
+    const double rhomax = (v0 != v0) ? v0 : fmax(v0, m1);
     int done = 0;
     if (j >= 2 && rhomax < ctl->thresh) done = 1;
     else if (j >= ctl->niter_cap) done = 2;
@@ -168,28 +232,35 @@ __device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, in
 
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
 template <class T, int IMASS>
-__global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgsT<T> a) {
+__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzArgsT<T> a) {
+    constexpr int NF = LzShape<T>::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
     if (ctl->done) return;
     const int j = ctl->iter;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    T* rn = ring(a, j + 1);
+    const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
-    if (p < a.g.npts) {
+#pragma unroll 1
+    for (int64_t base = R.begin; base < R.end; base += LzShape<T>::unit) {
+        int64_t p;
+        int f0;
+        lz_lane<T>(base, &p, &f0);
+        if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
-        T acc[2][4];
-        dwf_apply_point<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, a.chif, a.diag, a.hpin,
-                                     a.apbc != 0);
-        T* rn = ring(a, j + 1);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
+        for (int f = f0; f < f0 + NF; f++) {
+            T acc[4];
+            dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag,
+                                           a.hpin, a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const int64_t e = p + a.g.cs * (d + 4 * f);
-                const T v = three_term(a, acc[f][d], e, j);
+                const T v = three_term(a, acc[d], e, j);
                 rn[e] = v;
                 const double2 w = widen(v);
                 loc += w.x * w.x + w.y * w.y;
             }
+        }
     }
     double tot;
     if (!last_block_sum(loc, a.part, &ctl->count2, &tot)) return;
@@ -202,27 +273,33 @@ __global__ void __launch_bounds__(kThreads) k_lz1_Md(LzArgsT<T> a) {
 }
 
 // ---- pass 2: regenerate q_j and accumulate --------------------------------
+// One block pass per block (grid lz_direct_blocks).
 template <class T, int IMASS, int IFLAG>
-__global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgsT<T> a, int j, int apply) {
+__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_M(LzArgsT<T> a, int j,
+                                                                            int apply) {
     typedef typename real_of<T>::type Real;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    constexpr int NF = LzShape<T>::split ? 1 : 2;
+    int64_t p;
+    int f0;
+    lz_lane<T>((int64_t)blockIdx.x * LzShape<T>::unit, &p, &f0);
     if (p >= a.g.npts) return;
     const PointIdx q = point_of(a.g, p);
     const Real ib = (Real)a.h.invbeta[j];
     const T* rj = ring(a, j);
     if (apply) {
-        T acc[2][4];
-        dwf_apply_point<false, IMASS>(acc, LdScaledT<T>{rj, ib}, a.g, q, a.chif, a.diag, a.hpin,
-                                      a.apbc != 0);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
+        for (int f = f0; f < f0 + NF; f++) {
+            T acc[4];
+            dwf_apply_flavour<false, IMASS>(acc, LdScaledT<T>{rj, ib}, a.g, q, f, a.chif, a.diag,
+                                            a.hpin, a.apbc != 0);
 #pragma unroll
-            for (int d = 0; d < 4; d++) a.vt[p + a.g.cs * (d + 4 * f)] = acc[f][d];
+            for (int d = 0; d < 4; d++) a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
+        }
     }
     if (IFLAG == 0) {
         const double cj = a.h.c[j];
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
+        for (int c = 4 * f0; c < 4 * (f0 + NF); c++) {
             const int64_t e = p + a.g.cs * c;
             const double2 qj = widen(zscal(ib, __ldg(rj + e)));
             double2 xv = a.x[e];
@@ -237,15 +314,15 @@ __global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgsT<T> a, int j, int app
         const int64_t cs2 = 2 * (int64_t)a.g.kvol, kf2 = 8 * cs2;
         const int64_t H = kMaxIter + 2;
         const int n = a.npole;
-        double2 qv[8];
+        double2 qv[4 * NF];
 #pragma unroll
-        for (int c = 0; c < 8; c++) qv[c] = widen(zscal(ib, __ldg(rj + p + a.g.cs * c)));
-        const int64_t base = sw + 2 * (int64_t)q.site;
+        for (int c = 0; c < 4 * NF; c++) qv[c] = widen(zscal(ib, __ldg(rj + p + a.g.cs * (c + 4 * f0))));
+        const int64_t base = sw + 2 * (int64_t)q.site + cs2 * (4 * f0);
         for (int k = 0; k < n; k++) {
             const double y = a.h.y[k * H + j];
             double2* xk = a.xw + k * kf2 + base;
 #pragma unroll
-            for (int c = 0; c < 8; c++) {
+            for (int c = 0; c < 4 * NF; c++) {
                 double2 xv = xk[cs2 * c];
                 xv.x += y * qv[c].x;
                 xv.y += y * qv[c].y;
@@ -256,21 +333,45 @@ __global__ void __launch_bounds__(kThreads) k_lz2_M(LzArgsT<T> a, int j, int app
 }
 
 template <class T, int IMASS>
-__global__ void __launch_bounds__(kThreads) k_lz2_Md(LzArgsT<T> a, int j) {
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_Md(LzArgsT<T> a, int j) {
+    constexpr int NF = LzShape<T>::split ? 1 : 2;
+    int64_t p;
+    int f0;
+    lz_lane<T>((int64_t)blockIdx.x * LzShape<T>::unit, &p, &f0);
     if (p >= a.g.npts) return;
     const PointIdx q = point_of(a.g, p);
-    T acc[2][4];
-    dwf_apply_point<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, a.chif, a.diag, a.hpin,
-                                 a.apbc != 0);
     T* rn = ring(a, j + 1);
 #pragma unroll
-    for (int f = 0; f < 2; f++)
+    for (int f = f0; f < f0 + NF; f++) {
+        T acc[4];
+        dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag, a.hpin,
+                                       a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             const int64_t e = p + a.g.cs * (d + 4 * f);
-            rn[e] = three_term(a, acc[f][d], e, j);
+            rn[e] = three_term(a, acc[d], e, j);
         }
+    }
+}
+
+template <class T>
+static unsigned lz_direct_blocks(int64_t npts) {
+    return (unsigned)((npts + LzShape<T>::unit - 1) / LzShape<T>::unit);
+}
+
+// Persistent pass-1 grid: the resident blocks of both pass-1 kernels on all
+// SMs, at most one block pass per block.
+template <class T, int IMASS>
+static unsigned lz_pass1_blocks(int64_t npts) {
+    int dev = 0, nsm = 0, b1 = 0, b2 = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lz1_M<T, IMASS>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS>, kThreads, 0);
+    int64_t nb = (int64_t)nsm * (b1 < b2 ? b1 : b2);
+    const int64_t direct = lz_direct_blocks<T>(npts);
+    if (nb < 1 || nb > direct) nb = direct;
+    return (unsigned)nb;
 }
 
 // ---- between the passes: y_kj and c_j -------------------------------------
@@ -342,13 +443,51 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, Kern
     if (tm) tm->end(st);
 }
 
+// L2 residency of vt = M q_j: k_lz1_M writes it and k_lz1_Md reads it right
+// back, so its address range is marked persisting in L2 for the pass-1
+// launches instead of taking a DRAM round trip.  The persisting carve-out is
+// a limit of this process's context.  Returns the window (num_bytes 0 when
+// the device offers none).
+static constexpr bool kVtL2Window = true;
+
+static cudaAccessPolicyWindow vt_window(const void* vt, size_t bytes) {
+    cudaAccessPolicyWindow w{};
+    if (!kVtL2Window) return w;
+    int dev = 0, max_win = 0, max_persist = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
+    if (max_win <= 0 || max_persist <= 0) return w;
+    const size_t win = bytes < (size_t)max_win ? bytes : (size_t)max_win;
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t want = win < (size_t)max_persist ? win : (size_t)max_persist;
+    if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess)
+        cur = want;
+    cudaGetLastError();
+    if (cur == 0) return w;
+    w.base_ptr = const_cast<void*>(vt);
+    w.num_bytes = win;
+    w.hitRatio = cur >= win ? 1.0f : (float)((double)cur / (double)win);
+    w.hitProp = cudaAccessPropertyPersisting;
+    w.missProp = cudaAccessPropertyStreaming;
+    return w;
+}
+
+static void set_stream_window(cudaStream_t st, const cudaAccessPolicyWindow& w) {
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow = w;
+    cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaGetLastError();
+}
+
 // Pass 1 is a sequence of identical launch pairs (the iteration index and the
 // residual ring live in device memory), so a chunk of them is captured once
 // as a CUDA graph and replayed; the graph is rebuilt when any argument
 // changes.
 template <class T>
 static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned nb, int imass,
-                                   int chunk, cudaStream_t st) {
+                                   int chunk, cudaStream_t st, const cudaAccessPolicyWindow& win) {
     // pass-1 kernels never touch the pass-2 fields: clear them so one graph
     // serves every solve of this precision (heatbath, hamilton, force)
     LzArgsT<T> a = a_in;
@@ -375,6 +514,21 @@ static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned n
         cudaGetLastError();
         return nullptr;
     }
+    if (win.num_bytes) {                 // the L2 window on every captured launch
+        size_t nn = 0;
+        cudaGraphGetNodes(graph, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn && cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess) {
+            cudaKernelNodeAttrValue v{};
+            v.accessPolicyWindow = win;
+            for (cudaGraphNode_t nd : nodes) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+                    cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v);
+            }
+        }
+        cudaGetLastError();
+    }
     cudaGraphExec_t exec = nullptr;
     const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -391,8 +545,9 @@ static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned n
 }
 
 template <class T, int IMASS>
-static void launch_pass2(const LzArgsT<T>& a, unsigned nb, int j, int m, int iflag,
-                         cudaStream_t st, KernelTimer& tm) {
+static void launch_pass2(const LzArgsT<T>& a, int j, int m, int iflag, cudaStream_t st,
+                         KernelTimer& tm) {
+    const unsigned nb = lz_direct_blocks<T>(a.g.npts);
     const int apply = j < m;
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     const double acc = iflag == 0 ? 2.0 * a.g.kferm * sizeof(double2) + V : 0.0;
@@ -511,7 +666,7 @@ cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec) {
         hist.rho = hist_mem + 4 * H;
         hist.mu = hist.rho + kMaxPoles * H;
         hist.y = hist.mu + kMaxPoles * H;
-        const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+        const int64_t nb = split_blocks(g.npts);
         if ((e = cudaMalloc(&part, sizeof(double) * (nb + 2048)))) return e;
         if ((e = cudaHostAlloc(&hflag_host, sizeof(int), cudaHostAllocMapped))) return e;
         if ((e = cudaHostGetDevicePointer((void**)&hflag_dev, hflag_host, 0))) return e;
@@ -667,7 +822,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.x = x;
     a.xw = w.xw;
     a.npole = ndiag;
-    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const unsigned nb = imass == 3 ? lz_pass1_blocks<T, 3>(g.npts) : lz_pass1_blocks<T, 1>(g.npts);
     const int nbr = reduce_blocks(g.kferm);
     // r_1 lives where ring(a, 1) looks for it: the basis store when present
     T* r1 = a.hcap > 1 ? a.basis + g.kferm : a.rb1;
@@ -685,7 +840,10 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
     int launched = 0, nchunk = 0;
     // the per-launch path when kernels are being timed, else graph replays
-    cudaGraphExec_t gexec = w.timer.enabled ? nullptr : pass1_graph<T>(w, a, nb, imass, chunk, st);
+    const cudaAccessPolicyWindow win = vt_window(a.vt, sizeof(T) * (size_t)g.kferm);
+    if (win.num_bytes) set_stream_window(st, win);
+    cudaGraphExec_t gexec =
+        w.timer.enabled ? nullptr : pass1_graph<T>(w, a, nb, imass, chunk, st, win);
     while (launched < kMaxIter) {
         if (gexec) {
             cudaGraphLaunch(gexec, st);
@@ -729,6 +887,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     cudaEventSynchronize(ev[nchunk & 1]);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
+    if (win.num_bytes) set_stream_window(st, cudaAccessPolicyWindow{});
     if ((e = cudaGetLastError())) return e;
     LzCtl hr;
     if ((e = cudaMemcpyAsync(&hr, w.ctl, sizeof(hr), cudaMemcpyDeviceToHost, st))) return e;
@@ -763,8 +922,8 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         count_launches(1);
     } else {
         for (int j = 1; j <= m; j++) {
-            if (imass == 3) launch_pass2<T, 3>(a, nb, j, m, iflag, st, w.timer);
-            else launch_pass2<T, 1>(a, nb, j, m, iflag, st, w.timer);
+            if (imass == 3) launch_pass2<T, 3>(a, j, m, iflag, st, w.timer);
+            else launch_pass2<T, 1>(a, j, m, iflag, st, w.timer);
             if (w.timer.enabled && w.timer.used >= KernelTimer::kPool - 2) {
                 cudaStreamSynchronize(st);
                 w.timer.collect();

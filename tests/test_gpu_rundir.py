@@ -26,8 +26,8 @@ def run(tmp_path_factory):
     chb.run_dir(str(d), L, LT, LS)
     # the same chain through the API: cold start (no 'con'), default seed
     dt, beta, am3, am, hpin, imass, iterl, iter2 = MIDOUT
-    rz = {k: chb.read_remez(k, n, GOLD) for k, n in (("remez2", 25), ("remez4", 25),
-                                                     ("remez2g", 12))}
+    rz = {k: chb.read_remez(k, n, os.path.join(GOLD, k))
+          for k, n in (("remez2", 25), ("remez4", 25), ("remez2g", 12))}
     prog = chb.Program(L, LT, LS, dt, beta, am3, am, hpin, imass, iterl, rz["remez2"],
                        rz["remez4"], rz["remez2g"])
     seed0 = prog.read_con(str(d / "no_such_con"))
