@@ -25,7 +25,8 @@ constexpr int kThreads = 256;
 // rotation are read from here so every launch of the loop is identical
 // (and therefore capturable in a CUDA graph).
 struct LzCtl {
-    int iter;          // current Lanczos iteration j (1-based)
+    int it_m;          // iteration j of the next pass-1 M launch (written by M^dagger)
+    int it_md;         // iteration j of the next pass-1 M^dagger launch (written by M)
     int done;          // 0 running, 1 converged, 2 iteration cap
     int m;             // iteration at which the loop ended
     int npole;
@@ -37,7 +38,6 @@ struct LzCtl {
     double d[kMaxPoles];
     double rho[kMaxPoles];
     double anum[kMaxPoles];    // a_1..a_n (force weights / solution weights)
-    unsigned count1, count2;   // last-block counters of the two reductions
 };
 
 // Per-iteration scalar history (device), sized for kMaxIter iterations.

@@ -30,23 +30,6 @@
 
 namespace chdwf {
 
-template <class T> struct LdScaledT;
-template <> struct LdScaledT<double2> {
-    const double2* __restrict__ p;
-    double s;
-    __device__ __forceinline__ double2 operator()(int64_t j) const {
-        const double2 v = __ldg(p + j);
-        return make_double2(__dmul_rn(v.x, s), __dmul_rn(v.y, s));
-    }
-};
-template <> struct LdScaledT<float2> {
-    const float2* __restrict__ p;
-    float s;
-    __device__ __forceinline__ float2 operator()(int64_t j) const {
-        const float2 v = __ldg(p + j);
-        return make_float2(v.x * s, v.y * s);
-    }
-};
 template <class T> struct LdPlainT {
     const T* __restrict__ p;
     __device__ __forceinline__ T operator()(int64_t j) const { return __ldg(p + j); }
@@ -64,29 +47,17 @@ __device__ __forceinline__ T* ring(const LzArgsT<T>& a, int j) {
 
 static_assert(kSplitThreads == kThreads, "the reductions assume kThreads-wide blocks");
 
-// Deterministic last-block reduction of the per-block partial sums.
-__device__ __forceinline__ bool last_block_sum(double v, double* part, unsigned* count,
-                                               double* total) {
+// Sum of the n chunk partials part[0..n) in a fixed order; every block that
+// calls it gets the same value.  Valid in all threads.
+__device__ __forceinline__ double sum_partials(const double* part, int n) {
     __shared__ double sh[kThreads / 32];
-    __shared__ bool is_last;
-    v = block_sum<kThreads>(v, sh);
-    if (threadIdx.x == 0) {
-        part[blockIdx.x] = v;
-        __threadfence();
-        const unsigned t = atomicAdd(count, 1u);
-        is_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!is_last) return false;
-    __threadfence();
+    __shared__ double total;
     double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += ((volatile double*)part)[i];
+    for (int i = threadIdx.x; i < n; i += kThreads) s += __ldcg(part + i);
     s = block_sum<kThreads>(s, sh);
-    if (threadIdx.x == 0) {
-        *total = s;
-        *count = 0;
-    }
-    return true;
+    if (threadIdx.x == 0) total = s;
+    __syncthreads();
+    return total;
 }
 
 // ---- thread mapping ----------------------------------------------------------
@@ -108,7 +79,9 @@ template <> struct LzShape<float2> {
 
 // Pass 1 runs on a persistent grid (a whole number of blocks per SM); block b
 // owns the contiguous, warp-aligned point range below, so every SM gets the
-// same amount of work and none idles through a partial last wave.
+// same amount of work and none idles through a partial last wave.  Each
+// block leaves its |.|^2 partial in part[b]; the kernel that needs the sum
+// adds the partials itself, in block order, so no block waits on another.
 struct PtRange { int64_t begin, end; };
 __device__ __forceinline__ PtRange block_range(int64_t npts) {
     const int64_t nb = gridDim.x, b = blockIdx.x;
@@ -130,15 +103,41 @@ __device__ __forceinline__ void lz_lane(int64_t base, int64_t* p, int* f0) {
     }
 }
 
-// ---- pass 1, kernel 1: vt = M q_j, alpha~_j = |vt|^2, pole recurrences -----
+// vt = M q_j with q_j = r_j / beta_j, formed as (1/beta_j) (M r_j): one
+// scaling per output element instead of one per stencil load.  The pass-1
+// kernel and the regenerating pass 2 use this same sequence.
+template <bool DAG, int IMASS, class T>
+__device__ __forceinline__ void apply_scaled(T acc[4], const T* r, typename real_of<T>::type ib,
+                                             const LzArgsT<T>& a, const PointIdx& q, int f) {
+    dwf_apply_flavour<DAG, IMASS>(acc, LdPlainT<T>{r}, a.g, q, f, a.chif, a.diag, a.hpin,
+                                  a.apbc != 0);
+#pragma unroll
+    for (int d = 0; d < 4; d++) acc[d] = zscal(ib, acc[d]);
+}
+
+// ---- pass 1, kernel 1: vt = M q_j and the block partials of |vt|^2 ---------
+// beta_j is the sum of the previous M^dagger launch's partials (beta_1 comes
+// from the source), formed by every block.  The partial buffers: part[0..nb)
+// for this kernel, part[nb..2nb) for M^dagger.
 template <class T, int IMASS>
 __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzArgsT<T> a) {
     typedef typename real_of<T>::type Real;
     constexpr int NF = LzShape<T>::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
     if (ctl->done) return;
-    const int j = ctl->iter;
-    const LdScaledT<T> ld{ring(a, j), (Real)a.h.invbeta[j]};
+    const int j = ctl->it_m;
+    const int nb = gridDim.x;
+    const double bj = j == 1 ? a.h.beta[1] : sqrt(sum_partials(a.part + nb, nb));
+    const double ibj = j == 1 ? a.h.invbeta[1] : 1.0 / bj;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->it_md = j;
+        if (j > 1) {
+            a.h.beta[j] = bj;
+            a.h.invbeta[j] = ibj;
+        }
+    }
+    const T* rj = ring(a, j);
+    const Real ib = (Real)ibj;
     const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
 #pragma unroll 1
@@ -151,8 +150,7 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzAr
 #pragma unroll
         for (int f = f0; f < f0 + NF; f++) {
             T acc[4];
-            dwf_apply_flavour<false, IMASS>(acc, ld, a.g, q, f, a.chif, a.diag, a.hpin,
-                                            a.apbc != 0);
+            apply_scaled<false, IMASS>(acc, rj, ib, a, q, f);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
@@ -161,16 +159,17 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzAr
             }
         }
     }
-    double tot;
-    __shared__ double sh_tot;
-    if (!last_block_sum(loc, a.part, &ctl->count1, &tot)) return;
-    if (threadIdx.x == 0) sh_tot = tot;
-    __syncthreads();
-    if (threadIdx.x >= 32) return;
-    // scalar recurrences of qmrherm (cheisdwf.f:666-715): the poles are
-    // independent, one lane each
+    __shared__ double sh[kThreads / 32];
+    loc = block_sum<kThreads>(loc, sh);
+    if (threadIdx.x == 0) a.part[blockIdx.x] = loc;
+}
+
+// Scalar recurrences of qmrherm for iteration j (cheisdwf.f:666-715), one
+// lane per pole (the poles are independent), and the stopping test.
+template <class T>
+__device__ __forceinline__ void pole_step(const LzArgsT<T>& a, int j, double at) {
+    LzCtl* ctl = a.ctl;
     const int k = threadIdx.x;
-    const double at = sh_tot;
     const double beta0 = a.h.beta[j];
     if (k == 0) a.h.alphat[j] = at;
     const int n = ctl->npole;
@@ -217,13 +216,29 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzAr
     }
 }
 
+// alpha~_j from M(j)'s partials (the same sum, in the same order, as the
+// M^dagger blocks form), the pole recurrences and the stopping test.  One
+// block, launched on a side stream next to M^dagger(j): it overlaps that
+// kernel instead of lengthening either pass-1 kernel.  A converged solve
+// stops before M(j+1).
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_lz_pole(LzArgsT<T> a, int nb) {
+    LzCtl* ctl = a.ctl;
+    if (ctl->done) return;
+    const int j = ctl->it_md;
+    const double at = sum_partials(a.part, nb);
+    if (threadIdx.x == 0) ctl->it_m = j + 1;
+    if (threadIdx.x < 32) pole_step(a, j, at);
+}
+
 // r_{j+1} = x3 - alpha~ q_j - beta_j q_{j-1} at one point (cheisdwf.f:655)
 template <class T>
-__device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, int j) {
+__device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, int j,
+                                        double alphat) {
     typedef typename real_of<T>::type Real;
     const T* rj = ring(a, j);
     const T* rjm = ring(a, j - 1);
-    const Real ib = (Real)a.h.invbeta[j], at = (Real)a.h.alphat[j], bj = (Real)a.h.beta[j];
+    const Real ib = (Real)a.h.invbeta[j], at = (Real)alphat, bj = (Real)a.h.beta[j];
     const T qj = zscal(ib, rj[e]);
     T v = zsub(x3, zscal(at, qj));
     if (j > 1) v = zsub(v, zscal(bj, zscal((Real)a.h.invbeta[j - 1], rjm[e])));
@@ -231,12 +246,15 @@ __device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, in
 }
 
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
+// alpha~_j is the sum of M(j)'s partials, formed by every block.
 template <class T, int IMASS>
 __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzArgsT<T> a) {
     constexpr int NF = LzShape<T>::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
     if (ctl->done) return;
-    const int j = ctl->iter;
+    const int j = ctl->it_md;
+    const int nb = gridDim.x;
+    const double at = sum_partials(a.part, nb);
     T* rn = ring(a, j + 1);
     const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
@@ -255,21 +273,16 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzA
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const int64_t e = p + a.g.cs * (d + 4 * f);
-                const T v = three_term(a, acc[d], e, j);
+                const T v = three_term(a, acc[d], e, j, at);
                 rn[e] = v;
                 const double2 w = widen(v);
                 loc += w.x * w.x + w.y * w.y;
             }
         }
     }
-    double tot;
-    if (!last_block_sum(loc, a.part, &ctl->count2, &tot)) return;
-    if (threadIdx.x == 0) {
-        const double b = sqrt(tot);
-        a.h.beta[j + 1] = b;
-        a.h.invbeta[j + 1] = 1.0 / b;
-        ctl->iter = j + 1;
-    }
+    __shared__ double sh[kThreads / 32];
+    loc = block_sum<kThreads>(loc, sh);
+    if (threadIdx.x == 0) a.part[nb + blockIdx.x] = loc;
 }
 
 // ---- pass 2: regenerate q_j and accumulate --------------------------------
@@ -290,8 +303,7 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_M(LzAr
 #pragma unroll
         for (int f = f0; f < f0 + NF; f++) {
             T acc[4];
-            dwf_apply_flavour<false, IMASS>(acc, LdScaledT<T>{rj, ib}, a.g, q, f, a.chif, a.diag,
-                                            a.hpin, a.apbc != 0);
+            apply_scaled<false, IMASS>(acc, rj, ib, a, q, f);
 #pragma unroll
             for (int d = 0; d < 4; d++) a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
         }
@@ -349,7 +361,7 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_Md(LzA
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             const int64_t e = p + a.g.cs * (d + 4 * f);
-            rn[e] = three_term(a, acc[d], e, j);
+            rn[e] = three_term(a, acc[d], e, j, a.h.alphat[j]);
         }
     }
 }
@@ -375,25 +387,45 @@ static unsigned lz_pass1_blocks(int64_t npts) {
 }
 
 // ---- between the passes: y_kj and c_j -------------------------------------
-__global__ void k_lz_coeffs(LzCtl* ctl, LzHist h, int iflag) {
+// The backward recurrence is sequential in i for each pole: the block stages
+// rho and mu in shared memory a chunk of iterations at a time, so each pole's
+// lane runs its chain from shared memory; c_j of the chunk follows in
+// parallel, summed over the poles in order.
+__global__ void __launch_bounds__(kThreads) k_lz_coeffs(LzCtl* ctl, LzHist h, int iflag) {
+    constexpr int CH = 48;
+    __shared__ double s_rho[kMaxPoles][CH], s_mu[kMaxPoles][CH], s_y[kMaxPoles][CH];
+    __shared__ double s_anum[kMaxPoles];
     const int m = ctl->m, n = ctl->npole;
     const int64_t H = kMaxIter + 2;
     const int k = threadIdx.x;
-    if (k < n) {
-        double y = h.rho[k * H + m];
-        h.y[k * H + m] = y;
-        for (int i = m - 1; i >= 1; i--) {
-            y = __dsub_rn(h.rho[k * H + i], __dmul_rn(h.mu[k * H + i + 1], y));
-            h.y[k * H + i] = y;
+    if (k < n) s_anum[k] = ctl->anum[k];
+    double y = 0.0;
+    for (int hi = m; hi >= 1; hi -= CH) {
+        const int lo = hi - CH + 1 > 1 ? hi - CH + 1 : 1;
+        const int len = hi - lo + 1;
+        for (int t = threadIdx.x; t < n * len; t += blockDim.x) {
+            const int kk = t / len, o = t - kk * len;
+            s_rho[kk][o] = h.rho[kk * H + lo + o];
+            s_mu[kk][o] = h.mu[kk * H + lo + o + 1];
         }
-    }
-    __syncthreads();
-    if (iflag == 0) {
-        for (int i = 1 + threadIdx.x; i <= m; i += blockDim.x) {
-            double c = 0.0;
-            for (int kk = 0; kk < n; kk++) c = __dadd_rn(c, __dmul_rn(ctl->anum[kk], h.y[kk * H + i]));
-            h.c[i] = c;
+        __syncthreads();
+        if (k < n) {
+            for (int o = len - 1; o >= 0; o--) {
+                const int i = lo + o;
+                y = i == m ? s_rho[k][o] : __dsub_rn(s_rho[k][o], __dmul_rn(s_mu[k][o], y));
+                s_y[k][o] = y;
+                h.y[k * H + i] = y;
+            }
         }
+        __syncthreads();
+        if (iflag == 0) {
+            for (int o = threadIdx.x; o < len; o += blockDim.x) {
+                double c = 0.0;
+                for (int kk = 0; kk < n; kk++) c = __dadd_rn(c, __dmul_rn(s_anum[kk], s_y[kk][o]));
+                h.c[lo + o] = c;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -431,16 +463,23 @@ __global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* part, int nb) {
 }
 
 template <class T, int IMASS>
-static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, KernelTimer* tm) {
+static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
+                         KernelTimer* tm) {
     // algorithmic bytes: M reads q, writes vt; M^dagger reads vt, r_j, r_{j-1}
     // and writes r_{j+1}; both read chi as REAL*4
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     if (tm) tm->begin(0, st, 2 * V + chi);
     k_lz1_M<T, IMASS><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
+    // the scalar step of iteration j on the side stream, beside M^dagger(j)
+    cudaEventRecord(side.fork, st);
+    cudaStreamWaitEvent(side.stream, side.fork, 0);
+    k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
+    cudaEventRecord(side.join, side.stream);
     if (tm) tm->begin(1, st, 4 * V + chi);
     k_lz1_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
+    cudaStreamWaitEvent(st, side.join, 0);
 }
 
 // L2 residency of vt = M q_j: k_lz1_M writes it and k_lz1_Md reads it right
@@ -507,8 +546,8 @@ static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned n
         return nullptr;
     }
     for (int c = 0; c < chunk; c++) {
-        if (imass == 3) launch_pass1<T, 3>(a, nb, st, nullptr);
-        else launch_pass1<T, 1>(a, nb, st, nullptr);
+        if (imass == 3) launch_pass1<T, 3>(a, nb, st, w.side, nullptr);
+        else launch_pass1<T, 1>(a, nb, st, w.side, nullptr);
     }
     if (cudaStreamEndCapture(st, &graph) != cudaSuccess || !graph) {
         cudaGetLastError();
@@ -626,6 +665,10 @@ void LzWork::release() {
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
         gr = LzGraph();
     }
+    if (side.fork) cudaEventDestroy(side.fork);
+    if (side.join) cudaEventDestroy(side.join);
+    if (side.stream) cudaStreamDestroy(side.stream);
+    side = LzSide();
     if (ctl) cudaFree(ctl);
     if (hist_mem) cudaFree(hist_mem);
     if (part) cudaFree(part);
@@ -666,9 +709,14 @@ cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec) {
         hist.rho = hist_mem + 4 * H;
         hist.mu = hist.rho + kMaxPoles * H;
         hist.y = hist.mu + kMaxPoles * H;
-        const int64_t nb = split_blocks(g.npts);
+        // block partials of the two pass-1 kernels (at most split_blocks
+        // blocks each), and the source norm's block partials
+        const int64_t nb = 2 * (int64_t)split_blocks(g.npts);
         if ((e = cudaMalloc(&part, sizeof(double) * (nb + 2048)))) return e;
         if ((e = cudaHostAlloc(&hflag_host, sizeof(int), cudaHostAllocMapped))) return e;
+        if ((e = cudaStreamCreateWithFlags(&side.stream, cudaStreamNonBlocking))) return e;
+        if ((e = cudaEventCreateWithFlags(&side.fork, cudaEventDisableTiming))) return e;
+        if ((e = cudaEventCreateWithFlags(&side.join, cudaEventDisableTiming))) return e;
         if ((e = cudaHostGetDevicePointer((void**)&hflag_dev, hflag_host, 0))) return e;
     }
     if (prec == kPrecF64 && !rb[0]) {
@@ -730,7 +778,7 @@ void set_ring<float2>(LzArgsT<float2>& a, LzWork& w) {
 // x += sum_j c_j q_j, q_j = r_j / beta_j, j = 1..m, in j order per element
 // (the same sequence of operations as the regenerating pass 2).
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int m) {
+__global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int j0, int j1) {
     typedef typename real_of<T>::type Real;
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= a.g.kferm) return;
@@ -738,7 +786,7 @@ __global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int m) {
     const T* b = a.basis + e;
     const int64_t stride = a.g.kferm;
 #pragma unroll 4
-    for (int j = 1; j <= m; j++) {
+    for (int j = j0; j <= j1; j++) {
         const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(b + j * stride)));
         const double cj = a.h.c[j];
         xv.x += cj * qj.x;
@@ -746,6 +794,8 @@ __global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int m) {
     }
     a.x[e] = xv;
 }
+
+static constexpr int kAccumChunk = 64;
 
 // Two-slice x_k of every pole from the stored basis (force solves):
 // thread per wall element (slice, component, site), poles in chunks of 8.
@@ -794,7 +844,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     cudaError_t e;
     LzCtl hc;
     memset(&hc, 0, sizeof(hc));
-    hc.iter = 1;
+    hc.it_m = 1;
     hc.npole = ndiag;
     hc.niter_cap = kMaxIter;
     const float resid = sqrtf((float)g.kferm * res * res);   // :621
@@ -848,12 +898,12 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         if (gexec) {
             cudaGraphLaunch(gexec, st);
             launched += chunk;
-            count_launches(2 * chunk);
+            count_launches(3 * chunk);
         } else {
             for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
-                if (imass == 3) launch_pass1<T, 3>(a, nb, st, &w.timer);
-                else launch_pass1<T, 1>(a, nb, st, &w.timer);
-                count_launches(2);
+                if (imass == 3) launch_pass1<T, 3>(a, nb, st, w.side, &w.timer);
+                else launch_pass1<T, 1>(a, nb, st, w.side, &w.timer);
+                count_launches(3);
             }
         }
         cudaEventRecord(ev[nchunk & 1], st);
@@ -871,7 +921,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         int keep = 0;
         for (int i = 0, it = 0; i < w.timer.used; i++) {
             if (w.timer.cls[i] == 0) it++;
-            const bool real = it <= hm.m && !(w.timer.cls[i] == 1 && it >= hm.m);
+            const bool real = it <= hm.m;      // M^dagger(m) completes too
             if (real) {
                 w.timer.cls[keep] = w.timer.cls[i];
                 std::swap(w.timer.ev[2 * keep], w.timer.ev[2 * i]);
@@ -880,7 +930,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
             }
         }
         w.timer.launches[0] -= launched - hm.m;
-        w.timer.launches[1] -= launched - hm.m + 1;
+        w.timer.launches[1] -= launched - hm.m;
         w.timer.used = keep;
         w.timer.collect();
     }
@@ -913,13 +963,22 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
             ? (double)m * g.kferm * vb + 2.0 * g.kferm * sizeof(double2)
             : (double)m * 16.0 * g.kvol * vb + (double)ndiag * 16.0 * g.kvol * sizeof(double2);
         w.timer.begin(2, st, nbytes);
-        if (iflag == 0)
-            k_lz_accum_x<T><<<(unsigned)((g.kferm + kThreads - 1) / kThreads), kThreads, 0, st>>>(a, m);
-        else
+        if (iflag == 0) {
+            // a chunk of stored vectors per launch: x (FP64) is carried in
+            // memory between chunks, so each element still sums j = 1..m in
+            // order, and the pages a launch touches stay few
+            const unsigned nbx = (unsigned)((g.kferm + kThreads - 1) / kThreads);
+            for (int j0 = 1; j0 <= m; j0 += kAccumChunk) {
+                const int j1 = j0 + kAccumChunk - 1 < m ? j0 + kAccumChunk - 1 : m;
+                k_lz_accum_x<T><<<nbx, kThreads, 0, st>>>(a, j0, j1);
+                count_launches(1);
+            }
+        } else {
             k_lz_accum_walls<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads),
                                   kThreads, 0, st>>>(a, m);
+            count_launches(1);
+        }
         w.timer.end(st);
-        count_launches(1);
     } else {
         for (int j = 1; j <= m; j++) {
             if (imass == 3) launch_pass2<T, 3>(a, j, m, iflag, st, w.timer);

@@ -66,8 +66,16 @@ struct LzGraph {
     int imass = 0, chunk = 0;
 };
 
+// Side stream of the pass-1 loop: the scalar step of each iteration runs
+// there, beside the M^dagger kernel, forked and joined with events.
+struct LzSide {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
 struct LzWork {
     Geom geom{};
+    LzSide side;
     LzGraph graph[2];                 // pass-1 chunk graph per vector precision
     LzCtl* ctl = nullptr;
     double* hist_mem = nullptr;
