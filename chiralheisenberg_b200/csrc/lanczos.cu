@@ -60,6 +60,15 @@ __device__ __forceinline__ double sum_partials(const double* part, int n) {
     return total;
 }
 
+// The stop flag, read once per block: every thread of a block takes the same
+// branch (the scalar step may set it while an M^dagger block starts).
+__device__ __forceinline__ bool block_stopped(const LzCtl* ctl) {
+    __shared__ int s_done;
+    if (threadIdx.x == 0) s_done = *(const volatile int*)&ctl->done;
+    __syncthreads();
+    return s_done != 0;
+}
+
 // ---- thread mapping ----------------------------------------------------------
 // FP64 vectors: two threads per point, one per flavour (split_point /
 // split_flavour), which halves the accumulator registers and doubles the
@@ -124,7 +133,7 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzAr
     typedef typename real_of<T>::type Real;
     constexpr int NF = LzShape<T>::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
-    if (ctl->done) return;
+    if (block_stopped(ctl)) return;
     const int j = ctl->it_m;
     const int nb = gridDim.x;
     const double bj = j == 1 ? a.h.beta[1] : sqrt(sum_partials(a.part + nb, nb));
@@ -224,7 +233,7 @@ __device__ __forceinline__ void pole_step(const LzArgsT<T>& a, int j, double at)
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_lz_pole(LzArgsT<T> a, int nb) {
     LzCtl* ctl = a.ctl;
-    if (ctl->done) return;
+    if (block_stopped(ctl)) return;
     const int j = ctl->it_md;
     const double at = sum_partials(a.part, nb);
     if (threadIdx.x == 0) ctl->it_m = j + 1;
@@ -251,7 +260,7 @@ template <class T, int IMASS>
 __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzArgsT<T> a) {
     constexpr int NF = LzShape<T>::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
-    if (ctl->done) return;
+    if (block_stopped(ctl)) return;
     const int j = ctl->it_md;
     const int nb = gridDim.x;
     const double at = sum_partials(a.part, nb);
@@ -882,12 +891,13 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     k_lz_init<<<1, kThreads, 0, st>>>(w.ctl, w.hist, w.part, nbr);
     count_launches(2);
 
-    // pass 1: launch chunks of iterations, poll the mapped flag with one
-    // chunk in flight ahead of the one being checked
+    // pass 1: launch chunks of iterations and poll the mapped flag with
+    // kAhead chunks queued beyond the one being checked, so a host thread
+    // that wakes late still finds the GPU busy
     const int chunk = 16;
-    cudaEvent_t ev[2];
-    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    constexpr int kAhead = 2;
+    cudaEvent_t ev[kAhead + 1];
+    for (cudaEvent_t& e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     int launched = 0, nchunk = 0;
     // the per-launch path when kernels are being timed, else graph replays
     const cudaAccessPolicyWindow win = vt_window(a.vt, sizeof(T) * (size_t)g.kferm);
@@ -906,9 +916,9 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
                 count_launches(3);
             }
         }
-        cudaEventRecord(ev[nchunk & 1], st);
-        if (nchunk >= 1) {
-            cudaEventSynchronize(ev[(nchunk - 1) & 1]);
+        cudaEventRecord(ev[nchunk % (kAhead + 1)], st);
+        if (nchunk >= kAhead) {
+            cudaEventSynchronize(ev[(nchunk - kAhead) % (kAhead + 1)]);
             if (*(volatile int*)w.hflag_host) break;
         }
         nchunk++;
@@ -934,9 +944,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         w.timer.used = keep;
         w.timer.collect();
     }
-    cudaEventSynchronize(ev[nchunk & 1]);
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
+    for (cudaEvent_t& e : ev) cudaEventDestroy(e);   // the stream sync below covers them
     if (win.num_bytes) set_stream_window(st, cudaAccessPolicyWindow{});
     if ((e = cudaGetLastError())) return e;
     LzCtl hr;
