@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--Ls", type=int, default=24)
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--operator-sweep", action="store_true",
+                    help="operator GB/s over L in {16,24,32,48}, Ls in {16,24,32}, FP64/FP32/FP16")
     ap.add_argument("--profile-solve", action="store_true",
                     help="bounded work for profilers: one heatbath and one force evaluation")
     ap.add_argument("--profile-res", type=float, default=0.0,
@@ -305,6 +307,79 @@ def run_profile_solve(args, local_rank):
     prog.close()
 
 
+def run_operator_sweep(args, local_rank):
+    """M and M^dagger on device buffers, one JSON line per (L, Ls, storage):
+    median of 20 applications, each timed alone with CUDA events on the
+    library stream after a 256 MB write that evicts L2.  Algorithmic bytes =
+    2 V sizeof(complex) + 3 kvol 4 (chi as REAL*4); the timed call also
+    rounds chi to REAL*4 (one small kernel, included)."""
+    import ctypes as C
+    import torch
+    import chiralheisenberg_b200 as chb
+    torch.cuda.set_device(local_rank)
+    peak, kind = peaks()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+    for L in (16, 24, 32, 48):
+        for Ls in (16, 24, 32):
+            kvol = L * L * L                  # ksize^2 * ksizet with ksizet = ksize
+            V = 8 * kvol * Ls
+            if 3 * V * 16 > 60e9:
+                continue
+            lat = chb.Lattice(L, L, Ls, device=local_rank)
+            stream = torch.cuda.ExternalStream(lat.lib.chdwf_get_stream(lat.h), device=local_rank)
+            g = torch.Generator(device=f"cuda:{local_rank}").manual_seed(L * 100 + Ls)
+            R64 = torch.randn(2 * V, dtype=torch.float64, device=f"cuda:{local_rank}", generator=g)
+            chi = torch.randn(3 * kvol, dtype=torch.float64, device=f"cuda:{local_rank}", generator=g)
+            for prec, name, elem in ((0, "f64", 16), (1, "f32", 8), (2, "f16", 4)):
+                if prec == 0:
+                    src = R64
+                elif prec == 1:
+                    src = R64.to(torch.float32)
+                else:
+                    src = R64.to(torch.float16)
+                out = torch.empty_like(src)
+                for dag in (0, 1):
+                    def apply():
+                        if prec == 0:
+                            rc = lat.lib.chdwf_dslash_dev(lat.h, C.c_void_p(out.data_ptr()),
+                                                          C.c_void_p(src.data_ptr()),
+                                                          C.c_void_p(chi.data_ptr()), 0.3, 1, dag,
+                                                          None)
+                        else:
+                            rc = lat.lib.chdwf_dslash_dev_lp(lat.h, C.c_void_p(out.data_ptr()),
+                                                             C.c_void_p(src.data_ptr()),
+                                                             C.c_void_p(chi.data_ptr()), 0.3, 1,
+                                                             dag, prec, None)
+                        if rc != 0:
+                            raise RuntimeError(f"operator rc={rc}")
+                    for _ in range(3):
+                        apply()
+                    torch.cuda.synchronize()
+                    ts = []
+                    for i in range(20):
+                        with torch.cuda.stream(stream):
+                            flush.fill_(i & 255)
+                            e0 = torch.cuda.Event(enable_timing=True)
+                            e1 = torch.cuda.Event(enable_timing=True)
+                            e0.record(stream)
+                            apply()
+                            e1.record(stream)
+                        e1.synchronize()
+                        ts.append(e0.elapsed_time(e1))
+                    ms = statistics.median(ts)
+                    nbytes = 2 * V * elem + 12 * kvol
+                    gbs = nbytes / (ms * 1e-3) / 1e9
+                    print(json.dumps({"operator": "M^dagger" if dag else "M", "L": L, "Lt": L,
+                                      "Ls": Ls, "storage": name, "us": round(ms * 1e3, 2),
+                                      "algorithmic_bytes": nbytes, "GBps": round(gbs, 1),
+                                      "frac_of_hbm": round(gbs / peak, 3), "peak_kind": kind,
+                                      "l2": "evicted before each application"}), flush=True)
+                del out
+            lat.close()
+            del R64, chi
+            torch.cuda.empty_cache()
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import chiralheisenberg_b200 as chb
@@ -459,6 +534,9 @@ def main():
         return
     if args.profile_solve:
         run_profile_solve(args, local_rank)
+        return
+    if args.operator_sweep:
+        run_operator_sweep(args, int(os.environ.get("LOCAL_RANK", "0")))
         return
     if world > 1:
         import datetime
