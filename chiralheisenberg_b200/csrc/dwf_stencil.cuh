@@ -202,6 +202,117 @@ __device__ __forceinline__ void dwf_apply_point(T acc[2][4], const Ld& ld, const
     dwf_apply_flavour<DAG, IMASS>(acc[1], ld, g, q, 1, chif, diag, hpin, apbc);
 }
 
+struct LdF2 {
+    const float2* __restrict__ p;
+    __device__ __forceinline__ float2 operator()(int64_t j) const { return __ldg(p + j); }
+};
+
+// Two adjacent points (s, s+1), s even, of flavour f on FP32 storage.  Each
+// load is one 16-byte float4 holding both points' components (the spinor
+// layout has s innermost, so an even point and its successor are adjacent),
+// which doubles the bytes per load instruction; each point's elements go
+// through the same operation sequence as dwf_apply_flavour.  Needs Ls even.
+template <bool DAG, int IMASS>
+__device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
+                                                       const float2* __restrict__ in,
+                                                       const Geom& g, const PointIdx& q, int f,
+                                                       const float* __restrict__ chif, float diag,
+                                                       float hpin, bool apbc) {
+    constexpr int SF = DAG ? -1 : 1;
+    const int L = g.L, Lt = g.Lt, Ls = g.Ls;
+    const int64_t LsI = Ls, cs = g.cs, fo = g.cs * (4 * f);
+    auto ld2 = [&](int64_t n, float2& r0, float2& r1) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(in + n));
+        r0 = make_float2(v.x, v.y);
+        r1 = make_float2(v.z, v.w);
+    };
+    // diagonal term (:2651-2667)
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        float2 r0, r1;
+        ld2(q.p + fo + cs * d, r0, r1);
+        acc[0][d] = zscal(diag, r0);
+        acc[1][d] = zscal(diag, r1);
+    }
+    const int xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
+    const int yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
+    const int tp = q.it + 1 == Lt ? 0 : q.it + 1, tm = q.it == 0 ? Lt - 1 : q.it - 1;
+    const int64_t sb = q.s + fo;
+    const int64_t rowb = (int64_t)L * (q.iy + (int64_t)L * q.it);
+    const int64_t n_xp = sb + LsI * (xp + rowb), n_xm = sb + LsI * (xm + rowb);
+    const int64_t colb = q.ix + (int64_t)L * L * q.it;
+    const int64_t n_yp = sb + LsI * (colb + (int64_t)L * yp), n_ym = sb + LsI * (colb + (int64_t)L * ym);
+    const int64_t plb = q.ix + (int64_t)L * q.iy;
+    const int64_t n_tp = sb + LsI * (plb + (int64_t)L * L * tp), n_tm = sb + LsI * (plb + (int64_t)L * L * tm);
+    float2 r0[4], r1[4];
+#define CHDWF_PAIR_HOP(N, MU, SIG, NEG)                                         \
+    {                                                                          \
+        _Pragma("unroll") for (int d = 0; d < 4; d++) ld2((N) + cs * d, r0[d], r1[d]); \
+        hop<MU, SIG, NEG>(acc[0], r0);                                         \
+        hop<MU, SIG, NEG>(acc[1], r1);                                         \
+    }
+    CHDWF_PAIR_HOP(n_xp, 0, SF, false)
+    CHDWF_PAIR_HOP(n_xm, 0, -SF, false)
+    CHDWF_PAIR_HOP(n_yp, 1, SF, false)
+    CHDWF_PAIR_HOP(n_ym, 1, -SF, false)
+    CHDWF_PAIR_HOP(n_tp, 2, SF, false)
+    CHDWF_PAIR_HOP(n_tm, 2, -SF, false)
+    // kappa = 1/2 (:2815-2829)
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        acc[0][d] = zscal(0.5f, acc[0][d]);
+        acc[1][d] = zscal(0.5f, acc[1][d]);
+    }
+    // antiperiodic boundary in t (:2831-2876)
+    if (apbc) {
+        if (q.it == Lt - 1) CHDWF_PAIR_HOP(n_tp, 2, SF, true)
+        if (q.it == 0) CHDWF_PAIR_HOP(n_tm, 2, -SF, true)
+    }
+#undef CHDWF_PAIR_HOP
+    // s hops (:2879-2908; M^dagger :3313-3342).  Point 0 is s, point 1 is s+1:
+    // the pair fed from s+1 takes point 0's value from this pair and point 1's
+    // from the next pair; the pair fed from s-1 takes point 0's value from the
+    // previous pair and point 1's from this pair.
+    constexpr int UP = DAG ? 0 : 2;
+    constexpr int DN = DAG ? 2 : 0;
+#pragma unroll
+    for (int d = UP; d < UP + 2; d++) {
+        float2 c0, c1;
+        ld2(q.p + fo + cs * d, c0, c1);
+        acc[0][d] = zsub(acc[0][d], c1);
+        if (q.s + 2 < Ls) {
+            float2 n0, n1;
+            ld2(q.p + 2 + fo + cs * d, n0, n1);
+            acc[1][d] = zsub(acc[1][d], n0);
+        }
+    }
+#pragma unroll
+    for (int d = DN; d < DN + 2; d++) {
+        float2 c0, c1;
+        ld2(q.p + fo + cs * d, c0, c1);
+        if (q.s > 0) {
+            float2 p0, p1;
+            ld2(q.p - 2 + fo + cs * d, p0, p1);
+            acc[0][d] = zsub(acc[0][d], p1);
+        }
+        acc[1][d] = zsub(acc[1][d], c0);
+    }
+    // wall coupling: point 1 at s=Ls (pair WA, reads s=1), point 0 at s=1
+    // (pair WB, reads s=Ls)
+    constexpr int WA = DAG ? 0 : 2;
+    constexpr int WB = DAG ? 2 : 0;
+    const bool atL = (q.s + 2 == Ls), at0 = (q.s == 0);
+    if (!(atL || at0)) return;
+    const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
+                c3f = __ldg(chif + 2 * g.kvol + q.site);
+    const bool pin = (q.site == 0);
+    if (atL)
+        wall_terms<DAG, IMASS, WA, 0>(acc[1], LdF2{in}, cs, LsI * q.site, f, c1f, c2f, c3f, pin, hpin);
+    if (at0)
+        wall_terms<DAG, IMASS, WB, 1>(acc[0], LdF2{in}, cs, LsI * q.site + Ls - 1, f, c1f, c2f, c3f,
+                                      pin, hpin);
+}
+
 // Thread -> (point, flavour) map of the flavour-split kernels: a block of
 // kSplitThreads threads covers kSplitThreads/2 consecutive points, the first
 // half of its threads flavour 0 and the second half flavour 1, so every warp

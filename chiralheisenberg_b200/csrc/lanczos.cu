@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <type_traits>
 #include <utility>
 
 #include "dwf_stencil.cuh"
@@ -72,18 +73,24 @@ __device__ __forceinline__ bool block_stopped(const LzCtl* ctl) {
 // ---- thread mapping ----------------------------------------------------------
 // FP64 vectors: two threads per point, one per flavour (split_point /
 // split_flavour), which halves the accumulator registers and doubles the
-// warps in flight.  FP32 vectors: one thread per point and both flavours,
-// the faster shape when the registers already allow full occupancy.
-template <class T> struct LzShape;
-template <> struct LzShape<double2> {
+// warps in flight.  FP32 vectors with Ls even (PAIR): a thread takes two
+// adjacent points of one flavour, loading both with one 16-byte float4.
+// FP32 otherwise: one thread per point and both flavours.
+template <class T, bool PAIR = false> struct LzShape;
+template <> struct LzShape<double2, false> {
     static constexpr bool split = true;
     static constexpr int min_blocks = 3;          // <= 85 registers: no spills
     static constexpr int unit = kSplitPoints;     // points per block pass
 };
-template <> struct LzShape<float2> {
+template <> struct LzShape<float2, false> {
     static constexpr bool split = false;
     static constexpr int min_blocks = 3;          // <= 85 registers a thread
     static constexpr int unit = kThreads;
+};
+template <> struct LzShape<float2, true> {
+    static constexpr bool split = true;
+    static constexpr int min_blocks = 3;
+    static constexpr int unit = 2 * kSplitPoints; // 128 point pairs per flavour
 };
 
 // Pass 1 runs on a persistent grid (a whole number of blocks per SM); block b
@@ -100,16 +107,30 @@ __device__ __forceinline__ PtRange block_range(int64_t npts) {
     return r;
 }
 
-// One block pass over points [base, base + unit) of flavour(s) f0..f0+NF-1.
-template <class T>
+// One block pass over points [base, base + unit) of flavour(s) f0..f0+NF-1
+// (PAIR: p is the even point of the thread's pair).
+template <class T, bool PAIR = false>
 __device__ __forceinline__ void lz_lane(int64_t base, int64_t* p, int* f0) {
-    if (LzShape<T>::split) {
+    if (PAIR) {
+        *p = base + 2 * (threadIdx.x & (kSplitPoints - 1));
+        *f0 = split_flavour();
+    } else if (LzShape<T>::split) {
         *p = base + (threadIdx.x & (kSplitPoints - 1));
         *f0 = split_flavour();
     } else {
         *p = base + threadIdx.x;
         *f0 = 0;
     }
+}
+
+// 16-byte access to two adjacent FP32 complex numbers (e even).
+__device__ __forceinline__ void ld_pair(const float2* b, int64_t e, float2& v0, float2& v1) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(b + e));
+    v0 = make_float2(v.x, v.y);
+    v1 = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void st_pair(float2* b, int64_t e, float2 v0, float2 v1) {
+    *reinterpret_cast<float4*>(b + e) = make_float4(v0.x, v0.y, v1.x, v1.y);
 }
 
 // vt = M q_j with q_j = r_j / beta_j, formed as (1/beta_j) (M r_j): one
@@ -128,10 +149,11 @@ __device__ __forceinline__ void apply_scaled(T acc[4], const T* r, typename real
 // beta_j is the sum of the previous M^dagger launch's partials (beta_1 comes
 // from the source), formed by every block.  The partial buffers: part[0..nb)
 // for this kernel, part[nb..2nb) for M^dagger.
-template <class T, int IMASS>
-__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzArgsT<T> a) {
+template <class T, int IMASS, bool PAIR>
+__global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz1_M(LzArgsT<T> a) {
     typedef typename real_of<T>::type Real;
-    constexpr int NF = LzShape<T>::split ? 1 : 2;
+    typedef LzShape<T, PAIR> S;
+    constexpr int NF = S::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
     if (block_stopped(ctl)) return;
     const int j = ctl->it_m;
@@ -150,21 +172,35 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_M(LzAr
     const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
 #pragma unroll 1
-    for (int64_t base = R.begin; base < R.end; base += LzShape<T>::unit) {
+    for (int64_t base = R.begin; base < R.end; base += S::unit) {
         int64_t p;
         int f0;
-        lz_lane<T>(base, &p, &f0);
+        lz_lane<T, PAIR>(base, &p, &f0);
         if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
-#pragma unroll
-        for (int f = f0; f < f0 + NF; f++) {
-            T acc[4];
-            apply_scaled<false, IMASS>(acc, rj, ib, a, q, f);
+        if constexpr (PAIR) {
+            float2 acc[2][4];
+            dwf_apply_flavour_pair<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                 a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
-                a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
-                const double2 w = widen(acc[d]);
-                loc += w.x * w.x + w.y * w.y;
+                const float2 v0 = zscal(ib, acc[0][d]), v1 = zscal(ib, acc[1][d]);
+                st_pair(a.vt, p + a.g.cs * (d + 4 * f0), v0, v1);
+                const double2 w0 = widen(v0), w1 = widen(v1);
+                loc += w0.x * w0.x + w0.y * w0.y;
+                loc += w1.x * w1.x + w1.y * w1.y;
+            }
+        } else {
+#pragma unroll
+            for (int f = f0; f < f0 + NF; f++) {
+                T acc[4];
+                apply_scaled<false, IMASS>(acc, rj, ib, a, q, f);
+#pragma unroll
+                for (int d = 0; d < 4; d++) {
+                    a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
+                    const double2 w = widen(acc[d]);
+                    loc += w.x * w.x + w.y * w.y;
+                }
             }
         }
     }
@@ -254,11 +290,32 @@ __device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, in
     return v;
 }
 
+// The same update for the two points of an FP32 pair (elements e, e+1).
+__device__ __forceinline__ void three_term_pair(const LzArgsT<float2>& a, float2 x0, float2 x1,
+                                                int64_t e, int j, double alphat, float2& v0,
+                                                float2& v1) {
+    const float2* rj = ring(a, j);
+    const float2* rjm = ring(a, j - 1);
+    const float ib = (float)a.h.invbeta[j], at = (float)alphat, bj = (float)a.h.beta[j];
+    float2 c0, c1;
+    ld_pair(rj, e, c0, c1);
+    v0 = zsub(x0, zscal(at, zscal(ib, c0)));
+    v1 = zsub(x1, zscal(at, zscal(ib, c1)));
+    if (j > 1) {
+        const float ibm = (float)a.h.invbeta[j - 1];
+        float2 m0, m1;
+        ld_pair(rjm, e, m0, m1);
+        v0 = zsub(v0, zscal(bj, zscal(ibm, m0)));
+        v1 = zsub(v1, zscal(bj, zscal(ibm, m1)));
+    }
+}
+
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
 // alpha~_j is the sum of M(j)'s partials, formed by every block.
-template <class T, int IMASS>
-__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzArgsT<T> a) {
-    constexpr int NF = LzShape<T>::split ? 1 : 2;
+template <class T, int IMASS, bool PAIR>
+__global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz1_Md(LzArgsT<T> a) {
+    typedef LzShape<T, PAIR> S;
+    constexpr int NF = S::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
     if (block_stopped(ctl)) return;
     const int j = ctl->it_md;
@@ -268,24 +325,40 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzA
     const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
 #pragma unroll 1
-    for (int64_t base = R.begin; base < R.end; base += LzShape<T>::unit) {
+    for (int64_t base = R.begin; base < R.end; base += S::unit) {
         int64_t p;
         int f0;
-        lz_lane<T>(base, &p, &f0);
+        lz_lane<T, PAIR>(base, &p, &f0);
         if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
-#pragma unroll
-        for (int f = f0; f < f0 + NF; f++) {
-            T acc[4];
-            dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag,
-                                           a.hpin, a.apbc != 0);
+        if constexpr (PAIR) {
+            float2 acc[2][4];
+            dwf_apply_flavour_pair<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
-                const int64_t e = p + a.g.cs * (d + 4 * f);
-                const T v = three_term(a, acc[d], e, j, at);
-                rn[e] = v;
-                const double2 w = widen(v);
-                loc += w.x * w.x + w.y * w.y;
+                const int64_t e = p + a.g.cs * (d + 4 * f0);
+                float2 v0, v1;
+                three_term_pair(a, acc[0][d], acc[1][d], e, j, at, v0, v1);
+                st_pair(rn, e, v0, v1);
+                const double2 w0 = widen(v0), w1 = widen(v1);
+                loc += w0.x * w0.x + w0.y * w0.y;
+                loc += w1.x * w1.x + w1.y * w1.y;
+            }
+        } else {
+#pragma unroll
+            for (int f = f0; f < f0 + NF; f++) {
+                T acc[4];
+                dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag,
+                                               a.hpin, a.apbc != 0);
+#pragma unroll
+                for (int d = 0; d < 4; d++) {
+                    const int64_t e = p + a.g.cs * (d + 4 * f);
+                    const T v = three_term(a, acc[d], e, j, at);
+                    rn[e] = v;
+                    const double2 w = widen(v);
+                    loc += w.x * w.x + w.y * w.y;
+                }
             }
         }
     }
@@ -295,32 +368,15 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz1_Md(LzA
 }
 
 // ---- pass 2: regenerate q_j and accumulate --------------------------------
-// One block pass per block (grid lz_direct_blocks).
-template <class T, int IMASS, int IFLAG>
-__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_M(LzArgsT<T> a, int j,
-                                                                            int apply) {
-    typedef typename real_of<T>::type Real;
-    constexpr int NF = LzShape<T>::split ? 1 : 2;
-    int64_t p;
-    int f0;
-    lz_lane<T>((int64_t)blockIdx.x * LzShape<T>::unit, &p, &f0);
-    if (p >= a.g.npts) return;
-    const PointIdx q = point_of(a.g, p);
-    const Real ib = (Real)a.h.invbeta[j];
-    const T* rj = ring(a, j);
-    if (apply) {
-#pragma unroll
-        for (int f = f0; f < f0 + NF; f++) {
-            T acc[4];
-            apply_scaled<false, IMASS>(acc, rj, ib, a, q, f);
-#pragma unroll
-            for (int d = 0; d < 4; d++) a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
-        }
-    }
+// One block pass per block (grid lz_direct_blocks).  The solution update of
+// one element of x (iflag 0) or of the wall fields (iflag 1).
+template <class T, int IFLAG>
+__device__ __forceinline__ void lz2_accumulate(const LzArgsT<T>& a, int j, const T* rj,
+                                               typename real_of<T>::type ib, int64_t p,
+                                               const PointIdx& q, int c0, int nc) {
     if (IFLAG == 0) {
         const double cj = a.h.c[j];
-#pragma unroll
-        for (int c = 4 * f0; c < 4 * (f0 + NF); c++) {
+        for (int c = c0; c < c0 + nc; c++) {
             const int64_t e = p + a.g.cs * c;
             const double2 qj = widen(zscal(ib, __ldg(rj + e)));
             double2 xv = a.x[e];
@@ -335,15 +391,17 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_M(LzAr
         const int64_t cs2 = 2 * (int64_t)a.g.kvol, kf2 = 8 * cs2;
         const int64_t H = kMaxIter + 2;
         const int n = a.npole;
-        double2 qv[4 * NF];
+        double2 qv[8];
 #pragma unroll
-        for (int c = 0; c < 4 * NF; c++) qv[c] = widen(zscal(ib, __ldg(rj + p + a.g.cs * (c + 4 * f0))));
-        const int64_t base = sw + 2 * (int64_t)q.site + cs2 * (4 * f0);
+        for (int c = 0; c < 8; c++)
+            if (c < nc) qv[c] = widen(zscal(ib, __ldg(rj + p + a.g.cs * (c + c0))));
+        const int64_t base = sw + 2 * (int64_t)q.site + cs2 * c0;
         for (int k = 0; k < n; k++) {
             const double y = a.h.y[k * H + j];
             double2* xk = a.xw + k * kf2 + base;
 #pragma unroll
-            for (int c = 0; c < 4 * NF; c++) {
+            for (int c = 0; c < 8; c++) {
+                if (c >= nc) break;
                 double2 xv = xk[cs2 * c];
                 xv.x += y * qv[c].x;
                 xv.y += y * qv[c].y;
@@ -353,44 +411,98 @@ __global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_M(LzAr
     }
 }
 
-template <class T, int IMASS>
-__global__ void __launch_bounds__(kThreads, LzShape<T>::min_blocks) k_lz2_Md(LzArgsT<T> a, int j) {
-    constexpr int NF = LzShape<T>::split ? 1 : 2;
+template <class T, int IMASS, int IFLAG, bool PAIR>
+__global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks))
+    k_lz2_M(LzArgsT<T> a, int j, int apply) {
+    typedef typename real_of<T>::type Real;
+    typedef LzShape<T, PAIR> S;
+    constexpr int NF = S::split ? 1 : 2;
     int64_t p;
     int f0;
-    lz_lane<T>((int64_t)blockIdx.x * LzShape<T>::unit, &p, &f0);
+    lz_lane<T, PAIR>((int64_t)blockIdx.x * S::unit, &p, &f0);
+    if (p >= a.g.npts) return;
+    const PointIdx q = point_of(a.g, p);
+    const Real ib = (Real)a.h.invbeta[j];
+    const T* rj = ring(a, j);
+    if constexpr (PAIR) {
+        if (apply) {
+            float2 acc[2][4];
+            dwf_apply_flavour_pair<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                 a.apbc != 0);
+#pragma unroll
+            for (int d = 0; d < 4; d++)
+                st_pair(a.vt, p + a.g.cs * (d + 4 * f0), zscal(ib, acc[0][d]), zscal(ib, acc[1][d]));
+        }
+        lz2_accumulate<T, IFLAG>(a, j, rj, ib, p, q, 4 * f0, 4);
+        const PointIdx q1 = point_of(a.g, p + 1);
+        lz2_accumulate<T, IFLAG>(a, j, rj, ib, p + 1, q1, 4 * f0, 4);
+    } else {
+        if (apply) {
+#pragma unroll
+            for (int f = f0; f < f0 + NF; f++) {
+                T acc[4];
+                apply_scaled<false, IMASS>(acc, rj, ib, a, q, f);
+#pragma unroll
+                for (int d = 0; d < 4; d++) a.vt[p + a.g.cs * (d + 4 * f)] = acc[d];
+            }
+        }
+        lz2_accumulate<T, IFLAG>(a, j, rj, ib, p, q, 4 * f0, 4 * NF);
+    }
+}
+
+template <class T, int IMASS, bool PAIR>
+__global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks))
+    k_lz2_Md(LzArgsT<T> a, int j) {
+    typedef LzShape<T, PAIR> S;
+    constexpr int NF = S::split ? 1 : 2;
+    int64_t p;
+    int f0;
+    lz_lane<T, PAIR>((int64_t)blockIdx.x * S::unit, &p, &f0);
     if (p >= a.g.npts) return;
     const PointIdx q = point_of(a.g, p);
     T* rn = ring(a, j + 1);
-#pragma unroll
-    for (int f = f0; f < f0 + NF; f++) {
-        T acc[4];
-        dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag, a.hpin,
-                                       a.apbc != 0);
+    if constexpr (PAIR) {
+        float2 acc[2][4];
+        dwf_apply_flavour_pair<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                            a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
-            const int64_t e = p + a.g.cs * (d + 4 * f);
-            rn[e] = three_term(a, acc[d], e, j, a.h.alphat[j]);
+            const int64_t e = p + a.g.cs * (d + 4 * f0);
+            float2 v0, v1;
+            three_term_pair(a, acc[0][d], acc[1][d], e, j, a.h.alphat[j], v0, v1);
+            st_pair(rn, e, v0, v1);
+        }
+    } else {
+#pragma unroll
+        for (int f = f0; f < f0 + NF; f++) {
+            T acc[4];
+            dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag,
+                                           a.hpin, a.apbc != 0);
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const int64_t e = p + a.g.cs * (d + 4 * f);
+                rn[e] = three_term(a, acc[d], e, j, a.h.alphat[j]);
+            }
         }
     }
 }
 
-template <class T>
+template <class T, bool PAIR = false>
 static unsigned lz_direct_blocks(int64_t npts) {
-    return (unsigned)((npts + LzShape<T>::unit - 1) / LzShape<T>::unit);
+    return (unsigned)((npts + LzShape<T, PAIR>::unit - 1) / LzShape<T, PAIR>::unit);
 }
 
 // Persistent pass-1 grid: the resident blocks of both pass-1 kernels on all
 // SMs, at most one block pass per block.
-template <class T, int IMASS>
+template <class T, int IMASS, bool PAIR>
 static unsigned lz_pass1_blocks(int64_t npts) {
     int dev = 0, nsm = 0, b1 = 0, b2 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lz1_M<T, IMASS>, kThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lz1_M<T, IMASS, PAIR>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS, PAIR>, kThreads, 0);
     int64_t nb = (int64_t)nsm * (b1 < b2 ? b1 : b2);
-    const int64_t direct = lz_direct_blocks<T>(npts);
+    const int64_t direct = lz_direct_blocks<T, PAIR>(npts);
     if (nb < 1 || nb > direct) nb = direct;
     return (unsigned)nb;
 }
@@ -471,14 +583,14 @@ __global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* part, int nb) {
     }
 }
 
-template <class T, int IMASS>
+template <class T, int IMASS, bool PAIR>
 static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
                          KernelTimer* tm) {
     // algorithmic bytes: M reads q, writes vt; M^dagger reads vt, r_j, r_{j-1}
     // and writes r_{j+1}; both read chi as REAL*4
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     if (tm) tm->begin(0, st, 2 * V + chi);
-    k_lz1_M<T, IMASS><<<nb, kThreads, 0, st>>>(a);
+    k_lz1_M<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
     // the scalar step of iteration j on the side stream, beside M^dagger(j)
     cudaEventRecord(side.fork, st);
@@ -486,7 +598,7 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
     k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
     cudaEventRecord(side.join, side.stream);
     if (tm) tm->begin(1, st, 4 * V + chi);
-    k_lz1_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a);
+    k_lz1_Md<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
     cudaStreamWaitEvent(st, side.join, 0);
 }
@@ -534,6 +646,10 @@ static void set_stream_window(cudaStream_t st, const cudaAccessPolicyWindow& w) 
 // as a CUDA graph and replayed; the graph is rebuilt when any argument
 // changes.
 template <class T>
+static void launch_pass1_any(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
+                             KernelTimer* tm, int imass);
+
+template <class T>
 static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned nb, int imass,
                                    int chunk, cudaStream_t st, const cudaAccessPolicyWindow& win) {
     // pass-1 kernels never touch the pass-2 fields: clear them so one graph
@@ -555,8 +671,7 @@ static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned n
         return nullptr;
     }
     for (int c = 0; c < chunk; c++) {
-        if (imass == 3) launch_pass1<T, 3>(a, nb, st, w.side, nullptr);
-        else launch_pass1<T, 1>(a, nb, st, w.side, nullptr);
+        launch_pass1_any<T>(a, nb, st, w.side, nullptr, imass);
     }
     if (cudaStreamEndCapture(st, &graph) != cudaSuccess || !graph) {
         cudaGetLastError();
@@ -592,24 +707,67 @@ static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned n
     return exec;
 }
 
-template <class T, int IMASS>
+template <class T, int IMASS, bool PAIR>
 static void launch_pass2(const LzArgsT<T>& a, int j, int m, int iflag, cudaStream_t st,
                          KernelTimer& tm) {
-    const unsigned nb = lz_direct_blocks<T>(a.g.npts);
+    const unsigned nb = lz_direct_blocks<T, PAIR>(a.g.npts);
     const int apply = j < m;
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     const double acc = iflag == 0 ? 2.0 * a.g.kferm * sizeof(double2) + V : 0.0;
     if (apply) tm.begin(3, st, 2 * V + chi + acc);
-    if (iflag == 0) k_lz2_M<T, IMASS, 0><<<nb, kThreads, 0, st>>>(a, j, apply);
-    else k_lz2_M<T, IMASS, 1><<<nb, kThreads, 0, st>>>(a, j, apply);
+    if (iflag == 0) k_lz2_M<T, IMASS, 0, PAIR><<<nb, kThreads, 0, st>>>(a, j, apply);
+    else k_lz2_M<T, IMASS, 1, PAIR><<<nb, kThreads, 0, st>>>(a, j, apply);
     count_launches(1);
     if (apply) {
         tm.end(st);
         tm.begin(3, st, 4 * V + chi);
-        k_lz2_Md<T, IMASS><<<nb, kThreads, 0, st>>>(a, j);
+        k_lz2_Md<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a, j);
         tm.end(st);
         count_launches(1);
     }
+}
+
+// Shape dispatch: FP32 vectors with Ls even take the two-point kernels.
+template <class T>
+static bool lz_pair(const Geom& g) {
+    return std::is_same<T, float2>::value && g.Ls % 2 == 0;
+}
+
+template <class T>
+static void launch_pass1_any(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
+                             KernelTimer* tm, int imass) {
+    if constexpr (std::is_same<T, float2>::value) {
+        if (lz_pair<T>(a.g)) {
+            if (imass == 3) launch_pass1<T, 3, true>(a, nb, st, side, tm);
+            else launch_pass1<T, 1, true>(a, nb, st, side, tm);
+            return;
+        }
+    }
+    if (imass == 3) launch_pass1<T, 3, false>(a, nb, st, side, tm);
+    else launch_pass1<T, 1, false>(a, nb, st, side, tm);
+}
+
+template <class T>
+static void launch_pass2_any(const LzArgsT<T>& a, int j, int m, int iflag, cudaStream_t st,
+                             KernelTimer& tm, int imass) {
+    if constexpr (std::is_same<T, float2>::value) {
+        if (lz_pair<T>(a.g)) {
+            if (imass == 3) launch_pass2<T, 3, true>(a, j, m, iflag, st, tm);
+            else launch_pass2<T, 1, true>(a, j, m, iflag, st, tm);
+            return;
+        }
+    }
+    if (imass == 3) launch_pass2<T, 3, false>(a, j, m, iflag, st, tm);
+    else launch_pass2<T, 1, false>(a, j, m, iflag, st, tm);
+}
+
+template <class T>
+static unsigned lz_pass1_blocks_any(const Geom& g, int imass) {
+    if constexpr (std::is_same<T, float2>::value) {
+        if (lz_pair<T>(g))
+            return imass == 3 ? lz_pass1_blocks<T, 3, true>(g.npts) : lz_pass1_blocks<T, 1, true>(g.npts);
+    }
+    return imass == 3 ? lz_pass1_blocks<T, 3, false>(g.npts) : lz_pass1_blocks<T, 1, false>(g.npts);
 }
 
 // ---- kernel timer ----------------------------------------------------------
@@ -881,7 +1039,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.x = x;
     a.xw = w.xw;
     a.npole = ndiag;
-    const unsigned nb = imass == 3 ? lz_pass1_blocks<T, 3>(g.npts) : lz_pass1_blocks<T, 1>(g.npts);
+    const unsigned nb = lz_pass1_blocks_any<T>(g, imass);
     const int nbr = reduce_blocks(g.kferm);
     // r_1 lives where ring(a, 1) looks for it: the basis store when present
     T* r1 = a.hcap > 1 ? a.basis + g.kferm : a.rb1;
@@ -911,8 +1069,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
             count_launches(3 * chunk);
         } else {
             for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
-                if (imass == 3) launch_pass1<T, 3>(a, nb, st, w.side, &w.timer);
-                else launch_pass1<T, 1>(a, nb, st, w.side, &w.timer);
+                launch_pass1_any<T>(a, nb, st, w.side, &w.timer, imass);
                 count_launches(3);
             }
         }
@@ -989,8 +1146,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         w.timer.end(st);
     } else {
         for (int j = 1; j <= m; j++) {
-            if (imass == 3) launch_pass2<T, 3>(a, j, m, iflag, st, w.timer);
-            else launch_pass2<T, 1>(a, j, m, iflag, st, w.timer);
+            launch_pass2_any<T>(a, j, m, iflag, st, w.timer, imass);
             if (w.timer.enabled && w.timer.used >= KernelTimer::kPool - 2) {
                 cudaStreamSynchronize(st);
                 w.timer.collect();

@@ -69,3 +69,29 @@ def test_mixed_precision_trajectory(remez):
     for a, b in zip(recs["f64"], recs["f32"]):
         assert a.nsteps == b.nsteps and a.accepted == b.accepted
         assert abs(a.dH - b.dH) <= 1e-8 * abs(a.H0), (a.dH, b.dH)
+
+
+@pytest.mark.parametrize("Ls", [5, 6])
+@pytest.mark.parametrize("store", [-1.0, 0.0])
+def test_mixed_force_thread_shapes(remez, Ls, store):
+    """The FP32 force solves on both of their thread shapes -- two adjacent
+    points per thread (Ls even) and one point with both flavours (Ls odd) --
+    with pass 2 from the stored basis (store < 0) and by regenerating the
+    vectors (store 0): the FP64 chain's decisions, dH within 1e-8 of H."""
+    L, Lt = 6, 6
+    beta = 0.475
+    chi = np.random.default_rng(99).standard_normal((3, L * L * Lt)) / np.sqrt(beta)
+    recs = {}
+    for mode in ("f64", "f32"):
+        prog = chb.Program(L, Lt, Ls, 0.1, beta, 1.0, 0.01, 0.0, 1, 5, remez["remez2"],
+                           remez["remez4"], remez["remez2g"])
+        prog.set_basis_store(store)
+        prog.set_chi(chi)
+        prog.startup(693764523745.0)
+        prog.set_measure(5, False)
+        prog.set_precision(md=mode, accept="f64")
+        recs[mode] = [prog.sweep() for _ in range(2)]
+        prog.close()
+    for a, b in zip(recs["f64"], recs["f32"]):
+        assert a.nsteps == b.nsteps and a.accepted == b.accepted
+        assert abs(a.dH - b.dH) <= 1e-8 * abs(a.H0), (a.dH, b.dH)
