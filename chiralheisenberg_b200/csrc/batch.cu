@@ -71,33 +71,35 @@ __device__ __forceinline__ bool sys_last_block(double v, double* part, unsigned*
 }
 
 template <bool DAG>
-__device__ __forceinline__ void apply_sys(double2 acc[2][4], const double2* in, const BSys& S,
-                                          const PointIdx& q, const float* chif) {
+__device__ __forceinline__ void apply_sys(double2 acc[4], const double2* in, const BSys& S,
+                                          const PointIdx& q, int f, const float* chif) {
     if (S.imass == 3)
-        dwf_apply_point<DAG, 3>(acc, LdB{in}, S.g, q, chif, S.diag, S.hpin, S.apbc != 0);
+        dwf_apply_flavour<DAG, 3>(acc, LdB{in}, S.g, q, f, chif, S.diag, S.hpin, S.apbc != 0);
     else
-        dwf_apply_point<DAG, 1>(acc, LdB{in}, S.g, q, chif, S.diag, S.hpin, S.apbc != 0);
+        dwf_apply_flavour<DAG, 1>(acc, LdB{in}, S.g, q, f, chif, S.diag, S.hpin, S.apbc != 0);
 }
 
 // x1 = M p ; alphad = |x1|^2 ; alpha = alphan/alphad (rhmc/cheisdwf.f:1093-1117)
-__global__ void __launch_bounds__(kThreads) k_bcg1(BArgs a) {
+// Flavour-split stencil kernels: a system's point blocks cover
+// kSplitPoints points each, two threads per point.
+__global__ void __launch_bounds__(kSplitThreads, 2) k_bcg1(BArgs a) {
     const int s = a.blk2sys[blockIdx.x];
     const BSys S = a.sys[s];
     CgCtl* c = a.ctl + s;
     if (c->done) return;
-    const int64_t p = (int64_t)(blockIdx.x - S.blk0) * blockDim.x + threadIdx.x;
+    const int64_t p = (int64_t)(blockIdx.x - S.blk0) * kSplitPoints +
+                      (threadIdx.x & (kSplitPoints - 1));
+    const int f = split_flavour();
     double loc = 0.0;
     if (p < S.g.npts) {
         const PointIdx q = point_of(S.g, p);
-        double2 acc[2][4];
-        apply_sys<false>(acc, a.p + S.off, S, q, a.chif + S.chioff);
+        double2 acc[4];
+        apply_sys<false>(acc, a.p + S.off, S, q, f, a.chif + S.chioff);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
-#pragma unroll
-            for (int d = 0; d < 4; d++) {
-                a.x1[S.off + p + S.g.cs * (d + 4 * f)] = acc[f][d];
-                loc += acc[f][d].x * acc[f][d].x + acc[f][d].y * acc[f][d].y;
-            }
+        for (int d = 0; d < 4; d++) {
+            a.x1[S.off + p + S.g.cs * (d + 4 * f)] = acc[d];
+            loc += acc[d].x * acc[d].x + acc[d].y * acc[d].y;
+        }
     }
     double tot;
     if (!sys_last_block(loc, a.part, &c->count1, S.blk0, S.nblk, &tot)) return;
@@ -105,29 +107,29 @@ __global__ void __launch_bounds__(kThreads) k_bcg1(BArgs a) {
 }
 
 // x2 = M^dagger x1 ; x += alpha p ; r -= alpha x2 ; betan = |r|^2 (:1119-1141)
-__global__ void __launch_bounds__(kThreads) k_bcg2(BArgs a) {
+__global__ void __launch_bounds__(kSplitThreads, 2) k_bcg2(BArgs a) {
     const int s = a.blk2sys[blockIdx.x];
     const BSys S = a.sys[s];
     CgCtl* c = a.ctl + s;
     if (c->done) return;
     const int nx = c->nx;
     const double alpha = (double)c->alpha;
-    const int64_t p = (int64_t)(blockIdx.x - S.blk0) * blockDim.x + threadIdx.x;
+    const int64_t p = (int64_t)(blockIdx.x - S.blk0) * kSplitPoints +
+                      (threadIdx.x & (kSplitPoints - 1));
+    const int f = split_flavour();
     double loc = 0.0;
     if (p < S.g.npts) {
         const PointIdx q = point_of(S.g, p);
-        double2 acc[2][4];
-        apply_sys<true>(acc, a.x1 + S.off, S, q, a.chif + S.chioff);
+        double2 acc[4];
+        apply_sys<true>(acc, a.x1 + S.off, S, q, f, a.chif + S.chioff);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
-#pragma unroll
-            for (int d = 0; d < 4; d++) {
-                const int64_t e = p + S.g.cs * (d + 4 * f);
-                if (nx > 1) S.x[e] = zadd(S.x[e], zscal(alpha, a.p[S.off + e]));
-                const double2 r = zsub(a.r[S.off + e], zscal(alpha, acc[f][d]));
-                a.r[S.off + e] = r;
-                loc += r.x * r.x + r.y * r.y;
-            }
+        for (int d = 0; d < 4; d++) {
+            const int64_t e = p + S.g.cs * (d + 4 * f);
+            if (nx > 1) S.x[e] = zadd(S.x[e], zscal(alpha, a.p[S.off + e]));
+            const double2 r = zsub(a.r[S.off + e], zscal(alpha, acc[d]));
+            a.r[S.off + e] = r;
+            loc += r.x * r.x + r.y * r.y;
+        }
     }
     double tot;
     if (!sys_last_block(loc, a.part, &c->count2, S.blk0, S.nblk, &tot)) return;
@@ -247,7 +249,7 @@ extern "C" int chdwf_congrad_batch(chdwf_ctx* ctx, const chdwf_cg_system* in, in
         b.apbc = s.ibound == -1;
         b.imass = s.imass;
         b.blk0 = (int)b2s.size();
-        b.nblk = (int)((b.g.npts + kThreads - 1) / kThreads);
+        b.nblk = (int)split_blocks(b.g.npts);
         for (int k = 0; k < b.nblk; k++) b2s.push_back(i);
         b.eblk0 = (int)e2s.size();
         b.neblk = (int)((b.g.kferm + kThreads - 1) / kThreads);

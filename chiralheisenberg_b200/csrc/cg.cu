@@ -41,24 +41,26 @@ __device__ __forceinline__ bool cg_last_block(double v, double* part, unsigned* 
     return true;
 }
 
+// The stencil kernels are flavour-split: two threads per point (one per
+// flavour), grid split_blocks(npts).
 // x1 = M p ; alphad = |x1|^2 ; alpha = alphan/alphad   (:1093-1117)
 template <int IMASS>
-__global__ void __launch_bounds__(kThreads) k_cg1(CgArgs a) {
+__global__ void __launch_bounds__(kSplitThreads, 3) k_cg1(CgArgs a) {
     CgCtl* c = a.ctl;
     if (c->done) return;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t p = split_point();
+    const int f = split_flavour();
     double loc = 0.0;
     if (p < a.g.npts) {
         const PointIdx q = point_of(a.g, p);
-        double2 acc[2][4];
-        dwf_apply_point<false, IMASS>(acc, LdCg{a.p}, a.g, q, a.chif, a.diag, a.hpin, a.apbc != 0);
+        double2 acc[4];
+        dwf_apply_flavour<false, IMASS>(acc, LdCg{a.p}, a.g, q, f, a.chif, a.diag, a.hpin,
+                                        a.apbc != 0);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
-#pragma unroll
-            for (int d = 0; d < 4; d++) {
-                a.x1[p + a.g.cs * (d + 4 * f)] = acc[f][d];
-                loc += acc[f][d].x * acc[f][d].x + acc[f][d].y * acc[f][d].y;
-            }
+        for (int d = 0; d < 4; d++) {
+            a.x1[p + a.g.cs * (d + 4 * f)] = acc[d];
+            loc += acc[d].x * acc[d].x + acc[d].y * acc[d].y;
+        }
     }
     double tot;
     if (!cg_last_block(loc, a.part, &c->count1, &tot)) return;
@@ -70,27 +72,27 @@ __global__ void __launch_bounds__(kThreads) k_cg1(CgArgs a) {
 
 // x2 = M^dagger x1 ; x += alpha p (nx>1) ; r -= alpha x2 ; betan = |r|^2 (:1119-1141)
 template <int IMASS>
-__global__ void __launch_bounds__(kThreads) k_cg2(CgArgs a) {
+__global__ void __launch_bounds__(kSplitThreads, 3) k_cg2(CgArgs a) {
     CgCtl* c = a.ctl;
     if (c->done) return;
     const int nx = c->nx;
     const double alpha = (double)c->alpha;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t p = split_point();
+    const int f = split_flavour();
     double loc = 0.0;
     if (p < a.g.npts) {
         const PointIdx q = point_of(a.g, p);
-        double2 acc[2][4];
-        dwf_apply_point<true, IMASS>(acc, LdCg{a.x1}, a.g, q, a.chif, a.diag, a.hpin, a.apbc != 0);
+        double2 acc[4];
+        dwf_apply_flavour<true, IMASS>(acc, LdCg{a.x1}, a.g, q, f, a.chif, a.diag, a.hpin,
+                                       a.apbc != 0);
 #pragma unroll
-        for (int f = 0; f < 2; f++)
-#pragma unroll
-            for (int d = 0; d < 4; d++) {
-                const int64_t e = p + a.g.cs * (d + 4 * f);
-                if (nx > 1) a.x[e] = zadd(a.x[e], zscal(alpha, a.p[e]));
-                const double2 r = zsub(a.r[e], zscal(alpha, acc[f][d]));
-                a.r[e] = r;
-                loc += r.x * r.x + r.y * r.y;
-            }
+        for (int d = 0; d < 4; d++) {
+            const int64_t e = p + a.g.cs * (d + 4 * f);
+            if (nx > 1) a.x[e] = zadd(a.x[e], zscal(alpha, a.p[e]));
+            const double2 r = zsub(a.r[e], zscal(alpha, acc[d]));
+            a.r[e] = r;
+            loc += r.x * r.x + r.y * r.y;
+        }
     }
     double tot;
     if (!cg_last_block(loc, a.part, &c->count2, &tot)) return;
@@ -146,7 +148,7 @@ cudaError_t CgWork::ensure(const Geom& g) {
     geom = g;
     cudaError_t e;
     if ((e = cudaMalloc(&ctl, sizeof(CgCtl)))) return e;
-    const int64_t nb = (g.npts + kThreads - 1) / kThreads;
+    const int64_t nb = split_blocks(g.npts);
     if ((e = cudaMalloc(&part, sizeof(double) * (nb + 64)))) return e;
     if ((e = cudaMalloc(&x1, sizeof(double2) * g.kferm))) return e;
     if ((e = cudaMalloc(&p, sizeof(double2) * g.kferm))) return e;
@@ -184,7 +186,7 @@ cudaError_t cg_solve(CgWork& w, const Geom& g, const double2* phi, float res, co
     a.ctl = w.ctl;
     a.part = w.part;
     a.hflag = w.hflag_dev;
-    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const unsigned nb = split_blocks(g.npts);
     const unsigned nbf = (unsigned)((g.kferm + kThreads - 1) / kThreads);
     const int chunk = 16;
     cudaEvent_t ev[2];
@@ -289,7 +291,7 @@ extern "C" int chdwf_congrad_static(const void* Phi, void* x, const void* chi, i
     a.ctl = ctl;
     a.part = part;
     a.hflag = nullptr;
-    const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
+    const unsigned nb = split_blocks(g.npts);
     const unsigned nbf = (unsigned)((g.kferm + kThreads - 1) / kThreads);
     // chunks of 16 iterations; the done flag is copied into a host stack
     // variable after each chunk (launches after convergence return at once)

@@ -78,8 +78,43 @@ __global__ void __launch_bounds__(kThreads) k_dslash_lp(void* __restrict__ out,
         }
 }
 
+// FP32 storage with Ls even: a thread takes two adjacent points of one
+// flavour with 16-byte loads (dwf_apply_flavour_pair); a block covers 128
+// point pairs of both flavours.
+template <bool DAG, int IMASS>
+__global__ void __launch_bounds__(kSplitThreads, 3)
+    k_dslash_f32_pair(float2* __restrict__ out, const float2* __restrict__ in,
+                      const float* __restrict__ chif, Geom g, float diag, float hpin, int apbc) {
+    const int64_t p = (int64_t)blockIdx.x * (2 * kSplitPoints) +
+                      2 * (threadIdx.x & (kSplitPoints - 1));
+    const int f = split_flavour();
+    if (p >= g.npts) return;
+    const PointIdx q = point_of(g, p);
+    float2 acc[2][4];
+    dwf_apply_flavour_pair<DAG, IMASS>(acc, in, g, q, f, chif, diag, hpin, apbc != 0);
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const int64_t e = p + g.cs * (d + 4 * f);
+        *reinterpret_cast<float4*>(out + e) =
+            make_float4(acc[0][d].x, acc[0][d].y, acc[1][d].x, acc[1][d].y);
+    }
+}
+
 void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
                       const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
+    if (!half && g.Ls % 2 == 0) {
+        const unsigned nb2 = (unsigned)((g.npts + 2 * kSplitPoints - 1) / (2 * kSplitPoints));
+        const float diag = diag_of(am3);
+        const int apbc = ibound == -1;
+        float2* o = (float2*)out;
+        const float2* i = (const float2*)in;
+#define PR(D, I) k_dslash_f32_pair<D, I><<<nb2, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
+        if (!dag) { if (imass == 3) PR(false, 3); else PR(false, 1); }
+        else { if (imass == 3) PR(true, 3); else PR(true, 1); }
+#undef PR
+        count_launches(1);
+        return;
+    }
     const unsigned nb = (unsigned)((g.npts + kThreads - 1) / kThreads);
     const float diag = diag_of(am3);
     const int apbc = ibound == -1;

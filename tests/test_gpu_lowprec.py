@@ -39,8 +39,11 @@ def _lp_apply(gl, R, chi, prec, dag, hpin=0.3):
 
 @pytest.mark.parametrize("prec,tol", [(1, 1e-6), (2, 2e-3)])
 @pytest.mark.parametrize("dag", [False, True])
-def test_operator_reduced_precision(prec, tol, dag):
-    L, Lt, Ls = 8, 8, 8
+@pytest.mark.parametrize("Ls", [8, 5])
+def test_operator_reduced_precision(prec, tol, dag, Ls):
+    """FP32 storage takes the two-point kernel when Ls is even and the
+    one-point kernel when it is odd; FP16 always the one-point kernel."""
+    L, Lt = 8, 8
     R, chi = random_fields(L, Lt, Ls, seed=31)
     lat = po.make_lat(L, Lt, Ls)
     ref = po.dslash(lat, R, chi, hpin=0.3, imass=1, dag=dag)
