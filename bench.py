@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--Ls", type=int, default=24)
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clock-interval-ms", type=int, default=200,
+                    help="nvidia-smi sampling interval during the timed region")
     ap.add_argument("--operator-sweep", action="store_true",
                     help="operator GB/s over L in {16,24,32,48}, Ls in {16,24,32}, FP64/FP32/FP16")
     ap.add_argument("--profile-solve", action="store_true",
@@ -87,8 +89,9 @@ def peaks():
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=200):
         self.gpu = gpu_index
+        self.interval = interval_ms
         self.proc = None
         self.lines = []
 
@@ -99,7 +102,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.interval)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
@@ -407,14 +410,15 @@ def run_b200(args, rank, world, local_rank):
         recs = []
         barrier()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ev[0].record(stream)
+        for k in range(args.steps):
             recs.append(prog.sweep())
-        e1.record(stream)
+            ev[k + 1].record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1)
+        ms = ev[0].elapsed_time(ev[-1])
+        timed.per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
         t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
         if world > 1:
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -425,15 +429,17 @@ def run_b200(args, rank, world, local_rank):
     # before the second
     chi0 = prog.get_chi()
     state0 = prog.get_state()
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(local_rank, args.clock_interval_ms)
     clocks.start()
     n0 = chb.kernel_launches()
     ms_value, recs = timed(staged=True)
+    step_ms_value = list(timed.per_step)
     launches = chb.kernel_launches() - n0
     clk = clocks.stop()
     prog.set_chi(chi0)
     prog.set_state(state0)
     ms_e2e, recs_e2e = timed(staged=False)
+    step_ms_e2e = list(timed.per_step)
     same = all(a.nsteps == b.nsteps and a.accepted == b.accepted and a.dH == b.dH
                for a, b in zip(recs, recs_e2e))
     mixed = None
@@ -488,13 +494,15 @@ def run_b200(args, rank, world, local_rank):
             "nforce": float(np.mean([r.nforce for r in recs]))}
     line = {"metric": "s/trajectory", "value": value, "unit": "s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_value / args.steps,
+            "step_ms": [round(x, 1) for x in step_ms_value],
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": f"RHMC trajectory L=Lt={L} Ls={Ls}", "precision": "fp64",
                        "parallelism": f"replicas{world}", "l2": "fields larger than L2 "
                        "(solver working set > 126 MB)", **CFG},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "same_trajectories_as_value": same},
+                    "d2h_bytes_per_step": d2h, "same_trajectories_as_value": same,
+                    "step_ms": [round(x, 1) for x in step_ms_e2e]},
             "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "what": KERNEL_WHAT[dom],
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

@@ -39,6 +39,10 @@ struct Draws {                       // the random numbers of one trajectory
 
 struct Staged {                      // a trajectory's random inputs already in HBM
     Draws d;
+    int slot = -1;                   // its device buffers in the driver's pool
+};
+
+struct StageSlot {                   // device buffers for one staged trajectory
     float* gauss_dev = nullptr;
     float* pp_dev = nullptr;
 };
@@ -58,6 +62,35 @@ struct chdwf_prog {
     int cg_caps = 0;                 // congrad iteration caps not yet reported
     std::string err;
     chdwf::Rng::State last_state{};  // generator after the last completed sweep
+    // Device buffers of staged trajectories, allocated on first use and
+    // reused: a sweep never allocates or frees device memory.
+    std::vector<StageSlot> pool;
+    std::vector<int> free_slots;
+
+    int take_slot() {
+        if (!free_slots.empty()) {
+            const int k = free_slots.back();
+            free_slots.pop_back();
+            return k;
+        }
+        StageSlot sl;
+        if (cudaMalloc(&sl.gauss_dev, sizeof(float) * 16 * (size_t)kvol * Ls) ||
+            cudaMalloc(&sl.pp_dev, sizeof(float) * 3 * (size_t)kvol)) {
+            cudaFree(sl.gauss_dev);
+            cudaGetLastError();
+            return -1;
+        }
+        pool.push_back(sl);
+        return (int)pool.size() - 1;
+    }
+    void release_pool() {
+        for (StageSlot& sl : pool) {
+            cudaFree(sl.gauss_dev);
+            cudaFree(sl.pp_dev);
+        }
+        pool.clear();
+        free_slots.clear();
+    }
 
     // Drop prefetched or staged draws and rewind the generator to the end
     // of the last completed sweep, so the stream continues exactly there.
@@ -66,10 +99,8 @@ struct chdwf_prog {
             next.wait();
             have_next = false;
         }
-        for (Staged& s : staged) {
-            cudaFree(s.gauss_dev);
-            cudaFree(s.pp_dev);
-        }
+        for (Staged& s : staged)
+            if (s.slot >= 0) free_slots.push_back(s.slot);
         staged.clear();
         rng.set_state(last_state);
     }
@@ -203,10 +234,7 @@ int chdwf_prog_create(chdwf_prog** out, int ksize, int ksizet, int kthird, float
 void chdwf_prog_destroy(chdwf_prog* p) {
     if (!p) return;
     if (p->have_next) p->next.wait();
-    for (Staged& s : p->staged) {
-        cudaFree(s.gauss_dev);
-        cudaFree(s.pp_dev);
-    }
+    p->release_pool();
     chdwf_destroy(p->ctx);
     delete p;
 }
@@ -229,13 +257,13 @@ int chdwf_prog_stage(chdwf_prog* p, int ntraj) {
         p->staged.push_back(std::move(s));
     }
     for (Staged& s : p->staged) {
-        if (s.gauss_dev) continue;
-        if (cudaMalloc(&s.gauss_dev, sizeof(float) * s.d.gauss.size()) ||
-            cudaMalloc(&s.pp_dev, sizeof(float) * s.d.pp.size()))
-            return CHDWF_CUDA_ERROR;
-        cudaMemcpy(s.gauss_dev, s.d.gauss.data(), sizeof(float) * s.d.gauss.size(),
+        if (s.slot >= 0) continue;
+        s.slot = p->take_slot();
+        if (s.slot < 0) return CHDWF_CUDA_ERROR;
+        const StageSlot& sl = p->pool[s.slot];
+        cudaMemcpy(sl.gauss_dev, s.d.gauss.data(), sizeof(float) * s.d.gauss.size(),
                    cudaMemcpyHostToDevice);
-        cudaMemcpy(s.pp_dev, s.d.pp.data(), sizeof(float) * s.d.pp.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(sl.pp_dev, s.d.pp.data(), sizeof(float) * s.d.pp.size(), cudaMemcpyHostToDevice);
     }
     return cudaDeviceSynchronize() == cudaSuccess ? CHDWF_OK : CHDWF_CUDA_ERROR;
 }
@@ -342,15 +370,17 @@ int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
     }
     Draws& d = stg.d;
     p->last_state = d.state_after;
-    struct Free {
-        Staged& s;
-        ~Free() { if (s.gauss_dev) { cudaFree(s.gauss_dev); cudaFree(s.pp_dev); } }
-    } free_guard{stg};
+    struct Back {                    // the slot returns to the pool, whatever the outcome
+        chdwf_prog* p;
+        int slot;
+        ~Back() { if (slot >= 0) p->free_slots.push_back(slot); }
+    } back{p, stg.slot};
+    const StageSlot* sl = stg.slot >= 0 ? &p->pool[stg.slot] : nullptr;
     int rc;
 #define CK(x) do { rc = (x); if (rc != CHDWF_OK) { p->err = chdwf_last_error(c); return rc; } } while (0)
     CK(chdwf_traj_begin(c));                                                        // :213-216
     if (from_stage)
-        CK(chdwf_traj_heatbath_dev(c, stg.gauss_dev, p->rescga, p->am, p->hpin, p->imass,
+        CK(chdwf_traj_heatbath_dev(c, sl->gauss_dev, p->rescga, p->am, p->hpin, p->imass,
                                    &rec->it_pf));                                   // :218-245
     else
         CK(chdwf_traj_heatbath(c, d.gauss.data(), p->rescga, p->am, p->hpin, p->imass,
@@ -358,7 +388,7 @@ int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
     chdwf_run_sums& A = p->sums;
     A.ancgpf = A.ancgpf + (float)rec->it_pf;                                       // :235
     if (p->staged.empty()) p->prefetch(p->isweep + 1);   // next trajectory's draws, overlapped
-    if (from_stage) CK(chdwf_traj_set_momenta_dev(c, stg.pp_dev));                 // :249-257
+    if (from_stage) CK(chdwf_traj_set_momenta_dev(c, sl->pp_dev));                 // :249-257
     else CK(chdwf_traj_set_momenta(c, d.pp.data()));
     double h[5];
     CK(chdwf_traj_hamilton(c, p->rescga, p->am, p->hpin, p->imass, h, &rec->it_h0));  // :261
