@@ -105,9 +105,14 @@ int chdwf_set_basis_store(chdwf_ctx* ctx, double max_bytes) {
     // drop the current store; the next solve allocates within the new limit
     if (c->lz.basis) cudaFree(c->lz.basis);
     if (c->lz.basis32) cudaFree(c->lz.basis32);
+    if (c->lz.wall) cudaFree(c->lz.wall);
+    if (c->lz.wall32) cudaFree(c->lz.wall32);
     c->lz.basis = nullptr;
     c->lz.basis32 = nullptr;
+    c->lz.wall = nullptr;
+    c->lz.wall32 = nullptr;
     c->lz.hcap = c->lz.hcap32 = 0;
+    c->lz.wcap = c->lz.wcap32 = 0;
     return c->status_of(cudaGetLastError(), "set_basis_store");
 }
 

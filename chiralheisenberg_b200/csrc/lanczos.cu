@@ -310,9 +310,21 @@ __device__ __forceinline__ void three_term_pair(const LzArgsT<float2>& a, float2
     }
 }
 
+// Force solves with a wall store: element e of r_{j+1} at point (s, site),
+// component c, also goes to the wall store when s is a wall.
+template <class T>
+__device__ __forceinline__ void wall_put(const LzArgsT<T>& a, int j1, int s, int site, int c,
+                                         T v) {
+    if (a.wcap == 0 || j1 >= a.wcap) return;
+    const int Ls = a.g.Ls;
+    if (s != 0 && s != Ls - 1) return;
+    const int64_t cs2 = 2 * (int64_t)a.g.kvol;
+    a.wbasis[(int64_t)j1 * 8 * cs2 + (s == 0 ? 0 : 1) + 2 * (int64_t)site + cs2 * c] = v;
+}
+
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
 // alpha~_j is the sum of M(j)'s partials, formed by every block.
-template <class T, int IMASS, bool PAIR>
+template <class T, int IMASS, bool PAIR, bool WALLS>
 __global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz1_Md(LzArgsT<T> a) {
     typedef LzShape<T, PAIR> S;
     constexpr int NF = S::split ? 1 : 2;
@@ -341,6 +353,10 @@ __global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz
                 float2 v0, v1;
                 three_term_pair(a, acc[0][d], acc[1][d], e, j, at, v0, v1);
                 st_pair(rn, e, v0, v1);
+                if (WALLS) {
+                    wall_put(a, j + 1, q.s, q.site, d + 4 * f0, v0);
+                    wall_put(a, j + 1, q.s + 1, q.site, d + 4 * f0, v1);
+                }
                 const double2 w0 = widen(v0), w1 = widen(v1);
                 loc += w0.x * w0.x + w0.y * w0.y;
                 loc += w1.x * w1.x + w1.y * w1.y;
@@ -356,6 +372,7 @@ __global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz
                     const int64_t e = p + a.g.cs * (d + 4 * f);
                     const T v = three_term(a, acc[d], e, j, at);
                     rn[e] = v;
+                    if (WALLS) wall_put(a, j + 1, q.s, q.site, d + 4 * f, v);
                     const double2 w = widen(v);
                     loc += w.x * w.x + w.y * w.y;
                 }
@@ -500,7 +517,10 @@ static unsigned lz_pass1_blocks(int64_t npts) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lz1_M<T, IMASS, PAIR>, kThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS, PAIR>, kThreads, 0);
+    int b3 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS, PAIR, false>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_lz1_Md<T, IMASS, PAIR, true>, kThreads, 0);
+    if (b3 < b2) b2 = b3;
     int64_t nb = (int64_t)nsm * (b1 < b2 ? b1 : b2);
     const int64_t direct = lz_direct_blocks<T, PAIR>(npts);
     if (nb < 1 || nb > direct) nb = direct;
@@ -598,7 +618,8 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
     k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
     cudaEventRecord(side.join, side.stream);
     if (tm) tm->begin(1, st, 4 * V + chi);
-    k_lz1_Md<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a);
+    if (a.wcap > 0) k_lz1_Md<T, IMASS, PAIR, true><<<nb, kThreads, 0, st>>>(a);
+    else k_lz1_Md<T, IMASS, PAIR, false><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
     cudaStreamWaitEvent(st, side.join, 0);
 }
@@ -658,7 +679,7 @@ static cudaGraphExec_t pass1_graph(LzWork& w, const LzArgsT<T>& a_in, unsigned n
     a.x = nullptr;
     a.xw = nullptr;
     a.npole = 0;
-    LzGraph& G = w.graph[sizeof(T) == sizeof(float2) ? 1 : 0];
+    LzGraph& G = w.graph[sizeof(T) == sizeof(float2) ? 1 : 0][a.wcap > 0 ? 1 : 0];
     const unsigned char* key = reinterpret_cast<const unsigned char*>(&a);
     if (G.exec && G.nb == nb && G.imass == imass && G.chunk == chunk &&
         G.key.size() == sizeof(a) && memcmp(G.key.data(), key, sizeof(a)) == 0)
@@ -828,10 +849,11 @@ LzWork::~LzWork() {
 }
 
 void LzWork::release() {
-    for (LzGraph& gr : graph) {
-        if (gr.exec) cudaGraphExecDestroy(gr.exec);
-        gr = LzGraph();
-    }
+    for (auto& row : graph)
+        for (LzGraph& gr : row) {
+            if (gr.exec) cudaGraphExecDestroy(gr.exec);
+            gr = LzGraph();
+        }
     if (side.fork) cudaEventDestroy(side.fork);
     if (side.join) cudaEventDestroy(side.join);
     if (side.stream) cudaStreamDestroy(side.stream);
@@ -848,9 +870,14 @@ void LzWork::release() {
     if (vt32) cudaFree(vt32);
     if (basis) cudaFree(basis);
     if (basis32) cudaFree(basis32);
+    if (wall) cudaFree(wall);
+    if (wall32) cudaFree(wall32);
     basis = nullptr;
     basis32 = nullptr;
+    wall = nullptr;
+    wall32 = nullptr;
     hcap = hcap32 = 0;
+    wcap = wcap32 = 0;
     if (xw) cudaFree(xw);
     if (x2w) cudaFree(x2w);
     ctl = nullptr; hist_mem = nullptr; part = nullptr; hflag_host = nullptr;
@@ -859,7 +886,7 @@ void LzWork::release() {
     xw_poles = 0;
 }
 
-cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec) {
+cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec, bool walls) {
     cudaError_t e;
     const bool same = ctl && g.kferm == geom.kferm && g.L == geom.L && g.Lt == geom.Lt;
     if (!same) {
@@ -915,6 +942,24 @@ cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec) {
             }
         }
     }
+    // Wall store: up to kMaxIter+2 two-slice vectors within 15% of the free
+    // HBM; force solves that outgrow it regenerate their vectors.
+    if (walls && basis_enabled && ((prec == kPrecF64 && !wall) || (prec == kPrecF32 && !wall32))) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        const size_t vb = (prec == kPrecF64 ? sizeof(double2) : sizeof(float2)) * 16 * (size_t)g.kvol;
+        int64_t cap = (int64_t)(0.15 * (double)fr / (double)vb);
+        if (cap > kMaxIter + 2) cap = kMaxIter + 2;
+        if (cap >= 8) {
+            void* ptr = nullptr;
+            if (cudaMalloc(&ptr, vb * (size_t)cap) == cudaSuccess) {
+                if (prec == kPrecF64) { wall = (double2*)ptr; wcap = (int)cap; }
+                else { wall32 = (float2*)ptr; wcap32 = (int)cap; }
+            } else {
+                cudaGetLastError();
+            }
+        }
+    }
     if (npole_max > xw_poles) {
         if (xw) cudaFree(xw);
         if (x2w) cudaFree(x2w);
@@ -939,6 +984,67 @@ void set_ring<float2>(LzArgsT<float2>& a, LzWork& w) {
     a.rb0 = w.rb32[0]; a.rb1 = w.rb32[1]; a.rb2 = w.rb32[2]; a.vt = w.vt32;
     a.basis = w.basis_enabled ? w.basis32 : nullptr;
     a.hcap = a.basis ? w.hcap32 : 0;
+}
+
+// Force solves with a wall store keep only the ring and the wall slices.
+template <class T>
+static void set_walls(LzArgsT<T>& a, LzWork& w) {
+    T* ws;
+    int cap;
+    if constexpr (std::is_same<T, double2>::value) { ws = w.wall; cap = w.wcap; }
+    else { ws = w.wall32; cap = w.wcap32; }
+    if (!w.basis_enabled || !ws) return;
+    a.wbasis = ws;
+    a.wcap = cap;
+    a.basis = nullptr;
+    a.hcap = 0;
+}
+
+// The two wall slices of r (s = 1 and s = Ls) into wall-store vector j, laid
+// out as the wall fields: element (slice sw, component c, site) at
+// sw + 2 site + 2 kvol c.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_lz_walls_of(LzArgsT<T> a, const T* __restrict__ r,
+                                                         int j) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t cs2 = 2 * (int64_t)a.g.kvol;
+    if (t >= 8 * cs2) return;
+    const int c = (int)(t / cs2);
+    const int64_t rr = t - c * cs2;
+    const int sw = (int)(rr & 1);
+    const int64_t site = rr >> 1;
+    a.wbasis[(int64_t)j * 8 * cs2 + t] = r[(sw ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * site + a.g.cs * c];
+}
+
+// q_j's wall slices (j = 1..m) from the wall store into every pole's two-slice
+// x_k: the same sums, in the same order, as from the full stored vectors.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_lz_accum_walls_c(LzArgsT<T> a, int m) {
+    typedef typename real_of<T>::type Real;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t cs2 = 2 * (int64_t)a.g.kvol, kf2 = 8 * cs2;
+    if (t >= kf2) return;
+    const int64_t H = kMaxIter + 2;
+    const int n = a.npole;
+    for (int k0 = 0; k0 < n; k0 += 8) {
+        double2 acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = make_double2(0.0, 0.0);
+        for (int j = 1; j <= m; j++) {
+            const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(a.wbasis + j * kf2 + t)));
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (k0 + k < n) {
+                    const double y = a.h.y[(k0 + k) * H + j];
+                    acc[k].x += y * qj.x;
+                    acc[k].y += y * qj.y;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (k0 + k < n) a.xw[(k0 + k) * kf2 + t] = acc[k];
+    }
 }
 
 // ---- pass 2 from the stored basis ---------------------------------------
@@ -1028,6 +1134,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     memset(&a, 0, sizeof(a));
     a.g = g;
     set_ring(a, w);
+    if (iflag) set_walls(a, w);
     a.chif = chif;
     a.diag = (Real)(2.0f * ((3.0f - am3) + 1.0f));
     a.hpin = (Real)hpin;
@@ -1048,6 +1155,11 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);
     k_lz_init<<<1, kThreads, 0, st>>>(w.ctl, w.hist, w.part, nbr);
     count_launches(2);
+    if (a.wcap > 1) {                    // r_1's wall slices (pass 1 adds r_2, r_3, ...)
+        k_lz_walls_of<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads), kThreads,
+                           0, st>>>(a, r1, 1);
+        count_launches(1);
+    }
 
     // pass 1: launch chunks of iterations and poll the mapped flag with
     // kAhead chunks queued beyond the one being checked, so a host thread
@@ -1119,9 +1231,9 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     count_launches(2);
     launch_scale(x, phi, anum[0], g.kferm, st);                       // x = a0 Phi (:628)
     if (iflag) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
-    if (m < a.hcap) {
-        // every q_j is still in HBM: one streaming pass over the basis
-        // reads the m stored vectors (whole or their two wall slices) and
+    if (a.wcap > 0 ? m < a.wcap : m < a.hcap) {
+        // every q_j (or, for the force, its wall slices) is still in HBM:
+        // one streaming pass over the store reads the m stored vectors and
         // the solution once
         const double vb = (double)sizeof(T);
         const double nbytes = iflag == 0
@@ -1138,6 +1250,10 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
                 k_lz_accum_x<T><<<nbx, kThreads, 0, st>>>(a, j0, j1);
                 count_launches(1);
             }
+        } else if (a.wcap > 0) {
+            k_lz_accum_walls_c<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads),
+                                    kThreads, 0, st>>>(a, m);
+            count_launches(1);
         } else {
             k_lz_accum_walls<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads),
                                   kThreads, 0, st>>>(a, m);
@@ -1175,7 +1291,7 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
                      float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
                      int* itercg, int* status, LzStats* stats, cudaStream_t st, int prec) {
     if (ndiag < 1 || ndiag > kMaxPoles) return cudaErrorInvalidValue;
-    cudaError_t e = w.ensure(g, iflag ? ndiag : 1, prec);
+    cudaError_t e = w.ensure(g, iflag ? ndiag : 1, prec, iflag != 0);
     if (e) return e;
     if (prec == kPrecF32)
         return lz_solve_t<float2>(w, g, phi, res, ndiag, anum, aden, iflag, chif, am3, hpin,

@@ -27,6 +27,8 @@ struct LzArgsT {
     double2* x;                 // solution (iflag 0), FP64
     double2* xw;                // two-slice x_k per pole (iflag 1), FP64
     int npole;
+    T* wbasis;                  // force solves: the two wall slices of each r_j,
+    int wcap;                   // j < wcap, at wbasis + j*16*kvol (0: no wall store)
 };
 
 struct LzStats {
@@ -76,7 +78,8 @@ struct LzSide {
 struct LzWork {
     Geom geom{};
     LzSide side;
-    LzGraph graph[2];                 // pass-1 chunk graph per vector precision
+    LzGraph graph[2][2];              // pass-1 chunk graph per vector precision and
+                                      // per basis mode (full vectors / wall slices)
     LzCtl* ctl = nullptr;
     double* hist_mem = nullptr;
     LzHist hist{};
@@ -90,6 +93,12 @@ struct LzWork {
     double2* basis = nullptr;
     float2* basis32 = nullptr;
     int hcap = 0, hcap32 = 0;
+    // Wall store of the force solves: the two wall slices of every Lanczos
+    // vector (2/Ls of a vector), all that their pass 2 reads; their pass 1
+    // then keeps only the three-vector ring, which stays in L2 for FP32.
+    double2* wall = nullptr;
+    float2* wall32 = nullptr;
+    int wcap = 0, wcap32 = 0;
     int basis_enabled = 1;
     double basis_max_bytes = -1.0;   // per precision; < 0: 40% of the free HBM
     double2* xw = nullptr;
@@ -100,7 +109,7 @@ struct LzWork {
     KernelTimer timer;
     ~LzWork();
     void release();
-    cudaError_t ensure(const Geom& g, int npole_max, int prec);
+    cudaError_t ensure(const Geom& g, int npole_max, int prec, bool walls);
 };
 
 // Precision of the Krylov vectors.
