@@ -50,7 +50,8 @@ EXPORTS = (
     "chdwf_prog_create", "chdwf_prog_destroy", "chdwf_prog_context", "chdwf_prog_set_remez",
     "chdwf_prog_set_chi", "chdwf_prog_get_chi", "chdwf_prog_startup", "chdwf_prog_seed",
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
-    "chdwf_prog_correlators", "chdwf_prog_last_error",
+    "chdwf_prog_correlators", "chdwf_prog_last_error", "chdwf_prog_measure",
+    "chdwf_traj_noise_solve",
     "chdwf_prog_sums", "chdwf_prog_reset_sums", "chdwf_prog_averages", "chdwf_prog_take_cg_caps",
     "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
@@ -128,6 +129,8 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_prog_set_residuals.argtypes = [P, F, F, F]
     L.chdwf_prog_sweep.argtypes = [P, P]
     L.chdwf_prog_correlators.argtypes = [P, P]
+    L.chdwf_prog_measure.argtypes = [P, F, C.POINTER(F), C.POINTER(F), C.POINTER(F), P]
+    L.chdwf_traj_noise_solve.argtypes = [P, P, I, I, F, F, F, I, P, PI]
     L.chdwf_prog_last_error.argtypes = [P]
     L.chdwf_prog_last_error.restype = C.c_char_p
     L.chdwf_prog_stage.argtypes = [P, I]
@@ -291,6 +294,7 @@ class Program:
         if rc != CHDWF_OK:
             raise ChdwfError(rc, self.lib.chdwf_last_error(None).decode())
         self.h = h
+        self._rescgm = 0.000000001                    # rhmc/cheisdwf.f:33
         for which, r in ((2, remez2), (4, remez4), (22, remez2g)):
             arrs = [np.ascontiguousarray(r[k], dtype=np.float64)
                     for k in ("anum", "aden", "bnum", "bden")]
@@ -323,6 +327,7 @@ class Program:
 
     def set_residuals(self, rescga, rescgg, rescgm):
         self._check(self.lib.chdwf_prog_set_residuals(self.h, rescga, rescgg, rescgm))
+        self._rescgm = rescgm
 
     def sweep(self) -> SweepRecord:
         rec = SweepRecord()
@@ -333,6 +338,18 @@ class Program:
         cf = np.empty((2, 2, self.Lt, 2), dtype=np.float32)
         self._check(self.lib.chdwf_prog_correlators(self.h, _ptr(cf)))
         return cf
+
+    def measure(self, res=None):
+        """measure() of rhmc/cheisdwf.f:1164-1453 on the current chi: returns
+        (psibarpsi, susclsing, aviter, parts) with parts[inoise] = (re p1,
+        im p1, re p2, im p2), the unit-100 record of each noise vector.
+        res defaults to the measurement residual rescgm."""
+        pb, su, av = C.c_float(), C.c_float(), C.c_float()
+        parts = np.empty((10, 4), dtype=np.float64)
+        r = self._rescgm if res is None else res
+        self._check(self.lib.chdwf_prog_measure(self.h, r, C.byref(pb), C.byref(su), C.byref(av),
+                                                _ptr(parts)))
+        return pb.value, su.value, av.value, parts
 
     def sums(self) -> RunSums:
         out = RunSums()

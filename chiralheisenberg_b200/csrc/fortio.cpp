@@ -1,6 +1,7 @@
 // fortio.cpp -- the reference program's on-disk formats (see fortio.h).
 #include "fortio.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -86,6 +87,7 @@ std::string edit_e(double v, int w, int d) {
 // E form with one digit before the point.
 std::string edit_g_list(double v, int w, int d, int e) {
     if (!std::isfinite(v)) return nonfinite(v, w);
+    d = std::min(std::max(d, 1), 40);            // gfortran uses 9 (REAL*4) and 17 (REAL*8)
     const double a = std::fabs(v);
     const std::string sign = std::signbit(v) ? "-" : "";
     const int tail = e + 2;

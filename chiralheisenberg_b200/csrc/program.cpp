@@ -480,6 +480,84 @@ int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
     return CHDWF_OK;
 }
 
+int chdwf_prog_measure(chdwf_prog* p, float res, float* psibarpsi, float* susclsing,
+                       float* aviter, double* parts) {
+    // measure(psibarpsi, res, aviter, am, hpin, imass), rhmc/cheisdwf.f:1164-1453,
+    // on chi with the program's am, hpin, imass (1 or 3)
+    if (!p || !psibarpsi || !susclsing || !aviter) return CHDWF_BAD_ARG;
+    if (p->imass != 1 && p->imass != 3) return CHDWF_BAD_ARG;
+    chdwf_ctx* c = p->ctx;
+    const int64_t kvol = p->kvol;
+    constexpr int knoise = 10;
+    p->discard_pending();                 // the draws continue the generator's stream
+    int rc = chdwf_traj_begin(c);         // the solves run on chit = chi
+    if (rc != CHDWF_OK) { p->err = chdwf_last_error(c); return rc; }
+    std::vector<float> ps(2 * kvol), pt(2 * kvol);
+    std::vector<double> slice(4 * kvol);
+    float pbp[knoise];
+    int iter = 0;
+    for (int inoise = 0; inoise < knoise; inoise++) {
+        p->rng.gauss0(kvol, ps.data());                                            // :1187
+        p->rng.gauss0(kvol, pt.data());                                            // :1189
+        double p1r = 0.0, p1i = 0.0, p2r = 0.0, p2i = 0.0;
+        for (int idsource = 1; idsource <= 2; idsource++) {
+            for (int w = 0; w < 2; w++) {
+                // w=0: ps on s=1, Dirac idsource, read s=kthird (:1194-1294);
+                // w=1: pt on s=kthird, Dirac idsource+2, read s=1 (:1303-1393)
+                const float* eta = w == 0 ? ps.data() : pt.data();
+                const int d = w == 0 ? idsource : idsource + 2;
+                int it = 0;
+                rc = chdwf_traj_noise_solve(c, eta, w == 0 ? 1 : p->Ls, d, res, p->am, p->hpin,
+                                            p->imass, slice.data(), &it);
+                if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) {
+                    p->err = chdwf_last_error(c);
+                    p->last_state = p->rng.state();
+                    return rc;
+                }
+                if (rc == CHDWF_ITER_CAP) p->cg_caps++;
+                iter += it;
+                double ar = w == 0 ? p1r : p2r, ai = w == 0 ? p1i : p2i;
+                for (int64_t t = 0; t < 2 * kvol; t++) {       // f outer, i inner
+                    const int64_t i = t % kvol;
+                    const double xr = (double)eta[i], xi = (double)eta[kvol + i];
+                    const double yr = slice[2 * t], yi = slice[2 * t + 1];
+                    // conjg(x)*y, then the running sum
+                    const double mr = xr * yr - (-xi) * yi, mi = xr * yi + (-xi) * yr;
+                    ar = ar + mr;
+                    ai = ai + mi;
+                }
+                if (w == 0) { p1r = ar; p1i = ai; } else { p2r = ar; p2i = ai; }
+            }
+        }
+        const double kv = (double)kvol;
+        if (p->imass == 1) {                                                      // :1418-1421
+            p1r = p1r / kv; p1i = p1i / kv;
+            p2r = p2r / kv; p2i = p2i / kv;
+        } else {                                                                  // :1422-1425
+            // (0,-1)*p1 and (0,+1)*p2 as complex products
+            const double a1 = 0.0 * p1r - (-1.0) * p1i, b1 = 0.0 * p1i + (-1.0) * p1r;
+            const double a2 = 0.0 * p2r - 1.0 * p2i, b2 = 0.0 * p2i + 1.0 * p2r;
+            p1r = a1 / kv; p1i = b1 / kv;
+            p2r = a2 / kv; p2i = b2 / kv;
+        }
+        pbp[inoise] = (float)(p1r + p2r);
+        if (parts) {                                                              // write(100)
+            parts[4 * inoise] = p1r; parts[4 * inoise + 1] = p1i;
+            parts[4 * inoise + 2] = p2r; parts[4 * inoise + 3] = p2i;
+        }
+    }
+    p->last_state = p->rng.state();
+    float pb = 0.0f, sus = 0.0f;                                                  // :1440-1449
+    for (int i = 0; i < knoise; i++) {
+        pb = pb + pbp[i];
+        for (int j = knoise - 1; j >= i + 1; j--) sus = sus + pbp[i] * pbp[j];
+    }
+    *psibarpsi = pb / (float)knoise;
+    *susclsing = (float)(2 * kvol) * sus / (float)(knoise * (knoise - 1));
+    *aviter = (float)iter / (float)(4 * knoise);                                  // :1451
+    return CHDWF_OK;
+}
+
 const char* chdwf_prog_last_error(chdwf_prog* p) { return p ? p->err.c_str() : ""; }
 
 int chdwf_prog_sums(chdwf_prog* p, chdwf_run_sums* out) {

@@ -75,6 +75,28 @@ __global__ void k_extract_walls(const double2* __restrict__ xi, Geom g, double2*
     out[t] = xi[s + (int64_t)g.Ls * i + g.cs * (d + 4 * f)];
 }
 
+// noise source of measure(): xi(s, i, d, f) = cmplx(eta(i,1), eta(i,2)) for
+// both flavours (rhmc/cheisdwf.f:1196-1208, :1226-1242); xi is zero elsewhere
+__global__ void k_noise_source(double2* __restrict__ xi, Geom g, const float* __restrict__ eta,
+                               int s, int d) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= 2 * (int64_t)g.kvol) return;
+    const int64_t i = t % g.kvol;
+    const int f = (int)(t / g.kvol);
+    xi[s + (int64_t)g.Ls * i + g.cs * (d + 4 * f)] =
+        make_double2((double)eta[i], (double)eta[g.kvol + i]);
+}
+
+// one wall slice of one Dirac component, both flavours -> out[f][kvol]
+__global__ void k_extract_slice(const double2* __restrict__ xi, Geom g, int s, int d,
+                                double2* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= 2 * (int64_t)g.kvol) return;
+    const int64_t i = t % g.kvol;
+    const int f = (int)(t / g.kvol);
+    out[t] = xi[s + (int64_t)g.Ls * i + g.cs * (d + 4 * f)];
+}
+
 static unsigned nblk(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 cudaError_t Ctx::ensure_traj() {
@@ -302,6 +324,38 @@ int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, flo
     cudaMemcpyAsync(walls, c->walls, sizeof(double2) * 8 * g.kvol, cudaMemcpyDeviceToHost, c->stream);
     e = cudaStreamSynchronize(c->stream);
     return traj_solver_status(c, e, st, "propagator");
+}
+
+int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idirac, float res,
+                           float am, float hpin, int imass, double* slice, int* itercg) {
+    (void)am;
+    CTX_OR_BAD(ctx);
+    const Geom& g = c->g;
+    if (!eta || !slice || !itercg || (swall != 1 && swall != g.Ls) || idirac < 1 || idirac > 4 ||
+        (imass != 1 && imass != 3))
+        return CHDWF_BAD_ARG;
+    double2* xi = c->spin[0];
+    double2* Phi = c->spin[1];
+    float* eta_d = c->gauss;                       // heatbath scratch, free between sweeps
+    cudaMemcpyAsync(eta_d, eta, sizeof(float) * 2 * g.kvol, cudaMemcpyHostToDevice, c->stream);
+    cudaMemsetAsync(xi, 0, sizeof(double2) * g.kferm, c->stream);
+    k_noise_source<<<nblk(2 * (int64_t)g.kvol), kThreads, 0, c->stream>>>(
+        xi, g, eta_d, swall - 1, idirac - 1); count_launches(1);
+    launch_round_chi(c->chit, c->chif, g.kvol, c->stream);
+    launch_dslash64(true, imass, Phi, xi, c->chif, g, c->am3, hpin, c->ibound, c->stream);  // :1273
+    cudaMemcpyAsync(xi, Phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice, c->stream);  // :1277-1282
+    int st = 0;
+    cudaError_t e = cg_solve(c->cg, g, Phi, res, c->chif, c->am3, hpin, imass, c->ibound, xi,
+                             itercg, &st, c->stream);                              // :1284
+    if (e) return traj_solver_status(c, e, st, "noise solve");
+    if (st == 1) fprintf(stdout, " # iterations of congrad exceeds niterc\n");
+    const int sread = swall == 1 ? g.Ls - 1 : 0;
+    k_extract_slice<<<nblk(2 * (int64_t)g.kvol), kThreads, 0, c->stream>>>(
+        xi, g, sread, idirac - 1, c->walls); count_launches(1);
+    cudaMemcpyAsync(slice, c->walls, sizeof(double2) * 2 * g.kvol, cudaMemcpyDeviceToHost,
+                    c->stream);
+    e = cudaStreamSynchronize(c->stream);
+    return traj_solver_status(c, e, st, "noise solve");
 }
 
 }  // extern "C"

@@ -234,6 +234,16 @@ int chdwf_traj_sync(chdwf_ctx* ctx);
  * complex128 [(w*2 + dd)*2 + f][kvol] (w=0: s=1, dd: Dirac pair index). */
 int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, float am, float hpin,
                           int imass, double* walls, int* itercg);
+/* One noise-source solve of measure() (rhmc/cheisdwf.f:1192-1403; the
+ * reference routine replaced is the body of its idsource loop):
+ * source cmplx(eta(i,1), eta(i,2)) (eta: REAL*4 (kvol,2), as gauss0 fills
+ * ps and pt) on wall s=swall (1 or kthird), Dirac idirac, both flavours;
+ * Phi = M^dag xi; CGNE from x0 = Phi on the current chit.  slice receives
+ * the solution on the opposite wall (s=kthird for swall=1, s=1 for
+ * swall=kthird), Dirac idirac, both flavours, as complex128 [f][kvol].
+ * imass 1 or 3. */
+int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idirac, float res,
+                           float am, float hpin, int imass, double* slice, int* itercg);
 
 #ifdef __cplusplus
 }

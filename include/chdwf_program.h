@@ -93,6 +93,17 @@ int chdwf_prog_stage(chdwf_prog* p, int ntraj);
  * complex64 (re, im) pair at [it + Lt*flavour] (written by the reference to
  * fort.5001/5002 and 5011/5012, :1036-1047) */
 int chdwf_prog_correlators(chdwf_prog* p, float* cferm);
+/* measure(psibarpsi, res, aviter, am, hpin, imass) (rhmc/cheisdwf.f:1164-1453)
+ * on the current chi with the program's am, hpin and imass (1 or 3): the
+ * noisy psibar psi estimator over knoise = 10 Gaussian noise vectors drawn
+ * from the program's generator (two gauss0 calls per noise), four CGNE
+ * solves per noise at residual res.  psibarpsi and susclsing are the
+ * values the reference writes to unit 200; aviter = iterations / 40.
+ * parts (40 doubles, or NULL) receives re/im of psibarpsi1 and psibarpsi2
+ * per noise, the unit-100 records.  The main program of the reference does
+ * not call it (:392); this entry point leaves the running sums alone. */
+int chdwf_prog_measure(chdwf_prog* p, float res, float* psibarpsi, float* susclsing,
+                       float* aviter, double* parts);
 const char* chdwf_prog_last_error(chdwf_prog* p);
 
 /* The running sums since creation (or the last reset); they are part of

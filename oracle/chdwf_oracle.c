@@ -619,6 +619,28 @@ void orc_derivs(const orc_lat* lat, const double* R, const double* X2, double an
     }
 }
 
+/* REAL*4 sum of |v_i|^2 over n complex entries, as congrad's
+ * !$OMP PARALLEL DO REDUCTION(+:alphad) / (+:betan) forms it (cheisdwf.f:1105-1108,
+ * :1133-1136): each term is added in REAL*8 and the sum rounded to REAL*4 at
+ * every step.  With nth > 1 the loop is split as OpenMP's static schedule
+ * splits it (the first n % nth threads take one entry more), each thread
+ * sums its contiguous chunk from zero, and the partials are added to the
+ * shared REAL*4 sum in thread order (one of the orders the runtime may
+ * take).  nth = 1 is the sequential loop. */
+static float r4_norm2(const double* v, int64_t n, int nth) {
+    if (nth < 1) nth = 1;
+    const int64_t q0 = n / nth, rem = n % nth;
+    float s = 0.0f;
+    for (int t = 0; t < nth; t++) {
+        const int64_t q = q0 + (t < rem ? 1 : 0), s0 = q0 * t + (t < rem ? t : rem);
+        float part = 0.0f;
+        for (int64_t i = s0; i < s0 + q; i++)
+            part = (float)((double)part + v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1]);
+        s = s + part;
+    }
+    return s;
+}
+
 /* ======================================================================
  * congrad: CGNE on M^dagger M with REAL*4 scalars (cheisdwf.f:1064-1157)
  * ==================================================================== */
@@ -645,17 +667,13 @@ int orc_congrad(const orc_lat* lat, const double* Phi, float res, int* itercg,
         alphad = 0.0f;
         orc_dslash(lat, x1, p, chi, am, hpin, imass);
         if (nx != 1) {
-            alphad = 0.0f;
-            for (int64_t i = 0; i < kferm; i++)
-                alphad = (float)((double)alphad + x1[2 * i] * x1[2 * i] + x1[2 * i + 1] * x1[2 * i + 1]);
+            alphad = r4_norm2(x1, kferm, lat->threads);
             alpha = alphan / alphad;
             for (int64_t i = 0; i < kferm; i++) st(x, i, cadd(ld(x, i), cscal((double)alpha, ld(p, i))));
         }
         orc_dslashd(lat, x2, x1, chi, am, hpin, imass);
         for (int64_t i = 0; i < kferm; i++) st(r, i, csub(ld(r, i), cscal((double)alpha, ld(x2, i))));
-        betan = 0.0f;
-        for (int64_t i = 0; i < kferm; i++)
-            betan = (float)((double)betan + r[2 * i] * r[2 * i] + r[2 * i + 1] * r[2 * i + 1]);
+        betan = r4_norm2(r, kferm, lat->threads);
         beta = betan / betad;
         betad = betan;
         alphan = betan;
@@ -665,6 +683,87 @@ int orc_congrad(const orc_lat* lat, const double* Phi, float res, int* itercg,
     }
     free(x1); free(x2); free(p); free(r);
     return capped;
+}
+
+/* ======================================================================
+ * measure (cheisdwf.f:1164-1453): noisy estimator of psibar psi and its
+ * disconnected susceptibility, knoise = 10 noise vectors, each with sources
+ * on the s=1 and s=Ls walls for Dirac indices 1, 2.  imass 1 or 3 (the
+ * operator of this code has no imass 5 term).  xi: /vector/ scratch.
+ * parts (4*knoise doubles, or NULL): re/im of psibarpsi1 and psibarpsi2 of
+ * each noise, the record written to fort.100 (:1433-1434).
+ * ==================================================================== */
+void orc_measure(const orc_lat* lat, orc_rng* g, float res, float am, float hpin, int imass,
+                 const double* chi, double* xi, float* psibarpsi, float* susclsing,
+                 float* aviter, double* parts) {
+    const int64_t Ls = lat->Ls, kvol = orc_kvol(lat), kferm = orc_kferm(lat);
+    enum { knoise = 10 };
+    float* ps = malloc(sizeof(float) * 2 * kvol);
+    float* pt = malloc(sizeof(float) * 2 * kvol);
+    double* Phi = malloc(sizeof(double) * 2 * kferm);
+    float pbp[knoise];
+    int iter = 0;
+    for (int inoise = 0; inoise < knoise; inoise++) {
+        orc_gauss0(g, kvol, ps);                                               /* :1187 */
+        cx p1 = {0.0, 0.0};
+        orc_gauss0(g, kvol, pt);                                               /* :1189 */
+        cx p2 = {0.0, 0.0};
+        for (int idsource = 1; idsource <= 2; idsource++) {
+            for (int wall = 0; wall < 2; wall++) {
+                /* wall 0: source x = cmplx(ps) on s=1 for Dirac idsource
+                 * (:1194-1235); wall 1: x = cmplx(pt) on s=Ls for idsource+2
+                 * (:1303-1346) */
+                const float* nz = wall == 0 ? ps : pt;
+                const int d = wall == 0 ? idsource - 1 : idsource + 1;
+                const int64_t s_src = wall == 0 ? 0 : Ls - 1;
+                const int64_t s_read = wall == 0 ? Ls - 1 : 0;
+                memset(xi, 0, sizeof(double) * 2 * kferm);
+                for (int f = 0; f < 2; f++)
+                    for (int64_t i = 0; i < kvol; i++) {
+                        cx x = {(double)nz[i], (double)nz[kvol + i]};
+                        st(xi, SIDX(s_src, i, d, f), x);
+                    }
+                orc_dslashd(lat, Phi, xi, chi, am, hpin, imass);               /* :1273, :1372 */
+                memcpy(xi, Phi, sizeof(double) * 2 * kferm);
+                int itercg = 0;
+                orc_congrad(lat, Phi, res, &itercg, am, hpin, imass, chi, xi);  /* :1284, :1383 */
+                iter += itercg;
+                cx acc = wall == 0 ? p1 : p2;
+                for (int f = 0; f < 2; f++)                                    /* :1289-1294, :1388-1393 */
+                    for (int64_t i = 0; i < kvol; i++) {
+                        cx x = {(double)nz[i], (double)nz[kvol + i]};
+                        acc = cadd(acc, cmul(cconj(x), ld(xi, SIDX(s_read, i, d, f))));
+                    }
+                if (wall == 0) p1 = acc;
+                else p2 = acc;
+            }
+        }
+        const double kv = (double)kvol;
+        if (imass == 1) {                                                      /* :1418-1421 */
+            p1.re /= kv; p1.im /= kv;
+            p2.re /= kv; p2.im /= kv;
+        } else {                                                               /* :1422-1425 */
+            const cx mi = {0.0, -1.0}, pi = {0.0, 1.0};
+            p1 = cmul(mi, p1); p1.re /= kv; p1.im /= kv;
+            p2 = cmul(pi, p2); p2.re /= kv; p2.im /= kv;
+        }
+        pbp[inoise] = (float)(p1.re + p2.re);
+        if (parts) {
+            parts[4 * inoise] = p1.re; parts[4 * inoise + 1] = p1.im;
+            parts[4 * inoise + 2] = p2.re; parts[4 * inoise + 3] = p2.im;
+        }
+    }
+    float pb = 0.0f, sus = 0.0f;                                               /* :1440-1449 */
+    for (int inoise = 0; inoise < knoise; inoise++) {
+        pb = pb + pbp[inoise];
+        for (int jnoise = knoise - 1; jnoise >= inoise + 1; jnoise--) sus = sus + pbp[inoise] * pbp[jnoise];
+    }
+    pb = pb / (float)knoise;
+    sus = (float)(2 * kvol) * sus / (float)(knoise * (knoise - 1));
+    *psibarpsi = pb;
+    *susclsing = sus;
+    *aviter = (float)iter / (float)(4 * knoise);                               /* :1451 */
+    free(ps); free(pt); free(Phi);
 }
 
 /* ======================================================================

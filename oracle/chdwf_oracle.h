@@ -102,6 +102,10 @@ void orc_hamilton(const orc_lat* lat, const double* Phi, float res2, float am,
 
 /* fermion (cheisdwf.f:897-1058): returns aviter; cferm1/cferm2 receive the
  * averaged correlators as complex64 pairs [(it, flavour)] = 2*(it + Lt*f). */
+/* measure (cheisdwf.f:1164-1453): the noisy psibar psi estimator; imass 1 or 3. */
+void orc_measure(const orc_lat* lat, orc_rng* g, float res, float am, float hpin, int imass,
+                 const double* chi, double* xi, float* psibarpsi, float* susclsing,
+                 float* aviter, double* parts);
 float orc_fermion(const orc_lat* lat, orc_rng* g, float res, float am,
                   float hpin, int imass, const double* chi, double* x,
                   float* cferm1, float* cferm2);

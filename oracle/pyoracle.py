@@ -92,6 +92,9 @@ def lib():
                                    P, P]
         L.orc_fermion.argtypes = [P, P, C.c_float, C.c_float, C.c_float, C.c_int, P, P, P, P]
         L.orc_fermion.restype = C.c_float
+        L.orc_measure.argtypes = [P, P, C.c_float, C.c_float, C.c_float, C.c_int, P, P,
+                                  C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                  C.POINTER(C.c_float), P]
         L.orc_state_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
                                     C.c_float, C.c_float, C.c_int, C.c_int]
         L.orc_state_new.restype = C.POINTER(State)
@@ -208,6 +211,18 @@ class Sweeper:
         rec = TrajRec()
         self.lib.orc_sweep(self.st, C.byref(rec))
         return rec
+
+    def measure(self, res=1e-9):
+        """measure() (cheisdwf.f:1164-1453) on chi with the state's am, hpin,
+        imass and generator: (psibarpsi, susclsing, aviter, parts[10, 4])."""
+        st = self.st.contents
+        xi = np.empty(2 * 8 * self.kvol * st.lat.Ls, dtype=np.float64)
+        parts = np.empty((10, 4), dtype=np.float64)
+        pb, su, av = C.c_float(), C.c_float(), C.c_float()
+        self.lib.orc_measure(C.byref(st.lat), C.byref(st.rng), res, st.am, st.hpin, st.imass,
+                             C.cast(st.chi, C.c_void_p), _p(xi), C.byref(pb), C.byref(su),
+                             C.byref(av), _p(parts))
+        return pb.value, su.value, av.value, parts
 
     def close(self):
         if self.st:

@@ -1,0 +1,66 @@
+"""measure (rhmc/cheisdwf.f:1164-1453), the noisy psibar psi estimator, on
+the GPU driver (chdwf_prog_measure: host noise and sums, device solves
+through chdwf_traj_noise_solve) against the oracle on the same chi and seed.
+
+Workload: L=Lt=6, Ls=8, beta=0.475, am3=1, hpin=0, imass 1 and 3, res 1e-9
+(rescgm); chi from a seeded N(0, 1/beta); the reference's default seed.
+
+Tolerances:
+  unit-100 records (re/im of psibarpsi1, psibarpsi2 per noise vector)
+      |gpu - oracle| <= 1e-6 * max|oracle|.  Each record comes from a CGNE
+      stopped at |r|^2 < kferm res^2; at res 1e-9 the oracle's records lie
+      within 8.3e-8 (imass 1) and 3.9e-8 (imass 3) relative of the same
+      solves converged to 1e-11 on this workload, so two independent solves
+      differ by at most about 2e-7.
+  psibarpsi (REAL*4)   relative 1e-5
+  susclsing (REAL*4)   |gpu - oracle| <= 1e-5 * kvol * max pbp^2
+  aviter               within +-5 iterations of the oracle on 8 threads
+  generator            identical after the 20 gauss0 calls
+
+congrad sums alphad and betan in REAL*4 under !$OMP REDUCTION
+(rhmc/cheisdwf.f:1105, :1133), so the reference's iteration count depends on
+its thread count.  On this workload (imass 1) the oracle, which models that
+reduction, gives aviter 474.4 on 1 thread, 462.3 on 2, 461.1 on 4 and 460.4
+on 8, with the records unchanged to 1e-7.  The GPU sums in FP64 and rounds
+once, which is the many-thread end of that range.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import chiralheisenberg_b200 as chb
+
+pytestmark = pytest.mark.gpu
+
+CFG = dict(L=6, Lt=6, Ls=8, beta=0.475, am3=1.0, dt=0.1, am=0.01, hpin=0.0, iterl=10)
+SEED = 693764523745.0
+RES = 1e-9
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_measure_against_oracle(remez, imass):
+    c = CFG
+    kvol = c["L"] ** 2 * c["Lt"]
+    chi = np.random.default_rng(3).standard_normal((3, kvol)) / np.sqrt(c["beta"])
+    r0 = po.Remez()
+    sw = po.Sweeper(c["L"], c["Lt"], c["Ls"], c["beta"], c["am3"], c["dt"], c["am"], c["hpin"],
+                    imass, c["iterl"], r0, r0, r0, chi=chi, seed=SEED, measure=False, threads=8)
+    pb_o, su_o, av_o, parts_o = sw.measure(RES)
+    seed_o = po.lib().orc_rranget(po.C.byref(sw.st.contents.rng))
+    sw.close()
+
+    prog = chb.Program(c["L"], c["Lt"], c["Ls"], c["dt"], c["beta"], c["am3"], c["am"], c["hpin"],
+                       imass, c["iterl"], remez["remez2"], remez["remez4"], remez["remez2g"])
+    prog.set_chi(chi)
+    prog.startup(SEED)
+    pb_g, su_g, av_g, parts_g = prog.measure(RES)
+    seed_g = prog.seed()
+    prog.close()
+
+    scale = np.abs(parts_o).max()
+    assert np.abs(parts_g - parts_o).max() <= 1e-6 * scale
+    assert abs(pb_g - pb_o) <= 1e-5 * abs(pb_o), (pb_g, pb_o)
+    pbp = parts_o[:, 0] + parts_o[:, 2]
+    assert abs(su_g - su_o) <= 1e-5 * kvol * np.max(pbp ** 2), (su_g, su_o)
+    assert abs(av_g - av_o) <= 5, (av_g, av_o)
+    assert seed_g == seed_o

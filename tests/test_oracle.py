@@ -224,3 +224,80 @@ def test_oracle_thread_envelope(remez):
     assert max(its) - min(its) <= 4
     for _, x in runs[1:]:
         assert np.linalg.norm(x - runs[0][1]) <= 1e-12 * np.linalg.norm(runs[0][1])
+
+
+def test_congrad_thread_model():
+    """congrad's REAL*4 sums under !$OMP REDUCTION (cheisdwf.f:1105, :1133),
+    modelled with the static schedule for threads > 1: the solve is the
+    same to the residual's accuracy and converges for every thread count."""
+    Phi, chi = random_fields(4, 4, 8, seed=7)
+    runs = []
+    for th in (1, 2, 3, 8):
+        lat = po.make_lat(4, 4, 8, threads=th)
+        x, it, capped = po.congrad(lat, Phi, chi, Phi, 1e-9)
+        assert not capped
+        runs.append((it, x))
+    its = [it for it, _ in runs]
+    assert max(its) - min(its) <= 3
+    for _, x in runs[1:]:
+        assert np.linalg.norm(x - runs[0][1]) <= 1e-9 * np.linalg.norm(runs[0][1])
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_measure_matches_dense_solve(imass):
+    """measure (cheisdwf.f:1164-1453): each noise vector's unit-100 record
+    (psibarpsi1, psibarpsi2) against x^dag [M^-1 xi] read on the opposite
+    wall from a dense solve; the unit-200 pair (psibarpsi, susclsing) from
+    those records in REAL*4, bit for bit; the generator advanced by exactly
+    two gauss0 calls per noise vector (:1187, :1189)."""
+    L, Lt, Ls = 4, 4, 8             # congrad's cap niterc = kthird*kvol = 512
+    kvol = L * L * Lt
+    seed = 693764523745.0
+    chi = np.random.default_rng(11).standard_normal((3, kvol)) / np.sqrt(0.475)
+    r0 = po.Remez()
+    sw = po.Sweeper(L, Lt, Ls, 0.475, 1.0, 0.1, 0.01, 0.0, imass, 10, r0, r0, r0, chi=chi,
+                    seed=seed, measure=False)
+    # res 1e-12: the CGNE stops at |r|^2 < kferm res^2, so the records
+    # carry an error of order sqrt(kferm) res / lambda_min(M^dag M)
+    pb, su, av, parts = sw.measure(1e-12)
+    seed_after = po.lib().orc_rranget(po.C.byref(sw.st.contents.rng))
+    sw.close()
+
+    lat = po.make_lat(L, Lt, Ls)
+    sh = po.spinor_shape(lat)
+    M = _dense(lat, chi, imass=imass)
+    rand = po.Rand(seed)
+    noise, rhs = [], []
+    for _ in range(10):
+        ps, pt = rand.gauss0(kvol), rand.gauss0(kvol)
+        xs, xt = ps[0] + 1j * ps[1].astype(np.float64), pt[0] + 1j * pt[1].astype(np.float64)
+        noise.append((xs, xt))
+        for d in (1, 2):
+            for w, (x, dd, s) in enumerate(((xs, d, 0), (xt, d + 2, Ls - 1))):
+                xi = np.zeros(sh, complex)
+                xi[:, dd - 1, ..., s] = x.reshape(Lt, L, L)
+                rhs.append(xi.reshape(-1))
+    Y = np.linalg.solve(M, np.array(rhs).T).T.reshape((10, 2, 2) + sh)
+    dense = np.zeros((10, 4))
+    for k, (xs, xt) in enumerate(noise):
+        p = [0j, 0j]
+        for di, d in enumerate((1, 2)):
+            p[0] += np.vdot(np.tile(xs, 2), Y[k, di, 0][:, d - 1, ..., Ls - 1].reshape(-1))
+            p[1] += np.vdot(np.tile(xt, 2), Y[k, di, 1][:, d + 1, ..., 0].reshape(-1))
+        if imass == 3:
+            p = [-1j * p[0], 1j * p[1]]
+        dense[k] = [p[0].real / kvol, p[0].imag / kvol, p[1].real / kvol, p[1].imag / kvol]
+    assert np.abs(parts - dense).max() <= 1e-9 * np.abs(dense).max()
+
+    f32 = np.float32
+    pbp = (parts[:, 0] + parts[:, 2]).astype(f32)
+    s_pb, s_su = f32(0), f32(0)
+    for i in range(10):
+        s_pb = f32(s_pb + pbp[i])
+        for j in range(9, i, -1):
+            s_su = f32(s_su + f32(pbp[i] * pbp[j]))
+    assert pb == f32(s_pb / f32(10))
+    assert su == f32(f32(f32(2 * kvol) * s_su) / f32(90))
+    iters = round(float(av) * 40)
+    assert 0 < iters < 40 * Ls * kvol and av == np.float32(iters) / np.float32(40)
+    assert seed_after == rand.seed()
