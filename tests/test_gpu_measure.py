@@ -19,10 +19,11 @@ Tolerances:
 
 congrad sums alphad and betan in REAL*4 under !$OMP REDUCTION
 (rhmc/cheisdwf.f:1105, :1133), so the reference's iteration count depends on
-its thread count.  On this workload (imass 1) the oracle, which models that
+its thread count.  On this workload the oracle, which models that
 reduction, gives aviter 474.4 on 1 thread, 462.3 on 2, 461.1 on 4 and 460.4
-on 8, with the records unchanged to 1e-7.  The GPU sums in FP64 and rounds
-once, which is the many-thread end of that range.
+on 8 (imass 1), and 533.8 on 1 and 530.6 on 8 (imass 3), with the records
+equal to 6e-9.  The GPU sums in FP64 and rounds once, which is the
+many-thread end of that range.
 """
 import numpy as np
 import pytest
