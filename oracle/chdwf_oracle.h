@@ -151,6 +151,55 @@ void orc_state_set_remez(orc_state* st, int which, const orc_remez* r);
 /* One sweep of the main loop (cheisdwf.f:207-399). */
 void orc_sweep(orc_state* st, orc_traj_rec* rec);
 
+/* --- the HMC predecessor, mh/cheisdwf_hmc.f (chdwf_oracle_hmc.c) --------
+ * single precision: spinors complex64 (re, im float pairs), chi REAL*4. */
+void orc_hmc_dslash(const orc_lat* lat, float* Phi, const float* R, const float* chi,
+                    int imass, int dag);
+int orc_hmc_congrad(const orc_lat* lat, const float* Phi, float res, int* itercg, int imass,
+                    const float* chi, float* x);
+void orc_hmc_derivs(const orc_lat* lat, const float* X1, const float* chi, int imass,
+                    float* dSdchi);
+int orc_hmc_force(const orc_lat* lat, const float* Phi, float* X0, float* X1, const float* chi,
+                  float res1, int imass, float* dSdchi, int* itercg);
+int orc_hmc_hamilton(const orc_lat* lat, const float* Phi, float* X0, const float* chi,
+                     const float* pp, float res2, int imass, double* out, int* itercg);
+
+typedef struct {
+    double H0, H1, dH, dS, S0, S1, hg, hp;
+    float y, x;
+    int drew_x, accepted, nsteps;
+    int it_h0, it_h1, it_force, nforce;
+    float action, gaction, paction, vel2;
+    int measured;
+    float cond[3], susc[3], condmod, susctot;
+} orc_hmc_rec;
+
+typedef struct {
+    orc_lat lat;
+    orc_rng rng;
+    float dt, am;
+    int imass, iterl, iprint;
+    float rescga, rescgg;
+    float* chi;        /* /chi/ chi(kvol,3), REAL*4 */
+    float* chit;       /* /trial/ chit      */
+    float* pp;         /* /trial/ pp        */
+    float* dSdchi;
+    float* Phi;        /* pseudofermion     */
+    float* X0;         /* solver guess, extrapolated by force */
+    float* X1;         /* /vector/          */
+    float* R;          /* /dum1/ R          */
+    float* ps;         /* /dum1/ ps(kvol,2) */
+    int isweep, itot, naccp;
+    float action, gaction, paction;   /* main-program variables kept across sweeps */
+    float actiona, vel2a, yav, yyav;
+} orc_hmc_state;
+
+orc_hmc_state* orc_hmc_new(int L, int Lt, int Ls, float beta, float am3, float dt, float am,
+                           int imass, int iterl);
+void orc_hmc_free(orc_hmc_state* st);
+/* One sweep of the main loop of mh/cheisdwf_hmc.f (:140-320). */
+void orc_hmc_sweep(orc_hmc_state* st, orc_hmc_rec* rec);
+
 /* Remez file reader (format of rhmc/remez*): returns 0 on success. */
 int orc_read_remez(const char* path, int n, orc_remez* r);
 

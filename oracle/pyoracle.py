@@ -66,6 +66,31 @@ class State(C.Structure):
                 ("gaction", C.c_float)]
 
 
+class HmcRec(C.Structure):
+    _fields_ = [("H0", C.c_double), ("H1", C.c_double), ("dH", C.c_double), ("dS", C.c_double),
+                ("S0", C.c_double), ("S1", C.c_double), ("hg", C.c_double), ("hp", C.c_double),
+                ("y", C.c_float), ("x", C.c_float), ("drew_x", C.c_int), ("accepted", C.c_int),
+                ("nsteps", C.c_int), ("it_h0", C.c_int), ("it_h1", C.c_int),
+                ("it_force", C.c_int), ("nforce", C.c_int), ("action", C.c_float),
+                ("gaction", C.c_float), ("paction", C.c_float), ("vel2", C.c_float),
+                ("measured", C.c_int), ("cond", C.c_float * 3), ("susc", C.c_float * 3),
+                ("condmod", C.c_float), ("susctot", C.c_float)]
+
+
+class HmcState(C.Structure):
+    _fields_ = [("lat", Lat), ("rng", Rng), ("dt", C.c_float), ("am", C.c_float),
+                ("imass", C.c_int), ("iterl", C.c_int), ("iprint", C.c_int),
+                ("rescga", C.c_float), ("rescgg", C.c_float),
+                ("chi", C.POINTER(C.c_float)), ("chit", C.POINTER(C.c_float)),
+                ("pp", C.POINTER(C.c_float)), ("dSdchi", C.POINTER(C.c_float)),
+                ("Phi", C.POINTER(C.c_float)), ("X0", C.POINTER(C.c_float)),
+                ("X1", C.POINTER(C.c_float)), ("R", C.POINTER(C.c_float)),
+                ("ps", C.POINTER(C.c_float)), ("isweep", C.c_int), ("itot", C.c_int),
+                ("naccp", C.c_int), ("action", C.c_float), ("gaction", C.c_float),
+                ("paction", C.c_float), ("actiona", C.c_float), ("vel2a", C.c_float),
+                ("yav", C.c_float), ("yyav", C.c_float)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -102,6 +127,16 @@ def lib():
         L.orc_state_set_remez.argtypes = [C.POINTER(State), C.c_int, P]
         L.orc_sweep.argtypes = [C.POINTER(State), P]
         L.orc_read_remez.argtypes = [C.c_char_p, C.c_int, P]
+        L.orc_hmc_dslash.argtypes = [P, P, P, P, C.c_int, C.c_int]
+        L.orc_hmc_congrad.argtypes = [P, P, C.c_float, P, C.c_int, P, P]
+        L.orc_hmc_derivs.argtypes = [P, P, P, C.c_int, P]
+        L.orc_hmc_force.argtypes = [P, P, P, P, P, C.c_float, C.c_int, P, P]
+        L.orc_hmc_hamilton.argtypes = [P, P, P, P, P, C.c_float, C.c_int, P, P]
+        L.orc_hmc_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                  C.c_float, C.c_int, C.c_int]
+        L.orc_hmc_new.restype = C.POINTER(HmcState)
+        L.orc_hmc_free.argtypes = [C.POINTER(HmcState)]
+        L.orc_hmc_sweep.argtypes = [C.POINTER(HmcState), P]
         _lib = L
     return _lib
 
@@ -158,6 +193,69 @@ def congrad(lat, Phi, chi, x0, res, hpin=0.0, imass=1, am=0.0):
     capped = lib().orc_congrad(C.byref(lat), _p(np.ascontiguousarray(Phi)), res, C.byref(it), am,
                                hpin, imass, _p(np.ascontiguousarray(chi)), _p(x))
     return x, it.value, capped
+
+
+# ---- the HMC predecessor (mh/cheisdwf_hmc.f), single precision ----------
+def hmc_dslash(lat, R, chi, imass=1, dag=False):
+    R = np.ascontiguousarray(R, dtype=np.complex64)
+    chi = np.ascontiguousarray(chi, dtype=np.float32)
+    out = np.empty_like(R)
+    lib().orc_hmc_dslash(C.byref(lat), _p(out), _p(R), _p(chi), imass, 1 if dag else 0)
+    return out
+
+
+def hmc_congrad(lat, Phi, chi, x0, res, imass=1):
+    x = np.ascontiguousarray(x0, dtype=np.complex64).copy()
+    it = C.c_int(0)
+    capped = lib().orc_hmc_congrad(C.byref(lat), _p(np.ascontiguousarray(Phi, dtype=np.complex64)),
+                                   res, C.byref(it), imass,
+                                   _p(np.ascontiguousarray(chi, dtype=np.float32)), _p(x))
+    return x, it.value, capped
+
+
+def hmc_derivs(lat, X1, chi, imass=1):
+    dS = np.empty((3, kvol(lat)), dtype=np.float32)
+    lib().orc_hmc_derivs(C.byref(lat), _p(np.ascontiguousarray(X1, dtype=np.complex64)),
+                         _p(np.ascontiguousarray(chi, dtype=np.float32)), imass, _p(dS))
+    return dS
+
+
+class HmcSweeper:
+    """The main loop of mh/cheisdwf_hmc.f (:140-320) over the oracle."""
+
+    def __init__(self, L, Lt, Ls, beta, am3, dt, am, imass, iterl, chi=None, seed=None,
+                 iprint=5):
+        self.lib = lib()
+        self.st = self.lib.orc_hmc_new(L, Lt, Ls, beta, am3, dt, am, imass, iterl)
+        self.st.contents.iprint = iprint
+        self.kvol = L * L * Lt
+        if chi is not None:
+            self.chi[:] = np.asarray(chi, dtype=np.float32).reshape(-1)
+        if seed is not None:
+            self.lib.orc_rng_startup(C.byref(self.st.contents.rng), float(seed))
+
+    @property
+    def chi(self):
+        return np.ctypeslib.as_array(self.st.contents.chi, shape=(3 * self.kvol,))
+
+    def seed(self):
+        return self.lib.orc_rranget(C.byref(self.st.contents.rng))
+
+    def sweep(self) -> HmcRec:
+        rec = HmcRec()
+        self.lib.orc_hmc_sweep(self.st, C.byref(rec))
+        return rec
+
+    def close(self):
+        if self.st:
+            self.lib.orc_hmc_free(self.st)
+            self.st = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def remez_struct(a0, anum, aden, b0, bnum, bden) -> Remez:
