@@ -52,6 +52,10 @@ EXPORTS = (
     "chdwf_prog_set_measure", "chdwf_prog_set_residuals", "chdwf_prog_sweep",
     "chdwf_prog_correlators", "chdwf_prog_last_error", "chdwf_prog_measure",
     "chdwf_traj_noise_solve",
+    "chdwf_hmc_create", "chdwf_hmc_destroy", "chdwf_hmc_last_error", "chdwf_hmc_dslash",
+    "chdwf_hmc_dslashd", "chdwf_hmc_congrad", "chdwf_hmc_derivs", "chdwf_hmc_set_chi",
+    "chdwf_hmc_get_chi", "chdwf_hmc_startup", "chdwf_hmc_seed", "chdwf_hmc_set_measure",
+    "chdwf_hmc_set_residuals", "chdwf_hmc_sweep",
     "chdwf_prog_sums", "chdwf_prog_reset_sums", "chdwf_prog_averages", "chdwf_prog_take_cg_caps",
     "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
@@ -131,6 +135,23 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_prog_correlators.argtypes = [P, P]
     L.chdwf_prog_measure.argtypes = [P, F, C.POINTER(F), C.POINTER(F), C.POINTER(F), P]
     L.chdwf_traj_noise_solve.argtypes = [P, P, I, I, F, F, F, I, P, PI]
+    L.chdwf_hmc_create.argtypes = [C.POINTER(P), I, I, I, F, F, F, F, I, I, I]
+    L.chdwf_hmc_destroy.argtypes = [P]
+    L.chdwf_hmc_destroy.restype = None
+    L.chdwf_hmc_last_error.argtypes = [P]
+    L.chdwf_hmc_last_error.restype = C.c_char_p
+    L.chdwf_hmc_dslash.argtypes = [P, P, P, P, I]
+    L.chdwf_hmc_dslashd.argtypes = [P, P, P, P, I]
+    L.chdwf_hmc_congrad.argtypes = [P, P, F, PI, I, P, P]
+    L.chdwf_hmc_derivs.argtypes = [P, P, P, I, P]
+    L.chdwf_hmc_set_chi.argtypes = [P, P]
+    L.chdwf_hmc_get_chi.argtypes = [P, P]
+    L.chdwf_hmc_startup.argtypes = [P, D]
+    L.chdwf_hmc_seed.argtypes = [P]
+    L.chdwf_hmc_seed.restype = D
+    L.chdwf_hmc_set_measure.argtypes = [P, I]
+    L.chdwf_hmc_set_residuals.argtypes = [P, F, F]
+    L.chdwf_hmc_sweep.argtypes = [P, P]
     L.chdwf_prog_last_error.argtypes = [P]
     L.chdwf_prog_last_error.restype = C.c_char_p
     L.chdwf_prog_stage.argtypes = [P, I]
@@ -606,3 +627,112 @@ def reference_remez() -> dict:
     remez4 (25 poles), remez2g (12 poles)."""
     return {"remez2": read_remez("remez2", 25), "remez4": read_remez("remez4", 25),
             "remez2g": read_remez("remez2g", 12)}
+
+
+class HmcRecord(C.Structure):
+    """chdwf_hmc_record (include/chdwf_hmc.h)."""
+    _fields_ = [("H0", C.c_double), ("H1", C.c_double), ("dH", C.c_double), ("dS", C.c_double),
+                ("S0", C.c_double), ("S1", C.c_double), ("hg", C.c_double), ("hp", C.c_double),
+                ("y", C.c_float), ("x", C.c_float), ("drew_x", C.c_int), ("accepted", C.c_int),
+                ("nsteps", C.c_int), ("it_h0", C.c_int), ("it_h1", C.c_int),
+                ("it_force", C.c_int), ("nforce", C.c_int), ("action", C.c_float),
+                ("gaction", C.c_float), ("paction", C.c_float), ("vel2", C.c_float),
+                ("measured", C.c_int), ("cond", C.c_float * 3), ("susc", C.c_float * 3),
+                ("condmod", C.c_float), ("susctot", C.c_float)]
+
+
+class Hmc:
+    """The HMC predecessor mh/cheisdwf_hmc.f on the GPU (include/chdwf_hmc.h):
+    single-precision operator, congrad, chi force and main loop.  Spinors are
+    complex64 of shape (2, 4, ksizet, ksize, ksize, kthird), chi float32
+    (3, kvol)."""
+
+    def __init__(self, ksize, ksizet, kthird, dt, beta, am3, am, imass, iterl, device=0):
+        self.lib = load_library()
+        self.kvol = ksize * ksize * ksizet
+        self.shape = (2, 4, ksizet, ksize, ksize, kthird)
+        self.imass = imass
+        h = C.c_void_p()
+        rc = self.lib.chdwf_hmc_create(C.byref(h), ksize, ksizet, kthird, dt, beta, am3, am,
+                                       imass, iterl, device)
+        if rc != CHDWF_OK:
+            raise ChdwfError(rc, self.lib.chdwf_hmc_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != CHDWF_OK:
+            msg = self.lib.chdwf_hmc_last_error(self.h).decode()
+            raise (IterationCapError if rc == CHDWF_ITER_CAP else ChdwfError)(rc, msg)
+
+    def _spinor(self, a):
+        a = np.ascontiguousarray(a, dtype=np.complex64)
+        if a.size != int(np.prod(self.shape)):
+            raise ValueError(f"spinor has {a.size} entries, expected shape {self.shape}")
+        return a
+
+    def _chi(self, chi):
+        chi = np.ascontiguousarray(chi, dtype=np.float32)
+        if chi.size != 3 * self.kvol:
+            raise ValueError(f"chi has {chi.size} entries, expected {3 * self.kvol}")
+        return chi
+
+    def dslash(self, R, chi, imass=None, dag=False):
+        R, chi = self._spinor(R), self._chi(chi)
+        out = np.empty(self.shape, dtype=np.complex64)
+        f = self.lib.chdwf_hmc_dslashd if dag else self.lib.chdwf_hmc_dslash
+        self._check(f(self.h, _ptr(out), _ptr(R), _ptr(chi), self.imass if imass is None else imass))
+        return out
+
+    def congrad(self, Phi, chi, x0, res, imass=None):
+        """x with M^dag M x = Phi from the guess x0; returns (x, itercg, capped)."""
+        Phi, chi = self._spinor(Phi), self._chi(chi)
+        x = self._spinor(x0).copy()
+        it = C.c_int(0)
+        rc = self.lib.chdwf_hmc_congrad(self.h, _ptr(Phi), res, C.byref(it),
+                                        self.imass if imass is None else imass, _ptr(chi), _ptr(x))
+        if rc not in (CHDWF_OK, CHDWF_ITER_CAP):
+            self._check(rc)
+        return x.reshape(self.shape), it.value, rc == CHDWF_ITER_CAP
+
+    def derivs(self, X1, chi, imass=None):
+        X1, chi = self._spinor(X1), self._chi(chi)
+        dS = np.empty((3, self.kvol), dtype=np.float32)
+        self._check(self.lib.chdwf_hmc_derivs(self.h, _ptr(X1), _ptr(chi),
+                                              self.imass if imass is None else imass, _ptr(dS)))
+        return dS
+
+    def set_chi(self, chi):
+        self._check(self.lib.chdwf_hmc_set_chi(self.h, _ptr(self._chi(chi))))
+
+    def get_chi(self):
+        chi = np.empty((3, self.kvol), dtype=np.float32)
+        self._check(self.lib.chdwf_hmc_get_chi(self.h, _ptr(chi)))
+        return chi
+
+    def startup(self, seed):
+        self._check(self.lib.chdwf_hmc_startup(self.h, float(seed)))
+
+    def seed(self):
+        return self.lib.chdwf_hmc_seed(self.h)
+
+    def set_measure(self, iprint):
+        self._check(self.lib.chdwf_hmc_set_measure(self.h, iprint))
+
+    def set_residuals(self, rescga, rescgg):
+        self._check(self.lib.chdwf_hmc_set_residuals(self.h, rescga, rescgg))
+
+    def sweep(self) -> HmcRecord:
+        rec = HmcRecord()
+        self._check(self.lib.chdwf_hmc_sweep(self.h, C.byref(rec)))
+        return rec
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chdwf_hmc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

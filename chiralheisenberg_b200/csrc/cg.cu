@@ -20,25 +20,7 @@ struct LdCg {
 
 __device__ __forceinline__ bool cg_last_block(double v, double* part, unsigned* count,
                                               double* total) {
-    __shared__ double sh[kThreads / 32];
-    __shared__ bool is_last;
-    v = block_sum<kThreads>(v, sh);
-    if (threadIdx.x == 0) {
-        part[blockIdx.x] = v;
-        __threadfence();
-        is_last = (atomicAdd(count, 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!is_last) return false;
-    __threadfence();
-    double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += ((volatile double*)part)[i];
-    s = block_sum<kThreads>(s, sh);
-    if (threadIdx.x == 0) {
-        *total = s;
-        *count = 0;
-    }
-    return true;
+    return last_block_total<kThreads>(v, part, count, total);
 }
 
 // The stencil kernels are flavour-split: two threads per point (one per

@@ -109,4 +109,33 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return r;  // valid in thread 0
 }
 
+// Grid-wide sum of one double per thread: each block writes its block sum to
+// part[blockIdx.x]; the block that arrives last (counted in *count) adds the
+// partials in block order, stores the total in *total (thread 0), resets the
+// counter for the next launch and returns true.  Every other block returns
+// false.  The result does not depend on the order in which blocks finish.
+template <int NT>
+__device__ __forceinline__ bool last_block_total(double v, double* part, unsigned* count,
+                                                 double* total) {
+    __shared__ double sh[NT / 32];
+    __shared__ bool is_last;
+    v = block_sum<NT>(v, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = v;
+        __threadfence();
+        is_last = (atomicAdd(count, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += ((volatile double*)part)[i];
+    s = block_sum<NT>(s, sh);
+    if (threadIdx.x == 0) {
+        *total = s;
+        *count = 0;
+    }
+    return true;
+}
+
 }  // namespace chdwf
