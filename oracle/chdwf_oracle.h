@@ -200,6 +200,61 @@ void orc_hmc_free(orc_hmc_state* st);
 /* One sweep of the main loop of mh/cheisdwf_hmc.f (:140-320). */
 void orc_hmc_sweep(orc_hmc_state* st, orc_hmc_rec* rec);
 
+/* --- the bulk Thirring RHMC, bulk_rhmc.f (chdwf_oracle_thirring.c) ------
+ * spinors R(s, site, d) complex128 (4 Dirac components, one flavour); link
+ * angles theta(kvol,3) REAL*4; links u(kvol,3) complex128. */
+void orc_thr_coef(const orc_lat* lat, const float* theta, double* u);
+void orc_thr_dslash(const orc_lat* lat, double* Phi, const double* R, const double* u, float am,
+                    int imass, int dag);
+void orc_thr_derivs(const orc_lat* lat, const double* R, const double* X2, double anum,
+                    int iflag, float* dSdpi);
+int orc_thr_qmrherm(const orc_lat* lat, const double* Phi, float res, int* itercg, float am,
+                    int imass, const double* anum, const double* aden, int ndiag, int iflag,
+                    const double* u, double* x, double* Phi0, float* dSdpi);
+
+typedef struct {
+    double H0, H1, dH, dS, S0, S1, hg, hp;
+    float y, x;
+    int drew_x, accepted, nsteps;
+    int it_pf, it_pfpv, it_h0, it_h0pv, it_h1, it_h1pv;
+    int it_force[4];   /* summed per force solve: PV (iflag 1), m, DWF force, PV force */
+    int nforce;
+    float action, gaction, paction, vel2;
+} orc_thr_rec;
+
+typedef struct {
+    orc_lat lat;
+    orc_rng rng;
+    orc_remez r2, r4, r2g, r4g;
+    float dt, am;
+    int imass, iterl, iprint;
+    float rescga, rescgg;
+    float* theta;      /* /gauge/ theta(kvol,3) */
+    float* thetat;     /* /trial/ thetat     */
+    float* pp;         /* /trial/ pp         */
+    float* dSdpi;      /* /gforce/           */
+    double* ut;        /* /trial/ ut         */
+    double* Phi;       /* pseudofermion      */
+    double* X1;        /* /vector/           */
+    double* R;         /* /dum1/ R           */
+    double* Phi0;      /* /phi0/ Phi0(kferm,25) */
+    float* ps;         /* /dum1/ ps(kvol,2)  */
+    int isweep, itot, naccp;
+    float action, gaction, paction;
+    float actiona, vel2a, yav, yyav;
+} orc_thr_state;
+
+orc_thr_state* orc_thr_new(int L, int Lt, int Ls, float beta, float am3, float dt, float am,
+                           int imass, int iterl);
+void orc_thr_free(orc_thr_state* st);
+/* which: 2, 4 (remez2, remez4), 22, 44 (remez2g, remez4g) */
+void orc_thr_set_remez(orc_thr_state* st, int which, const orc_remez* r);
+void orc_thr_force(orc_thr_state* st, float res1, int* its);
+void orc_thr_hamilton(orc_thr_state* st, float res2, double* out, int* its);
+/* One sweep of the main loop of bulk_rhmc.f (:205-400) without its
+ * measurement (measure, every iprint-th sweep). */
+void orc_thr_sweep(orc_thr_state* st, orc_thr_rec* rec);
+
 /* Remez file reader (format of rhmc/remez*): returns 0 on success. */
 int orc_read_remez(const char* path, int n, orc_remez* r);
 

@@ -91,6 +91,32 @@ class HmcState(C.Structure):
                 ("yav", C.c_float), ("yyav", C.c_float)]
 
 
+class ThrRec(C.Structure):
+    _fields_ = [("H0", C.c_double), ("H1", C.c_double), ("dH", C.c_double), ("dS", C.c_double),
+                ("S0", C.c_double), ("S1", C.c_double), ("hg", C.c_double), ("hp", C.c_double),
+                ("y", C.c_float), ("x", C.c_float), ("drew_x", C.c_int), ("accepted", C.c_int),
+                ("nsteps", C.c_int), ("it_pf", C.c_int), ("it_pfpv", C.c_int),
+                ("it_h0", C.c_int), ("it_h0pv", C.c_int), ("it_h1", C.c_int),
+                ("it_h1pv", C.c_int), ("it_force", C.c_int * 4), ("nforce", C.c_int),
+                ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
+                ("vel2", C.c_float)]
+
+
+class ThrState(C.Structure):
+    _fields_ = [("lat", Lat), ("rng", Rng), ("r2", Remez), ("r4", Remez), ("r2g", Remez),
+                ("r4g", Remez), ("dt", C.c_float), ("am", C.c_float), ("imass", C.c_int),
+                ("iterl", C.c_int), ("iprint", C.c_int), ("rescga", C.c_float),
+                ("rescgg", C.c_float), ("theta", C.POINTER(C.c_float)),
+                ("thetat", C.POINTER(C.c_float)), ("pp", C.POINTER(C.c_float)),
+                ("dSdpi", C.POINTER(C.c_float)), ("ut", C.POINTER(C.c_double)),
+                ("Phi", C.POINTER(C.c_double)), ("X1", C.POINTER(C.c_double)),
+                ("R", C.POINTER(C.c_double)), ("Phi0", C.POINTER(C.c_double)),
+                ("ps", C.POINTER(C.c_float)), ("isweep", C.c_int), ("itot", C.c_int),
+                ("naccp", C.c_int), ("action", C.c_float), ("gaction", C.c_float),
+                ("paction", C.c_float), ("actiona", C.c_float), ("vel2a", C.c_float),
+                ("yav", C.c_float), ("yyav", C.c_float)]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -137,6 +163,19 @@ def lib():
         L.orc_hmc_new.restype = C.POINTER(HmcState)
         L.orc_hmc_free.argtypes = [C.POINTER(HmcState)]
         L.orc_hmc_sweep.argtypes = [C.POINTER(HmcState), P]
+        L.orc_thr_coef.argtypes = [P, P, P]
+        L.orc_thr_dslash.argtypes = [P, P, P, P, C.c_float, C.c_int, C.c_int]
+        L.orc_thr_derivs.argtypes = [P, P, P, C.c_double, C.c_int, P]
+        L.orc_thr_qmrherm.argtypes = [P, P, C.c_float, P, C.c_float, C.c_int, P, P, C.c_int,
+                                      C.c_int, P, P, P, P]
+        L.orc_thr_new.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                  C.c_float, C.c_int, C.c_int]
+        L.orc_thr_new.restype = C.POINTER(ThrState)
+        L.orc_thr_free.argtypes = [C.POINTER(ThrState)]
+        L.orc_thr_set_remez.argtypes = [C.POINTER(ThrState), C.c_int, P]
+        L.orc_thr_force.argtypes = [C.POINTER(ThrState), C.c_float, P]
+        L.orc_thr_hamilton.argtypes = [C.POINTER(ThrState), C.c_float, P, P]
+        L.orc_thr_sweep.argtypes = [C.POINTER(ThrState), P]
         _lib = L
     return _lib
 
@@ -249,6 +288,88 @@ class HmcSweeper:
     def close(self):
         if self.st:
             self.lib.orc_hmc_free(self.st)
+            self.st = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- the bulk Thirring RHMC (bulk_rhmc.f) ---------------------------------
+def thr_shape(lat):
+    return (4, lat.Lt, lat.L, lat.L, lat.Ls)
+
+
+def thr_coef(lat, theta):
+    u = np.empty((3, kvol(lat)), dtype=np.complex128)
+    lib().orc_thr_coef(C.byref(lat), _p(np.ascontiguousarray(theta, dtype=np.float32)), _p(u))
+    return u
+
+
+def thr_dslash(lat, R, u, am, imass=1, dag=False):
+    R = np.ascontiguousarray(R, dtype=np.complex128)
+    out = np.empty_like(R)
+    lib().orc_thr_dslash(C.byref(lat), _p(out), _p(R), _p(np.ascontiguousarray(u)), am, imass,
+                         1 if dag else 0)
+    return out
+
+
+def thr_derivs(lat, R, X2, anum, iflag, dSdpi=None):
+    dS = np.zeros((3, kvol(lat)), dtype=np.float32) if dSdpi is None else dSdpi
+    lib().orc_thr_derivs(C.byref(lat), _p(np.ascontiguousarray(R)), _p(np.ascontiguousarray(X2)),
+                         float(anum), iflag, _p(dS))
+    return dS
+
+
+def thr_qmrherm(lat, Phi, u, res, am, imass, anum, aden, iflag=0, Phi0=None, dSdpi=None):
+    """Returns (x, itercg, capped, Phi0, dSdpi)."""
+    n = len(aden)
+    sh = thr_shape(lat)
+    x = np.empty(sh, dtype=np.complex128)
+    P0 = np.zeros((n,) + sh, dtype=np.complex128) if Phi0 is None else Phi0
+    dS = np.zeros((3, kvol(lat)), dtype=np.float32) if dSdpi is None else dSdpi
+    it = C.c_int(0)
+    capped = lib().orc_thr_qmrherm(
+        C.byref(lat), _p(np.ascontiguousarray(Phi, dtype=np.complex128)), res, C.byref(it), am,
+        imass, _p(np.ascontiguousarray(anum, dtype=np.float64)),
+        _p(np.ascontiguousarray(aden, dtype=np.float64)), n, iflag, _p(np.ascontiguousarray(u)),
+        _p(x), _p(P0), _p(dS))
+    return x, it.value, capped, P0, dS
+
+
+class ThrSweeper:
+    """The main loop of bulk_rhmc.f (:201-400) over the oracle, without the
+    measurement sweeps."""
+
+    def __init__(self, L, Lt, Ls, beta, am3, dt, am, imass, iterl, r2, r4, r2g, r4g,
+                 theta=None, seed=None):
+        self.lib = lib()
+        self.st = self.lib.orc_thr_new(L, Lt, Ls, beta, am3, dt, am, imass, iterl)
+        for which, r in ((2, r2), (4, r4), (22, r2g), (44, r4g)):
+            self.lib.orc_thr_set_remez(self.st, which, C.byref(r))
+        self.kvol = L * L * Lt
+        if theta is not None:
+            self.theta[:] = np.asarray(theta, dtype=np.float32).reshape(-1)
+        if seed is not None:
+            self.lib.orc_rng_startup(C.byref(self.st.contents.rng), float(seed))
+
+    @property
+    def theta(self):
+        return np.ctypeslib.as_array(self.st.contents.theta, shape=(3 * self.kvol,))
+
+    def seed(self):
+        return self.lib.orc_rranget(C.byref(self.st.contents.rng))
+
+    def sweep(self) -> ThrRec:
+        rec = ThrRec()
+        self.lib.orc_thr_sweep(self.st, C.byref(rec))
+        return rec
+
+    def close(self):
+        if self.st:
+            self.lib.orc_thr_free(self.st)
             self.st = None
 
     def __del__(self):

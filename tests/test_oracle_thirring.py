@@ -1,0 +1,195 @@
+"""CPU tests of the oracle's restatement of the bulk Thirring RHMC,
+bulk_rhmc.f (oracle/chdwf_oracle_thirring.c).
+
+Pins: at theta = 0 its operator equals the flavour-1 block of the RHMC
+operator of rhmc/cheisdwf.f (itself pinned by its two formulations) with
+chi = (0, 0, +-am); M^dagger is the adjoint of M for the three mass terms;
+derivs computes the identities its header states (R^dag (M^dag)' X2 and
+R^dag M' X2, times 2*anum) against the exact theta-derivative of M, which
+is linear in theta; qmrherm against a dense rational evaluation; the
+random stream of a sweep replayed draw by draw.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+
+SEED = 693764523745.0
+
+
+def _fields(lat, seed):
+    rng = np.random.default_rng(seed)
+    sh = po.thr_shape(lat)
+    R = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    theta = (0.3 * rng.standard_normal((3, po.kvol(lat)))).astype(np.float32)
+    return R, theta
+
+
+def _dense(lat, u, am, imass, dag=False):
+    sh = po.thr_shape(lat)
+    n = int(np.prod(sh))
+    M = np.zeros((n, n), complex)
+    e = np.zeros(n, complex)
+    for i in range(n):
+        e[:] = 0
+        e[i] = 1
+        M[:, i] = po.thr_dslash(lat, e.reshape(sh), u, am, imass, dag=dag).reshape(-1)
+    return M
+
+
+@pytest.mark.parametrize("imass,c3", [(1, 0.25), (3, -0.25)])
+def test_thirring_operator_free_field_is_rhmc_block(imass, c3):
+    lat = po.make_lat(4, 4, 4)
+    kv = po.kvol(lat)
+    R, _ = _fields(lat, 1)
+    u0 = po.thr_coef(lat, np.zeros((3, kv), np.float32))
+    Rf = np.zeros((2,) + R.shape, complex)
+    Rf[0] = R
+    chi = np.zeros((3, kv))
+    chi[2] = c3
+    for dag in (False, True):
+        a = po.thr_dslash(lat, R, u0, 0.25, imass, dag=dag)
+        b = po.dslash(lat, Rf, chi, imass=imass, dag=dag)
+        assert np.abs(a - b[0]).max() <= 1e-13 * np.abs(b[0]).max()
+        assert not b[1].any()
+
+
+@pytest.mark.parametrize("imass", [1, 3, 5])
+def test_thirring_operator_adjoint(imass):
+    lat = po.make_lat(4, 4, 4)
+    R, theta = _fields(lat, 2)
+    y, _ = _fields(lat, 3)
+    u = po.thr_coef(lat, theta)
+    lhs = np.vdot(y, po.thr_dslash(lat, R, u, 0.2, imass))
+    rhs = np.vdot(po.thr_dslash(lat, y, u, 0.2, imass, dag=True), R)
+    assert abs(lhs - rhs) <= 1e-13 * abs(lhs)
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_thirring_derivs_identities(imass):
+    """derivs(R, X2, anum, 0) = 2 anum Re R^dag (dM^dag/dtheta) X2 and
+    derivs(R, X2, anum, 1) = 2 anum Re R^dag (dM/dtheta) X2, after the sign
+    that force puts on the t links of the last slice (bulk_rhmc.f:520-525).
+    anum = 0.375 keeps 2*anum exact in the REAL*4 tzi."""
+    L, Lt, Ls, am, anum = 2, 4, 3, 0.2, 0.375
+    lat = po.make_lat(L, Lt, Ls)
+    kv = po.kvol(lat)
+    R, theta = _fields(lat, 4)
+    X2, _ = _fields(lat, 5)
+    M0 = _dense(lat, po.thr_coef(lat, theta), am, imass)
+    g_dag, g_m = np.zeros((3, kv)), np.zeros((3, kv))
+    for mu in range(3):
+        for i in range(kv):
+            th = theta.copy()
+            th[mu, i] += 1.0
+            dM = _dense(lat, po.thr_coef(lat, th), am, imass) - M0
+            g_m[mu, i] = np.vdot(R.reshape(-1), dM @ X2.reshape(-1)).real
+            g_dag[mu, i] = np.vdot(R.reshape(-1), dM.conj().T @ X2.reshape(-1)).real
+    last = np.arange((Lt - 1) * L * L, kv)
+    for iflag, g in ((0, g_dag), (1, g_m)):
+        d = po.thr_derivs(lat, R, X2, anum, iflag).astype(float)
+        d[2, last] *= -1
+        assert np.abs(d - 2 * anum * g).max() <= 1e-6 * np.abs(g).max() * 2 * anum
+
+
+def test_thirring_qmrherm_matches_dense_rational(remez):
+    lat = po.make_lat(2, 4, 4)
+    R, theta = _fields(lat, 6)
+    u = po.thr_coef(lat, theta)
+    for am, imass in ((0.2, 1), (1.0, 1), (0.2, 3)):
+        M = _dense(lat, u, am, imass)
+        w, V = np.linalg.eigh(M.conj().T @ M)
+        r = remez["remez4"]
+        x, it, capped, _, _ = po.thr_qmrherm(lat, R, u, 1e-9, am, imass, r["anum"], r["aden"])
+        assert not capped and 2 <= it < 7500
+        f = r["anum"][0] + sum(r["anum"][k + 1] / (w + r["aden"][k]) for k in range(len(r["aden"])))
+        exact = V @ (f * (V.conj().T @ R.reshape(-1)))
+        # alphatild and beta0 are REAL*4 in bulk_rhmc.f (implicit typing), so
+        # the Lanczos recurrences carry 1e-7 relative errors: 6e-8 measured
+        assert np.linalg.norm(x.reshape(-1) - exact) <= 1e-6 * np.linalg.norm(exact)
+
+
+def test_thirring_phi0_register_and_force_terms(remez):
+    """iflag 1 stores the pole solutions in Phi0; iflag 2 adds
+    -sum_k anum_k * 2 Re x_k^dag (M^dag M)' x_k (through derivs with M x_k),
+    iflag 3 the PV cross term from Phi0 -- checked against derivs called
+    directly on the same pole solutions."""
+    lat = po.make_lat(2, 4, 4)
+    R, theta = _fields(lat, 7)
+    u = po.thr_coef(lat, theta)
+    r = remez["remez2g"]
+    n = len(r["aden"])
+    x, _, _, P0, _ = po.thr_qmrherm(lat, R, u, 1e-9, 0.2, 1, r["anum"], r["aden"], iflag=1)
+    assert np.abs(P0).max() > 0
+    _, _, _, _, dS2 = po.thr_qmrherm(lat, R, u, 1e-9, 0.2, 1, r["anum"], r["aden"], iflag=2)
+    ref = np.zeros_like(dS2)
+    for k in range(n):
+        po.thr_derivs(lat, P0[k], po.thr_dslash(lat, P0[k], u, 0.2, 1), r["anum"][k + 1], 0, ref)
+    assert np.array_equal(dS2, ref)
+    _, _, _, _, dS3 = po.thr_qmrherm(lat, R, u, 1e-9, 0.2, 1, r["anum"], r["aden"], iflag=3,
+                                     Phi0=P0)
+    ref = np.zeros_like(dS3)
+    for k in range(n):
+        c = -r["anum"][k + 1]
+        po.thr_derivs(lat, P0[k], po.thr_dslash(lat, P0[k], u, 0.2, 1), c, 0, ref)
+        po.thr_derivs(lat, po.thr_dslash(lat, P0[k], u, 0.2, 1), P0[k], c, 1, ref)
+    assert np.array_equal(dS3, ref)
+
+
+def _remez_sets(remez):
+    """remez2, remez4, remez2g as shipped; the 12-pole remez4g of the Thirring
+    runs is not in the repository, so the 25-pole remez4 (the same function)
+    stands in for it."""
+    return [po.remez_struct(r["anum"][0], r["anum"][1:], r["aden"], r["bnum"][0], r["bnum"][1:],
+                            r["bden"]) for r in (remez["remez2"], remez["remez4"],
+                                                 remez["remez2g"], remez["remez4"])]
+
+
+def test_thirring_sweep_stream(remez):
+    """Two sweeps (no measurement sweep): the generator advances by exactly
+    4*kthird gauss0, 3 gaussp, one rano(yran) per MD step and one more only
+    when dH < 0 (bulk_rhmc.f:213-222, :255-260, :302, :333-336)."""
+    L, Lt, Ls, iterl = 2, 4, 4, 4
+    kv = L * L * Lt
+    theta = (0.2 * np.random.default_rng(8).standard_normal((3, kv))).astype(np.float32)
+    sw = po.ThrSweeper(L, Lt, Ls, 0.5, 1.0, 0.1, 0.2, 1, iterl, *_remez_sets(remez), theta=theta,
+                       seed=SEED)
+    rand = po.Rand(SEED)
+    proby = np.float32(1.0) / np.float32(iterl)
+    for _ in range(2):
+        rec = sw.sweep()
+        for _ in range(4 * Ls):
+            rand.gauss0(kv)
+        for _ in range(3):
+            rand.gaussp(kv)
+        n = 0
+        while True:
+            n += 1
+            if rand.rano("yran") < proby or n == 1000:
+                break
+        assert rec.nsteps == n and rec.nforce == n + 1
+        assert rec.drew_x == (rec.dH < 0)
+        if rec.drew_x:
+            assert rec.x == np.float32(rand.rano("yran"))
+        assert sw.seed() == rand.seed()
+    sw.close()
+
+
+def test_thirring_force_conserves_energy(remez):
+    """The force (both rational solves, the PV terms from Phi0, the
+    antiperiodic sign and beta*theta) is the gradient of the Hamiltonian:
+    over the same trajectories (the draws do not depend on dt) |dH| falls by
+    about 4x when dt is halved, and stays below 1e-4 |H|."""
+    L, Lt, Ls, iterl = 2, 4, 4, 4
+    kv = L * L * Lt
+    dHs = {}
+    for dt in (0.1, 0.05):
+        theta = (0.2 * np.random.default_rng(8).standard_normal((3, kv))).astype(np.float32)
+        sw = po.ThrSweeper(L, Lt, Ls, 0.5, 1.0, dt, 0.2, 1, iterl, *_remez_sets(remez),
+                           theta=theta, seed=SEED)
+        dHs[dt] = [(r.dH, r.H0, r.nsteps) for r in (sw.sweep(), sw.sweep())]
+        sw.close()
+    for (a, h, na), (b, _, nb) in zip(dHs[0.1], dHs[0.05]):
+        assert na == nb
+        assert abs(a) < 1e-4 * abs(h)
+        assert abs(b) < 0.35 * abs(a)
