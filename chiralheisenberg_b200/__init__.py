@@ -56,6 +56,10 @@ EXPORTS = (
     "chdwf_hmc_dslashd", "chdwf_hmc_congrad", "chdwf_hmc_derivs", "chdwf_hmc_set_chi",
     "chdwf_hmc_get_chi", "chdwf_hmc_startup", "chdwf_hmc_seed", "chdwf_hmc_set_measure",
     "chdwf_hmc_set_residuals", "chdwf_hmc_sweep",
+    "chdwf_thr_create", "chdwf_thr_destroy", "chdwf_thr_last_error", "chdwf_thr_set_remez",
+    "chdwf_thr_coef", "chdwf_thr_dslash", "chdwf_thr_dslashd", "chdwf_thr_derivs",
+    "chdwf_thr_qmrherm", "chdwf_thr_set_theta", "chdwf_thr_get_theta", "chdwf_thr_startup",
+    "chdwf_thr_seed", "chdwf_thr_sweep",
     "chdwf_prog_sums", "chdwf_prog_reset_sums", "chdwf_prog_averages", "chdwf_prog_take_cg_caps",
     "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
@@ -152,6 +156,23 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_hmc_set_measure.argtypes = [P, I]
     L.chdwf_hmc_set_residuals.argtypes = [P, F, F]
     L.chdwf_hmc_sweep.argtypes = [P, P]
+    L.chdwf_thr_create.argtypes = [C.POINTER(P), I, I, I, F, F, F, F, I, I, I]
+    L.chdwf_thr_destroy.argtypes = [P]
+    L.chdwf_thr_destroy.restype = None
+    L.chdwf_thr_last_error.argtypes = [P]
+    L.chdwf_thr_last_error.restype = C.c_char_p
+    L.chdwf_thr_set_remez.argtypes = [P, I, P, P, P, P, I]
+    L.chdwf_thr_coef.argtypes = [P, P, P]
+    L.chdwf_thr_dslash.argtypes = [P, P, P, P, F, I]
+    L.chdwf_thr_dslashd.argtypes = [P, P, P, P, F, I]
+    L.chdwf_thr_derivs.argtypes = [P, P, P, D, I, P]
+    L.chdwf_thr_qmrherm.argtypes = [P, P, F, PI, F, I, P, P, I, I, P, P, P, P]
+    L.chdwf_thr_set_theta.argtypes = [P, P]
+    L.chdwf_thr_get_theta.argtypes = [P, P]
+    L.chdwf_thr_startup.argtypes = [P, D]
+    L.chdwf_thr_seed.argtypes = [P]
+    L.chdwf_thr_seed.restype = D
+    L.chdwf_thr_sweep.argtypes = [P, P]
     L.chdwf_prog_last_error.argtypes = [P]
     L.chdwf_prog_last_error.restype = C.c_char_p
     L.chdwf_prog_stage.argtypes = [P, I]
@@ -729,6 +750,122 @@ class Hmc:
     def close(self):
         if getattr(self, "h", None):
             self.lib.chdwf_hmc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ThirringRecord(C.Structure):
+    """chdwf_thr_record (include/chdwf_thirring.h)."""
+    _fields_ = [("H0", C.c_double), ("H1", C.c_double), ("dH", C.c_double), ("dS", C.c_double),
+                ("S0", C.c_double), ("S1", C.c_double), ("hg", C.c_double), ("hp", C.c_double),
+                ("y", C.c_float), ("x", C.c_float), ("drew_x", C.c_int), ("accepted", C.c_int),
+                ("nsteps", C.c_int), ("it_pf", C.c_int), ("it_pfpv", C.c_int),
+                ("it_h0", C.c_int), ("it_h0pv", C.c_int), ("it_h1", C.c_int),
+                ("it_h1pv", C.c_int), ("it_force", C.c_int * 4), ("nforce", C.c_int),
+                ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
+                ("vel2", C.c_float)]
+
+
+class Thirring:
+    """The bulk Thirring RHMC of bulk_rhmc.f on the GPU
+    (include/chdwf_thirring.h).  Spinors are complex128 of shape
+    (4, ksizet, ksize, ksize, kthird), links u complex128 (3, kvol), link
+    angles theta and the force float32 (3, kvol)."""
+
+    def __init__(self, ksize, ksizet, kthird, dt, beta, am3, am, imass, iterl, device=0):
+        self.lib = load_library()
+        self.kvol = ksize * ksize * ksizet
+        self.shape = (4, ksizet, ksize, ksize, kthird)
+        h = C.c_void_p()
+        rc = self.lib.chdwf_thr_create(C.byref(h), ksize, ksizet, kthird, dt, beta, am3, am,
+                                       imass, iterl, device)
+        if rc != CHDWF_OK:
+            raise ChdwfError(rc, self.lib.chdwf_thr_last_error(None).decode())
+        self.h = h
+        self._keep = {}
+
+    def _check(self, rc):
+        if rc != CHDWF_OK:
+            msg = self.lib.chdwf_thr_last_error(self.h).decode()
+            raise (IterationCapError if rc == CHDWF_ITER_CAP else ChdwfError)(rc, msg)
+
+    def _spinor(self, a):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        if a.size != int(np.prod(self.shape)):
+            raise ValueError(f"spinor has {a.size} entries, expected shape {self.shape}")
+        return a
+
+    def set_remez(self, which, r):
+        """which: 2, 4 (remez2, remez4) or 22, 44 (remez2g, remez4g); r a dict
+        with anum, aden, bnum, bden as read from the file."""
+        arrs = [np.ascontiguousarray(r[k], dtype=np.float64) for k in ("anum", "aden", "bnum", "bden")]
+        self._check(self.lib.chdwf_thr_set_remez(self.h, which, *[_ptr(a) for a in arrs],
+                                                 len(arrs[1])))
+        self._keep[which] = arrs
+
+    def coef(self, theta):
+        u = np.empty((3, self.kvol), dtype=np.complex128)
+        self._check(self.lib.chdwf_thr_coef(self.h, _ptr(np.ascontiguousarray(theta, dtype=np.float32)),
+                                            _ptr(u)))
+        return u
+
+    def dslash(self, R, u, am, imass, dag=False):
+        R = self._spinor(R)
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        out = np.empty(self.shape, dtype=np.complex128)
+        f = self.lib.chdwf_thr_dslashd if dag else self.lib.chdwf_thr_dslash
+        self._check(f(self.h, _ptr(out), _ptr(R), _ptr(u), am, imass))
+        return out
+
+    def derivs(self, R, X2, anum, iflag, dSdpi=None):
+        dS = np.zeros((3, self.kvol), dtype=np.float32) if dSdpi is None else dSdpi
+        self._check(self.lib.chdwf_thr_derivs(self.h, _ptr(self._spinor(R)), _ptr(self._spinor(X2)),
+                                              float(anum), iflag, _ptr(dS)))
+        return dS
+
+    def qmrherm(self, Phi, u, res, am, imass, anum, aden, iflag=0, Phi0=None, dSdpi=None):
+        """Returns (x, itercg, capped, Phi0, dSdpi)."""
+        n = len(aden)
+        x = np.empty(self.shape, dtype=np.complex128)
+        P0 = np.zeros((n,) + self.shape, dtype=np.complex128) if Phi0 is None else Phi0
+        dS = np.zeros((3, self.kvol), dtype=np.float32) if dSdpi is None else dSdpi
+        it = C.c_int(0)
+        rc = self.lib.chdwf_thr_qmrherm(
+            self.h, _ptr(self._spinor(Phi)), res, C.byref(it), am, imass,
+            _ptr(np.ascontiguousarray(anum, dtype=np.float64)),
+            _ptr(np.ascontiguousarray(aden, dtype=np.float64)), n, iflag,
+            _ptr(np.ascontiguousarray(u, dtype=np.complex128)), _ptr(x), _ptr(P0), _ptr(dS))
+        if rc not in (CHDWF_OK, CHDWF_ITER_CAP):
+            self._check(rc)
+        return x, it.value, rc == CHDWF_ITER_CAP, P0, dS
+
+    def set_theta(self, theta):
+        self._check(self.lib.chdwf_thr_set_theta(self.h, _ptr(np.ascontiguousarray(theta, dtype=np.float32))))
+
+    def get_theta(self):
+        th = np.empty((3, self.kvol), dtype=np.float32)
+        self._check(self.lib.chdwf_thr_get_theta(self.h, _ptr(th)))
+        return th
+
+    def startup(self, seed):
+        self._check(self.lib.chdwf_thr_startup(self.h, float(seed)))
+
+    def seed(self):
+        return self.lib.chdwf_thr_seed(self.h)
+
+    def sweep(self) -> ThirringRecord:
+        rec = ThirringRecord()
+        self._check(self.lib.chdwf_thr_sweep(self.h, C.byref(rec)))
+        return rec
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chdwf_thr_destroy(self.h)
             self.h = None
 
     def __del__(self):

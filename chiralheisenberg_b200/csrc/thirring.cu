@@ -1,0 +1,829 @@
+// thirring.cu -- the bulk Thirring RHMC, bulk_rhmc.f, on the GPU: its link
+// operator, multi-shift solver with the Phi0 register, link force, force and
+// Hamiltonian with the Pauli-Villars terms, and main loop
+// (include/chdwf_thirring.h).
+//
+// The operator is a chain of sweeps in the reference (diagonal, Wilson and
+// Dirac hops through the links, s hops, wall mass term).  One thread per
+// spinor element replays the chain for its element in FP64 with
+// round-to-nearest intrinsics, so the result equals the sequential
+// evaluation bit for bit.  derivs gives one thread to each link (site, mu)
+// and adds its 8*kthird terms in the reference's order into a REAL*4
+// register, also bit for bit.  The multi-shift solver runs its scalar
+// recurrences on the host with the reference's implicit REAL*4 / REAL*8
+// types; its sums are FP64 block partials added in block order.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "chdwf_thirring.h"
+#include "common.cuh"
+#include "internal.h"
+#include "rng.h"
+
+namespace chdwf {
+namespace {
+
+constexpr int kThrMaxPoles = 25;
+constexpr int kRedBlocks = 592;           // 4 per SM, fixed: partials summed in block order
+
+struct TGeom {
+    int L, Lt, Ls, kvol;
+    int64_t kferm;                        // 4*kvol*Ls
+};
+
+// gamval(mu,idirac)*akappa, gamin(mu,idirac) - 1 (bulk_rhmc.f:1646-1722)
+__constant__ double2 c_tgv[3][4] = {{{0., -0.5}, {0., -0.5}, {0., 0.5}, {0., 0.5}},
+                                    {{-0.5, 0.}, {0.5, 0.}, {0.5, 0.}, {-0.5, 0.}},
+                                    {{0., -0.5}, {0., 0.5}, {0., 0.5}, {0., -0.5}}};
+__constant__ int c_tgi[3][4] = {{3, 2, 1, 0}, {3, 2, 1, 0}, {2, 3, 0, 1}};
+
+__device__ __forceinline__ int64_t tsite(int L, int x, int y, int t) {
+    return x + (int64_t)L * (y + (int64_t)L * t);
+}
+
+// the periodic neighbours up/down of site (x, y, t) in direction mu (addrc, :1746-1797)
+__device__ __forceinline__ void tnbr(const TGeom& g, int x, int y, int t, int mu, int64_t* up,
+                                     int64_t* dn) {
+    if (mu == 0) {
+        *up = tsite(g.L, x + 1 == g.L ? 0 : x + 1, y, t);
+        *dn = tsite(g.L, x == 0 ? g.L - 1 : x - 1, y, t);
+    } else if (mu == 1) {
+        *up = tsite(g.L, x, y + 1 == g.L ? 0 : y + 1, t);
+        *dn = tsite(g.L, x, y == 0 ? g.L - 1 : y - 1, t);
+    } else {
+        *up = tsite(g.L, x, y, t + 1 == g.Lt ? 0 : t + 1);
+        *dn = tsite(g.L, x, y, t == 0 ? g.Lt - 1 : t - 1);
+    }
+}
+
+// One element (s, site, d) of Phi = M R (DAG false, :1946-2069) or
+// Phi = M^dagger R (DAG true, :2071-2188).
+template <bool DAG, int IMASS>
+__device__ double2 thr_element(const double2* __restrict__ R, const double2* __restrict__ u,
+                               const TGeom& g, int s, int64_t i, int d, double diag, double2 zk) {
+    const int L = g.L, Ls = g.Ls;
+    const int64_t kvol = g.kvol;
+    auto at = [&](int ss, int64_t st, int dd) -> double2 {
+        return __ldg(R + ss + (int64_t)Ls * (st + kvol * dd));
+    };
+    const int x = (int)(i % L), y = (int)((i / L) % L), t = (int)(i / ((int64_t)L * L));
+    int64_t up[3], dn[3];
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) tnbr(g, x, y, t, mu, &up[mu], &dn[mu]);
+    double2 phi = zscal(diag, at(s, i, d));                                 // :1967-1974
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {                                         // Wilson, :1976-1987
+        const double2 uu = __ldg(u + i + kvol * mu), ud = zconj(__ldg(u + dn[mu] + kvol * mu));
+        const double2 w = zadd(zmul(uu, at(s, up[mu], d)), zmul(ud, at(s, dn[mu], d)));
+        phi = zsub(phi, zscal(0.5, w));
+    }
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {                                         // Dirac, :1989-2002
+        const int dg = c_tgi[mu][d];
+        const double2 uu = __ldg(u + i + kvol * mu), ud = zconj(__ldg(u + dn[mu] + kvol * mu));
+        const double2 tt = zmul(c_tgv[mu][d], zsub(zmul(uu, at(s, up[mu], dg)),
+                                                   zmul(ud, at(s, dn[mu], dg))));
+        phi = DAG ? zsub(phi, tt) : zadd(phi, tt);
+    }
+    // s hops (:2004-2020): M takes Dirac 3,4 from s+1, Dirac 1,2 from s-1;
+    // M^dagger the reverse (:2129-2145)
+    const bool from_up = DAG ? d < 2 : d >= 2;
+    if (from_up) {
+        if (s < Ls - 1) phi = zsub(phi, at(s + 1, i, d));
+    } else if (s > 0) {
+        phi = zsub(phi, at(s - 1, i, d));
+    }
+    // mass term (:2022-2067, :2147-2186): group A at s=kthird (the pair that
+    // takes s+1), group B at s=1 (the other pair)
+    const bool grpA = s == Ls - 1 && from_up, grpB = s == 0 && !from_up;
+    if (grpA || grpB) {
+        double2 src;
+        int sg;
+        if (IMASS == 5) {
+            src = at(s, i, d >= 2 ? d - 2 : d + 2);
+            sg = -1;
+        } else {
+            src = at(grpA ? 0 : Ls - 1, i, d);
+            sg = IMASS == 1 ? 1 : (grpA == !DAG ? -1 : 1);
+        }
+        const double2 tt = zmul(zk, src);
+        phi = sg > 0 ? zadd(phi, tt) : zsub(phi, tt);
+    }
+    return phi;
+}
+
+template <bool DAG, int IMASS>
+__global__ void __launch_bounds__(kThreads) k_thr_dslash(double2* __restrict__ out,
+                                                         const double2* __restrict__ in,
+                                                         const double2* __restrict__ u, TGeom g,
+                                                         double diag, double2 zk) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= g.kferm) return;
+    const int s = (int)(j % g.Ls);
+    const int64_t r = j / g.Ls;
+    out[j] = thr_element<DAG, IMASS>(in, u, g, s, r % g.kvol, (int)(r / g.kvol), diag, zk);
+}
+
+// derivs (:820-878), one thread per link (i, mu): for Dirac d and s in the
+// reference's order, the Wilson term then the Dirac term, each rounded to
+// REAL*4 as it is added.
+__global__ void __launch_bounds__(kThreads) k_thr_derivs(const double2* __restrict__ R,
+                                                         const double2* __restrict__ X2, TGeom g,
+                                                         double tz, int iflag,
+                                                         float* __restrict__ dS) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= 3 * (int64_t)g.kvol) return;
+    const int64_t kvol = g.kvol;
+    const int mu = (int)(j / kvol);
+    const int64_t i = j % kvol;
+    const int Ls = g.Ls;
+    const int x = (int)(i % g.L), y = (int)((i / g.L) % g.L), t = (int)(i / ((int64_t)g.L * g.L));
+    int64_t up, dn;
+    tnbr(g, x, y, t, mu, &up, &dn);
+    const double2 tzi = make_double2(0.0, tz);
+    float f = dS[j];
+    for (int d = 0; d < 4; d++) {
+        const int dg = c_tgi[mu][d];
+        const double2 tg = zmul(tzi, c_tgv[mu][d]);
+        for (int s = 0; s < Ls; s++) {
+            const double2 ri = zconj(R[s + (int64_t)Ls * (i + kvol * d)]);
+            const double2 ru = zconj(R[s + (int64_t)Ls * (up + kvol * d)]);
+            const double2 a = zmul(ri, X2[s + (int64_t)Ls * (up + kvol * d)]);
+            const double2 b = zmul(ru, X2[s + (int64_t)Ls * (i + kvol * d)]);
+            const double2 w = zmul(tzi, zsub(a, b));
+            f = __double2float_rn(__dsub_rn((double)f, __dmul_rn(0.5, w.x)));     // :843-850
+            const double2 a2 = zmul(ri, X2[s + (int64_t)Ls * (up + kvol * dg)]);
+            const double2 b2 = zmul(ru, X2[s + (int64_t)Ls * (i + kvol * dg)]);
+            const double2 w2 = zmul(tg, zadd(a2, b2));
+            f = __double2float_rn(iflag == 0 ? __dsub_rn((double)f, w2.x)             // :851-868
+                                             : __dadd_rn((double)f, w2.x));
+        }
+    }
+    dS[j] = f;
+}
+
+// coef (:1799-1827)
+__global__ void k_thr_coef(const float* __restrict__ theta, double2* __restrict__ u, TGeom g) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= 3 * (int64_t)g.kvol) return;
+    double2 v = make_double2(1.0, (double)theta[j]);
+    const int64_t i = j % g.kvol;
+    if (j / g.kvol == 2 && i >= (int64_t)(g.Lt - 1) * g.L * g.L) v = make_double2(-v.x, -v.y);
+    u[j] = v;
+}
+
+// ---- multi-shift solver kernels (qmrherm, :630-818) ------------------------
+struct PoleCoef {
+    double rho[kThrMaxPoles], amu[kThrMaxPoles];
+};
+
+// q = R/beta (:684-686)
+__global__ void k_thr_q(double2* __restrict__ q, const double2* __restrict__ R, double beta,
+                        int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j < n) q[j] = make_double2(__ddiv_rn(R[j].x, beta), __ddiv_rn(R[j].y, beta));
+}
+
+// block partials of sum Re(conjg(a)*b)
+__global__ void __launch_bounds__(kThreads) k_thr_dot(const double2* __restrict__ a,
+                                                      const double2* __restrict__ b, int64_t n,
+                                                      double* __restrict__ part) {
+    __shared__ double sh[kThreads / 32];
+    double loc = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        loc += zmul(zconj(a[j]), b[j]).x;
+    loc = block_sum<kThreads>(loc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = loc;
+}
+
+// R = x3 - alphatild q - beta qm1 ; qm1 = q ; partials of |R|^2 (:696-703)
+__global__ void __launch_bounds__(kThreads) k_thr_lanczos(double2* __restrict__ R,
+                                                          double2* __restrict__ qm1,
+                                                          const double2* __restrict__ q,
+                                                          const double2* __restrict__ x3,
+                                                          double alphat, double beta, int64_t n,
+                                                          double* __restrict__ part) {
+    __shared__ double sh[kThreads / 32];
+    double loc = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const double2 qj = q[j];
+        const double2 r = zsub(zsub(x3[j], zscal(alphat, qj)), zscal(beta, qm1[j]));
+        R[j] = r;
+        qm1[j] = qj;
+        loc += zmul(zconj(r), r).x;
+    }
+    loc = block_sum<kThreads>(loc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = loc;
+}
+
+// all poles at once: first iteration p_k = q, x_k = rho_k q; later
+// p_k = q - amu_k p_k, x_k += rho_k p_k (:712-747; pm1 equals p)
+__global__ void k_thr_poles(double2* __restrict__ p, double2* __restrict__ x1,
+                            const double2* __restrict__ q, PoleCoef c, int npole, int first,
+                            int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double2 qj = q[j];
+    for (int k = 0; k < npole; k++) {
+        const int64_t e = j + n * k;
+        if (first) {
+            p[e] = qj;
+            x1[e] = zscal(c.rho[k], qj);
+        } else {
+            const double2 pk = zsub(qj, zscal(c.amu[k], p[e]));
+            p[e] = pk;
+            x1[e] = zadd(x1[e], zscal(c.rho[k], pk));
+        }
+    }
+}
+
+// x = anum0 Phi, then x += anum_k x_k in pole order (:666, :766-772)
+__global__ void k_thr_combine(double2* __restrict__ x, const double2* __restrict__ Phi,
+                              const double2* __restrict__ x1, PoleCoef c, double a0, int npole,
+                              int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double2 v = zscal(a0, Phi[j]);
+    for (int k = 0; k < npole; k++) v = zadd(v, zscal(c.rho[k], x1[j + n * k]));
+    x[j] = v;
+}
+
+// R = x3 - ... helpers for the leapfrog: pp -= dS*d ; theta += d*pp
+__global__ void k_thr_update_p(float* __restrict__ pp, const float* __restrict__ dS, float d,
+                               int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j < n) pp[j] = __fsub_rn(pp[j], __fmul_rn(dS[j], d));
+}
+__global__ void k_thr_update_theta(float* __restrict__ th, const float* __restrict__ pp,
+                                   float d, int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j < n) th[j] = __fadd_rn(th[j], __fmul_rn(d, pp[j]));
+}
+
+// end of force (:520-532): the antiperiodic sign on the t links of the last
+// slice, then dSdpi + beta*Nf*theta
+__global__ void k_thr_force_end(float* __restrict__ dS, const float* __restrict__ theta,
+                                float b, TGeom g) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= 3 * (int64_t)g.kvol) return;
+    float v = dS[j];
+    if (j / g.kvol == 2 && j % g.kvol >= (int64_t)(g.Lt - 1) * g.L * g.L) v = -v;
+    dS[j] = __fadd_rn(v, __fmul_rn(b, theta[j]));
+}
+
+// R(s, i, d) = cmplx(ps(i,1), ps(i,2)) of gauss0 call d*kthird + s (:213-222)
+__global__ void k_thr_noise(double2* __restrict__ R, const float* __restrict__ gauss, TGeom g) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= g.kferm) return;
+    const int s = (int)(j % g.Ls);
+    const int64_t r = j / g.Ls;
+    const int64_t site = r % g.kvol;
+    const int64_t c = (r / g.kvol) * g.Ls + s;
+    const float* ps = gauss + c * 2 * g.kvol;
+    R[j] = make_double2((double)ps[site], (double)ps[g.kvol + site]);
+}
+
+unsigned tblk(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+}  // namespace
+}  // namespace chdwf
+
+using chdwf::TGeom;
+
+struct ThrRemez {
+    std::vector<double> anum, aden, bnum, bden;
+    int n = 0;
+};
+
+struct chdwf_thr {
+    int device = 0;
+    TGeom g{};
+    float dt = 0.1f, beta = 0.5f, am3 = 1.0f, am = 0.0f;
+    int imass = 1, iterl = 1;
+    float rescga = 0.000000001f, rescgg = 0.000001f;                   // :39
+    ThrRemez r2, r4, r2g, r4g;
+    cudaStream_t st = nullptr;
+    float *theta = nullptr, *thetat = nullptr, *pp = nullptr, *dS = nullptr, *gauss = nullptr;
+    double2 *ut = nullptr, *uio = nullptr;
+    double2 *Phi = nullptr, *X1 = nullptr, *R = nullptr, *X2 = nullptr, *Phi0 = nullptr;
+    double2 *q = nullptr, *qm1 = nullptr, *vt = nullptr, *x3 = nullptr, *rr = nullptr;
+    double2 *p = nullptr, *x1 = nullptr;
+    double* part = nullptr;
+    std::vector<double> hpart;
+    chdwf::Rng rng;
+    int isweep = 0, itot = 0, naccp = 0;
+    float action = 0.0f, gaction = 0.0f, paction = 0.0f;
+    float actiona = 0.0f, vel2a = 0.0f, yav = 0.0f, yyav = 0.0f;
+    std::string err;
+
+    double diag() const { return (double)((3.0f - am3) + 1.0f); }       // :1967
+    int fail(cudaError_t e, const char* where) {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return CHDWF_CUDA_ERROR;
+    }
+};
+
+namespace {
+
+thread_local std::string g_thr_create_err;
+
+template <class T>
+cudaError_t talloc(T** p, size_t n) { return cudaMalloc((void**)p, sizeof(T) * n); }
+
+void thr_dslash(chdwf_thr* h, bool dag, float am, int imass, double2* out, const double2* in,
+                const double2* u) {
+    const unsigned nb = chdwf::tblk(h->g.kferm);
+    double2 zk = imass == 1 ? make_double2((double)am, 0.0)
+                            : make_double2(0.0, dag ? (double)am : (double)(-am));
+    const double dg = h->diag();
+#define THR_LAUNCH(D, I) chdwf::k_thr_dslash<D, I><<<nb, chdwf::kThreads, 0, h->st>>>(out, in, u, h->g, dg, zk)
+    if (dag) {
+        if (imass == 1) THR_LAUNCH(true, 1); else if (imass == 3) THR_LAUNCH(true, 3); else THR_LAUNCH(true, 5);
+    } else {
+        if (imass == 1) THR_LAUNCH(false, 1); else if (imass == 3) THR_LAUNCH(false, 3); else THR_LAUNCH(false, 5);
+    }
+#undef THR_LAUNCH
+    chdwf::count_launches(1);
+}
+
+void thr_derivs(chdwf_thr* h, const double2* R, const double2* X2, double anum, int iflag) {
+    const double tz = (double)(float)(2.0 * anum);                         // tzi, :839
+    chdwf::k_thr_derivs<<<chdwf::tblk(3 * (int64_t)h->g.kvol), chdwf::kThreads, 0, h->st>>>(
+        R, X2, h->g, tz, iflag, h->dS);
+    chdwf::count_launches(1);
+}
+
+// sum of the block partials in block order
+cudaError_t thr_sum(chdwf_thr* h, double* out) {
+    cudaMemcpyAsync(h->hpart.data(), h->part, sizeof(double) * chdwf::kRedBlocks,
+                    cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    double s = 0.0;
+    for (int b = 0; b < chdwf::kRedBlocks; b++) s = s + h->hpart[b];
+    *out = s;
+    return e;
+}
+
+// qmrherm on device vectors (:630-818): Phi in, x out, Phi0 and dS of the
+// context; the scalars follow the reference's implicit typing.
+int thr_qmrherm(chdwf_thr* h, const double2* Phi, float res, int* itercg, float am, int imass,
+                const double* anum, const double* aden, int ndiag, int iflag, const double2* u,
+                double2* x) {
+    const int64_t n = h->g.kferm;
+    const unsigned nb = chdwf::tblk(n);
+    const int niterc = 7500;                                             // :635
+    const float resid = std::sqrt((float)n * res * res);                // :660
+    cudaError_t e;
+    cudaMemcpyAsync(h->rr, Phi, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);   // :662-667
+    cudaMemsetAsync(h->qm1, 0, sizeof(double2) * n, h->st);
+    chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(h->rr, h->rr, n, h->part);
+    chdwf::count_launches(1);
+    double beta;
+    if ((e = thr_sum(h, &beta))) return h->fail(e, "thr_qmrherm");
+    beta = std::sqrt(beta);
+    const float phimod = (float)beta;
+    double alpha[chdwf::kThrMaxPoles], d[chdwf::kThrMaxPoles], dm1[chdwf::kThrMaxPoles];
+    double rhom1[chdwf::kThrMaxPoles];
+    chdwf::PoleCoef c;
+    memset(&c, 0, sizeof(c));
+    int capped = 1;
+    *itercg = 0;
+    for (int niter = 1; niter <= niterc; niter++) {
+        (*itercg)++;
+        chdwf::k_thr_q<<<nb, chdwf::kThreads, 0, h->st>>>(h->q, h->rr, beta, n);
+        thr_dslash(h, false, am, imass, h->vt, h->q, u);
+        thr_dslash(h, true, am, imass, h->x3, h->vt, u);
+        chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(h->q, h->x3, n, h->part);
+        chdwf::count_launches(2);
+        double at;
+        if ((e = thr_sum(h, &at))) return h->fail(e, "thr_qmrherm");
+        const float alphatild = (float)at;                               // REAL*4 (:691-694)
+        chdwf::k_thr_lanczos<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(
+            h->rr, h->qm1, h->q, h->x3, (double)alphatild, beta, n, h->part);
+        chdwf::count_launches(1);
+        const float beta0 = (float)beta;
+        double b2;
+        if ((e = thr_sum(h, &b2))) return h->fail(e, "thr_qmrherm");
+        beta = std::sqrt(b2);
+        for (int k = 0; k < ndiag; k++) alpha[k] = (double)alphatild + aden[k];
+        float rhomax = 0.0f;
+        if (niter == 1) {                                                  // :712-724
+            for (int k = 0; k < ndiag; k++) {
+                d[k] = alpha[k];
+                c.rho[k] = (double)beta0 / alpha[k];
+                rhom1[k] = c.rho[k];
+            }
+        } else {                                                           // :725-747
+            for (int k = 0; k < ndiag; k++) {
+                c.amu[k] = (double)beta0 / d[k];
+                dm1[k] = d[k];
+                d[k] = alpha[k] - (double)beta0 * c.amu[k];
+                c.rho[k] = -(c.amu[k] * dm1[k] * rhom1[k] / d[k]);
+                const double rm = std::fabs((double)phimod * c.rho[k]);
+                if (k == 0) rhomax = (float)rm;
+                else if (rm > (double)rhomax) rhomax = (float)rm;
+                rhom1[k] = c.rho[k];
+            }
+        }
+        chdwf::k_thr_poles<<<nb, chdwf::kThreads, 0, h->st>>>(h->p, h->x1, h->q, c, ndiag,
+                                                               niter == 1, n);
+        chdwf::count_launches(1);
+        const float arelax = 2.0f;                                         // :750-757
+        if (niter > 1 && rhomax < arelax * resid) { capped = 0; break; }
+    }
+    if (iflag < 2) {                                                       // :766-780
+        chdwf::PoleCoef a;
+        for (int k = 0; k < ndiag; k++) a.rho[k] = anum[k + 1];
+        chdwf::k_thr_combine<<<nb, chdwf::kThreads, 0, h->st>>>(x, Phi, h->x1, a, anum[0], ndiag, n);
+        chdwf::count_launches(1);
+        if (iflag == 1)
+            cudaMemcpyAsync(h->Phi0, h->x1, sizeof(double2) * n * ndiag, cudaMemcpyDeviceToDevice,
+                            h->st);
+    } else {                                                               // :781-806
+        chdwf::k_thr_combine<<<nb, chdwf::kThreads, 0, h->st>>>(x, Phi, h->x1, c, anum[0], 0, n);
+        chdwf::count_launches(1);
+        for (int k = 0; k < ndiag; k++) {
+            const double2* xk = h->x1 + n * k;
+            thr_dslash(h, false, am, imass, h->X2, xk, u);
+            if (iflag == 2) {
+                thr_derivs(h, xk, h->X2, anum[k + 1], 0);
+            } else {
+                const double coeff = -anum[k + 1];
+                const double2* p0 = h->Phi0 + n * k;
+                thr_derivs(h, p0, h->X2, coeff, 0);
+                thr_dslash(h, false, am, imass, h->X2, p0, u);
+                thr_derivs(h, h->X2, xk, coeff, 1);
+            }
+        }
+    }
+    if ((e = cudaGetLastError())) return h->fail(e, "thr_qmrherm");
+    return capped ? CHDWF_ITER_CAP : CHDWF_OK;
+}
+
+// force (:449-535) on thetat/ut; its[4] receives the four solves' iterations
+int thr_force(chdwf_thr* h, float res1, int* its) {
+    const int64_t n = h->g.kferm;
+    cudaMemsetAsync(h->dS, 0, sizeof(float) * 3 * h->g.kvol, h->st);   // :477-481
+    int rc;
+    const ThrRemez& a4 = h->r4g;
+    const ThrRemez& r2 = h->r2g;
+    rc = thr_qmrherm(h, h->Phi, res1, &its[0], 1.0f, 1, a4.anum.data(), a4.aden.data(), a4.n, 1,
+                     h->ut, h->X1);                                       // :493
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    cudaMemcpyAsync(h->R, h->X1, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
+    rc = thr_qmrherm(h, h->R, res1, &its[1], h->am, h->imass, r2.bnum.data(), r2.bden.data(), r2.n,
+                     0, h->ut, h->X1);                                    // :500
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    cudaMemcpyAsync(h->R, h->X1, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
+    rc = thr_qmrherm(h, h->R, res1, &its[2], h->am, h->imass, r2.anum.data(), r2.aden.data(), r2.n,
+                     2, h->ut, h->X1);                                    // :509
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    rc = thr_qmrherm(h, h->R, res1, &its[3], 1.0f, 1, a4.anum.data(), a4.aden.data(), a4.n, 3,
+                     h->ut, h->X1);                                       // :514
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    const float b = h->beta * 1.0f;                                       // b = beta*Nf, :527
+    chdwf::k_thr_force_end<<<chdwf::tblk(3 * (int64_t)h->g.kvol), chdwf::kThreads, 0, h->st>>>(
+        h->dS, h->thetat, b, h->g);
+    chdwf::count_launches(1);
+    const cudaError_t e = cudaGetLastError();
+    return e ? h->fail(e, "thr_force") : CHDWF_OK;
+}
+
+// hamilton (:539-628): out = h, hg, hp, s; its = {mass m, PV}
+int thr_hamilton(chdwf_thr* h, float res2, double* out, int* its) {
+    const int64_t n = h->g.kferm, n3 = 3 * (int64_t)h->g.kvol;
+    std::vector<float> pp(n3), th(n3);
+    cudaMemcpyAsync(pp.data(), h->pp, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->st);
+    cudaMemcpyAsync(th.data(), h->thetat, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->st);
+    int rc = thr_qmrherm(h, h->Phi, res2, &its[1], 1.0f, 1, h->r4.anum.data(), h->r4.aden.data(),
+                         h->r4.n, 0, h->ut, h->X1);                       // :596
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    cudaMemcpyAsync(h->R, h->X1, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
+    rc = thr_qmrherm(h, h->R, res2, &its[0], h->am, h->imass, h->r2.bnum.data(), h->r2.bden.data(),
+                     h->r2.n, 0, h->ut, h->X1);                           // :603
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(h->R, h->X1, n, h->part);
+    chdwf::count_launches(1);
+    double hf;
+    const cudaError_t e = thr_sum(h, &hf);                                 // :607-609
+    if (e) return h->fail(e, "thr_hamilton");
+    double hp = 0.0, hg = 0.0;
+    for (int64_t j = 0; j < n3; j++) hp = hp + (double)(pp[j] * pp[j]);         // :571-575
+    hp = hp * 0.5;
+    for (int64_t j = 0; j < n3; j++) hg = hg + (double)(th[j] * th[j]);
+    hg = (double)(0.5f * 1.0f * h->beta) * hg;                          // :581
+    out[0] = hg + hp + hf;
+    out[1] = hg;
+    out[2] = hp;
+    out[3] = hg + hf;
+    return CHDWF_OK;
+}
+
+chdwf_thr* thr_ok(chdwf_thr* h) {
+    if (h) cudaSetDevice(h->device);
+    return h;
+}
+
+int thr_apply(chdwf_thr* h, bool dag, double* Phi, const double* R, const double* u, float am,
+              int imass) {
+    if (!thr_ok(h) || !Phi || !R || !u || (imass != 1 && imass != 3 && imass != 5))
+        return CHDWF_BAD_ARG;
+    const int64_t n = h->g.kferm;
+    cudaMemcpyAsync(h->R, R, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->uio, u, sizeof(double2) * 3 * h->g.kvol, cudaMemcpyHostToDevice, h->st);
+    thr_dslash(h, dag, am, imass, h->X2, h->R, h->uio);
+    cudaMemcpyAsync(Phi, h->X2, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    return e ? h->fail(e, "thr_dslash") : CHDWF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chdwf_thr_create(chdwf_thr** out, int ksize, int ksizet, int kthird, float dt, float beta,
+                     float am3, float am, int imass, int iterl, int device) {
+    if (!out) return CHDWF_BAD_ARG;
+    *out = nullptr;
+    if (!chdwf::geom_ok(ksize, ksizet, kthird) || (imass != 1 && imass != 3 && imass != 5) ||
+        iterl < 1) {
+        g_thr_create_err = "chdwf_thr_create: bad lattice, imass or iterl";
+        return CHDWF_BAD_ARG;
+    }
+    chdwf_thr* h = new chdwf_thr;
+    h->device = device;
+    h->g.L = ksize; h->g.Lt = ksizet; h->g.Ls = kthird;
+    h->g.kvol = ksize * ksize * ksizet;
+    h->g.kferm = 4 * (int64_t)h->g.kvol * kthird;
+    h->dt = dt; h->beta = beta; h->am3 = am3; h->am = am; h->imass = imass; h->iterl = iterl;
+    const int64_t n3 = 3 * (int64_t)h->g.kvol, n = h->g.kferm;
+    const int np = chdwf::kThrMaxPoles;
+    cudaError_t e = cudaSetDevice(device);
+    if (!e) e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    if (!e) e = talloc(&h->theta, n3);
+    if (!e) e = talloc(&h->thetat, n3);
+    if (!e) e = talloc(&h->pp, n3);
+    if (!e) e = talloc(&h->dS, n3);
+    if (!e) e = talloc(&h->gauss, 8 * (size_t)h->g.kvol * kthird);
+    if (!e) e = talloc(&h->ut, n3);
+    if (!e) e = talloc(&h->uio, n3);
+    for (double2** v : {&h->Phi, &h->X1, &h->R, &h->X2, &h->q, &h->qm1, &h->vt, &h->x3, &h->rr})
+        if (!e) e = talloc(v, n);
+    if (!e) e = talloc(&h->Phi0, n * np);
+    if (!e) e = talloc(&h->p, n * np);
+    if (!e) e = talloc(&h->x1, n * np);
+    if (!e) e = talloc(&h->part, chdwf::kRedBlocks);
+    if (!e) e = cudaMemsetAsync(h->theta, 0, sizeof(float) * n3, h->st);
+    if (!e) e = cudaMemsetAsync(h->Phi0, 0, sizeof(double2) * n * np, h->st);
+    if (!e) e = cudaStreamSynchronize(h->st);
+    if (e) {
+        g_thr_create_err = std::string("chdwf_thr_create: ") + cudaGetErrorString(e);
+        chdwf_thr_destroy(h);
+        return CHDWF_CUDA_ERROR;
+    }
+    h->hpart.resize(chdwf::kRedBlocks);
+    h->rng.startup((double)693764523745.0f);
+    *out = h;
+    return CHDWF_OK;
+}
+
+void chdwf_thr_destroy(chdwf_thr* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    for (float* v : {h->theta, h->thetat, h->pp, h->dS, h->gauss}) if (v) cudaFree(v);
+    for (double2* v : {h->ut, h->uio, h->Phi, h->X1, h->R, h->X2, h->Phi0, h->q, h->qm1, h->vt,
+                       h->x3, h->rr, h->p, h->x1})
+        if (v) cudaFree(v);
+    if (h->part) cudaFree(h->part);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+const char* chdwf_thr_last_error(chdwf_thr* h) {
+    return h ? h->err.c_str() : g_thr_create_err.c_str();
+}
+
+int chdwf_thr_set_remez(chdwf_thr* h, int which, const double* anum, const double* aden,
+                        const double* bnum, const double* bden, int ndiag) {
+    if (!h || !anum || !aden || !bnum || !bden || ndiag < 1 || ndiag > chdwf::kThrMaxPoles)
+        return CHDWF_BAD_ARG;
+    ThrRemez* r = which == 2 ? &h->r2 : which == 4 ? &h->r4 : which == 22 ? &h->r2g
+                : which == 44 ? &h->r4g : nullptr;
+    if (!r) return CHDWF_BAD_ARG;
+    r->anum.assign(anum, anum + ndiag + 1);
+    r->aden.assign(aden, aden + ndiag);
+    r->bnum.assign(bnum, bnum + ndiag + 1);
+    r->bden.assign(bden, bden + ndiag);
+    r->n = ndiag;
+    return CHDWF_OK;
+}
+
+int chdwf_thr_coef(chdwf_thr* h, const float* theta, double* u) {
+    if (!thr_ok(h) || !theta || !u) return CHDWF_BAD_ARG;
+    const int64_t n3 = 3 * (int64_t)h->g.kvol;
+    cudaMemcpyAsync(h->dS, theta, sizeof(float) * n3, cudaMemcpyHostToDevice, h->st);
+    chdwf::k_thr_coef<<<chdwf::tblk(n3), chdwf::kThreads, 0, h->st>>>(h->dS, h->uio, h->g);
+    chdwf::count_launches(1);
+    cudaMemcpyAsync(u, h->uio, sizeof(double2) * n3, cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    return e ? h->fail(e, "thr_coef") : CHDWF_OK;
+}
+
+int chdwf_thr_dslash(chdwf_thr* h, double* Phi, const double* R, const double* u, float am,
+                     int imass) {
+    return thr_apply(h, false, Phi, R, u, am, imass);
+}
+
+int chdwf_thr_dslashd(chdwf_thr* h, double* Phi, const double* R, const double* u, float am,
+                      int imass) {
+    return thr_apply(h, true, Phi, R, u, am, imass);
+}
+
+int chdwf_thr_derivs(chdwf_thr* h, const double* R, const double* X2, double anum, int iflag,
+                     float* dSdpi) {
+    if (!thr_ok(h) || !R || !X2 || !dSdpi || (iflag != 0 && iflag != 1)) return CHDWF_BAD_ARG;
+    const int64_t n = h->g.kferm, n3 = 3 * (int64_t)h->g.kvol;
+    cudaMemcpyAsync(h->R, R, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->X1, X2, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->dS, dSdpi, sizeof(float) * n3, cudaMemcpyHostToDevice, h->st);
+    thr_derivs(h, h->R, h->X1, anum, iflag);
+    cudaMemcpyAsync(dSdpi, h->dS, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    return e ? h->fail(e, "thr_derivs") : CHDWF_OK;
+}
+
+int chdwf_thr_qmrherm(chdwf_thr* h, const double* Phi, float res, int* itercg, float am,
+                      int imass, const double* anum, const double* aden, int ndiag, int iflag,
+                      const double* u, double* x, double* Phi0, float* dSdpi) {
+    if (!thr_ok(h) || !Phi || !itercg || !anum || !aden || !u || !x ||
+        ndiag < 1 || ndiag > chdwf::kThrMaxPoles || iflag < 0 || iflag > 3 ||
+        (imass != 1 && imass != 3 && imass != 5) || (iflag >= 1 && !Phi0) ||
+        (iflag >= 2 && !dSdpi))
+        return CHDWF_BAD_ARG;
+    const int64_t n = h->g.kferm, n3 = 3 * (int64_t)h->g.kvol;
+    cudaMemcpyAsync(h->Phi, Phi, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->uio, u, sizeof(double2) * n3, cudaMemcpyHostToDevice, h->st);
+    if (iflag == 3)
+        cudaMemcpyAsync(h->Phi0, Phi0, sizeof(double2) * n * ndiag, cudaMemcpyHostToDevice, h->st);
+    if (iflag >= 2) cudaMemcpyAsync(h->dS, dSdpi, sizeof(float) * n3, cudaMemcpyHostToDevice, h->st);
+    const int rc = thr_qmrherm(h, h->Phi, res, itercg, am, imass, anum, aden, ndiag, iflag, h->uio,
+                               h->X1);
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    cudaMemcpyAsync(x, h->X1, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->st);
+    if (iflag == 1)
+        cudaMemcpyAsync(Phi0, h->Phi0, sizeof(double2) * n * ndiag, cudaMemcpyDeviceToHost, h->st);
+    if (iflag >= 2) cudaMemcpyAsync(dSdpi, h->dS, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e) return h->fail(e, "thr_qmrherm");
+    return rc;
+}
+
+int chdwf_thr_set_theta(chdwf_thr* h, const float* theta) {
+    if (!thr_ok(h) || !theta) return CHDWF_BAD_ARG;
+    cudaMemcpyAsync(h->theta, theta, sizeof(float) * 3 * h->g.kvol, cudaMemcpyHostToDevice, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    return e ? h->fail(e, "thr_set_theta") : CHDWF_OK;
+}
+
+int chdwf_thr_get_theta(chdwf_thr* h, float* theta) {
+    if (!thr_ok(h) || !theta) return CHDWF_BAD_ARG;
+    cudaMemcpyAsync(theta, h->theta, sizeof(float) * 3 * h->g.kvol, cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    return e ? h->fail(e, "thr_get_theta") : CHDWF_OK;
+}
+
+int chdwf_thr_startup(chdwf_thr* h, double seed) {
+    if (!h) return CHDWF_BAD_ARG;
+    h->rng.startup(seed);
+    return CHDWF_OK;
+}
+
+double chdwf_thr_seed(chdwf_thr* h) { return h ? h->rng.seed() : 0.0; }
+
+int chdwf_thr_sweep(chdwf_thr* h, chdwf_thr_record* rec) {
+    if (!thr_ok(h) || !rec) return CHDWF_BAD_ARG;
+    if (h->r2.n < 1 || h->r4.n < 1 || h->r2g.n < 1 || h->r4g.n < 1) {
+        h->err = "thr_sweep: set remez2, remez4, remez2g and remez4g first";
+        return CHDWF_BAD_ARG;
+    }
+    memset(rec, 0, sizeof(*rec));
+    const TGeom& g = h->g;
+    const int64_t kvol = g.kvol, n = g.kferm, n3 = 3 * kvol;
+    const unsigned nb3 = chdwf::tblk(n3);
+    int rc;
+#define CK(x) do { rc = (x); if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc; } while (0)
+#define CKC(x, w) do { cudaError_t e_ = (x); if (e_) return h->fail(e_, w); } while (0)
+    h->isweep++;
+    cudaMemcpyAsync(h->thetat, h->theta, sizeof(float) * n3, cudaMemcpyDeviceToDevice, h->st);  // :203-208
+    chdwf::k_thr_coef<<<nb3, chdwf::kThreads, 0, h->st>>>(h->thetat, h->ut, g);
+    chdwf::count_launches(1);
+    std::vector<float> gauss(8 * (size_t)kvol * g.Ls);                    // :213-222
+    for (int c = 0; c < 4 * g.Ls; c++) h->rng.gauss0(kvol, gauss.data() + (size_t)c * 2 * kvol);
+    CKC(cudaMemcpyAsync(h->gauss, gauss.data(), sizeof(float) * gauss.size(),
+                        cudaMemcpyHostToDevice, h->st), "thr_sweep");
+    chdwf::k_thr_noise<<<chdwf::tblk(n), chdwf::kThreads, 0, h->st>>>(h->R, h->gauss, g);
+    chdwf::count_launches(1);
+    CK(thr_qmrherm(h, h->R, h->rescga, &rec->it_pf, h->am, h->imass, h->r4.anum.data(),
+                   h->r4.aden.data(), h->r4.n, 0, h->ut, h->X1));          // :226
+    cudaMemcpyAsync(h->R, h->X1, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
+    CK(thr_qmrherm(h, h->R, h->rescga, &rec->it_pfpv, 1.0f, 1, h->r4.bnum.data(),
+                   h->r4.bden.data(), h->r4.n, 0, h->ut, h->X1));          // :236
+    cudaMemcpyAsync(h->Phi, h->X1, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
+    std::vector<float> ps(2 * kvol), pp(n3);                               // :255-260
+    for (int mu = 0; mu < 3; mu++) {
+        h->rng.gaussp(kvol, ps.data());
+        memcpy(pp.data() + kvol * mu, ps.data(), sizeof(float) * kvol);
+    }
+    CKC(cudaMemcpyAsync(h->pp, pp.data(), sizeof(float) * n3, cudaMemcpyHostToDevice, h->st),
+        "thr_sweep");
+    double hh[4];
+    int ih[2];
+    CK(thr_hamilton(h, h->rescga, hh, ih));                               // :265
+    rec->it_h0 = ih[0];
+    rec->it_h0pv = ih[1];
+    rec->H0 = hh[0];
+    rec->S0 = hh[3];
+    if (h->isweep == 1) {                                                  // :267-271
+        h->action = (float)(hh[3] / (double)kvol);
+        h->gaction = (float)(hh[1] / (double)kvol);
+        h->paction = (float)(hh[2] / (double)kvol);
+    }
+    int fi[4];
+    CK(thr_force(h, h->rescgg, fi));                                      // :276
+    for (int k = 0; k < 4; k++) rec->it_force[k] += fi[k];
+    rec->nforce++;
+    float d = h->dt * 0.5f;
+    chdwf::k_thr_update_p<<<nb3, chdwf::kThreads, 0, h->st>>>(h->pp, h->dS, d, n3);
+    chdwf::count_launches(1);
+    const float proby = 1.0f / (float)h->iterl;                           // :151
+    for (int iter = 1; iter <= 1000; iter++) {                            // :285-320
+        d = h->dt;
+        chdwf::k_thr_update_theta<<<nb3, chdwf::kThreads, 0, h->st>>>(h->thetat, h->pp, d, n3);
+        chdwf::k_thr_coef<<<nb3, chdwf::kThreads, 0, h->st>>>(h->thetat, h->ut, g);
+        chdwf::count_launches(2);
+        CK(thr_force(h, h->rescgg, fi));
+        for (int k = 0; k < 4; k++) rec->it_force[k] += fi[k];
+        rec->nforce++;
+        rec->nsteps = iter;
+        const float ytest = h->rng.rano_yran();                            // :302
+        if (ytest < proby) {
+            d = h->dt * 0.5f;
+            chdwf::k_thr_update_p<<<nb3, chdwf::kThreads, 0, h->st>>>(h->pp, h->dS, d, n3);
+            chdwf::count_launches(1);
+            h->itot = h->itot + iter;
+            break;
+        }
+        d = h->dt;
+        chdwf::k_thr_update_p<<<nb3, chdwf::kThreads, 0, h->st>>>(h->pp, h->dS, d, n3);
+        chdwf::count_launches(1);
+    }
+    CK(thr_hamilton(h, h->rescga, hh, ih));                               // :325
+    rec->it_h1 = ih[0];
+    rec->it_h1pv = ih[1];
+    rec->H1 = hh[0];
+    rec->S1 = hh[3];
+    rec->hg = hh[1];
+    rec->hp = hh[2];
+    rec->dH = rec->H0 - rec->H1;
+    rec->dS = rec->S0 - rec->S1;
+    rec->y = (float)std::exp(rec->dH);                                    // :330
+    h->yav = h->yav + rec->y;
+    h->yyav = h->yyav + rec->y * rec->y;
+    int accept = 1;
+    if (rec->dH < 0.0) {                                                  // :333-336
+        rec->x = h->rng.rano_yran();
+        rec->drew_x = 1;
+        if (rec->x > rec->y) accept = 0;
+    }
+    if (accept) {                                                         // :338-348
+        cudaMemcpyAsync(h->theta, h->thetat, sizeof(float) * n3, cudaMemcpyDeviceToDevice, h->st);
+        h->naccp = h->naccp + 1;
+        h->action = (float)(rec->S1 / (double)kvol);
+        h->gaction = (float)(rec->hg / (double)kvol);
+        h->paction = (float)(rec->hp / (double)kvol);
+    }
+    rec->accepted = accept;
+    rec->action = h->action;
+    rec->gaction = h->gaction;
+    rec->paction = h->paction;
+    h->actiona = h->actiona + h->action;                                  // :350
+    CKC(cudaMemcpyAsync(pp.data(), h->pp, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->st),
+        "thr_sweep");
+    CKC(cudaStreamSynchronize(h->st), "thr_sweep");
+    float vel2 = 0.0f;                                                    // :351-357
+    for (int64_t j = 0; j < n3; j++) vel2 = vel2 + pp[j] * pp[j];
+    rec->vel2 = vel2 / (float)(3 * kvol);
+    h->vel2a = h->vel2a + rec->vel2;
+    CKC(cudaGetLastError(), "thr_sweep");
+#undef CK
+#undef CKC
+    return CHDWF_OK;
+}
+
+}  // extern "C"
