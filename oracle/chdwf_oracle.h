@@ -220,6 +220,8 @@ typedef struct {
     int it_force[4];   /* summed per force solve: PV (iflag 1), m, DWF force, PV force */
     int nforce;
     float action, gaction, paction, vel2;
+    int measured;
+    float pbp, ancgm;  /* measure's psibarpsi and aviter (measurement sweeps) */
 } orc_thr_rec;
 
 typedef struct {
@@ -251,8 +253,13 @@ void orc_thr_free(orc_thr_state* st);
 void orc_thr_set_remez(orc_thr_state* st, int which, const orc_remez* r);
 void orc_thr_force(orc_thr_state* st, float res1, int* its);
 void orc_thr_hamilton(orc_thr_state* st, float res2, double* out, int* its);
-/* One sweep of the main loop of bulk_rhmc.f (:205-400) without its
- * measurement (measure, every iprint-th sweep). */
+int orc_thr_congrad(const orc_lat* lat, const double* Phi, float res, int* itercg, float am,
+                    int imass, const double* u, double* x);
+void orc_thr_measure(const orc_lat* lat, orc_rng* g, float res, float am, int imass,
+                     const double* u, float* psibarpsi, float* susclsing, float* aviter,
+                     double* parts);
+/* One sweep of the main loop of bulk_rhmc.f (:201-400), with measure on
+ * every iprint-th sweep. */
 void orc_thr_sweep(orc_thr_state* st, orc_thr_rec* rec);
 
 /* Remez file reader (format of rhmc/remez*): returns 0 on success. */

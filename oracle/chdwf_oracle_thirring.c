@@ -358,6 +358,141 @@ void orc_thr_hamilton(orc_thr_state* st, float res2, double* out, int* its) {
     out[3] = hg + hf;
 }
 
+/* congrad (:931-1025): CGNE on M^dagger M, FP64 vectors with REAL*4 scalars;
+ * alphad and betan take each complex*16 term and round to REAL*4.  x: in =
+ * initial guess (/vector/), out = solution.  Returns 1 at the cap
+ * niterc = kthird*kvol. */
+int orc_thr_congrad(const orc_lat* lat, const double* Phi, float res, int* itercg, float am,
+                    int imass, const double* u, double* x) {
+    const int64_t kvol = orc_kvol(lat), kferm = 4 * kvol * lat->Ls;
+    const int64_t niterc = lat->Ls * kvol;                                  /* :934 */
+    const size_t vb = sizeof(double) * 2 * kferm;
+    double* x1 = malloc(vb);
+    double* x2 = malloc(vb);
+    double* p = malloc(vb);
+    double* r = malloc(vb);
+    const float resid = (float)kferm * res * res;                           /* :947 */
+    float betad = 1.0f, alpha = 1.0f, alphan = 0.0f;
+    int capped = 1;
+    *itercg = 0;
+    for (int64_t nx = 1; nx <= niterc; nx++) {
+        (*itercg)++;
+        if (nx == 1) {                                                       /* :951-962 */
+            memcpy(p, x, vb);
+            memcpy(r, Phi, vb);
+            betad = 1.0f;
+            alpha = 1.0f;
+        }
+        orc_thr_dslash(lat, x1, p, u, am, imass, 0);                         /* :966 */
+        if (nx != 1) {                                                       /* :970-983 */
+            float alphad = 0.0f;
+            for (int64_t i = 0; i < kferm; i++)
+                alphad = (float)((double)alphad + zmul(zconj(zld(x1, i)), zld(x1, i)).re);
+            alpha = alphan / alphad;
+            for (int64_t i = 0; i < kferm; i++)
+                zst(x, i, zadd(zld(x, i), zscal((double)alpha, zld(p, i))));
+        }
+        orc_thr_dslash(lat, x2, x1, u, am, imass, 1);                        /* :987 */
+        for (int64_t i = 0; i < kferm; i++) zst(r, i, zsub(zld(r, i), zscal((double)alpha, zld(x2, i))));
+        float betan = 0.0f;                                                  /* :996-1001 */
+        for (int64_t i = 0; i < kferm; i++)
+            betan = (float)((double)betan + zmul(zconj(zld(r, i)), zld(r, i)).re);
+        float beta = betan / betad;
+        betad = betan;
+        alphan = betan;
+        if (nx == 1) beta = 0.0f;
+        for (int64_t i = 0; i < kferm; i++) zst(p, i, zadd(zld(r, i), zscal((double)beta, zld(p, i))));
+        if (betan < resid) { capped = 0; break; }
+    }
+    free(x1); free(x2); free(p); free(r);
+    return capped;
+}
+
+/* measure (:1027-1285): the noisy psibar psi estimator, knoise = 10 noise
+ * vectors (two gauss0 calls each); per noise and Dirac source 1, 2 a
+ * source on the s=1 wall and one on the s=kthird wall (imass 5: the other
+ * chirality, negated), Phi = M^dagger xi, congrad from the source itself as
+ * initial guess, and the overlap with the opposite wall.  pbp is REAL*8;
+ * psibarpsi and susclsing REAL*4.  parts (40 doubles or NULL): re/im of
+ * psibarpsi1 and psibarpsi2 per noise (the unit-100 records). */
+void orc_thr_measure(const orc_lat* lat, orc_rng* g, float res, float am, int imass,
+                     const double* u, float* psibarpsi, float* susclsing, float* aviter,
+                     double* parts) {
+    const int64_t Ls = lat->Ls, kvol = orc_kvol(lat), kferm = 4 * kvol * Ls;
+    enum { knoise = 10 };
+    float* ps = malloc(sizeof(float) * 2 * kvol);
+    float* pt = malloc(sizeof(float) * 2 * kvol);
+    double* xi = malloc(sizeof(double) * 2 * kferm);
+    double* Phi = malloc(sizeof(double) * 2 * kferm);
+    double pbp[knoise];
+    int iter = 0;
+    for (int inoise = 0; inoise < knoise; inoise++) {
+        orc_gauss0(g, kvol, ps);                                             /* :1061 */
+        orc_gauss0(g, kvol, pt);                                             /* :1063 */
+        zc p1 = {0.0, 0.0}, p2 = {0.0, 0.0};
+        for (int idsource = 1; idsource <= 2; idsource++) {
+            for (int w = 0; w < 2; w++) {
+                /* w=0: ps on s=1 (:1066-1156); w=1: pt on s=kthird (:1157-1241).
+                 * dn: Dirac index of the noise x; dsrc: component of xi set;
+                 * sgn: -1 for the gamma_5 sources of imass 5. */
+                const float* nz = w == 0 ? ps : pt;
+                int dn, dsrc;
+                double sgn = 1.0;
+                if (imass != 5) {
+                    dn = w == 0 ? idsource : idsource + 2;
+                    dsrc = dn;
+                } else {
+                    dn = w == 0 ? idsource + 2 : idsource;
+                    dsrc = w == 0 ? dn - 2 : dn + 2;
+                    sgn = -1.0;
+                }
+                const int64_t s_src = w == 0 ? 0 : Ls - 1;
+                memset(xi, 0, sizeof(double) * 2 * kferm);
+                for (int64_t i = 0; i < kvol; i++) {
+                    zc x = {(double)nz[i], (double)nz[kvol + i]};
+                    if (sgn < 0) { x.re = -x.re; x.im = -x.im; }
+                    zst(xi, TIDX(s_src, i, dsrc - 1), x);
+                }
+                orc_thr_dslash(lat, Phi, xi, u, am, imass, 1);              /* :1136, :1220 */
+                int it = 0;
+                orc_thr_congrad(lat, Phi, res, &it, am, imass, u, xi);      /* :1138, :1225 */
+                iter += it;
+                /* read: imass != 5 the noise component on the opposite wall;
+                 * imass 5 the noise component on the same wall */
+                const int64_t s_rd = imass != 5 ? (w == 0 ? Ls - 1 : 0) : s_src;
+                zc acc = w == 0 ? p1 : p2;
+                for (int64_t i = 0; i < kvol; i++) {
+                    const zc x = {(double)nz[i], (double)nz[kvol + i]};
+                    acc = zadd(acc, zmul(zconj(x), zld(xi, TIDX(s_rd, i, dn - 1))));
+                }
+                if (w == 0) p1 = acc; else p2 = acc;
+            }
+        }
+        const double kv = (double)kvol;
+        if (imass == 1) {                                                    /* :1245-1257 */
+            p1.re /= kv; p1.im /= kv; p2.re /= kv; p2.im /= kv;
+        } else {
+            const zc m1 = {0.0, -1.0}, s2 = {0.0, imass == 3 ? 1.0 : -1.0};
+            p1 = zmul(m1, p1); p1.re /= kv; p1.im /= kv;
+            p2 = zmul(s2, p2); p2.re /= kv; p2.im /= kv;
+        }
+        pbp[inoise] = p1.re + p2.re;
+        if (parts) {
+            parts[4 * inoise] = p1.re; parts[4 * inoise + 1] = p1.im;
+            parts[4 * inoise + 2] = p2.re; parts[4 * inoise + 3] = p2.im;
+        }
+    }
+    float pb = 0.0f, sus = 0.0f;                                             /* :1266-1276 */
+    for (int i = 0; i < knoise; i++) {
+        pb = (float)((double)pb + pbp[i]);
+        for (int j = knoise - 1; j >= i + 1; j--) sus = (float)((double)sus + pbp[i] * pbp[j]);
+    }
+    *psibarpsi = pb / (float)knoise;
+    *susclsing = (float)(2 * kvol) * sus / (float)(knoise * (knoise - 1));
+    *aviter = (float)iter / (float)(4 * knoise);                             /* :1278 */
+    free(ps); free(pt); free(xi); free(Phi);
+}
+
 /* ---- program dwf3d of bulk_rhmc.f (:201-400) ----------------------------- */
 orc_thr_state* orc_thr_new(int L, int Lt, int Ls, float beta, float am3, float dt, float am,
                            int imass, int iterl) {
@@ -395,8 +530,7 @@ void orc_thr_set_remez(orc_thr_state* st, int which, const orc_remez* r) {
     else if (which == 44) st->r4g = *r;
 }
 
-/* One sweep without the measurement of isweep % iprint == 0 sweeps (its
- * measure call draws random numbers; the caller keeps such sweeps away). */
+/* One sweep, with measure on every iprint-th sweep (:360-374). */
 void orc_thr_sweep(orc_thr_state* st, orc_thr_rec* rec) {
     const orc_lat* lat = &st->lat;
     const int64_t Ls = lat->Ls, kvol = orc_kvol(lat), kferm = 4 * kvol * Ls;
@@ -496,4 +630,12 @@ void orc_thr_sweep(orc_thr_state* st, orc_thr_rec* rec) {
     for (int64_t j = 0; j < 3 * kvol; j++) vel2 = vel2 + st->pp[j] * st->pp[j];
     rec->vel2 = vel2 / (float)(3 * kvol);
     st->vel2a = st->vel2a + rec->vel2;
+    if ((st->isweep / st->iprint) * st->iprint == st->isweep) {              /* :361-371 */
+        memcpy(st->thetat, st->theta, sizeof(float) * 3 * kvol);
+        orc_thr_coef(lat, st->thetat, st->ut);
+        float sus = 0.0f;
+        orc_thr_measure(lat, &st->rng, 0.000001f, st->am, st->imass, st->ut, &rec->pbp, &sus,
+                        &rec->ancgm, NULL);                                  /* respbp, :39 */
+        rec->measured = 1;
+    }
 }

@@ -99,7 +99,8 @@ class ThrRec(C.Structure):
                 ("it_h0", C.c_int), ("it_h0pv", C.c_int), ("it_h1", C.c_int),
                 ("it_h1pv", C.c_int), ("it_force", C.c_int * 4), ("nforce", C.c_int),
                 ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
-                ("vel2", C.c_float)]
+                ("vel2", C.c_float), ("measured", C.c_int), ("pbp", C.c_float),
+                ("ancgm", C.c_float)]
 
 
 class ThrState(C.Structure):
@@ -176,6 +177,10 @@ def lib():
         L.orc_thr_force.argtypes = [C.POINTER(ThrState), C.c_float, P]
         L.orc_thr_hamilton.argtypes = [C.POINTER(ThrState), C.c_float, P, P]
         L.orc_thr_sweep.argtypes = [C.POINTER(ThrState), P]
+        L.orc_thr_congrad.argtypes = [P, P, C.c_float, P, C.c_float, C.c_int, P, P]
+        L.orc_thr_measure.argtypes = [P, P, C.c_float, C.c_float, C.c_int, P,
+                                      C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float), P]
         _lib = L
     return _lib
 
@@ -339,14 +344,34 @@ def thr_qmrherm(lat, Phi, u, res, am, imass, anum, aden, iflag=0, Phi0=None, dSd
     return x, it.value, capped, P0, dS
 
 
+def thr_congrad(lat, Phi, u, x0, res, am, imass=1):
+    x = np.ascontiguousarray(x0, dtype=np.complex128).copy()
+    it = C.c_int(0)
+    capped = lib().orc_thr_congrad(C.byref(lat), _p(np.ascontiguousarray(Phi, dtype=np.complex128)),
+                                   res, C.byref(it), am, imass, _p(np.ascontiguousarray(u)), _p(x))
+    return x, it.value, capped
+
+
+def thr_measure(lat, rand, u, res, am, imass):
+    """measure of bulk_rhmc.f on the generator of a Rand:
+    (psibarpsi, susclsing, aviter, parts[10, 4])."""
+    parts = np.empty((10, 4), dtype=np.float64)
+    pb, su, av = C.c_float(), C.c_float(), C.c_float()
+    lib().orc_thr_measure(C.byref(lat), C.byref(rand.g), res, am, imass,
+                          _p(np.ascontiguousarray(u)), C.byref(pb), C.byref(su), C.byref(av),
+                          _p(parts))
+    return pb.value, su.value, av.value, parts
+
+
 class ThrSweeper:
-    """The main loop of bulk_rhmc.f (:201-400) over the oracle, without the
-    measurement sweeps."""
+    """The main loop of bulk_rhmc.f (:201-400) over the oracle, with measure
+    on every iprint-th sweep."""
 
     def __init__(self, L, Lt, Ls, beta, am3, dt, am, imass, iterl, r2, r4, r2g, r4g,
-                 theta=None, seed=None):
+                 theta=None, seed=None, iprint=5):
         self.lib = lib()
         self.st = self.lib.orc_thr_new(L, Lt, Ls, beta, am3, dt, am, imass, iterl)
+        self.st.contents.iprint = iprint
         for which, r in ((2, r2), (4, r4), (22, r2g), (44, r4g)):
             self.lib.orc_thr_set_remez(self.st, which, C.byref(r))
         self.kvol = L * L * Lt

@@ -193,3 +193,78 @@ def test_thirring_force_conserves_energy(remez):
         assert na == nb
         assert abs(a) < 1e-4 * abs(h)
         assert abs(b) < 0.35 * abs(a)
+
+
+@pytest.mark.parametrize("imass", [1, 3, 5])
+def test_thirring_measure_matches_dense_solve(imass):
+    """measure (bulk_rhmc.f:1027-1285): each noise vector's unit-100 record
+    against x^dag [M^-1 xi] from a dense solve (congrad solves
+    M^dag M y = M^dag xi from the source itself); for imass 5 the sources are
+    the other chirality, negated, and the overlap is taken on the same wall."""
+    L, Lt, Ls = 4, 4, 4            # congrad's cap kthird*kvol = 256
+    lat = po.make_lat(L, Lt, Ls)
+    kv, sh = po.kvol(lat), po.thr_shape(lat)
+    theta = (0.3 * np.random.default_rng(3).standard_normal((3, kv))).astype(np.float32)
+    u = po.thr_coef(lat, theta)
+    am = np.float32(0.2)
+    pb, su, av, parts = po.thr_measure(lat, po.Rand(SEED), u, 1e-9, am, imass)
+    assert 0 < av < Ls * kv
+    M = _dense(lat, u, am, imass)
+    rand = po.Rand(SEED)
+    dense = np.zeros((10, 4))
+    for k in range(10):
+        ps, pt = rand.gauss0(kv), rand.gauss0(kv)
+        noise = (ps[0].astype(float) + 1j * ps[1], pt[0].astype(float) + 1j * pt[1])
+        p = [0j, 0j]
+        for d in (1, 2):
+            for w, x in enumerate(noise):
+                if imass != 5:
+                    dn = d if w == 0 else d + 2
+                    dsrc, sg = dn, 1
+                else:
+                    dn = d + 2 if w == 0 else d
+                    dsrc, sg = (dn - 2 if w == 0 else dn + 2), -1
+                s_src = 0 if w == 0 else Ls - 1
+                xi = np.zeros(sh, complex)
+                xi[dsrc - 1, ..., s_src] = sg * x.reshape(Lt, L, L)
+                y = np.linalg.solve(M, xi.reshape(-1)).reshape(sh)
+                s_rd = (Ls - 1 if w == 0 else 0) if imass != 5 else s_src
+                p[w] += np.vdot(x, y[dn - 1, ..., s_rd].reshape(-1))
+        if imass == 3:
+            p = [-1j * p[0], 1j * p[1]]
+        elif imass == 5:
+            p = [-1j * p[0], -1j * p[1]]
+        dense[k] = [p[0].real / kv, p[0].imag / kv, p[1].real / kv, p[1].imag / kv]
+    assert np.abs(parts - dense).max() <= 1e-7 * np.abs(dense).max()
+    pbp = parts[:, 0] + parts[:, 2]
+    assert abs(pb - pbp.mean()) <= 1e-6 * np.abs(pbp).max()
+
+
+def test_thirring_sweep_stream_with_measurement(remez):
+    """iprint = 1: every sweep ends with measure, whose 20 gauss0 calls come
+    after the Metropolis draw (bulk_rhmc.f:361-371)."""
+    L, Lt, Ls, iterl = 2, 4, 4, 4
+    kv = L * L * Lt
+    theta = (0.2 * np.random.default_rng(8).standard_normal((3, kv))).astype(np.float32)
+    sw = po.ThrSweeper(L, Lt, Ls, 0.5, 1.0, 0.1, 0.2, 1, iterl, *_remez_sets(remez), theta=theta,
+                       seed=SEED, iprint=1)
+    rand = po.Rand(SEED)
+    proby = np.float32(1.0) / np.float32(iterl)
+    for _ in range(2):
+        rec = sw.sweep()
+        for _ in range(4 * Ls):
+            rand.gauss0(kv)
+        for _ in range(3):
+            rand.gaussp(kv)
+        n = 0
+        while True:
+            n += 1
+            if rand.rano("yran") < proby or n == 1000:
+                break
+        if rec.drew_x:
+            assert rec.x == np.float32(rand.rano("yran"))
+        assert rec.measured == 1 and rec.ancgm > 0
+        for _ in range(20):
+            rand.gauss0(kv)
+        assert sw.seed() == rand.seed()
+    sw.close()
