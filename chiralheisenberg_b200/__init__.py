@@ -59,7 +59,8 @@ EXPORTS = (
     "chdwf_thr_create", "chdwf_thr_destroy", "chdwf_thr_last_error", "chdwf_thr_set_remez",
     "chdwf_thr_coef", "chdwf_thr_dslash", "chdwf_thr_dslashd", "chdwf_thr_derivs",
     "chdwf_thr_qmrherm", "chdwf_thr_set_theta", "chdwf_thr_get_theta", "chdwf_thr_startup",
-    "chdwf_thr_seed", "chdwf_thr_sweep",
+    "chdwf_thr_seed", "chdwf_thr_sweep", "chdwf_thr_congrad", "chdwf_thr_measure",
+    "chdwf_thr_set_measure",
     "chdwf_prog_sums", "chdwf_prog_reset_sums", "chdwf_prog_averages", "chdwf_prog_take_cg_caps",
     "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
@@ -173,6 +174,9 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_thr_seed.argtypes = [P]
     L.chdwf_thr_seed.restype = D
     L.chdwf_thr_sweep.argtypes = [P, P]
+    L.chdwf_thr_congrad.argtypes = [P, P, F, PI, F, I, P, P]
+    L.chdwf_thr_measure.argtypes = [P, F, P, C.POINTER(F), C.POINTER(F), C.POINTER(F), P]
+    L.chdwf_thr_set_measure.argtypes = [P, I]
     L.chdwf_prog_last_error.argtypes = [P]
     L.chdwf_prog_last_error.restype = C.c_char_p
     L.chdwf_prog_stage.argtypes = [P, I]
@@ -768,7 +772,8 @@ class ThirringRecord(C.Structure):
                 ("it_h0", C.c_int), ("it_h0pv", C.c_int), ("it_h1", C.c_int),
                 ("it_h1pv", C.c_int), ("it_force", C.c_int * 4), ("nforce", C.c_int),
                 ("action", C.c_float), ("gaction", C.c_float), ("paction", C.c_float),
-                ("vel2", C.c_float)]
+                ("vel2", C.c_float), ("measured", C.c_int), ("pbp", C.c_float),
+                ("ancgm", C.c_float)]
 
 
 class Thirring:
@@ -843,6 +848,29 @@ class Thirring:
         if rc not in (CHDWF_OK, CHDWF_ITER_CAP):
             self._check(rc)
         return x, it.value, rc == CHDWF_ITER_CAP, P0, dS
+
+    def congrad(self, Phi, u, x0, res, am, imass):
+        """congrad: x with M^dag M x = Phi from x0; returns (x, itercg, capped)."""
+        x = self._spinor(x0).copy()
+        it = C.c_int(0)
+        rc = self.lib.chdwf_thr_congrad(self.h, _ptr(self._spinor(Phi)), res, C.byref(it), am,
+                                        imass, _ptr(np.ascontiguousarray(u, dtype=np.complex128)),
+                                        _ptr(x))
+        if rc not in (CHDWF_OK, CHDWF_ITER_CAP):
+            self._check(rc)
+        return x.reshape(self.shape), it.value, rc == CHDWF_ITER_CAP
+
+    def measure(self, u, res=1e-6):
+        """measure with links u: (psibarpsi, susclsing, aviter, parts[10, 4])."""
+        pb, su, av = C.c_float(), C.c_float(), C.c_float()
+        parts = np.empty((10, 4), dtype=np.float64)
+        self._check(self.lib.chdwf_thr_measure(
+            self.h, res, _ptr(np.ascontiguousarray(u, dtype=np.complex128)), C.byref(pb),
+            C.byref(su), C.byref(av), _ptr(parts)))
+        return pb.value, su.value, av.value, parts
+
+    def set_measure(self, iprint):
+        self._check(self.lib.chdwf_thr_set_measure(self.h, iprint))
 
     def set_theta(self, theta):
         self._check(self.lib.chdwf_thr_set_theta(self.h, _ptr(np.ascontiguousarray(theta, dtype=np.float32))))

@@ -288,6 +288,58 @@ __global__ void k_thr_noise(double2* __restrict__ R, const float* __restrict__ g
     R[j] = make_double2((double)ps[site], (double)ps[g.kvol + site]);
 }
 
+// ---- congrad (:931-1025) and measure (:1027-1285) -------------------------
+// x += alpha p
+__global__ void k_thr_axpy(double2* __restrict__ x, const double2* __restrict__ p, double a,
+                           int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j < n) x[j] = zadd(x[j], zscal(a, p[j]));
+}
+
+// r -= alpha x2 ; block partials of |r|^2
+__global__ void __launch_bounds__(kThreads) k_thr_cg_r(double2* __restrict__ r,
+                                                       const double2* __restrict__ x2, double a,
+                                                       int64_t n, double* __restrict__ part) {
+    __shared__ double sh[kThreads / 32];
+    double loc = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = zsub(r[j], zscal(a, x2[j]));
+        r[j] = v;
+        loc += zmul(zconj(v), v).x;
+    }
+    loc = block_sum<kThreads>(loc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = loc;
+}
+
+// p = r + beta p
+__global__ void k_thr_xpay(double2* __restrict__ p, const double2* __restrict__ r, double b,
+                           int64_t n) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j < n) p[j] = zadd(r[j], zscal(b, p[j]));
+}
+
+// xi = 0 except component d at wall s: sgn*cmplx(eta(i,1), eta(i,2))
+__global__ void k_thr_wall_source(double2* __restrict__ xi, const float* __restrict__ eta,
+                                  int s, int d, double sgn, TGeom g) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= g.kferm) return;
+    const int sj = (int)(j % g.Ls);
+    const int64_t r = j / g.Ls;
+    const int64_t i = r % g.kvol;
+    const int dj = (int)(r / g.kvol);
+    double2 v = make_double2(0.0, 0.0);
+    if (sj == s && dj == d) v = make_double2(sgn * (double)eta[i], sgn * (double)eta[g.kvol + i]);
+    xi[j] = v;
+}
+
+// out[i] = x(s, i, d)
+__global__ void k_thr_slice(const double2* __restrict__ x, int s, int d, TGeom g,
+                            double2* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < g.kvol) out[i] = x[s + (int64_t)g.Ls * (i + (int64_t)g.kvol * d)];
+}
+
 unsigned tblk(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
 }  // namespace
@@ -304,8 +356,9 @@ struct chdwf_thr {
     int device = 0;
     TGeom g{};
     float dt = 0.1f, beta = 0.5f, am3 = 1.0f, am = 0.0f;
-    int imass = 1, iterl = 1;
+    int imass = 1, iterl = 1, iprint = 5;
     float rescga = 0.000000001f, rescgg = 0.000001f;                   // :39
+    float respbp = 0.000001f;                                            // :39
     ThrRemez r2, r4, r2g, r4g;
     cudaStream_t st = nullptr;
     float *theta = nullptr, *thetat = nullptr, *pp = nullptr, *dS = nullptr, *gauss = nullptr;
@@ -524,6 +577,138 @@ int thr_hamilton(chdwf_thr* h, float res2, double* out, int* its) {
     return CHDWF_OK;
 }
 
+// congrad (:931-1025) on device vectors: x in = guess, out = solution;
+// REAL*4 scalars, FP64 sums rounded once.  Returns CHDWF_ITER_CAP at the cap.
+int thr_congrad(chdwf_thr* h, const double2* Phi, float res, int* itercg, float am, int imass,
+                const double2* u, double2* x) {
+    const int64_t n = h->g.kferm;
+    const unsigned nb = chdwf::tblk(n);
+    const int64_t niterc = h->g.Ls * (int64_t)h->g.kvol;                 // :934
+    const float resid = (float)n * res * res;                            // :947
+    double2 *p = h->q, *r = h->rr, *x1 = h->vt, *x2 = h->x3;
+    cudaMemcpyAsync(p, x, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);   // :956-959
+    cudaMemcpyAsync(r, Phi, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
+    float betad = 1.0f, alpha = 1.0f, alphan = 0.0f;
+    cudaError_t e;
+    *itercg = 0;
+    for (int64_t nx = 1; nx <= niterc; nx++) {
+        (*itercg)++;
+        thr_dslash(h, false, am, imass, x1, p, u);                        // :966
+        if (nx != 1) {                                                    // :970-983
+            chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(x1, x1, n, h->part);
+            chdwf::count_launches(1);
+            double ad;
+            if ((e = thr_sum(h, &ad))) return h->fail(e, "thr_congrad");
+            alpha = alphan / (float)ad;
+            chdwf::k_thr_axpy<<<nb, chdwf::kThreads, 0, h->st>>>(x, p, (double)alpha, n);
+            chdwf::count_launches(1);
+        }
+        thr_dslash(h, true, am, imass, x2, x1, u);                        // :987
+        chdwf::k_thr_cg_r<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(r, x2, (double)alpha, n,
+                                                                          h->part);
+        chdwf::count_launches(1);
+        double bn;
+        if ((e = thr_sum(h, &bn))) return h->fail(e, "thr_congrad");
+        const float betan = (float)bn;                                    // :996-1001
+        float beta = betan / betad;
+        betad = betan;
+        alphan = betan;
+        if (nx == 1) beta = 0.0f;
+        chdwf::k_thr_xpay<<<nb, chdwf::kThreads, 0, h->st>>>(p, r, (double)beta, n);
+        chdwf::count_launches(1);
+        if (betan < resid) return CHDWF_OK;
+    }
+    return CHDWF_ITER_CAP;
+}
+
+// measure (:1027-1285) with links u: psibarpsi, susclsing, aviter and the
+// unit-100 records (parts, 40 doubles, or NULL).  Noise from the context's
+// generator (two gauss0 calls per noise vector); the overlaps are summed on
+// the host in the reference's order.
+int thr_measure(chdwf_thr* h, float res, float am, int imass, const double2* u, float* psibarpsi,
+                float* susclsing, float* aviter, double* parts) {
+    const TGeom& g = h->g;
+    const int64_t kvol = g.kvol, n = g.kferm;
+    const int Ls = g.Ls;
+    constexpr int knoise = 10;
+    std::vector<float> ps(2 * kvol), pt(2 * kvol);
+    std::vector<double2> slice(kvol);
+    double pbp[knoise];
+    int iter = 0;
+    double2* xi = h->X2;
+    double2* Phi = h->R;
+    for (int inoise = 0; inoise < knoise; inoise++) {
+        h->rng.gauss0(kvol, ps.data());                                   // :1061
+        h->rng.gauss0(kvol, pt.data());                                   // :1063
+        double p1r = 0.0, p1i = 0.0, p2r = 0.0, p2i = 0.0;
+        for (int idsource = 1; idsource <= 2; idsource++) {
+            for (int w = 0; w < 2; w++) {
+                const float* nz = w == 0 ? ps.data() : pt.data();
+                int dn, dsrc;
+                double sgn = 1.0;
+                if (imass != 5) {
+                    dn = w == 0 ? idsource : idsource + 2;
+                    dsrc = dn;
+                } else {
+                    dn = w == 0 ? idsource + 2 : idsource;
+                    dsrc = w == 0 ? dn - 2 : dn + 2;
+                    sgn = -1.0;
+                }
+                const int s_src = w == 0 ? 0 : Ls - 1;
+                cudaMemcpyAsync(h->gauss, nz, sizeof(float) * 2 * kvol, cudaMemcpyHostToDevice, h->st);
+                chdwf::k_thr_wall_source<<<chdwf::tblk(n), chdwf::kThreads, 0, h->st>>>(
+                    xi, h->gauss, s_src, dsrc - 1, sgn, g);
+                chdwf::count_launches(1);
+                thr_dslash(h, true, am, imass, Phi, xi, u);               // :1136, :1220
+                int it = 0;
+                const int rc = thr_congrad(h, Phi, res, &it, am, imass, u, xi);   // :1138, :1225
+                if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+                iter += it;
+                const int s_rd = imass != 5 ? (w == 0 ? Ls - 1 : 0) : s_src;
+                chdwf::k_thr_slice<<<chdwf::tblk(kvol), chdwf::kThreads, 0, h->st>>>(xi, s_rd, dn - 1,
+                                                                                 g, h->X1);
+                chdwf::count_launches(1);
+                cudaMemcpyAsync(slice.data(), h->X1, sizeof(double2) * kvol, cudaMemcpyDeviceToHost,
+                                h->st);
+                const cudaError_t e = cudaStreamSynchronize(h->st);
+                if (e) return h->fail(e, "thr_measure");
+                double ar = w == 0 ? p1r : p2r, ai = w == 0 ? p1i : p2i;
+                for (int64_t i = 0; i < kvol; i++) {                      // conjg(x)*xi, in order
+                    const double xr = (double)nz[i], xim = (double)nz[kvol + i];
+                    const double yr = slice[i].x, yi = slice[i].y;
+                    ar = ar + (xr * yr - (-xim) * yi);
+                    ai = ai + (xr * yi + (-xim) * yr);
+                }
+                if (w == 0) { p1r = ar; p1i = ai; } else { p2r = ar; p2i = ai; }
+            }
+        }
+        const double kv = (double)kvol;
+        if (imass == 1) {                                                 // :1245-1257
+            p1r = p1r / kv; p1i = p1i / kv; p2r = p2r / kv; p2i = p2i / kv;
+        } else {
+            // (0,-1)*p1 ; (0,+1)*p2 (imass 3) or (0,-1)*p2 (imass 5), as complex products
+            const double s2 = imass == 3 ? 1.0 : -1.0;
+            const double a1 = 0.0 * p1r - (-1.0) * p1i, b1 = 0.0 * p1i + (-1.0) * p1r;
+            const double a2 = 0.0 * p2r - s2 * p2i, b2 = 0.0 * p2i + s2 * p2r;
+            p1r = a1 / kv; p1i = b1 / kv; p2r = a2 / kv; p2i = b2 / kv;
+        }
+        pbp[inoise] = p1r + p2r;
+        if (parts) {
+            parts[4 * inoise] = p1r; parts[4 * inoise + 1] = p1i;
+            parts[4 * inoise + 2] = p2r; parts[4 * inoise + 3] = p2i;
+        }
+    }
+    float pb = 0.0f, sus = 0.0f;                                          // :1266-1276
+    for (int i = 0; i < knoise; i++) {
+        pb = (float)((double)pb + pbp[i]);
+        for (int j = knoise - 1; j >= i + 1; j--) sus = (float)((double)sus + pbp[i] * pbp[j]);
+    }
+    *psibarpsi = pb / (float)knoise;
+    *susclsing = (float)(2 * kvol) * sus / (float)(knoise * (knoise - 1));
+    *aviter = (float)iter / (float)(4 * knoise);                          // :1278
+    return CHDWF_OK;
+}
+
 chdwf_thr* thr_ok(chdwf_thr* h) {
     if (h) cudaSetDevice(h->device);
     return h;
@@ -684,6 +869,34 @@ int chdwf_thr_qmrherm(chdwf_thr* h, const double* Phi, float res, int* itercg, f
     return rc;
 }
 
+int chdwf_thr_congrad(chdwf_thr* h, const double* Phi, float res, int* itercg, float am,
+                      int imass, const double* u, double* x) {
+    if (!thr_ok(h) || !Phi || !itercg || !u || !x || (imass != 1 && imass != 3 && imass != 5))
+        return CHDWF_BAD_ARG;
+    const int64_t n = h->g.kferm;
+    cudaMemcpyAsync(h->R, Phi, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->X2, x, sizeof(double2) * n, cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->uio, u, sizeof(double2) * 3 * h->g.kvol, cudaMemcpyHostToDevice, h->st);
+    const int rc = thr_congrad(h, h->R, res, itercg, am, imass, h->uio, h->X2);
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    cudaMemcpyAsync(x, h->X2, sizeof(double2) * n, cudaMemcpyDeviceToHost, h->st);
+    const cudaError_t e = cudaStreamSynchronize(h->st);
+    return e ? h->fail(e, "thr_congrad") : rc;
+}
+
+int chdwf_thr_measure(chdwf_thr* h, float res, const double* u, float* psibarpsi,
+                      float* susclsing, float* aviter, double* parts) {
+    if (!thr_ok(h) || !u || !psibarpsi || !susclsing || !aviter) return CHDWF_BAD_ARG;
+    cudaMemcpyAsync(h->uio, u, sizeof(double2) * 3 * h->g.kvol, cudaMemcpyHostToDevice, h->st);
+    return thr_measure(h, res, h->am, h->imass, h->uio, psibarpsi, susclsing, aviter, parts);
+}
+
+int chdwf_thr_set_measure(chdwf_thr* h, int iprint) {
+    if (!h || iprint < 1) return CHDWF_BAD_ARG;
+    h->iprint = iprint;
+    return CHDWF_OK;
+}
+
 int chdwf_thr_set_theta(chdwf_thr* h, const float* theta) {
     if (!thr_ok(h) || !theta) return CHDWF_BAD_ARG;
     cudaMemcpyAsync(h->theta, theta, sizeof(float) * 3 * h->g.kvol, cudaMemcpyHostToDevice, h->st);
@@ -820,6 +1033,15 @@ int chdwf_thr_sweep(chdwf_thr* h, chdwf_thr_record* rec) {
     for (int64_t j = 0; j < n3; j++) vel2 = vel2 + pp[j] * pp[j];
     rec->vel2 = vel2 / (float)(3 * kvol);
     h->vel2a = h->vel2a + rec->vel2;
+    if ((h->isweep / h->iprint) * h->iprint == h->isweep) {               // :361-371
+        cudaMemcpyAsync(h->thetat, h->theta, sizeof(float) * n3, cudaMemcpyDeviceToDevice, h->st);
+        chdwf::k_thr_coef<<<nb3, chdwf::kThreads, 0, h->st>>>(h->thetat, h->ut, g);
+        chdwf::count_launches(1);
+        float sus = 0.0f;
+        CK(thr_measure(h, h->respbp, h->am, h->imass, h->ut, &rec->pbp, &sus, &rec->ancgm,
+                       nullptr));
+        rec->measured = 1;
+    }
     CKC(cudaGetLastError(), "thr_sweep");
 #undef CK
 #undef CKC

@@ -13,8 +13,8 @@
  *   chdwf_thr_dslash / _dslashd dslash, dslashd   (:1946-2069, :2071-2188)
  *   chdwf_thr_derivs           derivs             (:820-878)
  *   chdwf_thr_qmrherm          qmrherm, iflag 0-3 with the Phi0 register (:630-818)
- *   chdwf_thr_sweep            one pass of the main loop (:201-400) without
- *                              the measurement of every iprint-th sweep
+ *   chdwf_thr_congrad, _measure congrad, measure  (:931-1025, :1027-1285)
+ *   chdwf_thr_sweep            one pass of the main loop (:201-400)
  *
  * Layouts are the reference's: spinors R(kthird,kvol,4) complex128, s
  * fastest; links u(kvol,3) complex128; theta, pp, dSdpi (kvol,3) REAL*4;
@@ -48,6 +48,8 @@ typedef struct {
     int it_force[4];
     int nforce;
     float action, gaction, paction, vel2;
+    int measured;          /* isweep a multiple of iprint: measure ran */
+    float pbp, ancgm;      /* its psibarpsi and aviter (:367-370) */
 } chdwf_thr_record;
 
 /* Lattice and 'midout' parameters (dt, beta, am3, am, imass, iterl;
@@ -84,6 +86,19 @@ int chdwf_thr_derivs(chdwf_thr* h, const double* R, const double* X2, double anu
 int chdwf_thr_qmrherm(chdwf_thr* h, const double* Phi, float res, int* itercg, float am,
                       int imass, const double* anum, const double* aden, int ndiag, int iflag,
                       const double* u, double* x, double* Phi0, float* dSdpi);
+
+/* congrad (:931-1025): x (in: initial guess, out: solution) of
+ * M^dagger M x = Phi at mass (am, imass); CHDWF_ITER_CAP at kthird*kvol. */
+int chdwf_thr_congrad(chdwf_thr* h, const double* Phi, float res, int* itercg, float am,
+                      int imass, const double* u, double* x);
+/* measure (:1027-1285) with links u at the context's am and imass: the noisy
+ * psibar psi estimator over 10 noise vectors from the context's generator;
+ * parts (40 doubles or NULL) receives re/im of psibarpsi1 and psibarpsi2 per
+ * noise (the unit-100 records). */
+int chdwf_thr_measure(chdwf_thr* h, float res, const double* u, float* psibarpsi,
+                      float* susclsing, float* aviter, double* parts);
+/* Measure every iprint-th sweep (default 5, as the reference). */
+int chdwf_thr_set_measure(chdwf_thr* h, int iprint);
 
 /* The main loop: theta (REAL*4 (kvol,3)), the generator, one sweep. */
 int chdwf_thr_set_theta(chdwf_thr* h, const float* theta);

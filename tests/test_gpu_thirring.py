@@ -14,7 +14,8 @@ Tolerances:
       4^3x4, imass 1, 3, 5, res 1e-6 and 1e-9); dSdpi is REAL*4.
   sweeps: H0, S0, H1, S1, dH within 1e-6 |H0|; trajectory length, the
       Metropolis draw and decision identical while the oracle's margins
-      exceed that.  alphatild, beta0 and phimod are REAL*4 in the reference,
+      exceed that; every second sweep measures (its psibarpsi within 1e-4 of max(|pbp|, 0.1),
+      its draws keep the generators together).  alphatild, beta0 and phimod are REAL*4 in the reference,
       which limits one rational solve to about 1e-7 relative (6e-8 against
       a dense evaluation); H0 chains two heatbath and two hamilton solves,
       and GPU and oracle differ by 3e-7 relative on this workload.
@@ -95,6 +96,35 @@ def test_thirring_qmrherm(remez, am, imass):
         h.close()
 
 
+@pytest.mark.parametrize("imass", [1, 3, 5])
+def test_thirring_measure(imass):
+    """measure: the unit-100 records within 1e-6 of max (congrad in FP64
+    with REAL*4 scalars, stopped at |r|^2 < kferm res^2 with res 1e-9),
+    psibarpsi within 1e-5, aviter within 5 iterations, the generator
+    identical after its 20 gauss0 calls."""
+    L, Lt, Ls = 4, 4, 6
+    lat = po.make_lat(L, Lt, Ls)
+    kv = po.kvol(lat)
+    _, _, theta = _fields(lat, 13)
+    uo = po.thr_coef(lat, theta)
+    am = np.float32(0.2)
+    ro = po.Rand(SEED)
+    pb_o, su_o, av_o, parts_o = po.thr_measure(lat, ro, uo, 1e-9, am, imass)
+    h = chb.Thirring(L, Lt, Ls, 0.1, 0.5, 1.0, float(am), imass, 4)
+    try:
+        h.startup(SEED)
+        pb_g, su_g, av_g, parts_g = h.measure(uo, 1e-9)
+        seed_g = h.seed()
+    finally:
+        h.close()
+    assert np.abs(parts_g - parts_o).max() <= 1e-6 * np.abs(parts_o).max()
+    pbp = parts_o[:, 0] + parts_o[:, 2]
+    assert abs(pb_g - pb_o) <= 1e-5 * np.abs(pbp).max()
+    assert abs(su_g - su_o) <= 1e-5 * kv * np.max(pbp ** 2)
+    assert abs(av_g - av_o) <= 5
+    assert seed_g == ro.seed()
+
+
 def _oracle_sets(remez):
     return [po.remez_struct(r["anum"][0], r["anum"][1:], r["aden"], r["bnum"][0], r["bnum"][1:],
                             r["bden"]) for r in (remez["remez2"], remez["remez4"],
@@ -107,8 +137,9 @@ def test_thirring_sweeps_against_oracle(remez, imass):
     kv = L * L * Lt
     theta = (0.2 * np.random.default_rng(8).standard_normal((3, kv))).astype(np.float32)
     sw = po.ThrSweeper(L, Lt, Ls, 0.5, 1.0, dt, am, imass, iterl, *_oracle_sets(remez),
-                       theta=theta, seed=SEED)
+                       theta=theta, seed=SEED, iprint=2)
     h = chb.Thirring(L, Lt, Ls, dt, 0.5, 1.0, am, imass, iterl)
+    h.set_measure(2)
     for which, name in ((2, "remez2"), (4, "remez4"), (22, "remez2g"), (44, "remez4")):
         h.set_remez(which, remez[name])
     h.set_theta(theta)
@@ -131,6 +162,10 @@ def test_thirring_sweeps_against_oracle(remez, imass):
                 if abs(ro.x - ro.y) <= 2 * tol * abs(ro.y):
                     break
             assert rg.accepted == ro.accepted
+            assert rg.measured == ro.measured
+            if ro.measured:
+                # congrad at respbp 1e-6: records good to about 1e-6 of their scale
+                assert abs(rg.pbp - ro.pbp) <= 1e-4 * max(abs(ro.pbp), 0.1)
             assert h.seed() == sw.seed()
             th_g, th_o = h.get_theta(), sw.theta.reshape(3, -1)
             assert np.abs(th_g - th_o).max() <= 1e-5 * np.abs(th_o).max()
