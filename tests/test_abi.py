@@ -51,3 +51,28 @@ def test_null_context_is_rejected():
     lib = chb.load_library()
     assert lib.chdwf_set_para(None, 0.5, 1.0, -1) == chb.CHDWF_BAD_ARG
     assert lib.chdwf_dslash(None, None, None, None, 0.0, 0.0, 1) == chb.CHDWF_BAD_ARG
+
+
+def test_hmc_and_thirring_reject_bad_arguments():
+    """The single-precision HMC and the Thirring contexts validate their
+    arguments before touching a device: bad lattices, mass terms and
+    trajectory lengths are refused, and every entry point refuses a NULL
+    context."""
+    chbuild.build()
+    lib = chb.load_library()
+    h = C.c_void_p()
+    assert lib.chdwf_hmc_create(C.byref(h), 1, 4, 4, 0.1, 0.5, 1.0, 0.0, 1, 5, 0) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_hmc_create(C.byref(h), 4, 4, 4, 0.1, 0.5, 1.0, 0.0, 5, 5, 0) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_hmc_create(C.byref(h), 4, 4, 4, 0.1, 0.5, 1.0, 0.0, 1, 0, 0) == chb.CHDWF_BAD_ARG
+    assert b"bad lattice" in lib.chdwf_hmc_last_error(None)
+    assert lib.chdwf_thr_create(C.byref(h), 4, 1, 4, 0.1, 0.5, 1.0, 0.2, 1, 5, 0) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_thr_create(C.byref(h), 4, 4, 4, 0.1, 0.5, 1.0, 0.2, 2, 5, 0) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_thr_create(None, 4, 4, 4, 0.1, 0.5, 1.0, 0.2, 1, 5, 0) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_hmc_dslash(None, None, None, None, 1) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_hmc_sweep(None, None) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_hmc_set_measure(None, 2) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_thr_dslash(None, None, None, None, 0.2, 1) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_thr_sweep(None, None) == chb.CHDWF_BAD_ARG
+    z = (C.c_double * 26)()
+    assert lib.chdwf_thr_set_remez(None, 2, z, z, z, z, 25) == chb.CHDWF_BAD_ARG
+    assert lib.chdwf_thr_set_measure(None, 2) == chb.CHDWF_BAD_ARG
