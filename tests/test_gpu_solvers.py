@@ -143,3 +143,34 @@ def test_basis_store_and_regeneration_agree(remez, iflag):
     assert out[0][1] == out[1][1]
     assert rel(out[0][0], out[1][0]) <= 1e-14
     assert np.abs(out[0][2] - out[1][2]).max() <= 2 * np.spacing(np.float32(np.abs(out[1][2]).max()))
+
+
+def test_failures_are_reported_and_the_context_survives(remez):
+    """Failures are made on the host side of the boundary and come back as
+    status codes, never as a hang: a NaN injected into chi stops congrad
+    and qmrherm with CHDWF_NONFINITE; a residual below REAL*4 reach makes
+    congrad run to its cap kthird*kvol and return CHDWF_ITER_CAP (the
+    reference prints its message and goes on).  The context then solves
+    normally again."""
+    L, Lt, Ls = 4, 4, 4
+    R, chi = random_fields(L, Lt, Ls, seed=31)
+    lat = po.make_lat(L, Lt, Ls)
+    gl = chb.Lattice(L, Lt, Ls, beta=0.475)
+    try:
+        bad = chi.copy()
+        bad[1, 5] = np.nan
+        with pytest.raises(chb.ChdwfError) as e:
+            gl.congrad(R, 1e-9, bad, R)
+        assert e.value.code == chb.CHDWF_NONFINITE
+        r = remez["remez4"]
+        with pytest.raises(chb.ChdwfError) as e:
+            gl.qmrherm(R, 1e-9, r["anum"], r["aden"], 0, bad)
+        assert e.value.code == chb.CHDWF_NONFINITE
+        with pytest.raises(chb.IterationCapError):
+            gl.congrad(R, 1e-30, chi, R)
+        x, it = gl.congrad(R, 1e-9, chi, R)
+        xo, ito, capped = po.congrad(lat, R, chi, R, 1e-9)
+        assert not capped
+        assert rel(x, xo) <= 1e-6 and abs(it - ito) <= 2
+    finally:
+        gl.close()

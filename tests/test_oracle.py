@@ -301,3 +301,26 @@ def test_measure_matches_dense_solve(imass):
     iters = round(float(av) * 40)
     assert 0 < iters < 40 * Ls * kvol and av == np.float32(iters) / np.float32(40)
     assert seed_after == rand.seed()
+
+
+def test_leapfrog_dH_scales_as_dt_squared(remez):
+    """The RHMC trajectory (heatbath, leapfrog with the REAL*4 momenta and
+    force, the two Hamiltonian solves, rhmc/cheisdwf.f:207-345) conserves H
+    to O(dt^2): the first trajectory from the same chi and seed (the same
+    draws, so the same 16 steps) loses about 4x in |dH| when dt is halved."""
+    L, Lt, Ls = 4, 4, 4
+    kv = L * L * Lt
+    rs = [po.remez_struct(r["anum"][0], r["anum"][1:], r["aden"], r["bnum"][0], r["bnum"][1:],
+                          r["bden"]) for r in (remez["remez2"], remez["remez4"], remez["remez2g"])]
+    out = {}
+    for dt in (0.1, 0.05):
+        chi = np.random.default_rng(12345).standard_normal((3, kv)) / np.sqrt(0.475)
+        sw = po.Sweeper(L, Lt, Ls, 0.475, 1.0, dt, 0.01, 0.0, 1, 10, *rs, chi=chi,
+                        seed=693764523745.0, measure=False)
+        rec = sw.sweep()
+        out[dt] = (rec.dH, rec.H0, rec.nsteps)
+        sw.close()
+    (a, h, na), (b, _, nb) = out[0.1], out[0.05]
+    assert na == nb
+    assert abs(a) < 1e-3 * abs(h)
+    assert abs(b) < 0.35 * abs(a)
