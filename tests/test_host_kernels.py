@@ -1,0 +1,238 @@
+"""CPU check of the element arithmetic of two CUDA kernel families against
+the oracle, bit for bit, without a GPU.
+
+The single-precision HMC operator and force (chiralheisenberg_b200/csrc/
+hmc.cu) and the Thirring link operator, coef and derivs (csrc/thirring.cu)
+compute each output element in registers with round-to-nearest intrinsics
+(__fadd_rn, __dmul_rn, ...) and no fused multiply-add.  Host IEEE arithmetic
+compiled with -ffp-contract=off rounds the same way, so the same element
+functions, compiled for the host with those intrinsics mapped to plain
+operators, must reproduce the oracle's sequential sweeps exactly.  This test
+extracts the element functions and per-element kernels from the two .cu
+files (between the section comments named below), compiles them with g++
+into a small program, runs every element over random inputs, and compares.
+
+It checks the arithmetic of the kernel bodies only; the device build, the
+launch shapes and the solvers are checked by the -m gpu tests.
+"""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "chiralheisenberg_b200", "csrc")
+CUDA_INC = "/usr/local/cuda/include"
+
+PRELUDE = r'''
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#define __forceinline__
+#define __constant__
+static int64_t g_tid;
+static const int kThreads = 256;
+static inline float __fadd_rn(float a, float b) { return a + b; }
+static inline float __fsub_rn(float a, float b) { return a - b; }
+static inline float __fmul_rn(float a, float b) { return a * b; }
+static inline double __dadd_rn(double a, double b) { return a + b; }
+static inline double __dsub_rn(double a, double b) { return a - b; }
+static inline double __dmul_rn(double a, double b) { return a * b; }
+static inline float __double2float_rn(double a) { return (float)a; }
+template <class T> static inline T __ldg(const T* p) { return *p; }
+'''
+
+ZOPS = r'''
+static inline double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+static inline double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+static inline double2 zscal(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+static inline double2 zmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+static inline double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+'''
+
+HMC_MAIN = r'''
+struct Geom { int L, Lt, Ls; int kvol; int64_t npts, cs, kferm; };
+int main(int argc, char** argv) {
+    int L = atoi(argv[1]), Lt = atoi(argv[2]), Ls = atoi(argv[3]), imass = atoi(argv[4]);
+    float beta = atof(argv[5]);
+    Geom g; g.L = L; g.Lt = Lt; g.Ls = Ls; g.kvol = L * L * Lt; g.npts = (int64_t)g.kvol * Ls;
+    g.cs = g.npts; g.kferm = 8 * g.npts;
+    std::vector<float2> R(g.kferm), out(g.kferm), outd(g.kferm);
+    std::vector<float> chi(3 * g.kvol), dS(3 * g.kvol);
+    FILE* f = fopen(argv[6], "rb");
+    if (fread(R.data(), sizeof(float2), g.kferm, f) != (size_t)g.kferm) return 1;
+    if (fread(chi.data(), 4, 3 * g.kvol, f) != (size_t)(3 * g.kvol)) return 1;
+    fclose(f);
+    const float diag = (3.0f - 1.0f) + 1.0f;
+    for (g_tid = 0; g_tid < g.kferm; g_tid++) {
+        if (imass == 1) { k_hmc_dslash<false,1>(out.data(), R.data(), chi.data(), g, diag, 1);
+                          k_hmc_dslash<true,1>(outd.data(), R.data(), chi.data(), g, diag, 1); }
+        else { k_hmc_dslash<false,3>(out.data(), R.data(), chi.data(), g, diag, 1);
+               k_hmc_dslash<true,3>(outd.data(), R.data(), chi.data(), g, diag, 1); }
+    }
+    for (g_tid = 0; g_tid < g.kvol; g_tid++) {
+        if (imass == 1) k_hmc_derivs<1>(R.data(), chi.data(), g, 2.0f * beta, diag, 1, dS.data());
+        else k_hmc_derivs<3>(R.data(), chi.data(), g, 2.0f * beta, diag, 1, dS.data());
+    }
+    f = fopen(argv[7], "wb");
+    fwrite(out.data(), sizeof(float2), g.kferm, f); fwrite(outd.data(), sizeof(float2), g.kferm, f);
+    fwrite(dS.data(), 4, 3 * g.kvol, f); fclose(f);
+    return 0;
+}
+'''
+
+THR_MAIN = r'''
+int main(int argc, char** argv) {
+    int L = atoi(argv[1]), Lt = atoi(argv[2]), Ls = atoi(argv[3]), imass = atoi(argv[4]);
+    float am = atof(argv[5]); double anum = atof(argv[6]);
+    TGeom g; g.L = L; g.Lt = Lt; g.Ls = Ls; g.kvol = L * L * Lt; g.kferm = 4 * (int64_t)g.kvol * Ls;
+    const int64_t n3 = 3 * (int64_t)g.kvol;
+    std::vector<double2> R(g.kferm), X2(g.kferm), u(n3), out(g.kferm), outd(g.kferm);
+    std::vector<float> theta(n3), dS0(n3, 0.f), dS1(n3, 0.f);
+    FILE* f = fopen(argv[7], "rb");
+    if (fread(R.data(), 16, g.kferm, f) != (size_t)g.kferm) return 1;
+    if (fread(X2.data(), 16, g.kferm, f) != (size_t)g.kferm) return 1;
+    if (fread(theta.data(), 4, n3, f) != (size_t)n3) return 1;
+    fclose(f);
+    for (g_tid = 0; g_tid < n3; g_tid++) k_thr_coef(theta.data(), u.data(), g);
+    const double diag = (double)((3.0f - 1.0f) + 1.0f);
+    for (int dag = 0; dag < 2; dag++) {
+        double2 zk = imass == 1 ? make_double2((double)am, 0.0)
+                                : make_double2(0.0, dag ? (double)am : (double)(-am));
+        double2* o = dag ? outd.data() : out.data();
+        for (g_tid = 0; g_tid < g.kferm; g_tid++) {
+            if (!dag) { if (imass == 1) k_thr_dslash<false,1>(o, R.data(), u.data(), g, diag, zk);
+                        else if (imass == 3) k_thr_dslash<false,3>(o, R.data(), u.data(), g, diag, zk);
+                        else k_thr_dslash<false,5>(o, R.data(), u.data(), g, diag, zk); }
+            else { if (imass == 1) k_thr_dslash<true,1>(o, R.data(), u.data(), g, diag, zk);
+                   else if (imass == 3) k_thr_dslash<true,3>(o, R.data(), u.data(), g, diag, zk);
+                   else k_thr_dslash<true,5>(o, R.data(), u.data(), g, diag, zk); }
+        }
+    }
+    const double tz = (double)(float)(2.0 * anum);
+    for (g_tid = 0; g_tid < n3; g_tid++) {
+        k_thr_derivs(R.data(), X2.data(), g, tz, 0, dS0.data());
+        k_thr_derivs(R.data(), X2.data(), g, tz, 1, dS1.data());
+    }
+    f = fopen(argv[8], "wb");
+    fwrite(u.data(), 16, n3, f); fwrite(out.data(), 16, g.kferm, f); fwrite(outd.data(), 16, g.kferm, f);
+    fwrite(dS0.data(), 4, n3, f); fwrite(dS1.data(), 4, n3, f); fclose(f);
+    return 0;
+}
+'''
+
+
+def _section(src, start, end):
+    a, b = src.find(start), src.find(end)
+    assert a >= 0 and b > a, f"section markers moved: {start!r} .. {end!r}"
+    return src[a:b]
+
+
+def _hostify(body):
+    body = body.replace("__global__ void __launch_bounds__(kThreads)", "void")
+    body = body.replace("__global__ void", "void")
+    return body.replace("blockIdx.x * (int64_t)blockDim.x + threadIdx.x", "g_tid")
+
+
+def _build(tmp, name, code):
+    cxx = shutil.which("g++")
+    if cxx is None or not os.path.isdir(CUDA_INC):
+        pytest.skip("needs g++ and the CUDA headers")
+    src = os.path.join(tmp, name + ".cpp")
+    exe = os.path.join(tmp, name)
+    with open(src, "w") as f:
+        f.write(code)
+    subprocess.run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-w", "-I", CUDA_INC, "-o",
+                    exe, src], check=True)
+    return exe
+
+
+@pytest.fixture(scope="module")
+def hmc_exe(tmp_path_factory):
+    src = open(os.path.join(CSRC, "hmc.cu")).read()
+    body = _section(src, "// ---- REAL*4 complex arithmetic", "// ---- congrad (mh/cheisdwf_hmc.f:625-716)")
+    body += _section(src, "template <int IMASS>\n__global__ void __launch_bounds__(kThreads) k_hmc_derivs",
+                     "// R(s, i, d, f) = cmplx")
+    code = PRELUDE + HMC_MAIN.split("int main")[0] + "namespace X {\n" + _hostify(body) + \
+        "}\nusing namespace X;\nint main" + HMC_MAIN.split("int main")[1]
+    return _build(str(tmp_path_factory.mktemp("hmc")), "hmc", code)
+
+
+@pytest.fixture(scope="module")
+def thr_exe(tmp_path_factory):
+    src = open(os.path.join(CSRC, "thirring.cu")).read()
+    body = _section(src, "struct TGeom {", "// ---- multi-shift solver kernels")
+    code = PRELUDE + ZOPS + "namespace X {\n" + _hostify(body) + "}\nusing namespace X;\n" + THR_MAIN
+    return _build(str(tmp_path_factory.mktemp("thr")), "thr", code)
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 5), (6, 4, 8)])
+@pytest.mark.parametrize("imass", [1, 3])
+def test_hmc_element_kernels_match_oracle(hmc_exe, tmp_path, shape, imass):
+    L, Lt, Ls = shape
+    rng = np.random.default_rng(L * 100 + Lt * 10 + Ls + imass)
+    sh = (2, 4, Lt, L, L, Ls)
+    R = (rng.standard_normal(sh) + 1j * rng.standard_normal(sh)).astype(np.complex64)
+    chi = (0.7 * rng.standard_normal((3, L * L * Lt))).astype(np.float32)
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(fin, "wb") as f:
+        f.write(R.tobytes())
+        f.write(chi.tobytes())
+    subprocess.run([hmc_exe, str(L), str(Lt), str(Ls), str(imass), "0.475", fin, fout], check=True)
+    raw = np.fromfile(fout, dtype=np.uint8)
+    n = R.size * 8
+    out = np.frombuffer(raw[:n].tobytes(), dtype=np.complex64).reshape(sh)
+    outd = np.frombuffer(raw[n:2 * n].tobytes(), dtype=np.complex64).reshape(sh)
+    dS = np.frombuffer(raw[2 * n:].tobytes(), dtype=np.float32).reshape(3, -1)
+    lat = po.make_lat(L, Lt, Ls, beta=0.475)
+    assert np.array_equal(out, po.hmc_dslash(lat, R, chi, imass))
+    assert np.array_equal(outd, po.hmc_dslash(lat, R, chi, imass, dag=True))
+    assert np.array_equal(dS, po.hmc_derivs(lat, R, chi, imass))
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 5), (2, 6, 3)])
+@pytest.mark.parametrize("imass", [1, 3, 5])
+def test_thirring_element_kernels_match_oracle(thr_exe, tmp_path, shape, imass):
+    L, Lt, Ls = shape
+    lat = po.make_lat(L, Lt, Ls)
+    sh, kv = po.thr_shape(lat), po.kvol(lat)
+    rng = np.random.default_rng(L * 100 + Lt * 10 + Ls + imass)
+    R = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    X2 = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    theta = (0.3 * rng.standard_normal((3, kv))).astype(np.float32)
+    am, anum = np.float32(0.2), 0.3141592653589793
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(fin, "wb") as f:
+        f.write(R.tobytes())
+        f.write(X2.tobytes())
+        f.write(theta.tobytes())
+    subprocess.run([thr_exe, str(L), str(Lt), str(Ls), str(imass), repr(float(am)), repr(anum),
+                    fin, fout], check=True)
+    raw = np.fromfile(fout, dtype=np.uint8)
+    off = [0]
+
+    def take(count, dt):
+        size = count * np.dtype(dt).itemsize
+        v = np.frombuffer(raw[off[0]:off[0] + size].tobytes(), dtype=dt)
+        off[0] += size
+        return v
+
+    u = take(3 * kv, np.complex128).reshape(3, kv)
+    out = take(R.size, np.complex128).reshape(sh)
+    outd = take(R.size, np.complex128).reshape(sh)
+    d0 = take(3 * kv, np.float32).reshape(3, kv)
+    d1 = take(3 * kv, np.float32).reshape(3, kv)
+    uo = po.thr_coef(lat, theta)
+    assert np.array_equal(u, uo)
+    assert np.array_equal(out, po.thr_dslash(lat, R, uo, am, imass))
+    assert np.array_equal(outd, po.thr_dslash(lat, R, uo, am, imass, dag=True))
+    assert np.array_equal(d0, po.thr_derivs(lat, R, X2, anum, 0))
+    assert np.array_equal(d1, po.thr_derivs(lat, R, X2, anum, 1))
