@@ -1,16 +1,21 @@
-"""CPU check of the element arithmetic of two CUDA kernel families against
+"""CPU check of the element arithmetic of three CUDA kernel families against
 the oracle, bit for bit, without a GPU.
 
-The single-precision HMC operator and force (chiralheisenberg_b200/csrc/
-hmc.cu) and the Thirring link operator, coef and derivs (csrc/thirring.cu)
-compute each output element in registers with round-to-nearest intrinsics
-(__fadd_rn, __dmul_rn, ...) and no fused multiply-add.  Host IEEE arithmetic
+The FP64 RHMC operator (dwf_apply_flavour of chiralheisenberg_b200/csrc/
+dwf_stencil.cuh, the body of every FP64 M and M^dagger kernel), the
+single-precision HMC operator and force (csrc/hmc.cu) and the Thirring link
+operator, coef and derivs (csrc/thirring.cu) compute each output element in
+registers with round-to-nearest intrinsics (__dadd_rn, __fmul_rn, ...) and
+no fused multiply-add.  Host IEEE arithmetic
 compiled with -ffp-contract=off rounds the same way, so the same element
 functions, compiled for the host with those intrinsics mapped to plain
 operators, must reproduce the oracle's sequential sweeps exactly.  This test
-extracts the element functions and per-element kernels from the two .cu
-files (between the section comments named below), compiles them with g++
-into a small program, runs every element over random inputs, and compares.
+includes dwf_stencil.cuh as it is (with host stand-ins for the warp and
+atomic intrinsics of common.cuh, which the element function does not
+call), extracts the element functions and per-element kernels of the two
+.cu files (between the section comments named below), compiles each with
+g++ into a small program, runs every element over random inputs, and
+compares.
 
 It checks the arithmetic of the kernel bodies only; the device build, the
 launch shapes and the solvers are checked by the -m gpu tests.
@@ -130,6 +135,62 @@ int main(int argc, char** argv) {
 '''
 
 
+RHMC_PROGRAM = r'''
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#define __forceinline__ inline
+#define __shared__
+static inline double __dadd_rn(double a, double b) { return a + b; }
+static inline double __dsub_rn(double a, double b) { return a - b; }
+static inline double __dmul_rn(double a, double b) { return a * b; }
+template <class T> static inline T __ldg(const T* p) { return *p; }
+static uint3 threadIdx, blockIdx;
+static dim3 blockDim, gridDim;
+static inline double __shfl_down_sync(unsigned, double v, int) { return v; }
+static inline void __syncthreads() {}
+static inline void __threadfence() {}
+static inline unsigned atomicAdd(unsigned* p, unsigned v) { unsigned o = *p; *p += v; return o; }
+#include "dwf_stencil.cuh"
+using namespace chdwf;
+struct Ld { const double2* p; double2 operator()(int64_t j) const { return p[j]; } };
+int main(int argc, char** argv) {
+    int L = atoi(argv[1]), Lt = atoi(argv[2]), Ls = atoi(argv[3]), imass = atoi(argv[4]);
+    int dag = atoi(argv[5]);
+    double hpin = atof(argv[6]);
+    Geom g = make_geom(L, Lt, Ls);
+    std::vector<double2> R(g.kferm), out(g.kferm);
+    std::vector<float> chif(3 * g.kvol);
+    FILE* f = fopen(argv[7], "rb");
+    if (fread(R.data(), 16, g.kferm, f) != (size_t)g.kferm) return 1;
+    if (fread(chif.data(), 4, 3 * g.kvol, f) != (size_t)(3 * g.kvol)) return 1;
+    fclose(f);
+    const double diag = (double)(2.0f * ((3.0f - 1.0f) + 1.0f));
+    const Ld ld{R.data()};
+    for (int64_t p = 0; p < g.npts; p++) {
+        const PointIdx q = point_of(g, p);
+        for (int fl = 0; fl < 2; fl++) {
+            double2 acc[4];
+            if (dag) {
+                if (imass == 1) dwf_apply_flavour<true, 1>(acc, ld, g, q, fl, chif.data(), diag, hpin, true);
+                else dwf_apply_flavour<true, 3>(acc, ld, g, q, fl, chif.data(), diag, hpin, true);
+            } else {
+                if (imass == 1) dwf_apply_flavour<false, 1>(acc, ld, g, q, fl, chif.data(), diag, hpin, true);
+                else dwf_apply_flavour<false, 3>(acc, ld, g, q, fl, chif.data(), diag, hpin, true);
+            }
+            for (int d = 0; d < 4; d++) out[p + g.cs * (d + 4 * fl)] = acc[d];
+        }
+    }
+    f = fopen(argv[8], "wb");
+    fwrite(out.data(), 16, g.kferm, f);
+    fclose(f);
+    return 0;
+}
+'''
+
+
 def _section(src, start, end):
     a, b = src.find(start), src.find(end)
     assert a >= 0 and b > a, f"section markers moved: {start!r} .. {end!r}"
@@ -142,7 +203,7 @@ def _hostify(body):
     return body.replace("blockIdx.x * (int64_t)blockDim.x + threadIdx.x", "g_tid")
 
 
-def _build(tmp, name, code):
+def _build(tmp, name, code, extra=()):
     cxx = shutil.which("g++")
     if cxx is None or not os.path.isdir(CUDA_INC):
         pytest.skip("needs g++ and the CUDA headers")
@@ -150,9 +211,15 @@ def _build(tmp, name, code):
     exe = os.path.join(tmp, name)
     with open(src, "w") as f:
         f.write(code)
-    subprocess.run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-w", "-I", CUDA_INC, "-o",
-                    exe, src], check=True)
+    subprocess.run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-w", "-I", CUDA_INC,
+                    *extra, "-o", exe, src], check=True)
     return exe
+
+
+@pytest.fixture(scope="module")
+def rhmc_exe(tmp_path_factory):
+    return _build(str(tmp_path_factory.mktemp("rhmc")), "rhmc", RHMC_PROGRAM,
+                  extra=["-I", CSRC])
 
 
 @pytest.fixture(scope="module")
@@ -172,6 +239,28 @@ def thr_exe(tmp_path_factory):
     body = _section(src, "struct TGeom {", "// ---- multi-shift solver kernels")
     code = PRELUDE + ZOPS + "namespace X {\n" + _hostify(body) + "}\nusing namespace X;\n" + THR_MAIN
     return _build(str(tmp_path_factory.mktemp("thr")), "thr", code)
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 5), (6, 4, 8)])
+@pytest.mark.parametrize("imass", [1, 3])
+@pytest.mark.parametrize("dag", [0, 1])
+def test_rhmc_fp64_operator_element_matches_oracle(rhmc_exe, tmp_path, shape, imass, dag):
+    """The FP64 M and M^dagger element function, with the pinning term."""
+    L, Lt, Ls = shape
+    rng = np.random.default_rng(L * 100 + Lt * 10 + Ls + imass)
+    lat = po.make_lat(L, Lt, Ls, beta=0.475)
+    sh = po.spinor_shape(lat)
+    R = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    chi = rng.standard_normal((3, L * L * Lt))
+    hpin = np.float32(0.3)
+    fin, fout = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(fin, "wb") as f:
+        f.write(R.tobytes())
+        f.write(chi.astype(np.float32).tobytes())
+    subprocess.run([rhmc_exe, str(L), str(Lt), str(Ls), str(imass), str(dag), repr(float(hpin)),
+                    fin, fout], check=True)
+    out = np.fromfile(fout, dtype=np.complex128).reshape(sh)
+    assert np.array_equal(out, po.dslash(lat, R, chi, hpin=hpin, imass=imass, dag=bool(dag)))
 
 
 @pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 5), (6, 4, 8)])
