@@ -6,6 +6,7 @@
 // element by element in REAL*4 (:1105-1108, :1133-1136), an order no parallel
 // reduction can follow; here each sum is formed in FP64 with a fixed tree and
 // rounded to REAL*4 once.
+#include <cstdio>
 #include <cstring>
 
 #include "cg.h"
@@ -220,7 +221,11 @@ static __device__ __align__(256) unsigned char g_cg_scratch[kStaticBytes];
 
 namespace {
 constexpr int kMaxDevices = 64;
-unsigned char* g_scratch_addr[kMaxDevices] = {};   // device address per device ordinal
+// Device address of the array per device ordinal.  Two host threads making
+// their first call on a device at the same time both look it up and store
+// the same value: a benign race, since cudaGetSymbolAddress returns one
+// address per device.
+unsigned char* g_scratch_addr[kMaxDevices] = {};
 }  // namespace
 
 }  // namespace chdwf
@@ -229,10 +234,13 @@ extern "C" int chdwf_congrad_static(const void* Phi, void* x, const void* chi, i
                                     int ksizet, int kthird, float am3, int ibound, float res,
                                     float hpin, int imass, int* itercg, void* stream) {
     using namespace chdwf;
-    if (!Phi || !x || !chi || !itercg || ksize < 2 || ksizet < 2 || kthird < 2) return 4;
+    if (!Phi || !x || !chi || !itercg) return 4;
     if (imass != 1 && imass != 3) return 4;
+    // sizes in 64-bit arithmetic first: kvol = ksize^2*ksizet is a 32-bit
+    // int in the geometry and must not wrap before the size check
+    if (!geom_ok(ksize, ksizet, kthird)) return 4;
+    if (8 * (int64_t)ksize * ksize * ksizet * kthird > kStaticMaxFerm) return 4;
     const Geom g = make_geom(ksize, ksizet, kthird);
-    if (g.kferm > kStaticMaxFerm) return 4;          // beyond the static scratch
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 3;
     // once per device: the device address of the array (its host-side name
@@ -242,6 +250,9 @@ extern "C" int chdwf_congrad_static(const void* Phi, void* x, const void* chi, i
         if (cudaGetSymbolAddress(&ptr, g_cg_scratch) != cudaSuccess || !ptr) return 3;
         g_scratch_addr[dev] = (unsigned char*)ptr;
     }
+    // a sticky error from earlier work on this device fails here; a stale
+    // non-sticky one is cleared so that it is not reported as this call's
+    if (cudaGetLastError() != cudaSuccess && cudaPeekAtLastError() != cudaSuccess) return 3;
     unsigned char* base = g_scratch_addr[dev];
     CgCtl* ctl = reinterpret_cast<CgCtl*>(base);
     double* part = reinterpret_cast<double*>(base + 256);
@@ -288,14 +299,19 @@ extern "C" int chdwf_congrad_static(const void* Phi, void* x, const void* chi, i
             k_cg3<<<nbf, kThreads, 0, st>>>(a);
             count_launches(3);
         }
+        // a failed launch or copy ends the solve at once instead of launching
+        // on until the iteration cap
+        if (cudaGetLastError() != cudaSuccess) return 3;
         if (cudaMemcpyAsync(&hr, ctl, sizeof(hr), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
             return 3;
         if (hr.done) break;
     }
-    if (cudaGetLastError() != cudaSuccess) return 3;
     *itercg = hr.iters;
-    if (hr.done == 2) return 1;
+    if (hr.done == 2) {
+        fprintf(stdout, " # iterations of congrad exceeds niterc\n");   // :1151-1153
+        return 1;
+    }
     if (hr.done == 3) return 2;
     return 0;
 }
