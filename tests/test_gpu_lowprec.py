@@ -98,3 +98,21 @@ def test_mixed_force_thread_shapes(remez, Ls, store):
     for a, b in zip(recs["f64"], recs["f32"]):
         assert a.nsteps == b.nsteps and a.accepted == b.accepted
         assert abs(a.dH - b.dH) <= 1e-8 * abs(a.H0), (a.dH, b.dH)
+
+
+# FP32 and FP16 storage at the operator sweep's sizes, against the FP64
+# oracle: relative L2 error <= 1e-6 (FP32) and <= 2e-3 (FP16 storage, the
+# half-precision rounding of inputs and outputs).
+@pytest.mark.parametrize("L,Ls", [(16, 16), (24, 24), (32, 16)])
+@pytest.mark.parametrize("prec,tol", [(1, 1e-6), (2, 2e-3)])
+def test_operator_reduced_precision_sweep_sizes(L, Ls, prec, tol):
+    R, chi = random_fields(L, L, Ls, seed=3100 + L + Ls)
+    lat = po.make_lat(L, L, Ls)
+    gl = chb.Lattice(L, L, Ls)
+    for dag in (False, True):
+        ref = po.dslash(lat, R, chi, hpin=0.3, imass=1, dag=dag)
+        out = _lp_apply(gl, R, chi, prec, dag)
+        err = np.linalg.norm(out.reshape(-1) - ref.reshape(-1)) / np.linalg.norm(ref)
+        print(f"L={L} Ls={Ls} prec={prec} dag={dag}: relative error {err:.3e}")
+        assert err <= tol, err
+    gl.close()

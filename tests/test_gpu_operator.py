@@ -67,3 +67,22 @@ def test_operator_large_lattice_adjoint():
     Mlin = gl.dslash(2.5 * x + y, chi, hpin=0.2)
     My = gl.dslash(y, chi, hpin=0.2)
     assert np.linalg.norm(Mlin - (2.5 * Mx + My)) <= 1e-13 * np.linalg.norm(Mlin)
+
+
+# The operator sweep's lattices (L=Lt in {16, 24, 32, 48}, Ls in {16, 24,
+# 32}): FP64 M and M^dagger bit-exact against the oracle at the sizes the
+# sweep times.  48^3 x 16 (a 226 MB spinor) is checked for M only.
+SWEEP_CASES = [(16, 16, False), (16, 16, True), (16, 24, False), (16, 32, True),
+               (24, 16, True), (24, 24, False), (24, 24, True), (24, 32, False),
+               (32, 16, False), (32, 24, True), (48, 16, False)]
+
+
+@pytest.mark.parametrize("L,Ls,dag", SWEEP_CASES)
+def test_operator_bit_exact_sweep_sizes(L, Ls, dag):
+    R, chi = random_fields(L, L, Ls, seed=2024 + L + Ls)
+    lat = po.make_lat(L, L, Ls, beta=0.475, am3=1.0)
+    ref = po.dslash(lat, R, chi, hpin=0.0, imass=1, dag=dag)
+    gl = chb.Lattice(L, L, Ls, beta=0.475, am3=1.0)
+    out = (gl.dslashd if dag else gl.dslash)(R, chi, hpin=0.0, imass=1)
+    gl.close()
+    assert np.array_equal(out.view(np.float64), ref.view(np.float64))
