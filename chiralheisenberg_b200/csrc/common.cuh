@@ -66,13 +66,24 @@ __device__ __forceinline__ double2 zcomb(double2 x, double2 y, bool use_i, int s
     return sgn > 0 ? zadd(x, t) : zsub(x, t);
 }
 
-// ---- single-precision complex (mixed-precision path; contraction allowed) --
-__device__ __forceinline__ float2 zadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 zsub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// ---- single-precision complex (mixed-precision path) ----------------------
+// Also without contraction: every kernel that evaluates the same per-element
+// sequence (the pass-1 kernels and the regenerating pass 2, whatever their
+// thread shape) then produces the same bits, so regenerated Lanczos vectors
+// equal the first pass's.
+__device__ __forceinline__ float2 zadd(float2 a, float2 b) {
+    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 zsub(float2 a, float2 b) {
+    return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
+}
 __device__ __forceinline__ float2 zmuli(float2 a) { return make_float2(-a.y, a.x); }
-__device__ __forceinline__ float2 zscal(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+__device__ __forceinline__ float2 zscal(float s, float2 a) {
+    return make_float2(__fmul_rn(s, a.x), __fmul_rn(s, a.y));
+}
 __device__ __forceinline__ float2 zmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                       __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
 }
 __device__ __forceinline__ float2 zconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 zcomb(float2 x, float2 y, bool use_i, int sgn) {

@@ -2,8 +2,12 @@
 // and the chi-force contraction derivs (rhmc/cheisdwf.f:747-849).
 #include <cuda_fp16.h>
 
+#include <cstdlib>
+#include <cstring>
+
 #include "dwf_stencil.cuh"
 #include "internal.h"
+#include "row_stage.cuh"
 
 namespace chdwf {
 
@@ -29,11 +33,135 @@ __global__ void __launch_bounds__(kSplitThreads, kSplitMinBlocks)
 
 static inline float diag_of(float am3) { return 2.0f * ((3.0f - am3) + 1.0f); }  // :2652
 
+// ---- the operator on staged rows (row_stage.cuh) ------------------------------
+// S: storage type (double2, float2 or __half2), T: arithmetic type.  Per
+// element the operation sequence of k_dslash64 / k_dslash_lp.  A block
+// whose staged copy does not arrive within the bounded wait writes NaN over
+// its rows, so the failure reaches the caller's data.
+template <class T> __device__ __forceinline__ T row_store(T v, T*) { return v; }
+__device__ __forceinline__ __half2 row_store(float2 v, __half2*) { return __float22half2_rn(v); }
+
+template <class S, class T, bool DAG, int IMASS>
+struct OpRows {
+    typedef typename real_of<T>::type Real;
+    const S* __restrict__ in;
+    S* __restrict__ out;
+    const float* __restrict__ chif;
+    const Geom& g;
+    int Lrow;
+    Real diag, hpin;
+    int apbc;
+    T tp[4], tm[4];
+    __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
+        const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
+        const int64_t i = (int64_t)x * g.Ls + s;
+        const int64_t ep = i + (int64_t)Lrow * (y + (int64_t)g.L * tpi);
+        const int64_t em = i + (int64_t)Lrow * (y + (int64_t)g.L * tmi);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            tp[d] = RowCvt<T, S>::get(__ldg(in + ep + g.cs * (d + 4 * f)));
+            tm[d] = RowCvt<T, S>::get(__ldg(in + em + g.cs * (d + 4 * f)));
+        }
+    }
+    __device__ __forceinline__ void compute(const S* c, const S* yp, const S* ym, int f, int t,
+                                            int y, int x, int s, int i, int ixp, int ixm) {
+        const PointIdx q = row_point(g, t, y, x, s);
+        T acc[4];
+        dwf_apply_rows<DAG, IMASS>(acc, c, yp, ym, Lrow, i, ixp, ixm, tp, tm, in, g, q, f, chif,
+                                   diag, hpin, apbc != 0);
+#pragma unroll
+        for (int d = 0; d < 4; d++) out[q.p + g.cs * (d + 4 * f)] = row_store(acc[d], out);
+    }
+};
+
+template <class S, class T, bool DAG, int IMASS>
+__global__ void __maxnreg__(RowRegs<T>::value)
+    k_dslash_rows(S* __restrict__ out, const S* __restrict__ in, const float* __restrict__ chif,
+                  Geom g, RowPlan rp, typename real_of<T>::type diag,
+                  typename real_of<T>::type hpin, int apbc) {
+    extern __shared__ __align__(128) unsigned char row_smem[];
+    OpRows<S, T, DAG, IMASS> body{in, out, chif, g, rp.Lrow, diag, hpin, apbc};
+    if (row_sweep<S>(g, rp, row_smem, in, body)) return;
+    int rho0, rho1;
+    row_range(rp.nrows, &rho0, &rho1);
+    const T nan = zmake<T>((typename real_of<T>::type)NAN, (typename real_of<T>::type)NAN);
+    for (int rho = rho0; rho < rho1; rho++) {
+        const int run = rho / g.L, f = run / g.Lt, t = run - f * g.Lt, y = rho - run * g.L;
+        for (int i = threadIdx.x; i < rp.Lrow; i += blockDim.x)
+            for (int d = 0; d < 4; d++)
+                out[i + (int64_t)rp.Lrow * (y + (int64_t)g.L * t) + g.cs * (d + 4 * f)] =
+                    row_store(nan, out);
+    }
+}
+
+// Plan and grid of the row-staged operator, set up once per kernel, row
+// length and stencil_mode.
+template <class S, class T, bool DAG, int IMASS>
+static bool op_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
+    const int mode = stencil_mode();
+    if (mode == 1) return false;
+    if (!row_plan(g, sizeof(S), RowMaxThreads<T>::value, rp)) return false;
+    static int cached_lrow = -1, cached_nrows = -1, cached_mode = -1;
+    static unsigned cached_nb = 0;
+    if (cached_lrow == rp->Lrow && cached_nrows == rp->nrows && cached_mode == mode) {
+        *nb = cached_nb;
+        return cached_nb > 0;
+    }
+    const void* k = (const void*)k_dslash_rows<S, T, DAG, IMASS>;
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    unsigned n = 0;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp->smem) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, rp->nthreads, rp->smem) ==
+            cudaSuccess &&
+        per_sm >= 1) {
+        int64_t m = (int64_t)nsm * per_sm;
+        if (m > rp->nrows) m = rp->nrows;
+        if (m >= 1 && (mode == 2 || rp->nrows >= 3 * m)) n = (unsigned)m;
+    }
+    cudaGetLastError();
+    cached_lrow = rp->Lrow;
+    cached_nrows = rp->nrows;
+    cached_mode = mode;
+    cached_nb = n;
+    *nb = n;
+    return n > 0;
+}
+
+template <class S, class T, bool DAG, int IMASS>
+static bool launch_op_rows(S* out, const S* in, const float* chif, const Geom& g,
+                           typename real_of<T>::type diag, typename real_of<T>::type hpin,
+                           int apbc, cudaStream_t st) {
+    RowPlan rp;
+    unsigned nb = 0;
+    if (!op_rows_setup<S, T, DAG, IMASS>(g, &rp, &nb)) return false;
+    k_dslash_rows<S, T, DAG, IMASS><<<nb, rp.nthreads, rp.smem, st>>>(out, in, chif, g, rp, diag,
+                                                                      hpin, apbc);
+    count_launches(1);
+    return true;
+}
+
+template <class S, class T>
+static bool launch_op_rows_any(bool dag, int imass, S* out, const S* in, const float* chif,
+                               const Geom& g, typename real_of<T>::type diag,
+                               typename real_of<T>::type hpin, int apbc, cudaStream_t st) {
+    if (imass != 1 && imass != 3) return false;
+    if (!dag)
+        return imass == 1 ? launch_op_rows<S, T, false, 1>(out, in, chif, g, diag, hpin, apbc, st)
+                          : launch_op_rows<S, T, false, 3>(out, in, chif, g, diag, hpin, apbc, st);
+    return imass == 1 ? launch_op_rows<S, T, true, 1>(out, in, chif, g, diag, hpin, apbc, st)
+                      : launch_op_rows<S, T, true, 3>(out, in, chif, g, diag, hpin, apbc, st);
+}
+
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
     const unsigned nb = split_blocks(g.npts);
     const double diag = (double)diag_of(am3), hp = (double)hpin;
     const int apbc = ibound == -1;
+    if (launch_op_rows_any<double2, double2>(dag, imass, out, in, chif, g, diag, hp, apbc, st))
+        return;
 #define LAUNCH(D, I) k_dslash64<D, I><<<nb, kSplitThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc)
     if (!dag) {
         if (imass == 1) LAUNCH(false, 1); else if (imass == 3) LAUNCH(false, 3); else LAUNCH(false, 0);
@@ -102,6 +230,17 @@ __global__ void __launch_bounds__(kSplitThreads, 3)
 
 void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
                       const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
+    {
+        const float diag = diag_of(am3);
+        const int apbc = ibound == -1;
+        if (half ? launch_op_rows_any<__half2, float2>(dag, imass, (__half2*)out,
+                                                       (const __half2*)in, chif, g, diag, hpin,
+                                                       apbc, st)
+                 : launch_op_rows_any<float2, float2>(dag, imass, (float2*)out,
+                                                      (const float2*)in, chif, g, diag, hpin,
+                                                      apbc, st))
+            return;
+    }
     if (!half && g.Ls % 2 == 0) {
         const unsigned nb2 = (unsigned)((g.npts + 2 * kSplitPoints - 1) / (2 * kSplitPoints));
         const float diag = diag_of(am3);

@@ -27,7 +27,8 @@ constexpr int kThreads = 256;
 struct LzCtl {
     int it_m;          // iteration j of the next pass-1 M launch (written by M^dagger)
     int it_md;         // iteration j of the next pass-1 M^dagger launch (written by M)
-    int done;          // 0 running, 1 converged, 2 iteration cap
+    int done;          // 0 running, 1 converged, 2 iteration cap, 3 non-finite,
+                       // 4 a staged copy did not arrive (row kernels)
     int m;             // iteration at which the loop ended
     int npole;
     int niter_cap;

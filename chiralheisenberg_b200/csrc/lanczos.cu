@@ -384,6 +384,154 @@ __global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz
     if (threadIdx.x == 0) a.part[nb + blockIdx.x] = loc;
 }
 
+// ---- pass 1 on staged rows ---------------------------------------------------
+// The same two kernels with the stencil's input rows staged in shared memory
+// (row_stage.cuh): a persistent grid of the blocks that fit on all SMs at
+// once, each walking a contiguous range of output rows of one flavour at a
+// time.  Per element the operation sequence is that of k_lz1_M / k_lz1_Md,
+// so the vectors are the same bits and the regenerating pass 2 reproduces
+// them.  A copy that does not arrive within the bounded wait stops the solve
+// with done = 4 (reported as a CUDA error).
+__device__ __forceinline__ void row_fail(LzCtl* ctl, int* hflag) {
+    ctl->done = 4;
+    ctl->m = ctl->it_m;
+    if (hflag) {
+        *(volatile int*)hflag = 4;
+        __threadfence_system();
+    }
+}
+
+template <class T, int IMASS>
+struct LzRowsM {
+    typedef typename real_of<T>::type Real;
+    const LzArgsT<T>& a;
+    const T* rj;
+    Real ib;
+    double loc;
+    T tp[4], tm[4];
+    __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
+        const Geom& g = a.g;
+        const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
+        const int64_t i = (int64_t)x * g.Ls + s, Lrow = (int64_t)g.L * g.Ls;
+        const int64_t ep = i + Lrow * (y + (int64_t)g.L * tpi), em = i + Lrow * (y + (int64_t)g.L * tmi);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            tp[d] = __ldg(rj + ep + g.cs * (d + 4 * f));
+            tm[d] = __ldg(rj + em + g.cs * (d + 4 * f));
+        }
+    }
+    __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, int f, int t,
+                                            int y, int x, int s, int i, int ixp, int ixm) {
+        const Geom& g = a.g;
+        const PointIdx q = row_point(g, t, y, x, s);
+        T acc[4];
+        dwf_apply_rows<false, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, rj, g, q, f,
+                                     a.chif, a.diag, a.hpin, a.apbc != 0);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            acc[d] = zscal(ib, acc[d]);
+            a.vt[q.p + g.cs * (d + 4 * f)] = acc[d];
+            const double2 w = widen(acc[d]);
+            loc += w.x * w.x + w.y * w.y;
+        }
+    }
+};
+
+template <class T, int IMASS>
+__global__ void __maxnreg__(RowRegs<T>::value) k_lz1_M_rows(LzArgsT<T> a) {
+    extern __shared__ __align__(128) unsigned char row_smem[];
+    LzCtl* ctl = a.ctl;
+    if (block_stopped(ctl)) return;
+    const int j = ctl->it_m;
+    const int nb = gridDim.x;
+    const double bj = j == 1 ? a.h.beta[1] : sqrt(sum_partials_any(a.part + nb, nb));
+    const double ibj = j == 1 ? a.h.invbeta[1] : 1.0 / bj;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->it_md = j;
+        if (j > 1) {
+            a.h.beta[j] = bj;
+            a.h.invbeta[j] = ibj;
+        }
+    }
+    LzRowsM<T, IMASS> body{a, ring(a, j), (typename real_of<T>::type)ibj, 0.0};
+    const bool ok = row_sweep<T>(a.g, a.rp, row_smem, body.rj, body);
+    __shared__ double sh[32];
+    const double loc = block_sum_any(body.loc, sh);
+    if (threadIdx.x == 0) {
+        a.part[blockIdx.x] = loc;
+        if (!ok) row_fail(ctl, a.hflag);
+    }
+}
+
+template <class T, int IMASS, bool WALLS>
+struct LzRowsMd {
+    typedef typename real_of<T>::type Real;
+    const LzArgsT<T>& a;
+    const T* rj;
+    const T* rjm;
+    T* rn;
+    int j;
+    Real ib, at, bj, ibm;
+    double loc;
+    T tp[4], tm[4], cj[4], cm[4];
+    __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
+        const Geom& g = a.g;
+        const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
+        const int64_t i = (int64_t)x * g.Ls + s, Lrow = (int64_t)g.L * g.Ls;
+        const int64_t e0 = i + Lrow * (y + (int64_t)g.L * t);
+        const int64_t ep = i + Lrow * (y + (int64_t)g.L * tpi), em = i + Lrow * (y + (int64_t)g.L * tmi);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int64_t po = g.cs * (d + 4 * f);
+            tp[d] = __ldg(a.vt + ep + po);
+            tm[d] = __ldg(a.vt + em + po);
+            cj[d] = rj[e0 + po];
+            if (j > 1) cm[d] = rjm[e0 + po];
+        }
+    }
+    __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, int f, int t,
+                                            int y, int x, int s, int i, int ixp, int ixm) {
+        const Geom& g = a.g;
+        const PointIdx q = row_point(g, t, y, x, s);
+        T acc[4];
+        dwf_apply_rows<true, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, a.vt, g, q, f,
+                                    a.chif, a.diag, a.hpin, a.apbc != 0);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int64_t e = q.p + g.cs * (d + 4 * f);
+            // r_{j+1} = x3 - alpha~ q_j - beta_j q_{j-1}, as three_term (:655)
+            const T qj = zscal(ib, cj[d]);
+            T v = zsub(acc[d], zscal(at, qj));
+            if (j > 1) v = zsub(v, zscal(bj, zscal(ibm, cm[d])));
+            rn[e] = v;
+            if (WALLS) wall_put(a, j + 1, q.s, q.site, d + 4 * f, v);
+            const double2 w = widen(v);
+            loc += w.x * w.x + w.y * w.y;
+        }
+    }
+};
+
+template <class T, int IMASS, bool WALLS>
+__global__ void __maxnreg__(RowRegs<T>::value) k_lz1_Md_rows(LzArgsT<T> a) {
+    typedef typename real_of<T>::type Real;
+    extern __shared__ __align__(128) unsigned char row_smem[];
+    LzCtl* ctl = a.ctl;
+    if (block_stopped(ctl)) return;
+    const int j = ctl->it_md;
+    const int nb = gridDim.x;
+    const double at = sum_partials_any(a.part, nb);
+    LzRowsMd<T, IMASS, WALLS> body{a, ring(a, j), ring(a, j - 1), ring(a, j + 1), j,
+                                   (Real)a.h.invbeta[j], (Real)at, (Real)a.h.beta[j],
+                                   (Real)(j > 1 ? a.h.invbeta[j - 1] : 0.0), 0.0};
+    const bool ok = row_sweep<T>(a.g, a.rp, row_smem, a.vt, body);
+    __shared__ double sh[32];
+    const double loc = block_sum_any(body.loc, sh);
+    if (threadIdx.x == 0) {
+        a.part[nb + blockIdx.x] = loc;
+        if (!ok) row_fail(ctl, a.hflag);
+    }
+}
+
 // ---- pass 2: regenerate q_j and accumulate --------------------------------
 // One block pass per block (grid lz_direct_blocks).  The solution update of
 // one element of x (iflag 0) or of the wall fields (iflag 1).
@@ -624,6 +772,65 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
     cudaStreamWaitEvent(st, side.join, 0);
 }
 
+// Row-staged pass 1 (same protocol: M, the scalar step on the side stream,
+// M^dagger).  Grid: the blocks that fit on all SMs at once.
+template <class T, int IMASS>
+static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
+                              const LzSide& side, KernelTimer* tm) {
+    const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
+    const unsigned nt = (unsigned)a.rp.nthreads, sm = a.rp.smem;
+    if (tm) tm->begin(0, st, 2 * V + chi);
+    k_lz1_M_rows<T, IMASS><<<nb, nt, sm, st>>>(a);
+    if (tm) tm->end(st);
+    cudaEventRecord(side.fork, st);
+    cudaStreamWaitEvent(side.stream, side.fork, 0);
+    k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
+    cudaEventRecord(side.join, side.stream);
+    if (tm) tm->begin(1, st, 4 * V + chi);
+    if (a.wcap > 0) k_lz1_Md_rows<T, IMASS, true><<<nb, nt, sm, st>>>(a);
+    else k_lz1_Md_rows<T, IMASS, false><<<nb, nt, sm, st>>>(a);
+    if (tm) tm->end(st);
+    cudaStreamWaitEvent(st, side.join, 0);
+}
+
+// Whether pass 1 runs on the row-staged kernels, and their plan and grid.
+// Rows are used when the ring of staged rows fits a block's shared memory
+// and (stencil_mode) every block gets at least three output rows: the window
+// rows of a block's range cost two loads beyond its own rows.
+template <class T>
+static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
+    const int mode = stencil_mode();
+    if (mode == 1) return false;
+    if (!row_plan(g, sizeof(T), RowMaxThreads<T>::value, rp)) return false;
+    const void* kern[6] = {(const void*)k_lz1_M_rows<T, 1>, (const void*)k_lz1_M_rows<T, 3>,
+                           (const void*)k_lz1_Md_rows<T, 1, false>,
+                           (const void*)k_lz1_Md_rows<T, 1, true>,
+                           (const void*)k_lz1_Md_rows<T, 3, false>,
+                           (const void*)k_lz1_Md_rows<T, 3, true>};
+    int dev = 0, nsm = 0, per_sm = 1 << 20;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    for (const void* k : kern) {
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp->smem) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, rp->nthreads, rp->smem) !=
+                cudaSuccess || b < 1) {
+            cudaGetLastError();
+            return false;
+        }
+        if (b < per_sm) per_sm = b;
+    }
+    int64_t n = (int64_t)nsm * per_sm;
+    if (n > rp->nrows) n = rp->nrows;
+    if (n < 1 || (mode == 0 && rp->nrows < 3 * n)) return false;
+    *nb = (unsigned)n;
+    return true;
+}
+
 // L2 residency of vt = M q_j: k_lz1_M writes it and k_lz1_Md reads it right
 // back, so its address range is marked persisting in L2 for the pass-1
 // launches instead of taking a DRAM round trip.  The persisting carve-out is
@@ -757,6 +964,11 @@ static bool lz_pair(const Geom& g) {
 template <class T>
 static void launch_pass1_any(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
                              KernelTimer* tm, int imass) {
+    if (a.rows) {
+        if (imass == 3) launch_pass1_rows<T, 3>(a, nb, st, side, tm);
+        else launch_pass1_rows<T, 1>(a, nb, st, side, tm);
+        return;
+    }
     if constexpr (std::is_same<T, float2>::value) {
         if (lz_pair<T>(a.g)) {
             if (imass == 3) launch_pass1<T, 3, true>(a, nb, st, side, tm);
@@ -1146,7 +1358,9 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.x = x;
     a.xw = w.xw;
     a.npole = ndiag;
-    const unsigned nb = lz_pass1_blocks_any<T>(g, imass);
+    unsigned nb = 0;
+    a.rows = lz_rows_setup<T>(g, &a.rp, &nb) ? 1 : 0;
+    if (!a.rows) nb = lz_pass1_blocks_any<T>(g, imass);
     const int nbr = reduce_blocks(g.kferm);
     // r_1 lives where ring(a, 1) looks for it: the basis store when present
     T* r1 = a.hcap > 1 ? a.basis + g.kferm : a.rb1;
@@ -1221,6 +1435,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     if ((e = cudaStreamSynchronize(st))) return e;
     const int m = hr.m;
     *itercg = m;
+    if (hr.done == 4) return cudaErrorLaunchTimeout;   // a staged copy never arrived
     *status = hr.done == 1 ? 0 : (hr.done == 2 ? 1 : 2);
     if (stats) { stats->iters = m; stats->pass1_launches = 2 * launched; }
     if (m < 1) return cudaErrorUnknown;

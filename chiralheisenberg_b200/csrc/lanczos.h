@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "row_stage.cuh"
 
 namespace chdwf {
 
@@ -29,6 +30,8 @@ struct LzArgsT {
     int npole;
     T* wbasis;                  // force solves: the two wall slices of each r_j,
     int wcap;                   // j < wcap, at wbasis + j*16*kvol (0: no wall store)
+    int rows;                   // pass 1 on the row-staged kernels (plan rp)
+    RowPlan rp;
 };
 
 struct LzStats {

@@ -146,6 +146,9 @@ RHMC_PROGRAM = r'''
 static inline double __dadd_rn(double a, double b) { return a + b; }
 static inline double __dsub_rn(double a, double b) { return a - b; }
 static inline double __dmul_rn(double a, double b) { return a * b; }
+static inline float __fadd_rn(float a, float b) { return a + b; }
+static inline float __fsub_rn(float a, float b) { return a - b; }
+static inline float __fmul_rn(float a, float b) { return a * b; }
 template <class T> static inline T __ldg(const T* p) { return *p; }
 static uint3 threadIdx, blockIdx;
 static dim3 blockDim, gridDim;

@@ -1,0 +1,91 @@
+"""CPU model of the row-staged kernels' copy schedule (csrc/row_stage.cuh).
+
+The kernels' producer (thread 0 issuing bulk copies of window rows into a
+ring of slots) and consumer (every thread waiting for rows u, u+1, u+2 of
+an output row) are restated here line by line, and for many lattice shapes
+and grid sizes the model checks what the GPU code relies on:
+  * output row (f, t, y) reads window rows (f, t, y-1), (f, t, y), (f, t, y+1)
+    with y periodic;
+  * a slot is refilled only after every output row that reads it is done;
+  * every wait is on a copy already issued, and every issued copy is waited
+    on before the block ends (no copy in flight at exit);
+  * every copy is in bounds and starts on a 16-byte boundary.
+"""
+import pytest
+
+NS = 5   # kRowSlots
+
+
+def simulate(L, Lt, Ls, nb, elem):
+    Lrow = L * Ls
+    nrows = 2 * Lt * L
+    cs = L * L * Lt * Ls
+    kferm = 8 * cs
+    assert (Lrow * elem) % 16 == 0
+    for b in range(nb):
+        rho0, rho1 = b * nrows // nb, (b + 1) * nrows // nb
+        if rho0 >= rho1:
+            continue
+
+        def run_len(ra):
+            return min((ra // L + 1) * L, rho1) - ra
+
+        st = {"rho_a": rho0, "o": 0, "issued": 0, "len": run_len(rho0)}
+        slots, loads, done = {}, [], set()
+
+        def issue():
+            run = st["rho_a"] // L
+            f, t = run // Lt, run % Lt
+            y = (st["rho_a"] - run * L - 1 + st["o"]) % L
+            w = st["issued"]
+            if w % NS in slots:
+                assert slots[w % NS] in done, ("slot refilled before use ended", w)
+            slots[w % NS] = w
+            for d in range(4):
+                off = cs * (4 * f + d) + Lrow * (y + L * t)
+                assert 0 <= off and off + Lrow <= kferm
+                assert (off * elem) % 16 == 0
+            loads.append((f, t, y))
+            st["issued"] += 1
+            st["o"] += 1
+            if st["o"] == st["len"] + 2:
+                st["rho_a"] += st["len"]
+                st["o"] = 0
+                if st["rho_a"] < rho1:
+                    st["len"] = run_len(st["rho_a"])
+
+        while st["issued"] < NS and st["rho_a"] < rho1:
+            issue()
+        u, run_prev = 0, rho0 // L
+        for rho in range(rho0, rho1):
+            run = rho // L
+            if run != run_prev:
+                u += 2
+                run_prev = run
+            f, t, y = run // Lt, run % Lt, rho - run * L
+            for k in range(3):
+                assert u + k < st["issued"] and slots[(u + k) % NS] == u + k
+            assert loads[u] == (f, t, (y - 1) % L)
+            assert loads[u + 1] == (f, t, y)
+            assert loads[u + 2] == (f, t, (y + 1) % L)
+            u += 1
+            next_u = u + 2 if (rho + 1 < rho1 and (rho + 1) // L != run) else u
+            done.update(range(next_u))
+            while st["rho_a"] < rho1 and st["issued"] < next_u + NS:
+                issue()
+        assert st["issued"] <= u + 2   # all issued copies were waited on
+
+
+SHAPES = [(24, 24, 24), (16, 16, 16), (16, 16, 32), (12, 12, 8), (8, 8, 8), (4, 4, 4),
+          (3, 5, 2), (6, 4, 7), (24, 24, 16), (32, 32, 16), (2, 2, 4), (5, 3, 8), (6, 6, 5)]
+
+
+@pytest.mark.parametrize("L,Lt,Ls", SHAPES)
+def test_row_schedule(L, Lt, Ls):
+    nrows = 2 * Lt * L
+    for elem in (16, 8, 4):
+        if (L * Ls * elem) % 16:
+            continue
+        for nb in sorted({1, 2, 3, 7, 148, 296, max(1, nrows // 3), nrows}):
+            if 1 <= nb <= nrows:
+                simulate(L, Lt, Ls, nb, elem)
