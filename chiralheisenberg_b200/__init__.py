@@ -64,6 +64,8 @@ EXPORTS = (
     "chdwf_prog_sums", "chdwf_prog_reset_sums", "chdwf_prog_averages", "chdwf_prog_take_cg_caps",
     "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
+    "chdwf_ext_set_remez", "chdwf_ext_select_pf", "chdwf_ext_heatbath_dev", "chdwf_ext_action",
+    "chdwf_ext_force", "chdwf_ext_bosonic", "chdwf_prog_set_ext",
 )
 
 _lib = None
@@ -204,6 +206,13 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_format_list.argtypes = [C.c_char_p, I, C.c_char_p, P]
     L.chdwf_format_edit.argtypes = [C.c_char_p, I, C.c_char, I, I, D]
     L.chdwf_run_dir.argtypes = [C.c_char_p, I, I, I, I]
+    L.chdwf_ext_set_remez.argtypes = [P, I, P, P, I]
+    L.chdwf_ext_select_pf.argtypes = [P, I]
+    L.chdwf_ext_heatbath_dev.argtypes = [P, P, F, F, I, PI]
+    L.chdwf_ext_action.argtypes = [P, F, F, I, C.POINTER(D), PI]
+    L.chdwf_ext_force.argtypes = [P, F, F, I, I, PI]
+    L.chdwf_ext_bosonic.argtypes = [P, P]
+    L.chdwf_prog_set_ext.argtypes = [P, I, I, I, F]
     _lib = L
     return L
 
@@ -456,6 +465,26 @@ class Program:
         heatbath/hamilton solves (accept): "f64" (drop-in) or "f32"."""
         code = {"f64": 0, "f32": 1}
         self._check(self.lib.chdwf_set_precision(self.context, code[md], code[accept]))
+
+    def set_ext(self, npf, nsteps, hb, act, integrator="omelyan",
+                lam=0.1931833275037836):
+        """The multi-pseudofermion variant (include/chdwf_program.h,
+        chdwf_prog_set_ext): npf fields, nsteps integrator steps of dt.
+        hb, act: (num[0..n], den[0..n-1]) of the heatbath function
+        x^(1/(4 npf)) and of the action/force function x^(-1/(2 npf)),
+        e.g. from chiralheisenberg_b200.remez.  npf=0 returns to the
+        reference's sweep."""
+        ctx = self.context
+        if npf > 0:
+            keep = []
+            for which, (num, den) in ((0, hb), (1, act)):
+                num = np.ascontiguousarray(num, dtype=np.float64)
+                den = np.ascontiguousarray(den, dtype=np.float64)
+                keep.append((num, den))
+                self._check(self.lib.chdwf_ext_set_remez(ctx, which, _ptr(num), _ptr(den),
+                                                         len(den)))
+        code = {"leapfrog": 0, "omelyan": 1}[integrator]
+        self._check(self.lib.chdwf_prog_set_ext(self.h, npf, nsteps, code, lam))
 
     def timing_read(self):
         """Per solver-kernel class: (ms, timed launches, launches, bytes)."""

@@ -50,7 +50,9 @@ Ctx::~Ctx() {
     if (red) cudaFree(red);
     if (chit) cudaFree(chit);
     if (pp) cudaFree(pp);
-    if (phi) cudaFree(phi);
+    if (phi_slot[0] == nullptr && phi) phi_slot[0] = phi;   // field 0 is phi
+    for (int i = 0; i < kMaxPf; i++)
+        if (phi_slot[i]) cudaFree(phi_slot[i]);
     if (gauss) cudaFree(gauss);
     if (walls) cudaFree(walls);
     if (stream) cudaStreamDestroy(stream);

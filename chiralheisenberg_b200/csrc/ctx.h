@@ -41,6 +41,13 @@ struct Ctx {
     float* gauss = nullptr;             // staging of the heatbath Gaussians
     double2* walls = nullptr;           // propagator wall slices
     RemezSet rz2, rz4, rz2g;
+    // multi-pseudofermion variant (ext.cu): fields 1.. beyond phi, and its
+    // two rational functions (heatbath: x^(1/(4 npf)); action and force:
+    // x^(-1/(2 npf)))
+    static constexpr int kMaxPf = 4;
+    double2* phi_slot[kMaxPf] = {nullptr, nullptr, nullptr, nullptr};
+    int pf = 0;                         // the field phi points to
+    RemezSet rz_hb, rz_act;
     int prec_md = 0, prec_accept = 0;   // vector precision of the resident solves
     BatchWork* batch = nullptr;         // workspace of chdwf_congrad_batch
 

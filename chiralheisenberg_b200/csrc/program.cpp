@@ -54,6 +54,9 @@ struct chdwf_prog {
     float dt = 0.1f, beta = 0.5f, am3 = 1.0f, am = 0.0f, hpin = 0.0f;
     int imass = 1, iterl = 1, iprint = 5, measure = 1, isweep = 0;
     float rescga = 0.000000001f, rescgg = 0.000001f, rescgm = 0.000000001f;   // :32-33
+    // multi-pseudofermion variant (chdwf_prog_set_ext): npf > 0 selects it
+    int ext_npf = 0, ext_nsteps = 10, ext_integrator = 1;
+    float ext_lambda = 0.1931833275037836f;
     chdwf::Rng rng;
     bool have_next = false;
     std::future<Draws> next;
@@ -67,6 +70,11 @@ struct chdwf_prog {
     std::vector<StageSlot> pool;
     std::vector<int> free_slots;
 
+    // heatbath Gaussians of one trajectory: 2*4*kthird gauss0 calls of
+    // (kvol,2) per pseudofermion field
+    size_t gauss_floats() const {
+        return 16 * (size_t)kvol * Ls * (size_t)(ext_npf > 0 ? ext_npf : 1);
+    }
     int take_slot() {
         if (!free_slots.empty()) {
             const int k = free_slots.back();
@@ -74,7 +82,7 @@ struct chdwf_prog {
             return k;
         }
         StageSlot sl;
-        if (cudaMalloc(&sl.gauss_dev, sizeof(float) * 16 * (size_t)kvol * Ls) ||
+        if (cudaMalloc(&sl.gauss_dev, sizeof(float) * gauss_floats()) ||
             cudaMalloc(&sl.pp_dev, sizeof(float) * 3 * (size_t)kvol)) {
             cudaFree(sl.gauss_dev);
             cudaGetLastError();
@@ -107,6 +115,7 @@ struct chdwf_prog {
 
     // All random numbers of the next trajectory, in the reference's order.
     Draws draw(int sweep_index) {
+        if (ext_npf > 0) return draw_ext();
         Draws d;
         const int64_t kv = kvol;
         d.gauss.resize(16 * (size_t)kv * Ls);
@@ -126,6 +135,29 @@ struct chdwf_prog {
         d.x = rng.rano_yrun();                                                              // :329
         d.measured = measure && (sweep_index / iprint) * iprint == sweep_index;
         if (d.measured) d.yferm = rng.rano_yran();                                          // :929
+        d.state_after = rng.state();
+        return d;
+    }
+
+    // The multi-pseudofermion variant's random numbers: the heatbath
+    // Gaussians of each field in turn (the reference's gauss0 order within a
+    // field), the momenta as the reference draws them, and the Metropolis
+    // draw; the trajectory has a fixed number of steps, so there are no
+    // trajectory-end draws.  No measurement.
+    Draws draw_ext() {
+        Draws d;
+        const int64_t kv = kvol;
+        d.gauss.resize(gauss_floats());
+        for (int c = 0; c < 8 * Ls * ext_npf; c++)
+            rng.gauss0(kv, d.gauss.data() + (size_t)c * 2 * kv);
+        std::vector<float> ps(2 * kv);
+        d.pp.resize(3 * kv);
+        rng.gaussp(kv, ps.data());
+        std::memcpy(d.pp.data(), ps.data(), sizeof(float) * 2 * kv);
+        rng.gaussp(kv, ps.data());
+        std::memcpy(d.pp.data() + 2 * kv, ps.data(), sizeof(float) * kv);
+        d.x = rng.rano_yrun();
+        d.measured = false;
         d.state_after = rng.state();
         return d;
     }
@@ -352,10 +384,176 @@ int chdwf_prog_correlators(chdwf_prog* p, float* cferm) {
     return CHDWF_OK;
 }
 
+int chdwf_prog_set_ext(chdwf_prog* p, int npf, int nsteps, int integrator, float lambda) {
+    if (!p || npf < 0 || npf > 4 || nsteps < 1 || (integrator != 0 && integrator != 1))
+        return CHDWF_BAD_ARG;
+    p->discard_pending();
+    p->release_pool();                   // staged buffers are sized by npf
+    p->ext_npf = npf;
+    p->ext_nsteps = nsteps;
+    p->ext_integrator = integrator;
+    p->ext_lambda = lambda;
+    if (npf == 0) return chdwf_ext_select_pf(p->ctx, 0);
+    return CHDWF_OK;
+}
+
+namespace {
+
+// One trajectory of the multi-pseudofermion variant: heatbath of every
+// field, H0, a fixed number of integrator steps, H1 and the Metropolis test
+// (the reference's sequence, rhmc/cheisdwf.f:213-345, with npf fields and
+// the chosen integrator).  Omelyan's second-order minimum-norm integrator
+// (I.P. Omelyan, I.M. Mryglod, R. Folk, Comput. Phys. Commun. 151 (2003)
+// 272) per step: p -= l dt F; chi += dt/2 p; p -= (1-2l) dt F;
+// chi += dt/2 p; p -= l dt F, with the last force of a step shared with
+// the first of the next (2 nsteps + 1 force evaluations).  Leapfrog: the
+// reference's scheme with a fixed step count.
+int ext_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
+    chdwf_ctx* c = p->ctx;
+    const int kvol = p->kvol, npf = p->ext_npf;
+    Staged stg;
+    if (!p->staged.empty()) {
+        stg = std::move(p->staged.front());
+        p->staged.pop_front();
+    } else {
+        stg.d = p->have_next ? p->next.get() : p->draw_ext();
+        p->have_next = false;
+    }
+    Draws& d = stg.d;
+    p->last_state = d.state_after;
+    if (stg.slot < 0) {                  // draws not yet in HBM: copy them now
+        stg.slot = p->take_slot();
+        if (stg.slot < 0) return CHDWF_CUDA_ERROR;
+        const StageSlot& s0 = p->pool[stg.slot];
+        cudaMemcpy(s0.gauss_dev, d.gauss.data(), sizeof(float) * d.gauss.size(),
+                   cudaMemcpyHostToDevice);
+        cudaMemcpy(s0.pp_dev, d.pp.data(), sizeof(float) * d.pp.size(), cudaMemcpyHostToDevice);
+    }
+    struct Back {
+        chdwf_prog* p;
+        int slot;
+        ~Back() { if (slot >= 0) p->free_slots.push_back(slot); }
+    } back{p, stg.slot};
+    const StageSlot& sl = p->pool[stg.slot];
+    int rc;
+#define CK(x) do { rc = (x); if (rc != CHDWF_OK) { p->err = chdwf_last_error(c); return rc; } } while (0)
+    chdwf_run_sums& A = p->sums;
+    CK(chdwf_traj_begin(c));
+    const size_t per_pf = 16 * (size_t)kvol * p->Ls;
+    for (int i = 0; i < npf; i++) {
+        int it = 0;
+        CK(chdwf_ext_select_pf(c, i));
+        CK(chdwf_ext_heatbath_dev(c, sl.gauss_dev + per_pf * i, p->rescga, p->hpin, p->imass, &it));
+        rec->it_pf += it;
+    }
+    A.ancgpf = A.ancgpf + (float)rec->it_pf;
+    if (p->staged.empty()) p->prefetch(p->isweep + 1);
+    CK(chdwf_traj_set_momenta_dev(c, sl.pp_dev));
+    auto hamiltonian = [&](double* H, double* S, double* hg, double* hp, int* its) -> int {
+        double b[2];
+        int r2 = chdwf_ext_bosonic(c, b);
+        if (r2 != CHDWF_OK) return r2;
+        double hf = 0.0;
+        for (int i = 0; i < npf; i++) {
+            double h = 0.0;
+            int it = 0;
+            if ((r2 = chdwf_ext_select_pf(c, i)) != CHDWF_OK) return r2;
+            if ((r2 = chdwf_ext_action(c, p->rescga, p->hpin, p->imass, &h, &it)) != CHDWF_OK)
+                return r2;
+            hf += h;
+            *its += it;
+        }
+        *hp = b[0];
+        *hg = b[1];
+        *H = b[1] + b[0] + hf;
+        *S = b[1] + hf;
+        return CHDWF_OK;
+    };
+    double hg = 0.0, hp = 0.0;
+    CK(hamiltonian(&rec->H0, &rec->S0, &hg, &hp, &rec->it_h0));
+    A.ancgh = A.ancgh + (float)rec->it_h0;
+    if (p->isweep == 1) A.gaction = (float)(hg / (double)kvol);
+    rec->action = (float)(rec->S0 / (double)kvol);
+    rec->paction = (float)(hp / (double)kvol);
+    auto force = [&]() -> int {
+        for (int i = 0; i < npf; i++) {
+            int it = 0, r2;
+            if ((r2 = chdwf_ext_select_pf(c, i)) != CHDWF_OK) return r2;
+            if ((r2 = chdwf_ext_force(c, p->rescgg, p->hpin, p->imass, i == 0, &it)) != CHDWF_OK)
+                return r2;
+            rec->it_force += it;
+        }
+        rec->nforce++;
+        return CHDWF_OK;
+    };
+    const float dt = p->dt;
+    const int ns = p->ext_nsteps;
+    if (p->ext_integrator == 1) {
+        const float l = p->ext_lambda;
+        const float d_l = l * dt, d_m = (1.0f - 2.0f * l) * dt, d_2l = 2.0f * l * dt;
+        const float half = 0.5f * dt;
+        CK(force());
+        CK(chdwf_traj_update_momenta(c, d_l));
+        for (int k = 1; k <= ns; k++) {
+            CK(chdwf_traj_update_chi(c, half));
+            CK(force());
+            CK(chdwf_traj_update_momenta(c, d_m));
+            CK(chdwf_traj_update_chi(c, half));
+            CK(force());
+            CK(chdwf_traj_update_momenta(c, k < ns ? d_2l : d_l));
+        }
+    } else {
+        CK(force());
+        CK(chdwf_traj_update_momenta(c, 0.5f * dt));
+        for (int k = 1; k <= ns; k++) {
+            CK(chdwf_traj_update_chi(c, dt));
+            CK(force());
+            CK(chdwf_traj_update_momenta(c, k < ns ? dt : 0.5f * dt));
+        }
+    }
+    rec->nsteps = ns;
+    rec->ended = 1;
+    A.itot = A.itot + ns;
+    A.ancgf = A.ancgf + (float)rec->it_force;
+    CK(hamiltonian(&rec->H1, &rec->S1, &rec->hg, &rec->hp, &rec->it_h1));
+    A.ancgh = A.ancgh + (float)rec->it_h1;
+    rec->dH = rec->H0 - rec->H1;
+    rec->dS = rec->S0 - rec->S1;
+    rec->y = (float)std::exp(rec->dH);
+    A.yav = A.yav + rec->y;
+    A.yyav = A.yyav + rec->y * rec->y;
+    rec->x = d.x;
+    if (rec->x < rec->y) {
+        rec->accepted = 1;
+        CK(chdwf_traj_accept(c));
+        A.naccp = A.naccp + 1;
+        rec->action = (float)(rec->S1 / (double)kvol);
+        A.gaction = (float)(rec->hg / (double)kvol);
+        rec->paction = (float)(rec->hp / (double)kvol);
+    }
+    rec->gaction = A.gaction;
+    A.actiona = A.actiona + rec->action;
+    std::vector<float> pp(3 * (size_t)kvol);
+    CK(chdwf_traj_get_momenta(c, pp.data()));
+    float vel2 = 0.0f;
+    for (size_t i = 0; i < pp.size(); i++) vel2 = vel2 + pp[i] * pp[i];
+    rec->vel2 = vel2 / (float)kvol;
+    A.vel2a = A.vel2a + rec->vel2;
+    A.nsweep = A.nsweep + 1;
+#undef CK
+    return CHDWF_OK;
+}
+
+}  // namespace
+
 // One sweep of the main loop (rhmc/cheisdwf.f:207-399).
 int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec) {
     if (!p || !rec) return CHDWF_BAD_ARG;
     std::memset(rec, 0, sizeof(*rec));
+    if (p->ext_npf > 0) {
+        p->isweep++;
+        return ext_sweep(p, rec);
+    }
     chdwf_ctx* c = p->ctx;
     const int kvol = p->kvol;
     p->isweep++;

@@ -99,6 +99,16 @@ __global__ void k_extract_slice(const double2* __restrict__ xi, Geom g, int s, i
 
 static unsigned nblk(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
 
+// launchers shared with the multi-pseudofermion blocks (ext.cu)
+void launch_build_source(double2* R, const float* ps, const Geom& g, cudaStream_t st) {
+    k_build_source<<<nblk(8 * (int64_t)g.Ls * g.kvol), kThreads, 0, st>>>(R, ps, g);
+    count_launches(1);
+}
+void launch_hamilton_bos(const float* pp, const double* chi, int n, double* out, cudaStream_t st) {
+    k_hamilton_bos<<<1, kThreads, 0, st>>>(pp, chi, n, out);
+    count_launches(1);
+}
+
 cudaError_t Ctx::ensure_traj() {
     if (chit) return cudaSuccess;
     cudaError_t e;

@@ -245,6 +245,31 @@ int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, flo
 int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idirac, float res,
                            float am, float hpin, int imass, double* slice, int* itercg);
 
+/* ---- multi-pseudofermion variant (no reference counterpart) ---------------
+ * The reference samples det(M^dag M)^(1/2) with one pseudofermion
+ * (rhmc/cheisdwf.f:218-345).  These blocks split it over npf fields, each
+ * carrying det(M^dag M)^(1/(2 npf)): heatbath Phi_i = r_hb(M^dag M) R_i with
+ * r_hb ~ x^(1/(4 npf)); action Re Phi_i^dag r_act(M^dag M) Phi_i with
+ * r_act ~ x^(-1/(2 npf)); force from one multi-shift solve over r_act's poles
+ * (the per-pole derivs term of rhmc/cheisdwf.f:729-742).  Rational sets in
+ * the reference's partial-fraction form: num[0..n] = a0, a_k; den = sigma_k. */
+/* which = 0: r_hb, 1: r_act */
+int chdwf_ext_set_remez(chdwf_ctx* ctx, int which, const double* num, const double* den, int n);
+/* make field k (0..3) the one the resident blocks act on (field 0 is the
+ * reference's Phi) */
+int chdwf_ext_select_pf(chdwf_ctx* ctx, int k);
+/* Phi_k = r_hb(M^dag M) R, R from 2*4*kthird gauss0 outputs on the device
+ * (the layout of chdwf_traj_heatbath's ps), on chit */
+int chdwf_ext_heatbath_dev(chdwf_ctx* ctx, const void* ps_dev, float res, float hpin, int imass,
+                           int* itercg);
+/* hf = Re Phi_k^dag r_act(M^dag M) Phi_k on chit */
+int chdwf_ext_action(chdwf_ctx* ctx, float res, float hpin, int imass, double* hf, int* itercg);
+/* init = 1: dSdchi = 2 beta chit first (rhmc/cheisdwf.f:494-498); then
+ * dSdchi += d/dchi (Phi_k^dag r_act(M^dag M) Phi_k), REAL*4, resident */
+int chdwf_ext_force(chdwf_ctx* ctx, float res, float hpin, int imass, int init, int* itercg);
+/* hp_hg[0] = 0.5 sum pp^2, hp_hg[1] = beta sum chit^2 (rhmc/cheisdwf.f:546-559) */
+int chdwf_ext_bosonic(chdwf_ctx* ctx, double* hp_hg);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,17 @@ int chdwf_prog_set_measure(chdwf_prog* p, int iprint, int measure);
 int chdwf_prog_set_residuals(chdwf_prog* p, float rescga, float rescgg, float rescgm);
 /* one sweep (rhmc/cheisdwf.f:207-399) */
 int chdwf_prog_sweep(chdwf_prog* p, chdwf_sweep_record* rec);
+/* The multi-pseudofermion variant (no reference counterpart; the reference
+ * has one pseudofermion and a leapfrog of random length, rhmc/cheisdwf.f:
+ * 218-345).  npf > 0 makes every following sweep one trajectory with npf
+ * pseudofermion fields (rational sets by chdwf_ext_set_remez on the
+ * program's context), nsteps integrator steps of size dt, integrator 1 =
+ * Omelyan's second-order minimum-norm scheme with parameter lambda
+ * (0.1931833275037836 is its optimum), 0 = leapfrog; the same H0/H1,
+ * Metropolis draw and record.  Its random stream: npf blocks of 2*4*kthird
+ * gauss0 calls, the momenta, the Metropolis draw.  No measurement.
+ * npf = 0 returns to the reference's sweep. */
+int chdwf_prog_set_ext(chdwf_prog* p, int npf, int nsteps, int integrator, float lambda);
 /* Draw the random inputs (heatbath Gaussians, momenta, trajectory-end and
  * Metropolis draws) of the next ntraj sweeps now and place the field-sized
  * ones in HBM; those sweeps then start with every input resident.  The
