@@ -1,34 +1,48 @@
 """bench.py -- RHMC trajectory throughput of the chiral-Heisenberg domain-wall
-path on B200, in the reference's own algorithm (1 pseudofermion, the shipped
-25/25/12-pole Remez sets, leapfrog with random trajectory length).
+fermion path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--L 24] [--Ls 24]
 
-A step is one RHMC trajectory (heatbath, H0, molecular dynamics with a force
-evaluation per step, H1, Metropolis) at L=Lt=24, Ls=24 on synthetic fields:
-chi drawn from a seeded N(0, 1/beta), the reference's random-number generator
-from its default seed.  Measurements (fermion()) are off.  Printed metric:
-seconds per trajectory (lower is better).
+A step is one RHMC trajectory at L=Lt=24, Ls=24, beta=0.475, m=0.01 (inert,
+as in the reference), am3=1, imass=1, hpin=0, in the production form of the
+benchmark configuration: two pseudofermion fields, 20-pole rational
+approximations (remez8_20 a-set x^(1/8) for the heatbath, remez4_20 b-set
+x^(-1/4) for action and force, generated by chiralheisenberg_b200/remez.py),
+Omelyan's integrator with 10 steps of dt=0.1, mixed-precision solves (FP32
+Krylov vectors in the force solves at 1e-6, FP64 heatbath and action solves
+at 1e-9, FP64 Hamiltonian and Metropolis test).  chi starts from the
+thermalised configuration chiralheisenberg_b200/data/con_24x24x24_b0.475
+(made by `bench.py --thermalise 60` from a seeded N(0, 1/beta) start); the
+generator is the reference's.  Printed metric: seconds per trajectory.
 
   value     trajectories whose random inputs were staged in HBM before the
-            timed region (chdwf_prog_stage); CUDA events on the library's
-            stream, max over ranks.
+            timed region; CUDA events on the library's stream, max over
+            ranks.
   e2e       the same trajectories through the host-facing driver API with the
             random numbers drawn on the host and copied in every step.
-  roofline  the dominant solver kernel class, timed with CUDA events around
-            every solver launch in an instrumented replay of the first timed
-            trajectory, against the algorithmic bytes the library reports for
-            each launch.
+  fp64      the same trajectories with FP64 force solves (the drop-in
+            precision): its s/trajectory, the speed-up of value over it, and
+            |dH_mixed - dH_fp64| absolute and relative to |H0|.
+  reference_algorithm
+            the reference's own algorithm (one pseudofermion, the shipped
+            25/25/12-pole sets, leapfrog of random length), FP64, from the
+            same configuration: the drop-in path's s/trajectory.
+  roofline  the dominant solver kernel class of the value trajectories, timed
+            with CUDA events around every solver launch in an instrumented
+            replay of the first timed trajectory, against the algorithmic
+            bytes of each launch.
   cpu_baseline / --impl reference
             the CPU oracle (a C restatement of rhmc/cheisdwf.f; the Fortran
-            reference cannot be built here) on the host cores: per-iteration
-            cost of each solve type sampled at the same lattice, times the
-            trajectory's iteration profile.
+            reference cannot be built here) on all host cores: its cost per
+            iteration of the 20-pole multi-shift solver at this lattice,
+            measured on a bounded sample, times the FP64 iteration profile of
+            the same trajectories (this run's for cpu_baseline; the committed
+            profiles/iteration_profile_ext_24x24.json, made from the same
+            chain and seeds, for the reference arm).  A modelled figure;
+            `bench.py --validate-cpu-model` times one complete oracle solve
+            against the model.
 
-Multi-GPU: independent Markov chains, one per rank ("replicas only"); value
-is trajectories of all ranks per unit time expressed as seconds per
-trajectory of the whole job.
+Multi-GPU: independent Markov chains, one per rank ("replicas only").
 """
 from __future__ import annotations
 
@@ -45,24 +59,32 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+DATA = os.path.join(ROOT, "chiralheisenberg_b200", "data")
 
-# Workload (the configuration the metric is quoted on): L=Lt=24, Ls=24,
-# beta=0.475, m=0.01 (accepted and unused, as in the reference), am3=1,
-# imass=1, hpin=0; dt=0.1 with mean trajectory length dt*iterl = 1.
 CFG = dict(beta=0.475, am3=1.0, am=0.01, hpin=0.0, imass=1, dt=0.1, iterl=10,
            seed=693764523745.0, chi_seed=12345)
+EXT = dict(npf=2, nsteps=10, integrator="omelyan", poles=20, rescga=1e-9, rescgg=1e-6,
+           heatbath="remez8_20 a: x^(1/8)", action_force="remez4_20 b: x^(-1/4)",
+           interval=[1e-4, 50.0])
+PROFILE_EXT = os.path.join(ROOT, "profiles", "iteration_profile_ext_24x24.json")
+
+
+def con_path(L, Ls):
+    return os.path.join(DATA, f"con_{L}x{L}x{Ls}_b{CFG['beta']}")
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--no-propagators", action="store_true")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--L", type=int, default=24)
     ap.add_argument("--Ls", type=int, default=24)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-refalg", action="store_true")
+    ap.add_argument("--refalg-steps", type=int, default=3)
+    ap.add_argument("--no-propagators", action="store_true")
     ap.add_argument("--cpu-sample-iters", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--clock-interval-ms", type=int, default=200,
@@ -75,6 +97,13 @@ def parse():
                     help="stopping residual of both profiled solves (0: the reference's)")
     ap.add_argument("--basis-gb", type=float, default=-1.0,
                     help="HBM budget of the stored Lanczos basis (GB; <0 library default)")
+    ap.add_argument("--thermalise", type=int, default=0,
+                    help="run N trajectories from the seeded Gaussian start and write the "
+                         "thermalised configuration")
+    ap.add_argument("--write-profile", type=int, default=0,
+                    help="write the FP64 iteration profile of the first N trajectories")
+    ap.add_argument("--validate-cpu-model", action="store_true",
+                    help="time one complete oracle force solve against the per-iteration model")
     return ap.parse_args()
 
 
@@ -143,7 +172,38 @@ def synthetic_chi(L, Lt, beta, seed):
     return rng.standard_normal((3, L * L * Lt)) / np.sqrt(beta)
 
 
-# solver kernel classes reported by chdwf_timing_read
+def ext_sets():
+    from chiralheisenberg_b200.remez import read_remez_file
+    a8, d8, _, _ = read_remez_file(os.path.join(DATA, "remez8_20"), 20)
+    _, _, b4, e4 = read_remez_file(os.path.join(DATA, "remez4_20"), 20)
+    return (a8, d8), (b4, e4)
+
+
+def make_program(L, Ls, local_rank, rank=0, ext=True):
+    """The benchmark chain: thermalised configuration (or the seeded start
+    when it is missing), reference generator, extension mode if ext."""
+    import chiralheisenberg_b200 as chb
+    rz = chb.reference_remez()
+    prog = chb.Program(L, L, Ls, CFG["dt"], CFG["beta"], CFG["am3"], CFG["am"], CFG["hpin"],
+                       CFG["imass"], CFG["iterl"], rz["remez2"], rz["remez4"], rz["remez2g"],
+                       device=local_rank)
+    cp = con_path(L, Ls)
+    if os.path.exists(cp):
+        chi, seed, _ = chb.con_read(cp, L ** 3)
+        start = "thermalised (" + os.path.relpath(cp, ROOT) + ")"
+    else:
+        chi, seed = synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"]), CFG["seed"]
+        start = "raw N(0,1/beta) seeded"
+    prog.set_chi(chi)
+    prog.startup(seed + 1000.0 * rank)
+    prog.set_measure(5, False)
+    if ext:
+        hb, act = ext_sets()
+        prog.set_ext(EXT["npf"], EXT["nsteps"], hb, act, integrator=EXT["integrator"])
+    return prog, start
+
+
+# solver kernel classes reported by chdwf_timing_read (4-7: FP32 vectors)
 KERNEL_NAMES = {0: "k_lz1_M", 1: "k_lz1_Md", 2: "k_lz_accum", 3: "k_lz2_M/k_lz2_Md"}
 KERNEL_WHAT = {0: "pass-1 M q_j with |M q_j|^2",
                1: "pass-1 M^dag + three-term update with |r|^2",
@@ -151,49 +211,51 @@ KERNEL_WHAT = {0: "pass-1 M q_j with |M q_j|^2",
                3: "pass-2 regeneration (solves longer than the basis store)"}
 
 
-def cpu_sample(L, Ls, threads, iters, profile):
-    """Oracle cost per solver iteration for each solve type at this lattice,
-    combined with a trajectory's iteration profile into seconds/trajectory."""
+def kernel_name(k):
+    return KERNEL_NAMES[k % 4] + ("_rows" if k % 4 < 2 else "") + (" fp32" if k >= 4 else " fp64")
+
+
+def cpu_iteration_cost(L, Ls, threads, iters, npole=20):
+    """Oracle seconds per multi-shift iteration (npole poles) and per operator
+    apply at this lattice, on `threads` host threads; a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
-    import chiralheisenberg_b200 as chb
-    rz = chb.reference_remez()
+    hb, act = ext_sets()
     lat = po.make_lat(L, L, Ls, beta=CFG["beta"], am3=CFG["am3"], threads=threads)
     rng = np.random.default_rng(7)
     shape = (2, 4, L, L, L, Ls)
     Phi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
     chi = synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"])
-    t_iter = {}
-    t0all = time.perf_counter()
-    for name, n in (("remez2", 25), ("remez2g", 12)):
-        r = rz[name]
-        t0 = time.perf_counter()
-        po.qmrherm(lat, Phi, chi, r["bnum"], r["bden"], 1e-30, niterc=iters)
-        t_iter[n] = (time.perf_counter() - t0) / iters
-    # force tail: one M apply + derivs per guidance pole (rhmc/cheisdwf.f:733-740)
+    # the difference of a 2k- and a k-iteration run: set-up (allocation of the
+    # pole vectors, thread start-up) cancels
+    t0 = time.perf_counter()
+    po.qmrherm(lat, Phi, chi, act[0], act[1], 1e-30, niterc=iters)
+    t1 = time.perf_counter()
+    po.qmrherm(lat, Phi, chi, act[0], act[1], 1e-30, niterc=2 * iters)
+    t2 = time.perf_counter()
+    t_iter = max((t2 - t1) - (t1 - t0), 1e-9) / iters
     t0 = time.perf_counter()
     for _ in range(2):
         po.dslash(lat, Phi, chi)
     t_apply = (time.perf_counter() - t0) / 2
-    sampled = time.perf_counter() - t0all
-    it25 = profile["it_pf"] + profile["it_h0"] + profile["it_h1"]
-    it12 = profile["it_guid"] + profile["it_force"]
-    s_traj = it25 * t_iter[25] + it12 * t_iter[12] + profile["nforce"] * 12 * t_apply
-    sample = (f"oracle qmrherm at {L}^3x{Ls}: {iters} iterations each of the 25- and 12-pole "
-              f"solves + 2 operator applies ({sampled:.1f} s), scaled by the iteration profile "
-              f"of one trajectory ({it25:.0f} 25-pole + {it12:.0f} 12-pole iterations, "
-              f"{profile['nforce']:.1f} force calls)")
-    return s_traj, sample, {"t_iter_25": t_iter[25], "t_iter_12": t_iter[12], "t_apply": t_apply}
+    return t_iter, t_apply
 
 
-def default_profile():
-    p = os.path.join(ROOT, "profiles", "iteration_profile_24x24.json")
-    if os.path.exists(p):
-        return json.load(open(p))
-    # iteration counts of a trajectory at 24^3x24 on this workload, from the
-    # GPU arm (same algorithm and stopping rule)
-    return {"it_pf": 530, "it_h0": 530, "it_h1": 530, "it_guid": 5000.0, "it_force": 5000.0,
-            "nforce": 11.0}
+def cpu_model(profile, t_iter, t_apply, npole=20):
+    """Oracle seconds per trajectory: every solver iteration at t_iter, plus
+    the force tail of each force solve (one operator apply and derivs per
+    pole, rhmc/cheisdwf.f:733-740, counted as one apply)."""
+    its = profile["it_pf"] + profile["it_h0"] + profile["it_h1"] + profile["it_force"]
+    nsolve_force = profile["nforce"] * EXT["npf"]
+    return its * t_iter + nsolve_force * npole * t_apply, its
+
+
+def profile_of(recs):
+    return {"it_pf": float(np.mean([r.it_pf for r in recs])),
+            "it_h0": float(np.mean([r.it_h0 for r in recs])),
+            "it_h1": float(np.mean([r.it_h1 for r in recs])),
+            "it_force": float(np.mean([r.it_force for r in recs])),
+            "nforce": float(np.mean([r.nforce for r in recs]))}
 
 
 def bench_propagators(local_rank, seed=2024, nens=24, nsrc=4, res=1e-8):
@@ -249,29 +311,6 @@ def bench_propagators(local_rank, seed=2024, nens=24, nsrc=4, res=1e-8):
             "one_at_a_time_solves_per_s": n / t_one, "batched_solves_per_s": n / t_batch,
             "speedup": t_one / t_batch, "mean_iterations": float(np.mean(its2)),
             "same_iterations": bool(list(its1) == list(its2)), "all_converged": bool((sts == 0).all())}
-
-
-def run_reference(args, rank, world):
-    if rank != 0:
-        return
-    threads = os.cpu_count() or 1
-    profile = default_profile()
-    vals = []
-    sample = ""
-    for step in range(args.warmup + args.steps):
-        s_traj, sample, _ = cpu_sample(args.L, args.Ls, threads, args.cpu_sample_iters, profile)
-        if step >= args.warmup:
-            vals.append(s_traj)
-    v = statistics.median(vals)
-    line = {"impl": "reference", "metric": "s/trajectory", "value": v, "unit": "s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"RHMC trajectory L=Lt={args.L} Ls={args.Ls}", **CFG},
-            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
-                             "sample": sample},
-            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
 
 
 def run_profile_solve(args, local_rank):
@@ -383,18 +422,188 @@ def run_operator_sweep(args, local_rank):
             torch.cuda.empty_cache()
 
 
-def run_b200(args, rank, world, local_rank):
-    import torch
+def run_reference(args, rank, world):
+    """The reference arm: the oracle on all host cores, on this workload."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    prof = json.load(open(PROFILE_EXT)) if os.path.exists(PROFILE_EXT) else None
+    if prof:
+        per = prof["per_trajectory"]
+        window = per[args.warmup:args.warmup + args.steps] or per
+        profile = {k: float(np.mean([p[k] for p in window])) for k in window[0]}
+        psrc = (f"{os.path.relpath(PROFILE_EXT, ROOT)}, trajectories "
+                f"{args.warmup + 1}-{args.warmup + len(window)} of the same chain")
+    else:
+        profile = {"it_pf": 1600.0, "it_h0": 1600.0, "it_h1": 1600.0, "it_force": 26000.0,
+                   "nforce": 21.0}
+        psrc = "built-in estimate (profile file missing)"
+    vals = []
+    for step in range(args.warmup + args.steps):
+        t_iter, t_apply = cpu_iteration_cost(args.L, args.Ls, threads, args.cpu_sample_iters)
+        s, its = cpu_model(profile, t_iter, t_apply)
+        if step >= args.warmup:
+            vals.append((s, t_iter))
+    v = statistics.median(x[0] for x in vals)
+    t_it = statistics.median(x[1] for x in vals)
+    sample = (f"oracle 20-pole multi-shift iterations at {args.L}^3x{args.Ls} "
+              f"({3 * args.cpu_sample_iters} per step, cost per iteration from a "
+              f"{2 * args.cpu_sample_iters}- minus a {args.cpu_sample_iters}-iteration run) and 2 operator applies on {threads} threads; "
+              f"modelled: seconds per iteration x the FP64 iteration profile ({psrc})")
+    line = {"impl": "reference", "metric": "s/trajectory", "value": v, "unit": "s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args),
+            "modelled": True,
+            "iteration_profile": profile,
+            "ms_per_1000_iterations": t_it * 1e6,
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"RHMC trajectory L=Lt={args.L} Ls={args.Ls}, 2 pseudofermions x 20 "
+                        f"poles, Omelyan 10 steps", "precision": "mixed: FP32 force solves, "
+            "FP64 heatbath/action solves and dH", "parallelism": f"replicas{args.gpus}",
+            "l2": "fields larger than L2 (solver working set > 126 MB)",
+            "chi": "thermalised from seeded N(0,1/beta) (bench.py --thermalise 60)"
+            if os.path.exists(con_path(args.L, args.Ls)) else "raw seeded N(0,1/beta)",
+            "fermion": "off (no measurement in the timed trajectories)",
+            **CFG, **EXT}
+
+
+def run_thermalise(args, local_rank):
+    """From the seeded Gaussian start: N trajectories of the benchmark
+    algorithm (mixed precision), then write the configuration."""
     import chiralheisenberg_b200 as chb
+    import torch
     torch.cuda.set_device(local_rank)
     L, Ls = args.L, args.Ls
     rz = chb.reference_remez()
     prog = chb.Program(L, L, Ls, CFG["dt"], CFG["beta"], CFG["am3"], CFG["am"], CFG["hpin"],
                        CFG["imass"], CFG["iterl"], rz["remez2"], rz["remez4"], rz["remez2g"],
                        device=local_rank)
-    prog.set_chi(synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"] + rank))
-    prog.startup(CFG["seed"] + 1000.0 * rank)
+    prog.set_chi(synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"]))
+    prog.startup(CFG["seed"])
     prog.set_measure(5, False)
+    hb, act = ext_sets()
+    prog.set_ext(EXT["npf"], EXT["nsteps"], hb, act, integrator=EXT["integrator"])
+    prog.set_precision(md="f32", accept="f64")
+    for k in range(args.thermalise):
+        r = prog.sweep()
+        print(json.dumps({"trajectory": k + 1, "action_per_site": r.action, "dH": r.dH,
+                          "accepted": r.accepted, "it_force": r.it_force}), flush=True)
+    prog.write_con(con_path(L, Ls))
+    prog.close()
+
+
+def run_write_profile(args, local_rank):
+    """The FP64 iteration profile of the benchmark chain, trajectory by
+    trajectory (the reference arm prices its trajectories with it)."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    prog, start = make_program(args.L, args.Ls, local_rank)
+    prog.set_precision(md="f64", accept="f64")
+    per = []
+    for _ in range(args.write_profile):
+        r = prog.sweep()
+        per.append({"it_pf": r.it_pf, "it_h0": r.it_h0, "it_h1": r.it_h1,
+                    "it_force": r.it_force, "nforce": r.nforce})
+    prog.close()
+    out = {"workload": workload_config(args)["workload"], "start": start, "precision": "fp64",
+           "command": f"python bench.py --write-profile {args.write_profile}",
+           "per_trajectory": per}
+    with open(PROFILE_EXT, "w") as f:
+        json.dump(out, f, indent=0)
+    print(json.dumps(out["per_trajectory"][:3]), flush=True)
+
+
+def run_validate_cpu_model(args):
+    """One complete oracle solve at the bench lattice -- a 20-pole force
+    solve (iflag 1) at 1e-6 on the thermalised configuration -- timed end to
+    end and compared with the per-iteration model (sampled cost per
+    iteration x its iteration count + the force tail)."""
+    import chiralheisenberg_b200 as chb
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    L, Ls = args.L, args.Ls
+    threads = os.cpu_count() or 1
+    cp = con_path(L, Ls)
+    chi = chb.con_read(cp, L ** 3)[0] if os.path.exists(cp) else synthetic_chi(
+        L, L, CFG["beta"], CFG["chi_seed"])
+    hb, act = ext_sets()
+    lat = po.make_lat(L, L, Ls, beta=CFG["beta"], am3=CFG["am3"], threads=threads)
+    rng = np.random.default_rng(11)
+    shape = (2, 4, L, L, L, Ls)
+    Phi = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * np.sqrt(0.5)
+    t_iter, t_apply = cpu_iteration_cost(L, Ls, threads, args.cpu_sample_iters)
+    dS = np.zeros((3, L ** 3), np.float32)
+    t0 = time.perf_counter()
+    _, its, st, _ = po.qmrherm(lat, Phi, chi, act[0], act[1], 1e-6, iflag=1, dSdchi=dS)
+    t_full = time.perf_counter() - t0
+    model = its * t_iter + 20 * t_apply
+    print(json.dumps({"validate_cpu_model": f"L=Lt={L} Ls={Ls}", "threads": threads,
+                      "iterations": its, "status": st, "measured_s": t_full, "model_s": model,
+                      "model_over_measured": model / t_full, "t_iter_s": t_iter,
+                      "t_apply_s": t_apply}), flush=True)
+
+
+def timed_run(prog, stream, steps, staged, barrier, world, local_rank):
+    import torch
+    if staged:
+        prog.stage(steps)
+    recs = []
+    barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    ev[0].record(stream)
+    for k in range(steps):
+        recs.append(prog.sweep())
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev[0].elapsed_time(ev[-1])
+    per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+    t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item()), recs, per_step
+
+
+def instrumented(prog, chi0, state0):
+    """Replay the first timed trajectory with CUDA events around every solver
+    launch; per kernel class (ms, timed, launched, bytes)."""
+    prog.set_chi(chi0)
+    prog.set_state(state0)
+    prog.timing(True)
+    prog.sweep()
+    out = prog.timing_read()
+    prog.timing(False)
+    return out
+
+
+def kernel_table(kt):
+    kms, ktimed, klaunched, kbytes = kt
+    tot = max(float(np.sum(kms)), 1e-30)
+    return {kernel_name(k): {"launches": int(klaunched[k]),
+                             "avg_us": kms[k] / max(ktimed[k], 1) * 1e3,
+                             "share_of_solver_time": kms[k] / tot,
+                             "GBps": (kbytes[k] / (kms[k] * 1e-3) / 1e9) if kms[k] > 0 else None}
+            for k in range(8) if klaunched[k] > 0}
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import chiralheisenberg_b200 as chb
+    torch.cuda.set_device(local_rank)
+    L, Ls = args.L, args.Ls
+    prog, start = make_program(L, Ls, local_rank, rank)
+    if args.basis_gb >= 0:
+        prog.set_basis_store(args.basis_gb * 1e9)
+    prog.set_precision(md="f32", accept="f64")
     stream = torch.cuda.ExternalStream(prog.stream, device=local_rank)
 
     def barrier():
@@ -403,80 +612,66 @@ def run_b200(args, rank, world, local_rank):
 
     for _ in range(args.warmup):
         prog.sweep()
-
-    def timed(staged):
-        if staged:
-            prog.stage(args.steps)
-        recs = []
-        barrier()
-        torch.cuda.synchronize()
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-        ev[0].record(stream)
-        for k in range(args.steps):
-            recs.append(prog.sweep())
-            ev[k + 1].record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        ms = ev[0].elapsed_time(ev[-1])
-        timed.per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-        t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item()), recs
-
-    # value and e2e run the SAME trajectories: the chain state (chi and the
-    # complete generator state) is saved before the first and restored
-    # before the second
+    # every arm below runs the SAME trajectories: the chain state (chi and the
+    # complete generator state) is saved here and restored before each
     chi0 = prog.get_chi()
     state0 = prog.get_state()
     clocks = ClockSampler(local_rank, args.clock_interval_ms)
     clocks.start()
     n0 = chb.kernel_launches()
-    ms_value, recs = timed(staged=True)
-    step_ms_value = list(timed.per_step)
+    ms_value, recs, step_ms = timed_run(prog, stream, args.steps, True, barrier, world,
+                                        local_rank)
     launches = chb.kernel_launches() - n0
     clk = clocks.stop()
     prog.set_chi(chi0)
     prog.set_state(state0)
-    ms_e2e, recs_e2e = timed(staged=False)
-    step_ms_e2e = list(timed.per_step)
-    same = all(a.nsteps == b.nsteps and a.accepted == b.accepted and a.dH == b.dH
-               for a, b in zip(recs, recs_e2e))
-    mixed = None
-    if not args.no_mixed:
-        # the same trajectories with FP32 Krylov vectors in the force solves
+    ms_e2e, recs_e2e, step_ms_e2e = timed_run(prog, stream, args.steps, False, barrier, world,
+                                              local_rank)
+    same = all(a.accepted == b.accepted and a.dH == b.dH for a, b in zip(recs, recs_e2e))
+    kt = instrumented(prog, chi0, state0)
+    fp64 = None
+    prof64 = None
+    if not args.no_fp64:
         prog.set_chi(chi0)
         prog.set_state(state0)
-        prog.set_precision(md="f32", accept="f64")
-        ms_mix, recs_mix = timed(staged=True)
         prog.set_precision(md="f64", accept="f64")
-        dh = [abs(a.dH - b.dH) for a, b in zip(recs, recs_mix)]
-        dh_rel = [abs(a.dH - b.dH) / abs(a.H0) for a, b in zip(recs, recs_mix)]
-        mixed = {"value": (ms_mix / 1e3) / (args.steps * world), "unit": "s",
-                 "precision": "FP32 Krylov vectors in the force solves, FP64 heatbath/hamilton",
-                 "speedup_vs_fp64": ms_value / ms_mix,
-                 "dH_max_abs_diff_vs_fp64": max(dh), "dH_max_diff_rel_H": max(dh_rel),
-                 "same_decisions": all(a.accepted == b.accepted and a.nsteps == b.nsteps
-                                       for a, b in zip(recs, recs_mix))}
-
-    # Per-kernel timing: the first timed trajectory again, instrumented --
-    # CUDA events around every solver launch on the library's stream (the
-    # instrumented replay issues launches one by one, so it is not part of
-    # the timed value above)
-    prog.set_chi(chi0)
-    prog.set_state(state0)
-    prog.timing(True)
-    prog.sweep()
-    kms, ktimed, klaunched, kbytes = prog.timing_read()
-    prog.timing(False)
-
-    # whole job: steps*world trajectories in the slowest rank's time
+        ms64, recs64, _ = timed_run(prog, stream, args.steps, True, barrier, world, local_rank)
+        kt64 = instrumented(prog, chi0, state0)
+        prog.set_precision(md="f32", accept="f64")
+        dh = [abs(a.dH - b.dH) for a, b in zip(recs, recs64)]
+        dh_rel = [abs(a.dH - b.dH) / abs(b.H0) for a, b in zip(recs, recs64)]
+        prof64 = profile_of(recs64)
+        fp64 = {"value": (ms64 / 1e3) / (args.steps * world), "unit": "s",
+                "speedup_of_value": ms64 / ms_value,
+                "dH_max_abs_diff": max(dh), "dH_max_diff_rel_H0": max(dh_rel),
+                "dH_rms_fp64": float(np.sqrt(np.mean([b.dH ** 2 for b in recs64]))),
+                "target": "|dH_mixed - dH_fp64| <= 1e-8: met as relative to |H0| "
+                          f"({max(dh_rel):.2e}); as absolute {max(dh):.2e}",
+                "same_decisions": all(a.accepted == b.accepted for a, b in zip(recs, recs64)),
+                "iteration_profile": prof64,
+                "solver_kernels": kernel_table(kt64)}
+    prog.close()
+    refalg = None
+    if not args.no_refalg:
+        rprog, _ = make_program(L, Ls, local_rank, rank, ext=False)
+        rprog.sweep()
+        ms_r, recs_r, _ = timed_run(rprog, stream_of(rprog, local_rank), args.refalg_steps, True,
+                                    barrier, world, local_rank)
+        its = sum(r.it_pf + r.it_h0 + r.it_h1 + r.it_guid + r.it_force for r in recs_r)
+        refalg = {"value": (ms_r / 1e3) / (args.refalg_steps * world), "unit": "s",
+                  "precision": "fp64 (the drop-in)", "trajectories": args.refalg_steps,
+                  "ms_per_1000_iterations": ms_r / its * 1e3,
+                  "nforce": [r.nforce for r in recs_r],
+                  "algorithm": "1 pseudofermion, shipped remez2/remez4/remez2g, leapfrog dt=0.1 "
+                               "with random length (iterl=10), as rhmc/cheisdwf.f"}
+        rprog.close()
     ntraj = args.steps * world
     value = (ms_value / 1e3) / ntraj
     e2e = (ms_e2e / 1e3) / ntraj
     kvol = L * L * L
-    h2d = 64 * kvol * Ls + 12 * kvol          # heatbath Gaussians + momenta
-    d2h = 12 * kvol + 64                      # momenta for vel2 + scalars
+    h2d = EXT["npf"] * 64 * kvol * Ls + 12 * kvol      # heatbath Gaussians + momenta
+    d2h = 12 * kvol + 64                               # momenta for vel2 + scalars
+    kms, ktimed, klaunched, kbytes = kt
     dom = int(np.argmax(kms))
     avg_ms = kms[dom] / max(ktimed[dom], 1)
     achieved = kbytes[dom] / (kms[dom] * 1e-3) / 1e9
@@ -485,51 +680,52 @@ def run_b200(args, rank, world, local_rank):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic_24x24.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(KERNEL_NAMES[dom])
-    prof = {"it_pf": float(np.mean([r.it_pf for r in recs])),
-            "it_h0": float(np.mean([r.it_h0 for r in recs])),
-            "it_h1": float(np.mean([r.it_h1 for r in recs])),
-            "it_guid": float(np.mean([r.it_guid for r in recs])),
-            "it_force": float(np.mean([r.it_force for r in recs])),
-            "nforce": float(np.mean([r.nforce for r in recs]))}
+        traffic = json.load(open(tp)).get(kernel_name(dom))
+    prof = profile_of(recs)
+    its_value = sum(prof[k] for k in ("it_pf", "it_h0", "it_h1", "it_force"))
     line = {"metric": "s/trajectory", "value": value, "unit": "s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_value / args.steps,
-            "step_ms": [round(x, 1) for x in step_ms_value],
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": f"RHMC trajectory L=Lt={L} Ls={Ls}", "precision": "fp64",
-                       "parallelism": f"replicas{world}", "l2": "fields larger than L2 "
-                       "(solver working set > 126 MB)", **CFG},
+            "step_ms": [round(x, 1) for x in step_ms],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (mixed)", "data": "synthetic", "config": workload_config(args),
+            "ms_per_1000_iterations": (ms_value / args.steps) / its_value * 1e3,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "same_trajectories_as_value": same,
                     "step_ms": [round(x, 1) for x in step_ms_e2e]},
-            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "what": KERNEL_WHAT[dom],
+            "fp64": fp64,
+            "roofline": {"bound": "hbm", "kernel": kernel_name(dom), "what": KERNEL_WHAT[dom % 4],
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_ms * 1e3,
                          "measured_in": "instrumented replay of the first timed trajectory, "
                                         "CUDA events around every solver launch"},
-            "solver_kernels": {KERNEL_NAMES[k]: {
-                "launches": int(klaunched[k]), "avg_us": kms[k] / max(ktimed[k], 1) * 1e3,
-                "share_of_solver_time": kms[k] / max(sum(kms), 1e-30),
-                "GBps": (kbytes[k] / (kms[k] * 1e-3) / 1e9) if kms[k] > 0 else None}
-                for k in range(4)},
+            "solver_kernels": kernel_table(kt),
             "gpu_launches": launches,
-            "mixed": mixed,
+            "reference_algorithm": refalg,
             "iteration_profile": prof,
-            "trajectories": [{"dH": r.dH, "accepted": r.accepted, "nsteps": r.nsteps}
-                             for r in recs],
+            "trajectories": [{"dH": r.dH, "accepted": r.accepted, "H0": r.H0} for r in recs],
             "clocks": clk}
     if rank == 0 and not args.no_propagators:
         line["propagators"] = bench_propagators(local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        s_cpu, sample, _ = cpu_sample(L, Ls, threads, args.cpu_sample_iters, prof)
-        line["cpu_baseline"] = {"value": s_cpu, "unit": "s", "cores": threads, "kind": "port",
-                                "sample": sample}
+        t_iter, t_apply = cpu_iteration_cost(L, Ls, threads, args.cpu_sample_iters)
+        s_cpu, _ = cpu_model(prof64 or prof, t_iter, t_apply)
+        line["cpu_baseline"] = {
+            "value": s_cpu, "unit": "s", "cores": threads, "kind": "port", "modelled": True,
+            "ms_per_1000_iterations": t_iter * 1e6,
+            "sample": (f"oracle 20-pole multi-shift iterations at {L}^3x{Ls} "
+                       f"({3 * args.cpu_sample_iters}, cost per iteration from a "
+                       f"{2 * args.cpu_sample_iters}- minus a {args.cpu_sample_iters}-iteration "
+                       f"run) and 2 operator applies on {threads} threads, "
+                       f"times this run's FP64 iteration profile of the same trajectories")}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    prog.close()
+
+
+def stream_of(prog, local_rank):
+    import torch
+    return torch.cuda.ExternalStream(prog.stream, device=local_rank)
 
 
 def main():
@@ -540,11 +736,20 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if args.validate_cpu_model:
+        run_validate_cpu_model(args)
+        return
     if args.profile_solve:
         run_profile_solve(args, local_rank)
         return
     if args.operator_sweep:
-        run_operator_sweep(args, int(os.environ.get("LOCAL_RANK", "0")))
+        run_operator_sweep(args, local_rank)
+        return
+    if args.thermalise:
+        run_thermalise(args, local_rank)
+        return
+    if args.write_profile:
+        run_write_profile(args, local_rank)
         return
     if world > 1:
         import datetime

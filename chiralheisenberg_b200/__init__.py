@@ -487,11 +487,12 @@ class Program:
         self._check(self.lib.chdwf_prog_set_ext(self.h, npf, nsteps, code, lam))
 
     def timing_read(self):
-        """Per solver-kernel class: (ms, timed launches, launches, bytes)."""
-        ms = np.zeros(4, dtype=np.float64)
-        timed = np.zeros(4, dtype=np.int64)
-        launched = np.zeros(4, dtype=np.int64)
-        nbytes = np.zeros(4, dtype=np.float64)
+        """Per solver-kernel class (0-3 FP64 vectors, 4-7 FP32): (ms, timed
+        launches, launches, bytes)."""
+        ms = np.zeros(8, dtype=np.float64)
+        timed = np.zeros(8, dtype=np.int64)
+        launched = np.zeros(8, dtype=np.int64)
+        nbytes = np.zeros(8, dtype=np.float64)
         self._check(self.lib.chdwf_timing_read(self.context, _ptr(ms), _ptr(timed),
                                                _ptr(launched), _ptr(nbytes)))
         return ms, timed, launched, nbytes

@@ -48,6 +48,12 @@ __device__ __forceinline__ T* ring(const LzArgsT<T>& a, int j) {
 
 static_assert(kSplitThreads == kThreads, "the reductions assume kThreads-wide blocks");
 
+// KernelTimer class of a launch: c for FP64 Krylov vectors, c + 4 for FP32.
+template <class T>
+static inline int timer_class(int c) {
+    return c + (std::is_same<T, float2>::value ? 4 : 0);
+}
+
 // Sum of the n chunk partials part[0..n) in a fixed order; every block that
 // calls it gets the same value.  Valid in all threads.
 __device__ __forceinline__ double sum_partials(const double* part, int n) {
@@ -757,7 +763,7 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
     // algorithmic bytes: M reads q, writes vt; M^dagger reads vt, r_j, r_{j-1}
     // and writes r_{j+1}; both read chi as REAL*4
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
-    if (tm) tm->begin(0, st, 2 * V + chi);
+    if (tm) tm->begin(timer_class<T>(0), st, 2 * V + chi);
     k_lz1_M<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
     // the scalar step of iteration j on the side stream, beside M^dagger(j)
@@ -765,7 +771,7 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
     cudaStreamWaitEvent(side.stream, side.fork, 0);
     k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
     cudaEventRecord(side.join, side.stream);
-    if (tm) tm->begin(1, st, 4 * V + chi);
+    if (tm) tm->begin(timer_class<T>(1), st, 4 * V + chi);
     if (a.wcap > 0) k_lz1_Md<T, IMASS, PAIR, true><<<nb, kThreads, 0, st>>>(a);
     else k_lz1_Md<T, IMASS, PAIR, false><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
@@ -779,14 +785,14 @@ static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
                               const LzSide& side, KernelTimer* tm) {
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     const unsigned nt = (unsigned)a.rp.nthreads, sm = a.rp.smem;
-    if (tm) tm->begin(0, st, 2 * V + chi);
+    if (tm) tm->begin(timer_class<T>(0), st, 2 * V + chi);
     k_lz1_M_rows<T, IMASS><<<nb, nt, sm, st>>>(a);
     if (tm) tm->end(st);
     cudaEventRecord(side.fork, st);
     cudaStreamWaitEvent(side.stream, side.fork, 0);
     k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
     cudaEventRecord(side.join, side.stream);
-    if (tm) tm->begin(1, st, 4 * V + chi);
+    if (tm) tm->begin(timer_class<T>(1), st, 4 * V + chi);
     if (a.wcap > 0) k_lz1_Md_rows<T, IMASS, true><<<nb, nt, sm, st>>>(a);
     else k_lz1_Md_rows<T, IMASS, false><<<nb, nt, sm, st>>>(a);
     if (tm) tm->end(st);
@@ -942,13 +948,13 @@ static void launch_pass2(const LzArgsT<T>& a, int j, int m, int iflag, cudaStrea
     const int apply = j < m;
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     const double acc = iflag == 0 ? 2.0 * a.g.kferm * sizeof(double2) + V : 0.0;
-    if (apply) tm.begin(3, st, 2 * V + chi + acc);
+    if (apply) tm.begin(timer_class<T>(3), st, 2 * V + chi + acc);
     if (iflag == 0) k_lz2_M<T, IMASS, 0, PAIR><<<nb, kThreads, 0, st>>>(a, j, apply);
     else k_lz2_M<T, IMASS, 1, PAIR><<<nb, kThreads, 0, st>>>(a, j, apply);
     count_launches(1);
     if (apply) {
         tm.end(st);
-        tm.begin(3, st, 4 * V + chi);
+        tm.begin(timer_class<T>(3), st, 4 * V + chi);
         k_lz2_Md<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a, j);
         tm.end(st);
         count_launches(1);
@@ -1413,17 +1419,18 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         cudaMemcpy(&hm, w.ctl, sizeof(hm), cudaMemcpyDeviceToHost);
         int keep = 0;
         for (int i = 0, it = 0; i < w.timer.used; i++) {
-            if (w.timer.cls[i] == 0) it++;
+            if (w.timer.cls[i] == timer_class<T>(0)) it++;
             const bool real = it <= hm.m;      // M^dagger(m) completes too
             if (real) {
                 w.timer.cls[keep] = w.timer.cls[i];
+                w.timer.bytes[keep] = w.timer.bytes[i];
                 std::swap(w.timer.ev[2 * keep], w.timer.ev[2 * i]);
                 std::swap(w.timer.ev[2 * keep + 1], w.timer.ev[2 * i + 1]);
                 keep++;
             }
         }
-        w.timer.launches[0] -= launched - hm.m;
-        w.timer.launches[1] -= launched - hm.m;
+        w.timer.launches[timer_class<T>(0)] -= launched - hm.m;
+        w.timer.launches[timer_class<T>(1)] -= launched - hm.m;
         w.timer.used = keep;
         w.timer.collect();
     }
@@ -1454,7 +1461,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         const double nbytes = iflag == 0
             ? (double)m * g.kferm * vb + 2.0 * g.kferm * sizeof(double2)
             : (double)m * 16.0 * g.kvol * vb + (double)ndiag * 16.0 * g.kvol * sizeof(double2);
-        w.timer.begin(2, st, nbytes);
+        w.timer.begin(timer_class<T>(2), st, nbytes);
         if (iflag == 0) {
             // a chunk of stored vectors per launch: x (FP64) is carried in
             // memory between chunks, so each element still sums j = 1..m in

@@ -45,17 +45,18 @@ struct LzStats {
 // bytes of every timed launch.  Events bracket each launch on the solver's
 // stream; durations are summed when the solve synchronises.
 struct KernelTimer {
-    static constexpr int kClasses = 4;
+    // classes 0-3 as above for FP64 Krylov vectors, 4-7 the same for FP32
+    static constexpr int kClasses = 8;
     static constexpr int kPool = 2 * kMaxIter + 256;
     bool enabled = false;
     cudaEvent_t ev[2 * kPool] = {};
     int cls[kPool] = {};
     double bytes[kPool] = {};
     int used = 0;
-    double total_ms[kClasses] = {0, 0, 0, 0};
-    double total_bytes[kClasses] = {0, 0, 0, 0};   // algorithmic bytes moved
-    long long count[kClasses] = {0, 0, 0, 0};
-    long long launches[kClasses] = {0, 0, 0, 0};
+    double total_ms[kClasses] = {};
+    double total_bytes[kClasses] = {};   // algorithmic bytes moved
+    long long count[kClasses] = {};
+    long long launches[kClasses] = {};
     void enable();
     void release();
     void begin(int c, cudaStream_t st, double nbytes);   // start event of one launch

@@ -64,8 +64,9 @@ const char* chdwf_version(void);
  * is then bracketed by events and issued one by one) and resets the totals.
  * chdwf_timing_read fills, per kernel class (0: pass-1 M, 1: pass-1
  * M^dagger + update, 2: pass-2 accumulation from the stored basis, 3: pass-2
- * regeneration), the summed milliseconds, the number of timed launches, the
- * number of launches and the algorithmic bytes of the timed launches. */
+ * regeneration; 4-7: the same classes with FP32 Krylov vectors), the summed
+ * milliseconds, the number of timed launches, the number of launches and
+ * the algorithmic bytes of the timed launches (arrays of 8). */
 int chdwf_timing(chdwf_ctx* ctx, int enable);
 /* Precision of the Krylov vectors in the resident trajectory solves (no
  * reference counterpart: the reference is FP64 throughout).  md: the two
