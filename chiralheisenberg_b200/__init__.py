@@ -65,7 +65,7 @@ EXPORTS = (
     "chdwf_con_read", "chdwf_con_write", "chdwf_prog_read_con", "chdwf_prog_write_con",
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
     "chdwf_ext_set_remez", "chdwf_ext_select_pf", "chdwf_ext_heatbath_dev", "chdwf_ext_action",
-    "chdwf_ext_force", "chdwf_ext_bosonic", "chdwf_prog_set_ext",
+    "chdwf_ext_force", "chdwf_ext_bosonic", "chdwf_prog_set_ext", "chdwf_multishift_dev",
 )
 
 _lib = None
@@ -213,6 +213,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_ext_force.argtypes = [P, F, F, I, I, PI]
     L.chdwf_ext_bosonic.argtypes = [P, P]
     L.chdwf_prog_set_ext.argtypes = [P, I, I, I, F]
+    L.chdwf_multishift_dev.argtypes = [P, P, F, P, F, I, I, P, P, P, I, PI, PI]
     _lib = L
     return L
 
@@ -527,6 +528,7 @@ class Lattice:
     def __init__(self, ksize, ksizet, kthird, beta=0.475, am3=1.0, ibound=-1, device=0):
         self.lib = load_library()
         self.L, self.Lt, self.Ls = ksize, ksizet, kthird
+        self.device = device
         self.kvol = ksize * ksize * ksizet
         self.kferm = 8 * self.kvol * kthird
         self.shape = (2, 4, ksizet, ksize, ksize, kthird)
@@ -619,6 +621,29 @@ class Lattice:
                                            C.byref(it), am, hpin, imass, _ptr(self._chi(chi)),
                                            _ptr(x)))
         return x, it.value
+
+    def multishift(self, Phi, res, chi, sigma, prec="f64", hpin=0.0, imass=1):
+        """Per-shift solutions (M^dag M + sigma_k)^-1 Phi and their FP64 true
+        relative residuals (chdwf_multishift_dev).  prec "f64", or "f32":
+        FP32 Krylov vectors with FP64 defect correction.  Returns
+        (x[n, ...] complex128, true_res[n], iters, refine_iters)."""
+        import torch
+        sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+        n = len(sigma)
+        dev = torch.device("cuda", self.device)
+        Phi_t = torch.from_numpy(np.ascontiguousarray(_c128(Phi, self.shape))).to(dev)
+        chi_t = torch.from_numpy(self._chi(chi)).to(dev)
+        xs = [torch.empty_like(Phi_t) for _ in range(n)]
+        ptrs = (C.c_void_p * n)(*[x.data_ptr() for x in xs])
+        tr = np.zeros(n, dtype=np.float64)
+        it, rit = C.c_int(0), C.c_int(0)
+        code = {"f64": 0, "f32": 1}[prec]
+        self._check(self.lib.chdwf_multishift_dev(self.h, C.c_void_p(Phi_t.data_ptr()), res,
+                                                  C.c_void_p(chi_t.data_ptr()), hpin, imass, n,
+                                                  _ptr(sigma), ptrs, _ptr(tr), code,
+                                                  C.byref(it), C.byref(rit)))
+        torch.cuda.synchronize(dev)
+        return np.stack([x.cpu().numpy() for x in xs]), tr, it.value, rit.value
 
     def force(self, Phi, res1, chi, remez2g, am=0.0, hpin=0.0, imass=1):
         """dSdchi (rhmc/cheisdwf.f:470).  remez2g = (anum, aden, bnum, bden)."""

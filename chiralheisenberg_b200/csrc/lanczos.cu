@@ -1288,6 +1288,35 @@ __global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int j0, i
 
 static constexpr int kAccumChunk = 64;
 
+// Per-shift solutions (iflag 2): x_k = sum_j y_kj q_j for poles k0..k0+7,
+// every element summing j = 1..m in order; xk[k] are device pointers.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_lz_accum_poles(LzArgsT<T> a, int m, int k0,
+                                                             double2* const* xk) {
+    typedef typename real_of<T>::type Real;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= a.g.kferm) return;
+    const int64_t H = kMaxIter + 2, stride = a.g.kferm;
+    const int n = a.npole;
+    double2 acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = make_double2(0.0, 0.0);
+    for (int j = 1; j <= m; j++) {
+        const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(a.basis + j * stride + e)));
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if (k0 + k < n) {
+                const double y = a.h.y[(k0 + k) * H + j];
+                acc[k].x += y * qj.x;
+                acc[k].y += y * qj.y;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        if (k0 + k < n) xk[k0 + k][e] = acc[k];
+}
+
 // Two-slice x_k of every pole from the stored basis (force solves):
 // thread per wall element (slice, component, site), poles in chunks of 8.
 template <class T>
@@ -1352,7 +1381,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     memset(&a, 0, sizeof(a));
     a.g = g;
     set_ring(a, w);
-    if (iflag) set_walls(a, w);
+    if (iflag == 1) set_walls(a, w);
     a.chif = chif;
     a.diag = (Real)(2.0f * ((3.0f - am3) + 1.0f));
     a.hpin = (Real)hpin;
@@ -1451,8 +1480,19 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag);
     k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);
     count_launches(2);
+    if (iflag == 2) {
+        // every x_k from the stored basis, poles in chunks of 8 (one pass over
+        // the basis per chunk); needs the whole basis in HBM
+        if (!(m < a.hcap) || !w.pole_out) return cudaErrorInvalidValue;
+        const unsigned nbx = (unsigned)((g.kferm + kThreads - 1) / kThreads);
+        for (int k0 = 0; k0 < ndiag; k0 += 8) {
+            k_lz_accum_poles<T><<<nbx, kThreads, 0, st>>>(a, m, k0, w.pole_out);
+            count_launches(1);
+        }
+        return cudaGetLastError();
+    }
     launch_scale(x, phi, anum[0], g.kferm, st);                       // x = a0 Phi (:628)
-    if (iflag) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
+    if (iflag == 1) cudaMemsetAsync(w.xw, 0, sizeof(double2) * (size_t)ndiag * 16 * g.kvol, st);
     if (a.wcap > 0 ? m < a.wcap : m < a.hcap) {
         // every q_j (or, for the force, its wall slices) is still in HBM:
         // one streaming pass over the store reads the m stored vectors and
@@ -1495,7 +1535,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         cudaStreamSynchronize(st);
         w.timer.collect();
     }
-    if (iflag) {
+    if (iflag == 1) {
         // X2 = M x_k on the walls, then derivs pole by pole (:733-740)
         launch_wall_dslash64(ndiag, w.x2w, w.xw, chif, g, am3, hpin, ibound, imass, st);
         const double* anum_dev = reinterpret_cast<const double*>(
@@ -1513,7 +1553,7 @@ cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, in
                      float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,
                      int* itercg, int* status, LzStats* stats, cudaStream_t st, int prec) {
     if (ndiag < 1 || ndiag > kMaxPoles) return cudaErrorInvalidValue;
-    cudaError_t e = w.ensure(g, iflag ? ndiag : 1, prec, iflag != 0);
+    cudaError_t e = w.ensure(g, iflag == 1 ? ndiag : 1, prec, iflag == 1);
     if (e) return e;
     if (prec == kPrecF32)
         return lz_solve_t<float2>(w, g, phi, res, ndiag, anum, aden, iflag, chif, am3, hpin,

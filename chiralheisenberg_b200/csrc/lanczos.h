@@ -110,6 +110,7 @@ struct LzWork {
     int xw_poles = 0;
     int* hflag_host = nullptr;
     int* hflag_dev = nullptr;
+    double2* const* pole_out = nullptr;   // iflag 2: device array of the x_k pointers
     KernelTimer timer;
     ~LzWork();
     void release();
@@ -119,6 +120,8 @@ struct LzWork {
 // Precision of the Krylov vectors.
 enum { kPrecF64 = 0, kPrecF32 = 1 };
 
+// iflag 0: x = a0 Phi + sum_k a_k x_k; 1: force (see lanczos.cu); 2: every
+// x_k into w.pole_out[k] (needs the stored basis; anum unused).
 cudaError_t lz_solve(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
                      const double* anum, const double* aden, int iflag, const float* chif,
                      float am3, float hpin, int imass, int ibound, double2* x, float* dSdchi,

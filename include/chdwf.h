@@ -246,6 +246,24 @@ int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, flo
 int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idirac, float res,
                            float am, float hpin, int imass, double* slice, int* itercg);
 
+/* ---- per-shift multi-shift solutions --------------------------------------
+ * x_k = (M^dag M + sigma_k)^-1 Phi for k = 0..n-1 (n <= 32), each into the
+ * device buffer x[k] (complex128, reference layout), with its true relative
+ * residual |Phi - (M^dag M + sigma_k) x_k| / |Phi| computed in FP64 into
+ * true_res[k].  The reference's qmrherm keeps these x_k only internally
+ * (rhmc/cheisdwf.f:614, :689-695) and its testinv (:854-890) checks the same
+ * per-pole residuals.  prec = CHDWF_PREC_F64: the FP64 multi-shift solve
+ * (the reference's stopping rule at res).  CHDWF_PREC_F32: the multi-shift
+ * solve with FP32 Krylov vectors to max(res, 1e-6), the x_k accumulated in
+ * FP64, then per shift FP64 defect correction (FP32 CG on the FP64 true
+ * residual, added in FP64) until the true residual is below res.
+ * iters: multi-shift iterations; refine_iters: inner CG iterations summed.
+ * Phi, chi (real*8 (kvol,3)) are device pointers; the stored Lanczos basis
+ * must hold the solve (chdwf_set_basis_store).  Allocates its work space. */
+int chdwf_multishift_dev(chdwf_ctx* ctx, const void* Phi, float res, const void* chi, float hpin,
+                         int imass, int n, const double* sigma, void* const* x, double* true_res,
+                         int prec, int* iters, int* refine_iters);
+
 /* ---- multi-pseudofermion variant (no reference counterpart) ---------------
  * The reference samples det(M^dag M)^(1/2) with one pseudofermion
  * (rhmc/cheisdwf.f:218-345).  These blocks split it over npf fields, each
