@@ -208,6 +208,7 @@ void orc_thr_dslash(const orc_lat* lat, double* Phi, const double* R, const doub
                     int imass, int dag);
 void orc_thr_derivs(const orc_lat* lat, const double* R, const double* X2, double anum,
                     int iflag, float* dSdpi);
+void orc_thr_set_alphatild_fp64(int on);
 int orc_thr_qmrherm(const orc_lat* lat, const double* Phi, float res, int* itercg, float am,
                     int imass, const double* anum, const double* aden, int ndiag, int iflag,
                     const double* u, double* x, double* Phi0, float* dSdpi);

@@ -194,6 +194,16 @@ void orc_thr_derivs(const orc_lat* lat, const double* R, const double* X2, doubl
  * per pole; 3: the PV force, with coeff = -anum_k, derivs(Phi0_k, M x_k, 0)
  * then derivs(M Phi0_k, x_k, 1).  Phi0: ndiag*kferm complex, dSdpi: the force
  * accumulated into.  Returns 1 at the cap niterc = 7500. */
+/* How qmrherm forms alphatild, a REAL*4 variable by implicit typing
+ * (bulk_rhmc.f:691-694).  0 (default): as the reference, element by element
+ * with the REAL*4 sum rounded after every addition.  1: the sum in REAL*8,
+ * rounded to REAL*4 once -- the grouping a parallel reduction (the GPU's)
+ * can follow, so the GPU is compared with the same arithmetic; the
+ * difference between the two is the reference's own REAL*4 accumulation
+ * error, tested on the CPU. */
+static int g_alphatild_fp64 = 0;
+void orc_thr_set_alphatild_fp64(int on) { g_alphatild_fp64 = on != 0; }
+
 int orc_thr_qmrherm(const orc_lat* lat, const double* Phi, float res, int* itercg, float am,
                     int imass, const double* anum, const double* aden, int ndiag, int iflag,
                     const double* u, double* x, double* Phi0, float* dSdpi) {
@@ -227,8 +237,15 @@ int orc_thr_qmrherm(const orc_lat* lat, const double* Phi, float res, int* iterc
         orc_thr_dslash(lat, vt, q, u, am, imass, 0);
         orc_thr_dslash(lat, x3, vt, u, am, imass, 1);
         float alphatild = 0.0f;                                              /* :691-694 */
-        for (int64_t i = 0; i < kferm; i++)
-            alphatild = (float)((double)alphatild + zmul(zconj(zld(q, i)), zld(x3, i)).re);
+        if (g_alphatild_fp64) {
+            /* the GPU's grouping: the sum in REAL*8, rounded to REAL*4 once */
+            double a8 = 0.0;
+            for (int64_t i = 0; i < kferm; i++) a8 += zmul(zconj(zld(q, i)), zld(x3, i)).re;
+            alphatild = (float)a8;
+        } else {
+            for (int64_t i = 0; i < kferm; i++)
+                alphatild = (float)((double)alphatild + zmul(zconj(zld(q, i)), zld(x3, i)).re);
+        }
         for (int64_t i = 0; i < kferm; i++) {                                /* :696-699 */
             zst(R, i, zsub(zsub(zld(x3, i), zscal((double)alphatild, zld(q, i))),
                            zscal(beta, zld(qm1, i))));

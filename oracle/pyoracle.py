@@ -164,6 +164,8 @@ def lib():
         L.orc_hmc_new.restype = C.POINTER(HmcState)
         L.orc_hmc_free.argtypes = [C.POINTER(HmcState)]
         L.orc_hmc_sweep.argtypes = [C.POINTER(HmcState), P]
+        L.orc_thr_set_alphatild_fp64.argtypes = [C.c_int]
+        L.orc_thr_set_alphatild_fp64.restype = None
         L.orc_thr_coef.argtypes = [P, P, P]
         L.orc_thr_dslash.argtypes = [P, P, P, P, C.c_float, C.c_int, C.c_int]
         L.orc_thr_derivs.argtypes = [P, P, P, C.c_double, C.c_int, P]
@@ -303,6 +305,13 @@ class HmcSweeper:
 
 
 # ---- the bulk Thirring RHMC (bulk_rhmc.f) ---------------------------------
+def thr_alphatild_fp64(on: bool):
+    """Thirring qmrherm's alphatild: False (default) sums in REAL*4 element by
+    element as bulk_rhmc.f:691-694; True sums in REAL*8 and rounds once, the
+    grouping the GPU's parallel reduction follows."""
+    lib().orc_thr_set_alphatild_fp64(1 if on else 0)
+
+
 def thr_shape(lat):
     return (4, lat.Lt, lat.L, lat.L, lat.Ls)
 

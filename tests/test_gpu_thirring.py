@@ -12,13 +12,16 @@ Tolerances:
       sums in FP64 and rounds once.  A CPU model of the GPU's sums gives the
       same solutions to 1e-9 relative and iterations within 1 (2x4x4x4 and
       4^3x4, imass 1, 3, 5, res 1e-6 and 1e-9); dSdpi is REAL*4.
-  sweeps: H0, S0, H1, S1, dH within 1e-6 |H0|; trajectory length, the
+  sweeps: H0, S0, H1, S1, dH within 1e-7 |H0| against the oracle with
+      alphatild summed in REAL*8 and rounded once (the GPU's grouping; the
+      reference's element-by-element REAL*4 sum differs from it by its own
+      accumulation error, which test_oracle_thirring measures); trajectory length, the
       Metropolis draw and decision identical while the oracle's margins
       exceed that; every second sweep measures (its psibarpsi within 1e-4 of max(|pbp|, 0.1),
       its draws keep the generators together).  alphatild, beta0 and phimod are REAL*4 in the reference,
       which limits one rational solve to about 1e-7 relative (6e-8 against
-      a dense evaluation); H0 chains two heatbath and two hamilton solves,
-      and GPU and oracle differ by 3e-7 relative on this workload.
+      a dense evaluation); with the reference's element-by-element sum H0
+      (two heatbath and two hamilton solves) moves by 3e-7 relative.
 The 12-pole remez4g of the Thirring runs is not in the repository; the
 25-pole remez4 (the same function) stands in for it.
 """
@@ -145,10 +148,11 @@ def test_thirring_sweeps_against_oracle(remez, imass):
     h.set_theta(theta)
     h.startup(SEED)
     compared = 0
+    po.thr_alphatild_fp64(True)     # the GPU's grouping of the REAL*4 alphatild sum
     try:
         for _ in range(3):
             ro, rg = sw.sweep(), h.sweep()
-            tol = 1e-6 * abs(ro.H0)
+            tol = 1e-7 * abs(ro.H0)
             for f in ("H0", "S0", "H1", "S1", "dH"):
                 assert abs(getattr(rg, f) - getattr(ro, f)) <= tol, (f, getattr(rg, f),
                                                                       getattr(ro, f))
@@ -170,6 +174,7 @@ def test_thirring_sweeps_against_oracle(remez, imass):
             th_g, th_o = h.get_theta(), sw.theta.reshape(3, -1)
             assert np.abs(th_g - th_o).max() <= 1e-5 * np.abs(th_o).max()
     finally:
+        po.thr_alphatild_fp64(False)
         h.close()
         sw.close()
     assert compared >= 1

@@ -268,3 +268,33 @@ def test_thirring_sweep_stream_with_measurement(remez):
             rand.gauss0(kv)
         assert sw.seed() == rand.seed()
     sw.close()
+
+
+def test_alphatild_grouping_envelope():
+    """The two groupings of the REAL*4 alphatild sum (bulk_rhmc.f:691-694):
+    the reference's element-by-element REAL*4 accumulation and a REAL*8 sum
+    rounded once (what a parallel reduction can follow).  They give the same
+    solve to the reference's own REAL*4 accumulation error: iterations within
+    2 and x within 1e-6 relative; the GPU test compares with the second."""
+    L, Lt, Ls = 2, 4, 4
+    lat = po.make_lat(L, Lt, Ls)
+    kv = L * L * Lt
+    rng = np.random.default_rng(17)
+    theta = (0.2 * rng.standard_normal((3, kv))).astype(np.float32)
+    u = po.thr_coef(lat, theta)
+    shape = po.thr_shape(lat)
+    Phi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    an = np.concatenate([[0.3], np.linspace(0.1, 1.0, 6)])
+    ad = np.logspace(-3, 1, 6)
+    out = []
+    for on in (False, True):
+        po.thr_alphatild_fp64(on)
+        try:
+            x, it, _, _, _ = po.thr_qmrherm(lat, Phi, u, 1e-9, 0.2, 1, an, ad)
+        finally:
+            po.thr_alphatild_fp64(False)
+        out.append((x, it))
+    (x0, i0), (x1, i1) = out
+    assert abs(i0 - i1) <= 2
+    d = np.linalg.norm(x1 - x0) / np.linalg.norm(x0)
+    assert d < 1e-6, d
