@@ -183,11 +183,30 @@ struct BatchWork {
     double* part = nullptr;
     int* hflag_host = nullptr;
     int* hflag_dev = nullptr;
+    // a chunk of CG iterations captured as a CUDA graph, reused while the
+    // batch layout (kernel arguments and grids) stays the same
+    cudaGraphExec_t chunk = nullptr;
+    std::vector<unsigned char> chunk_key;
+    void drop_graph() {
+        if (chunk) cudaGraphExecDestroy(chunk);
+        chunk = nullptr;
+        chunk_key.clear();
+    }
     void release() {
+        drop_graph();
         cudaFree(p); cudaFree(r); cudaFree(x1); cudaFree(chif); cudaFree(sys);
         cudaFree(blk2sys); cudaFree(eblk2sys); cudaFree(active); cudaFree(ctl); cudaFree(part);
         if (hflag_host) cudaFreeHost(hflag_host);
-        *this = BatchWork();
+        hflag_host = nullptr;
+        cap_elems = cap_chi = 0;
+        cap_sys = cap_blk = cap_eblk = 0;
+        p = r = x1 = nullptr;
+        chif = nullptr;
+        sys = nullptr;
+        blk2sys = eblk2sys = active = nullptr;
+        ctl = nullptr;
+        part = nullptr;
+        hflag_dev = nullptr;
     }
     cudaError_t reserve(int64_t elems, int64_t chis, int nsys, int nblk, int neblk) {
         if (p && elems <= cap_elems && chis <= cap_chi && nsys <= cap_sys && nblk <= cap_blk &&
@@ -289,6 +308,7 @@ extern "C" int chdwf_congrad_batch(chdwf_ctx* ctx, const chdwf_cg_system* in, in
         count_launches(1);
     }
     BArgs a;
+    memset(&a, 0, sizeof(a));    // padding too: the struct is the graph's key
     a.sys = w.sys;
     a.blk2sys = w.blk2sys;
     a.eblk2sys = w.eblk2sys;
@@ -299,17 +319,51 @@ extern "C" int chdwf_congrad_batch(chdwf_ctx* ctx, const chdwf_cg_system* in, in
     a.active = w.active;
     a.hflag = w.hflag_dev;
     const unsigned nb = (unsigned)b2s.size(), nbe = (unsigned)e2s.size();
+    // the chunk of kChunk iterations as a graph: every launch of the loop is
+    // identical (the iteration state lives in the per-system control blocks),
+    // so one capture serves every chunk of this and later batches of the
+    // same layout
+    constexpr int kChunk = 16;
+    {
+        std::vector<unsigned char> key(sizeof(a) + 2 * sizeof(unsigned));
+        memcpy(key.data(), &a, sizeof(a));
+        memcpy(key.data() + sizeof(a), &nb, sizeof(unsigned));
+        memcpy(key.data() + sizeof(a) + sizeof(unsigned), &nbe, sizeof(unsigned));
+        if (!w.chunk || w.chunk_key != key) {
+            w.drop_graph();
+            cudaGraph_t g = nullptr;
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                for (int k = 0; k < kChunk; k++) {
+                    k_bcg1<<<nb, kThreads, 0, st>>>(a);
+                    k_bcg2<<<nb, kThreads, 0, st>>>(a);
+                    k_bcg3<<<nbe, kThreads, 0, st>>>(a);
+                }
+                if (cudaStreamEndCapture(st, &g) == cudaSuccess && g) {
+                    if (cudaGraphInstantiate(&w.chunk, g, 0) != cudaSuccess) w.chunk = nullptr;
+                    cudaGraphDestroy(g);
+                }
+            }
+            cudaGetLastError();
+            if (w.chunk) w.chunk_key = key;
+        }
+    }
     cudaEvent_t ev[2];
     cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
     int64_t launched = 0;
     int nchunk = 0;
     while (launched < maxcap) {
-        for (int k = 0; k < 16 && launched < maxcap; k++, launched++) {
-            k_bcg1<<<nb, kThreads, 0, st>>>(a);
-            k_bcg2<<<nb, kThreads, 0, st>>>(a);
-            k_bcg3<<<nbe, kThreads, 0, st>>>(a);
-            count_launches(3);
+        if (w.chunk) {
+            cudaGraphLaunch(w.chunk, st);
+            launched += kChunk;
+            count_launches(3 * kChunk);
+        } else {
+            for (int k = 0; k < kChunk && launched < maxcap; k++, launched++) {
+                k_bcg1<<<nb, kThreads, 0, st>>>(a);
+                k_bcg2<<<nb, kThreads, 0, st>>>(a);
+                k_bcg3<<<nbe, kThreads, 0, st>>>(a);
+                count_launches(3);
+            }
         }
         cudaEventRecord(ev[nchunk & 1], st);
         if (nchunk >= 1) {
