@@ -704,6 +704,7 @@ def run_b200(args, rank, world, local_rank):
             "reference_algorithm": refalg,
             "iteration_profile": prof,
             "trajectories": [{"dH": r.dH, "accepted": r.accepted, "H0": r.H0} for r in recs],
+            "autotune": chb.autotune_report(),
             "clocks": clk}
     if rank == 0 and not args.no_propagators:
         line["propagators"] = bench_propagators(local_rank)

@@ -66,6 +66,7 @@ EXPORTS = (
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
     "chdwf_ext_set_remez", "chdwf_ext_select_pf", "chdwf_ext_heatbath_dev", "chdwf_ext_action",
     "chdwf_ext_force", "chdwf_ext_bosonic", "chdwf_prog_set_ext", "chdwf_multishift_dev",
+    "chdwf_autotune_report",
 )
 
 _lib = None
@@ -214,6 +215,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_ext_bosonic.argtypes = [P, P]
     L.chdwf_prog_set_ext.argtypes = [P, I, I, I, F]
     L.chdwf_multishift_dev.argtypes = [P, P, F, P, F, I, I, P, P, P, I, PI, PI]
+    L.chdwf_autotune_report.argtypes = [C.c_char_p, I]
     _lib = L
     return L
 
@@ -275,6 +277,16 @@ class RunAverages(C.Structure):
                                   "ancgma", "condmoda", "susca")] + \
         [("conda", C.c_float * 3), ("pbpa", C.c_float), ("vel2a", C.c_float),
          ("actiona", C.c_float)]
+
+
+def autotune_report():
+    """The stencil autotuner's choices in this process (chdwf_autotune_report)."""
+    import json
+    lib = load_library()
+    n = lib.chdwf_autotune_report(None, 0)
+    buf = C.create_string_buffer(n)
+    lib.chdwf_autotune_report(buf, n)
+    return json.loads(buf.value.decode())
 
 
 def con_read(path, kvol):

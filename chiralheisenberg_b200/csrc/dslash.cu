@@ -94,16 +94,14 @@ __global__ void __maxnreg__(RowRegs<T>::value)
     }
 }
 
-// Plan and grid of the row-staged operator, set up once per kernel, row
-// length and stencil_mode.
+// Plan and grid of the row-staged operator, set up once per kernel and row
+// length: the blocks that fit on all SMs at once, at most one per row.
 template <class S, class T, bool DAG, int IMASS>
 static bool op_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
-    const int mode = stencil_mode();
-    if (mode == 1) return false;
     if (!row_plan(g, sizeof(S), RowMaxThreads<T>::value, rp)) return false;
-    static int cached_lrow = -1, cached_nrows = -1, cached_mode = -1;
+    static int cached_lrow = -1, cached_nrows = -1;
     static unsigned cached_nb = 0;
-    if (cached_lrow == rp->Lrow && cached_nrows == rp->nrows && cached_mode == mode) {
+    if (cached_lrow == rp->Lrow && cached_nrows == rp->nrows) {
         *nb = cached_nb;
         return cached_nb > 0;
     }
@@ -119,12 +117,11 @@ static bool op_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
         per_sm >= 1) {
         int64_t m = (int64_t)nsm * per_sm;
         if (m > rp->nrows) m = rp->nrows;
-        if (m >= 1 && (mode == 2 || rp->nrows >= 3 * m)) n = (unsigned)m;
+        if (m >= 1) n = (unsigned)m;
     }
     cudaGetLastError();
     cached_lrow = rp->Lrow;
     cached_nrows = rp->nrows;
-    cached_mode = mode;
     cached_nb = n;
     *nb = n;
     return n > 0;
@@ -156,11 +153,14 @@ static bool launch_op_rows_any(bool dag, int imass, S* out, const S* in, const f
 }
 
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
-                     const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
+                     const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
+                     int variant) {
     const unsigned nb = split_blocks(g.npts);
     const double diag = (double)diag_of(am3), hp = (double)hpin;
     const int apbc = ibound == -1;
-    if (launch_op_rows_any<double2, double2>(dag, imass, out, in, chif, g, diag, hp, apbc, st))
+    const bool rows = variant < 0 ? use_rows(g, 16, st) : variant == 1;
+    if (rows &&
+        launch_op_rows_any<double2, double2>(dag, imass, out, in, chif, g, diag, hp, apbc, st))
         return;
 #define LAUNCH(D, I) k_dslash64<D, I><<<nb, kSplitThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc)
     if (!dag) {
@@ -229,8 +229,9 @@ __global__ void __launch_bounds__(kSplitThreads, 3)
 }
 
 void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
-                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st) {
-    {
+                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
+                      int variant) {
+    if (variant < 0 ? use_rows(g, half ? 4 : 8, st) : variant == 1) {
         const float diag = diag_of(am3);
         const int apbc = ibound == -1;
         if (half ? launch_op_rows_any<__half2, float2>(dag, imass, (__half2*)out,

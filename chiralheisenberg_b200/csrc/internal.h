@@ -53,13 +53,24 @@ struct LzHist {
 };
 
 // Operator launchers (FP64, exact evaluation order).
+// variant: -1 the tuned choice (use_rows), 0 the point-gather kernel, 1 the
+// row-staged kernel wherever its shared memory fits.
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
-                     const Geom& g, float am3, float hpin, int ibound, cudaStream_t st);
+                     const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
+                     int variant = -1);
 
 // Operator on FP32 (half=0, complex64) or FP16 (half=1, two halves per
 // complex) storage with FP32 arithmetic.
 void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
-                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st);
+                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
+                      int variant = -1);
+
+// Autotuner (tune.cu): whether the row-staged stencil kernels run for this
+// lattice and element size (16: FP64, 8: FP32, 4: FP16 storage).  With
+// CHDWF_STENCIL unset the first call for a (L, Lt, Ls, elem) times the
+// row-staged and the point-gather operator on scratch vectors on stream st
+// and keeps the faster; "legacy" / "rows" force a choice.
+bool use_rows(const Geom& g, int elem, cudaStream_t st);
 
 // Wall-slice operator for npole stacked two-slice fields (s'=0 <-> s=1,
 // s'=1 <-> s=Ls): computes M on the Ls=2 lattice of each pole.

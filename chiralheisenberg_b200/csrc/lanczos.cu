@@ -799,14 +799,11 @@ static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
     cudaStreamWaitEvent(st, side.join, 0);
 }
 
-// Whether pass 1 runs on the row-staged kernels, and their plan and grid.
-// Rows are used when the ring of staged rows fits a block's shared memory
-// and (stencil_mode) every block gets at least three output rows: the window
-// rows of a block's range cost two loads beyond its own rows.
+// Whether pass 1 runs on the row-staged kernels (the autotuner's choice,
+// use_rows), and their plan and grid.
 template <class T>
-static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
-    const int mode = stencil_mode();
-    if (mode == 1) return false;
+static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb, cudaStream_t st) {
+    if (!use_rows(g, (int)sizeof(T), st)) return false;
     if (!row_plan(g, sizeof(T), RowMaxThreads<T>::value, rp)) return false;
     const void* kern[6] = {(const void*)k_lz1_M_rows<T, 1>, (const void*)k_lz1_M_rows<T, 3>,
                            (const void*)k_lz1_Md_rows<T, 1, false>,
@@ -832,7 +829,7 @@ static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
     }
     int64_t n = (int64_t)nsm * per_sm;
     if (n > rp->nrows) n = rp->nrows;
-    if (n < 1 || (mode == 0 && rp->nrows < 3 * n)) return false;
+    if (n < 1) return false;
     *nb = (unsigned)n;
     return true;
 }
@@ -1394,7 +1391,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.xw = w.xw;
     a.npole = ndiag;
     unsigned nb = 0;
-    a.rows = lz_rows_setup<T>(g, &a.rp, &nb) ? 1 : 0;
+    a.rows = lz_rows_setup<T>(g, &a.rp, &nb, st) ? 1 : 0;
     if (!a.rows) nb = lz_pass1_blocks_any<T>(g, imass);
     const int nbr = reduce_blocks(g.kferm);
     // r_1 lives where ring(a, 1) looks for it: the basis store when present

@@ -50,9 +50,9 @@ template <> struct RowRegs<double2> { static constexpr int value = 112; };
 template <> struct RowRegs<float2> { static constexpr int value = 80; };
 
 // Which stencil kernels run, from the environment variable CHDWF_STENCIL:
-// 0 (unset): row kernels where they fit and every block gets at least three
-// rows; 1 ("legacy"): the point-gather kernels only; 2 ("rows"): row
-// kernels wherever they fit (tests use it to run them on small lattices).
+// 0 (unset): the autotuner's choice per lattice and precision (tune.cu);
+// 1 ("legacy"): the point-gather kernels only; 2 ("rows"): row kernels
+// wherever they fit (tests use it to run them on small lattices).
 inline int stencil_mode() {
     const char* v = getenv("CHDWF_STENCIL");
     if (!v) return 0;

@@ -1,0 +1,136 @@
+// tune.cu -- the autotuner of the stencil kernels.
+//
+// Two kernel shapes apply the domain-wall operator: the point-gather kernels
+// (dwf_stencil.cuh: one thread per point and flavour, every neighbour read
+// through L1/L2) and the row-staged kernels (row_stage.cuh: rows y-1..y+1
+// staged in shared memory by bulk copies).  Which is faster depends on the
+// lattice: the row kernels need a row of L*Ls points to fill a block and
+// several rows per block to amortise the two extra window rows.  On the
+// first use of a (L, Lt, Ls, element size) the tuner applies M both ways to
+// scratch vectors on the caller's stream -- 2 warm-up and 5 timed
+// applications each, CUDA events, L2 not flushed (both see the same cache
+// state) -- and keeps the faster.  The choice holds for the operator and
+// for the multi-shift solver's pass 1, which use the same stencil.  The
+// table is per process; chdwf_autotune_report prints it.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/chdwf.h"
+#include "internal.h"
+#include "row_stage.cuh"
+
+namespace chdwf {
+namespace {
+
+struct TuneEntry {
+    int L, Lt, Ls, elem, device;
+    bool rows;
+    float us_rows, us_gather;
+};
+
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune;
+
+int max_threads_of(int elem) {
+    return elem == 16 ? RowMaxThreads<double2>::value : RowMaxThreads<float2>::value;
+}
+
+// median microseconds of 5 applications (after 2) of variant v
+float time_variant(const Geom& g, int elem, int v, void* out, const void* in, const float* chif,
+                   cudaStream_t st) {
+    auto apply = [&] {
+        if (elem == 16)
+            launch_dslash64(false, 1, (double2*)out, (const double2*)in, chif, g, 1.0f, 0.0f, -1,
+                            st, v);
+        else
+            launch_dslash_lp(false, 1, elem == 4 ? 1 : 0, out, in, chif, g, 1.0f, 0.0f, -1, st,
+                             v);
+    };
+    for (int k = 0; k < 2; k++) apply();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<float> ts;
+    for (int k = 0; k < 5; k++) {
+        cudaEventRecord(e0, st);
+        apply();
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ts.push_back(ms * 1e3f);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::sort(ts.begin(), ts.end());
+    return ts[ts.size() / 2];
+}
+
+}  // namespace
+
+bool use_rows(const Geom& g, int elem, cudaStream_t st) {
+    const int mode = stencil_mode();
+    if (mode == 1) return false;
+    RowPlan rp;
+    if (!row_plan(g, (size_t)elem, max_threads_of(elem), &rp)) return false;
+    if (mode == 2) return true;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (const TuneEntry& t : g_tune)
+            if (t.L == g.L && t.Lt == g.Lt && t.Ls == g.Ls && t.elem == elem && t.device == dev)
+                return t.rows;
+    }
+    // measure on scratch vectors (zeros: the same memory traffic)
+    void *in = nullptr, *out = nullptr;
+    float* chif = nullptr;
+    const size_t bytes = (size_t)elem * g.kferm;
+    TuneEntry t{g.L, g.Lt, g.Ls, elem, dev, false, 0.0f, 0.0f};
+    if (cudaMalloc(&in, bytes) == cudaSuccess && cudaMalloc(&out, bytes) == cudaSuccess &&
+        cudaMalloc(&chif, sizeof(float) * 3 * (size_t)g.kvol) == cudaSuccess) {
+        cudaMemsetAsync(in, 0, bytes, st);
+        cudaMemsetAsync(chif, 0, sizeof(float) * 3 * (size_t)g.kvol, st);
+        t.us_rows = time_variant(g, elem, 1, out, in, chif, st);
+        t.us_gather = time_variant(g, elem, 0, out, in, chif, st);
+        t.rows = t.us_rows < t.us_gather;
+    }
+    cudaGetLastError();
+    cudaFree(in);
+    cudaFree(out);
+    cudaFree(chif);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune.push_back(t);
+    return t.rows;
+}
+
+}  // namespace chdwf
+
+extern "C" int chdwf_autotune_report(char* buf, int cap) {
+    using namespace chdwf;
+    std::string s = "[";
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (size_t i = 0; i < g_tune.size(); i++) {
+            const TuneEntry& t = g_tune[i];
+            char line[256];
+            snprintf(line, sizeof(line),
+                     "%s{\"L\": %d, \"Lt\": %d, \"Ls\": %d, \"elem_bytes\": %d, \"device\": %d, "
+                     "\"rows_us\": %.2f, \"gather_us\": %.2f, \"choice\": \"%s\"}",
+                     i ? ", " : "", t.L, t.Lt, t.Ls, t.elem, t.device, t.us_rows, t.us_gather,
+                     t.rows ? "rows" : "gather");
+            s += line;
+        }
+    }
+    s += "]";
+    if (!buf || cap <= 0) return (int)s.size() + 1;
+    const int n = (int)s.size() < cap - 1 ? (int)s.size() : cap - 1;
+    memcpy(buf, s.data(), n);
+    buf[n] = 0;
+    return (int)s.size() + 1;
+}

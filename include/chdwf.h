@@ -246,6 +246,13 @@ int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, flo
 int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idirac, float res,
                            float am, float hpin, int imass, double* slice, int* itercg);
 
+/* The stencil autotuner's choices so far in this process (no reference
+ * counterpart): a JSON array with one entry per (lattice, element size) of
+ * the median microseconds of the row-staged and the point-gather operator
+ * and the kernel chosen.  Writes at most cap bytes (NUL-terminated) and
+ * returns the length the full text needs, including the NUL. */
+int chdwf_autotune_report(char* buf, int cap);
+
 /* ---- per-shift multi-shift solutions --------------------------------------
  * x_k = (M^dag M + sigma_k)^-1 Phi for k = 0..n-1 (n <= 32), each into the
  * device buffer x[k] (complex128, reference layout), with its true relative
