@@ -66,7 +66,7 @@ EXPORTS = (
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
     "chdwf_ext_set_remez", "chdwf_ext_select_pf", "chdwf_ext_heatbath_dev", "chdwf_ext_action",
     "chdwf_ext_force", "chdwf_ext_bosonic", "chdwf_prog_set_ext", "chdwf_multishift_dev",
-    "chdwf_autotune_report",
+    "chdwf_autotune_report", "chdwf_traj_propagators",
 )
 
 _lib = None
@@ -216,6 +216,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_prog_set_ext.argtypes = [P, I, I, I, F]
     L.chdwf_multishift_dev.argtypes = [P, P, F, P, F, I, I, P, P, P, I, PI, PI]
     L.chdwf_autotune_report.argtypes = [C.c_char_p, I]
+    L.chdwf_traj_propagators.argtypes = [P, I, P, P, F, F, F, I, P, P]
     _lib = L
     return L
 

@@ -54,6 +54,8 @@ Ctx::~Ctx() {
     for (int i = 0; i < kMaxPf; i++)
         if (phi_slot[i]) cudaFree(phi_slot[i]);
     if (gauss) cudaFree(gauss);
+    if (prop_x) cudaFree(prop_x);
+    if (prop_phi) cudaFree(prop_phi);
     if (walls) cudaFree(walls);
     if (stream) cudaStreamDestroy(stream);
 }

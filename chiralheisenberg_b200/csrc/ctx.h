@@ -50,6 +50,9 @@ struct Ctx {
     RemezSet rz_hb, rz_act;
     int prec_md = 0, prec_accept = 0;   // vector precision of the resident solves
     BatchWork* batch = nullptr;         // workspace of chdwf_congrad_batch
+    double2* prop_x = nullptr;          // chdwf_traj_propagators: solutions and
+    double2* prop_phi = nullptr;        // right-hand sides of nsrc sources
+    int prop_cap = 0;
 
     ~Ctx();
     bool fail(cudaError_t e, const char* where);

@@ -183,15 +183,31 @@ int fermion(chdwf_prog* p, float yferm, float* aviter) {
     int iter = 0;
     const int ittt0 = (int)((float)Lt * yferm) + 1;                              // :929
     int ittt = 0;
+    // the 2*nsource congrad solves of the loops below (:937-996) are
+    // independent and share chi: they run as one batched solve, each with
+    // the arithmetic of its own congrad call
+    std::vector<int> src_t, src_d, its(2 * nsource);
+    for (int ksource = 1; ksource <= nsource; ksource++)
+        for (int idsource = 3; idsource <= 4; idsource++) {
+            src_t.push_back((ittt0 + ksource * (Lt / nsource)) % Lt + 1);
+            src_d.push_back(idsource);
+        }
+    std::vector<double> all_walls(2 * 8 * (size_t)kvol * 2 * nsource);
+    {
+        const int rc = chdwf_traj_propagators(p->ctx, 2 * nsource, src_t.data(), src_d.data(),
+                                              p->rescgm, p->am, p->hpin, p->imass,
+                                              all_walls.data(), its.data());
+        if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+        for (int i = 0; i < 2 * nsource; i++)
+            if (its[i] >= p->Ls * kvol) p->cg_caps++;    // congrad's message (:1151-1153)
+    }
     for (int ksource = 1; ksource <= nsource; ksource++) {
         ittt = (ittt0 + ksource * (Lt / nsource)) % Lt + 1;                        // :937
         for (int idsource = 3; idsource <= 4; idsource++) {
-            int it = 0;
-            const int rc = chdwf_traj_propagator(p->ctx, ittt, idsource, p->rescgm, p->am, p->hpin,
-                                                 p->imass, walls.data(), &it);
-            if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
-            if (rc == CHDWF_ITER_CAP) p->cg_caps++;     // congrad's message (:1151-1153)
-            iter += it;
+            const int isrc = 2 * (ksource - 1) + (idsource - 3);
+            std::memcpy(walls.data(), all_walls.data() + 2 * 8 * (size_t)kvol * isrc,
+                        sizeof(double) * 2 * 8 * (size_t)kvol);
+            iter += its[isrc];
             // walls[(w*2 + dd)*2 + f][kvol]: w=0 s=1 Dirac 1,2; w=1 s=Ls Dirac 3,4
             for (int f = 0; f < 2; f++)
                 for (int dd = 0; dd < 2; dd++)

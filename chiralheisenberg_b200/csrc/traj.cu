@@ -3,7 +3,9 @@
 // updates, acceptance and the propagator solve of fermion(), with chi, chit,
 // pp, dSdchi and Phi kept in HBM.
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "../../include/chdwf.h"
 #include "cg.h"
@@ -334,6 +336,61 @@ int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, flo
     cudaMemcpyAsync(walls, c->walls, sizeof(double2) * 8 * g.kvol, cudaMemcpyDeviceToHost, c->stream);
     e = cudaStreamSynchronize(c->stream);
     return traj_solver_status(c, e, st, "propagator");
+}
+
+int chdwf_traj_propagators(chdwf_ctx* ctx, int nsrc, const int* ittt, const int* idsource,
+                           float res, float am, float hpin, int imass, double* walls,
+                           int* itercg) {
+    (void)am;
+    CTX_OR_BAD(ctx);
+    const Geom& g = c->g;
+    if (nsrc < 1 || !ittt || !idsource || !walls || !itercg) return CHDWF_BAD_ARG;
+    for (int i = 0; i < nsrc; i++)
+        if (ittt[i] < 1 || ittt[i] > g.Lt || idsource[i] < 1 || idsource[i] > 4)
+            return CHDWF_BAD_ARG;
+    if (nsrc > c->prop_cap) {
+        cudaFree(c->prop_x);
+        cudaFree(c->prop_phi);
+        c->prop_x = c->prop_phi = nullptr;
+        c->prop_cap = 0;
+        cudaError_t e;
+        if ((e = cudaMalloc(&c->prop_x, sizeof(double2) * g.kferm * nsrc)) ||
+            (e = cudaMalloc(&c->prop_phi, sizeof(double2) * g.kferm * nsrc)))
+            return c->status_of(e, "propagators");
+        c->prop_cap = nsrc;
+    }
+    const int64_t ksize2 = (int64_t)g.L * g.L;
+    const double val = (double)(1.0f / (float)ksize2);                             // :961
+    launch_round_chi(c->chit, c->chif, g.kvol, c->stream);
+    std::vector<chdwf_cg_system> sys(nsrc);
+    for (int i = 0; i < nsrc; i++) {
+        double2* xi = c->prop_x + g.kferm * i;
+        double2* Phi = c->prop_phi + g.kferm * i;
+        cudaMemsetAsync(xi, 0, sizeof(double2) * g.kferm, c->stream);             // :945-953
+        k_wall_source<<<nblk(ksize2), kThreads, 0, c->stream>>>(
+            xi, g, (int64_t)(ittt[i] - 1) * ksize2, idsource[i], val);
+        count_launches(1);
+        launch_dslash64(true, imass, Phi, xi, c->chif, g, c->am3, hpin, c->ibound,
+                        c->stream);                                                // :979
+        cudaMemcpyAsync(xi, Phi, sizeof(double2) * g.kferm, cudaMemcpyDeviceToDevice,
+                        c->stream);                                                // :983-991
+        sys[i] = chdwf_cg_system{g.L, g.Lt, g.Ls, imass, hpin, c->am3, c->ibound, Phi, xi,
+                                 c->chit};
+    }
+    std::vector<int> status(nsrc);
+    int rc = chdwf_congrad_batch(ctx, sys.data(), nsrc, res, itercg, status.data());   // :996
+    if (rc != CHDWF_OK && rc != CHDWF_ITER_CAP) return rc;
+    for (int i = 0; i < nsrc; i++) {
+        if (status[i] == CHDWF_ITER_CAP) fprintf(stdout, " # iterations of congrad exceeds niterc\n");
+        k_extract_walls<<<nblk(8 * (int64_t)g.kvol), kThreads, 0, c->stream>>>(
+            c->prop_x + g.kferm * i, g, c->walls);
+        count_launches(1);
+        cudaMemcpyAsync(walls + (size_t)16 * g.kvol * i, c->walls, sizeof(double2) * 8 * g.kvol,
+                        cudaMemcpyDeviceToHost, c->stream);
+    }
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e) return c->status_of(e, "propagators");
+    return rc;
 }
 
 int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idirac, float res,

@@ -235,6 +235,16 @@ int chdwf_traj_sync(chdwf_ctx* ctx);
  * complex128 [(w*2 + dd)*2 + f][kvol] (w=0: s=1, dd: Dirac pair index). */
 int chdwf_traj_propagator(chdwf_ctx* ctx, int ittt, int idsource, float res, float am, float hpin,
                           int imass, double* walls, int* itercg);
+/* nsrc wall-source propagators of fermion() in one batched solve (the
+ * reference runs them one after the other, rhmc/cheisdwf.f:937-1012): source
+ * i on timeslice ittt[i], Dirac idsource[i], as chdwf_traj_propagator; all
+ * share chit, so chdwf_congrad_batch runs them as multi-right-hand-side
+ * groups.  Each solve's arithmetic is that of chdwf_traj_propagator.  walls
+ * receives nsrc blocks of 8*kvol complex128 in chdwf_traj_propagator's
+ * layout, itercg[i] the iterations of source i. */
+int chdwf_traj_propagators(chdwf_ctx* ctx, int nsrc, const int* ittt, const int* idsource,
+                           float res, float am, float hpin, int imass, double* walls,
+                           int* itercg);
 /* One noise-source solve of measure() (rhmc/cheisdwf.f:1192-1403; the
  * reference routine replaced is the body of its idsource loop):
  * source cmplx(eta(i,1), eta(i,2)) (eta: REAL*4 (kvol,2), as gauss0 fills

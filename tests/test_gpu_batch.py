@@ -46,3 +46,39 @@ def test_batch_matches_one_at_a_time():
         assert its[k] == itr
         err = (torch.linalg.norm(x - xr) / torch.linalg.norm(xr)).item()
         assert err <= 1e-12, (k, err)
+
+
+def test_batched_propagators_equal_sequential(remez):
+    """chdwf_traj_propagators (the sources of fermion() as one batched,
+    multi-right-hand-side solve) gives the same walls, bit for bit, and the
+    same iterations as chdwf_traj_propagator source by source
+    (rhmc/cheisdwf.f:937-1012)."""
+    import ctypes as C
+    L, Lt, Ls = 6, 8, 6
+    beta = 0.475
+    prog = chb.Program(L, Lt, Ls, 0.1, beta, 1.0, 0.01, 0.2, 1, 10, remez["remez2"],
+                       remez["remez4"], remez["remez2g"])
+    chi = np.random.default_rng(5).standard_normal((3, L * L * Lt)) / np.sqrt(beta)
+    prog.set_chi(chi)
+    lib, ctx = prog.lib, prog.context
+    assert lib.chdwf_traj_begin(ctx) == 0
+    kvol = L * L * Lt
+    srcs = [(2, 3), (2, 4), (5, 3), (5, 4), (8, 3), (8, 4)]
+    seq_w, seq_it = [], []
+    for t, d in srcs:
+        w = np.empty(16 * kvol)
+        it = C.c_int()
+        assert lib.chdwf_traj_propagator(ctx, t, d, 1e-9, 0.0, 0.2, 1,
+                                         w.ctypes.data_as(C.c_void_p), C.byref(it)) == 0
+        seq_w.append(w)
+        seq_it.append(it.value)
+    tt = (C.c_int * len(srcs))(*[t for t, _ in srcs])
+    dd = (C.c_int * len(srcs))(*[d for _, d in srcs])
+    its = (C.c_int * len(srcs))()
+    wb = np.empty(16 * kvol * len(srcs))
+    assert lib.chdwf_traj_propagators(ctx, len(srcs), tt, dd, 1e-9, 0.0, 0.2, 1,
+                                      wb.ctypes.data_as(C.c_void_p), its) == 0
+    prog.close()
+    assert list(its) == seq_it
+    for i, w in enumerate(seq_w):
+        assert np.array_equal(wb[16 * kvol * i:16 * kvol * (i + 1)], w), i
