@@ -438,12 +438,14 @@ def run_reference(args, rank, world):
         profile = {"it_pf": 1600.0, "it_h0": 1600.0, "it_h1": 1600.0, "it_force": 26000.0,
                    "nforce": 21.0}
         psrc = "built-in estimate (profile file missing)"
-    vals = []
+    vals, walls = [], []
     for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         t_iter, t_apply = cpu_iteration_cost(args.L, args.Ls, threads, args.cpu_sample_iters)
         s, its = cpu_model(profile, t_iter, t_apply)
         if step >= args.warmup:
             vals.append((s, t_iter))
+            walls.append(time.perf_counter() - t0)
     v = statistics.median(x[0] for x in vals)
     t_it = statistics.median(x[1] for x in vals)
     sample = (f"oracle 20-pole multi-shift iterations at {args.L}^3x{args.Ls} "
@@ -456,6 +458,9 @@ def run_reference(args, rank, world):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(args),
             "modelled": True,
+            "consistency": {"sample_wall_s_per_step": statistics.median(walls),
+                            "note": "each step measures the oracle's cost per iteration on a "
+                                    "bounded sample; value prices a whole trajectory with it"},
             "iteration_profile": profile,
             "ms_per_1000_iterations": t_it * 1e6,
             "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
