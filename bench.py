@@ -96,7 +96,8 @@ def parse():
     ap.add_argument("--profile-res", type=float, default=0.0,
                     help="stopping residual of both profiled solves (0: the reference's)")
     ap.add_argument("--basis-gb", type=float, default=-1.0,
-                    help="HBM budget of the stored Lanczos basis (GB; <0 library default)")
+                    help="HBM budget of the stored Lanczos basis per vector precision (GB; "
+                         "<0: 60 GB in the timed runs, the library default elsewhere)")
     ap.add_argument("--thermalise", type=int, default=0,
                     help="run N trajectories from the seeded Gaussian start and write the "
                          "thermalised configuration")
@@ -211,8 +212,11 @@ KERNEL_WHAT = {0: "pass-1 M q_j with |M q_j|^2",
                3: "pass-2 regeneration (solves longer than the basis store)"}
 
 
-def kernel_name(k):
-    return KERNEL_NAMES[k % 4] + ("_rows" if k % 4 < 2 else "") + (" fp32" if k >= 4 else " fp64")
+def kernel_name(k, rows=False):
+    """Timer class k (4-7: FP32 vectors); rows: pass 1 ran the row-staged
+    kernels (the autotuner's choice for this lattice and precision)."""
+    return KERNEL_NAMES[k % 4] + ("_rows" if rows and k % 4 < 2 else "") + \
+        (" fp32" if k >= 4 else " fp64")
 
 
 def cpu_iteration_cost(L, Ls, threads, iters, npole=20):
@@ -590,10 +594,20 @@ def instrumented(prog, chi0, state0):
     return out
 
 
-def kernel_table(kt):
+def rows_chosen(L, Ls, k):
+    """Whether the autotuner chose the row-staged kernels for class k."""
+    import chiralheisenberg_b200 as chb
+    elem = 8 if k >= 4 else 16
+    for t in chb.autotune_report():
+        if (t["L"], t["Lt"], t["Ls"], t["elem_bytes"]) == (L, L, Ls, elem):
+            return t["choice"] == "rows"
+    return False
+
+
+def kernel_table(kt, L, Ls):
     kms, ktimed, klaunched, kbytes = kt
     tot = max(float(np.sum(kms)), 1e-30)
-    return {kernel_name(k): {"launches": int(klaunched[k]),
+    return {kernel_name(k, rows_chosen(L, Ls, k)): {"launches": int(klaunched[k]),
                              "avg_us": kms[k] / max(ktimed[k], 1) * 1e3,
                              "share_of_solver_time": kms[k] / tot,
                              "GBps": (kbytes[k] / (kms[k] * 1e-3) / 1e9) if kms[k] > 0 else None}
@@ -606,8 +620,10 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     L, Ls = args.L, args.Ls
     prog, start = make_program(L, Ls, local_rank, rank)
-    if args.basis_gb >= 0:
-        prog.set_basis_store(args.basis_gb * 1e9)
+    # the basis store of each vector precision (FP32 and FP64 solves run in
+    # the same program): a fixed budget each, so the FP64 arm is not left
+    # with what the FP32 arm did not take
+    prog.set_basis_store((args.basis_gb if args.basis_gb >= 0 else 60.0) * 1e9)
     prog.set_precision(md="f32", accept="f64")
     stream = torch.cuda.ExternalStream(prog.stream, device=local_rank)
 
@@ -654,7 +670,7 @@ def run_b200(args, rank, world, local_rank):
                           f"({max(dh_rel):.2e}); as absolute {max(dh):.2e}",
                 "same_decisions": all(a.accepted == b.accepted for a, b in zip(recs, recs64)),
                 "iteration_profile": prof64,
-                "solver_kernels": kernel_table(kt64)}
+                "solver_kernels": kernel_table(kt64, L, Ls)}
     prog.close()
     refalg = None
     if not args.no_refalg:
@@ -685,7 +701,7 @@ def run_b200(args, rank, world, local_rank):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic_24x24.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(kernel_name(dom))
+        traffic = json.load(open(tp)).get(kernel_name(dom, rows_chosen(L, Ls, dom)))
     prof = profile_of(recs)
     its_value = sum(prof[k] for k in ("it_pf", "it_h0", "it_h1", "it_force"))
     line = {"metric": "s/trajectory", "value": value, "unit": "s", "n_gpus": world,
@@ -698,13 +714,14 @@ def run_b200(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h, "same_trajectories_as_value": same,
                     "step_ms": [round(x, 1) for x in step_ms_e2e]},
             "fp64": fp64,
-            "roofline": {"bound": "hbm", "kernel": kernel_name(dom), "what": KERNEL_WHAT[dom % 4],
+            "roofline": {"bound": "hbm", "kernel": kernel_name(dom, rows_chosen(L, Ls, dom)),
+                         "what": KERNEL_WHAT[dom % 4],
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_ms * 1e3,
                          "measured_in": "instrumented replay of the first timed trajectory, "
                                         "CUDA events around every solver launch"},
-            "solver_kernels": kernel_table(kt),
+            "solver_kernels": kernel_table(kt, L, Ls),
             "gpu_launches": launches,
             "reference_algorithm": refalg,
             "iteration_profile": prof,

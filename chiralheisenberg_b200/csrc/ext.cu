@@ -9,16 +9,17 @@
 //             R_i from the same Gaussians as the reference's (gauss0, variance
 //             1/2 per component), so S_i = R_i^dag R_i at the start;
 //   action    S_i = Re Phi_i^dag r_act(M^dag M) Phi_i,   r_act ~ x^(-1/(2 npf));
-//   force     dS_i/dchi from one multi-shift solve with r_act's poles, the
-//             same per-pole derivs term the reference's qmrherm(iflag=1)
-//             accumulates (rhmc/cheisdwf.f:729-742): for
-//             r(x) = a0 + sum a_k/(x + sigma_k) the derivative of
-//             Phi^dag r(M^dag M) Phi is -sum_k a_k x_k^dag d(M^dag M) x_k.
+//   force     dS_i/dchi from one multi-shift solve with r_act's poles and
+//             the per-pole derivs term of the reference's qmrherm(iflag=1)
+//             (rhmc/cheisdwf.f:729-742): for r(x) = a0 + sum a_k/(x + sigma_k)
+//             the derivative of Phi^dag r(M^dag M) Phi is
+//             -sum_k a_k x_k^dag d(M^dag M) x_k, x_k = (M^dag M + sigma_k)^-1 Phi.
 // For npf = 1 these are the reference's remez4 (heatbath) and remez2
 // (action) functions; its force instead splits (M^dag M)^(-1/2) into a
 // guidance solve and a second set (rhmc/cheisdwf.f:470-518), equal in exact
 // arithmetic.  The rational sets are made by chiralheisenberg_b200/remez.py.
 #include <cstring>
+#include <vector>
 
 #include "../../include/chdwf.h"
 #include "ctx.h"
@@ -108,8 +109,16 @@ int chdwf_ext_force(chdwf_ctx* ctx, float res, float hpin, int imass, int init, 
     if (!itercg || c->rz_act.n < 1) return CHDWF_BAD_ARG;
     launch_round_chi(c->chit, c->chif, c->g.kvol, c->stream);
     if (init) launch_dsdchi_init(c->chit, 2 * c->beta, c->dS, c->g.kvol, c->stream);
+    // qmrherm(iflag=1) with weights a_k adds -X^dag d r(M^dag M) X to dSdchi:
+    // in the reference's force, X = r_b(M^dag M) Phi ~ (M^dag M)^(-1/2) Phi and
+    // r ~ x^(1/2), and -X^dag d(M^dag M)^(1/2) X is the derivative of
+    // Phi^dag (M^dag M)^(-1/2) Phi (rhmc/cheisdwf.f:470-518).  The derivative
+    // of Phi^dag r_act(M^dag M) Phi is +Phi^dag d r_act Phi: the same solve
+    // with the weights negated.
+    std::vector<double> w(c->rz_act.anum);
+    for (size_t k = 1; k < w.size(); k++) w[k] = -w[k];
     int st = 0;
-    cudaError_t e = lz_solve(c->lz, c->g, c->phi, res, c->rz_act.n, c->rz_act.anum.data(),
+    cudaError_t e = lz_solve(c->lz, c->g, c->phi, res, c->rz_act.n, w.data(),
                              c->rz_act.aden.data(), 1, c->chif, c->am3, hpin, imass, c->ibound,
                              c->spin[2], c->dS, itercg, &st, &c->last_lz, c->stream, c->prec_md);
     return ext_status(c, e, st, "ext force");

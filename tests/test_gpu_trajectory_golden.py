@@ -17,8 +17,10 @@ What must agree, and how closely (the numbers in TOL):
   * the random stream: MD step counts, the Metropolis draw x, the final
     seed -- identical;
   * the accept/reject decision sequence -- identical;
-  * H0, S0 (before the molecular dynamics): the 25-pole solves at 1e-9 of
-    the GPU and of the oracle agree to about 1e-13 relative;
+  * H0, S0 (before the molecular dynamics): from the same chi (the first
+    trajectory) the 25-pole solves at 1e-9 of the GPU and of the oracle give
+    H0 to about 1e-14 relative; later trajectories start from chains whose
+    chi differ at the REAL*4 level of the momenta (below);
   * H1, S1, hg and dH (after it): the momenta and forces are REAL*4, as in
     the reference, and the GPU's FP64 reductions are summed in another
     order than the oracle's loop, so a force solve's last-bit difference can
@@ -43,8 +45,14 @@ from conftest import GOLDEN
 pytestmark = pytest.mark.gpu
 
 ITER_ENVELOPE = 5
-# relative bounds; dH is bounded relative to |H0|
-TOL = {"H0": 1e-11, "S0": 1e-11, "H1": 1e-9, "S1": 1e-9, "hg": 1e-9, "dH_rel_H0": 1e-9}
+# Relative bounds (dH also absolutely), about 3x the largest difference
+# measured on a B200 over the 12 trajectories at 8^3x8: H0, S0 1.7e-10 (the
+# chains' chi drift apart at the REAL*4 level after accepted trajectories;
+# from the same chi, trajectory 1, H0 agrees to 5e-15), H1 4.4e-10,
+# S1 2.4e-10, hg 6.2e-9, dH 1.35e-5 absolute = 3.9e-10 |H0|.
+TOL = {"H0": 5e-10, "S0": 5e-10, "H1": 1.5e-9, "S1": 1.5e-9, "hg": 2e-8, "dH_rel_H0": 1.2e-9}
+TOL_DH_ABS = 4e-5
+TOL_FIRST_H0 = 1e-13   # trajectory 1 starts from the same chi on both sides
 WORKLOADS = ["traj_8x8_b0.475", "traj_12x8_rhmc"]
 
 
@@ -114,6 +122,8 @@ def test_hamiltonians_within_measured_envelope(golden_run):
     for k, d in enumerate(diffs):
         for f in ("H0", "S0", "H1", "S1", "hg", "dH_rel_H0"):
             assert d[f] <= TOL[f], (name, k, f, d[f])
+        assert d["dH_abs"] <= TOL_DH_ABS, (name, k, d["dH_abs"])
+    assert diffs[0]["H0"] <= TOL_FIRST_H0 and diffs[0]["S0"] <= TOL_FIRST_H0
 
 
 def test_iterations_and_single_precision_outputs(golden_run):
