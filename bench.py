@@ -93,6 +93,8 @@ def parse():
                     help="operator GB/s over L in {16,24,32,48}, Ls in {16,24,32}, FP64/FP32/FP16")
     ap.add_argument("--profile-solve", action="store_true",
                     help="bounded work for profilers: one heatbath and one force evaluation")
+    ap.add_argument("--profile-prec", default="f64", choices=["f64", "f32"],
+                    help="Krylov-vector precision of the profiled force evaluation")
     ap.add_argument("--profile-res", type=float, default=0.0,
                     help="stopping residual of both profiled solves (0: the reference's)")
     ap.add_argument("--basis-gb", type=float, default=-1.0,
@@ -332,6 +334,7 @@ def run_profile_solve(args, local_rank):
         prog.set_basis_store(args.basis_gb * 1e9)
     prog.set_chi(synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"]))
     prog.startup(CFG["seed"])
+    prog.set_precision(md=args.profile_prec, accept="f64")
     lib, ctx = prog.lib, prog.context
     import ctypes as C
     kvol = L ** 3
