@@ -100,6 +100,10 @@ def parse():
     ap.add_argument("--basis-gb", type=float, default=-1.0,
                     help="HBM budget of the stored Lanczos basis per vector precision (GB; "
                          "<0: 60 GB in the timed runs, the library default elsewhere)")
+    ap.add_argument("--profile-operator", default="",
+                    choices=["", "f64", "f32", "f16"],
+                    help="bounded work for profilers: 5 applications of M at --L/--Ls in the "
+                         "given storage (CHDWF_STENCIL selects the kernel shape)")
     ap.add_argument("--thermalise", type=int, default=0,
                     help="run N trajectories from the seeded Gaussian start and write the "
                          "thermalised configuration")
@@ -487,6 +491,39 @@ def workload_config(args):
             **CFG, **EXT}
 
 
+def run_profile_operator(args, local_rank):
+    """Five applications of M on device buffers (a bounded launch sequence
+    for profilers), after the autotuner's first call."""
+    import ctypes as C
+    import torch
+    import chiralheisenberg_b200 as chb
+    torch.cuda.set_device(local_rank)
+    L, Ls = args.L, args.Ls
+    lat = chb.Lattice(L, L, Ls, device=local_rank)
+    V = 8 * L ** 3 * Ls
+    dev = f"cuda:{local_rank}"
+    g = torch.Generator(device=dev).manual_seed(1)
+    R = torch.randn(2 * V, dtype=torch.float64, device=dev, generator=g)
+    chi = torch.randn(3 * L ** 3, dtype=torch.float64, device=dev, generator=g)
+    prec = {"f64": 0, "f32": 1, "f16": 2}[args.profile_operator]
+    src = R if prec == 0 else (R.to(torch.float32) if prec == 1 else R.to(torch.float16))
+    out = torch.empty_like(src)
+    for _ in range(5):
+        if prec == 0:
+            rc = lat.lib.chdwf_dslash_dev(lat.h, C.c_void_p(out.data_ptr()),
+                                          C.c_void_p(src.data_ptr()), C.c_void_p(chi.data_ptr()),
+                                          0.3, 1, 0, None)
+        else:
+            rc = lat.lib.chdwf_dslash_dev_lp(lat.h, C.c_void_p(out.data_ptr()),
+                                             C.c_void_p(src.data_ptr()),
+                                             C.c_void_p(chi.data_ptr()), 0.3, 1, 0, prec, None)
+        assert rc == 0
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_operator": args.profile_operator, "L": L, "Ls": Ls,
+                      "autotune": chb.autotune_report()}), flush=True)
+    lat.close()
+
+
 def run_thermalise(args, local_rank):
     """From the seeded Gaussian start: N trajectories of the benchmark
     algorithm (mixed precision), then write the configuration."""
@@ -770,6 +807,9 @@ def main():
         return
     if args.operator_sweep:
         run_operator_sweep(args, local_rank)
+        return
+    if args.profile_operator:
+        run_profile_operator(args, local_rank)
         return
     if args.thermalise:
         run_thermalise(args, local_rank)
