@@ -52,6 +52,7 @@ struct OpRows {
     Real diag, hpin;
     int apbc;
     T tp[4], tm[4];
+    RowWall<T> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
         const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
         const int64_t i = (int64_t)x * g.Ls + s;
@@ -62,13 +63,14 @@ struct OpRows {
             tp[d] = RowCvt<T, S>::get(__ldg(in + ep + g.cs * (d + 4 * f)));
             tm[d] = RowCvt<T, S>::get(__ldg(in + em + g.cs * (d + 4 * f)));
         }
+        row_wall_prefetch<DAG>(rw, in, g, f, t, y, x, s, chif);
     }
     __device__ __forceinline__ void compute(const S* c, const S* yp, const S* ym, int f, int t,
                                             int y, int x, int s, int i, int ixp, int ixm) {
         const PointIdx q = row_point(g, t, y, x, s);
         T acc[4];
-        dwf_apply_rows<DAG, IMASS>(acc, c, yp, ym, Lrow, i, ixp, ixm, tp, tm, in, g, q, f, chif,
-                                   diag, hpin, apbc != 0);
+        dwf_apply_rows<DAG, IMASS>(acc, c, yp, ym, Lrow, i, ixp, ixm, tp, tm, rw, g, q, f, diag,
+                                   hpin, apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) out[q.p + g.cs * (d + 4 * f)] = row_store(acc[d], out);
     }

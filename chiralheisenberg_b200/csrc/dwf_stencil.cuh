@@ -71,6 +71,48 @@ __device__ __forceinline__ void load4(T* r, const Ld& ld, const Geom& g, int64_t
     for (int d = 0; d < 4; d++) r[d] = ld(n + g.cs * (d + 4 * f));
 }
 
+// One element of the wall coupling: a of flavour f takes r1 (flavour 0) and
+// r2 (flavour 1), the other wall's components of the same Dirac index.
+template <bool DAG, int IMASS, int SIDE, class T>
+__device__ __forceinline__ void wall_elem(T& a, T r1, T r2, int f, float c1f, float c2f,
+                                          float c3f, bool pin, typename real_of<T>::type hpin) {
+    typedef typename real_of<T>::type R;
+    if (IMASS == 1) {
+        // spm = cmplx(chi3, 0) (:2912-2946 / :3345-3379), pinning
+        // (:2948-2959 / :3381-3392), spm = cmplx(chi1, -chi2)
+        // (:2962-2995 / :3395-3428)
+        const T spm = zmake<T>((R)c3f, (R)0);
+        const T sp = zmake<T>((R)c1f, (R)(-c2f));
+        if (f == 0) {
+            a = zadd(a, zmul(spm, r1));
+            if (pin) a = zadd(a, zscal(hpin, r1));
+            a = zadd(a, zmul(sp, r2));
+        } else {
+            a = zsub(a, zmul(spm, r2));
+            if (pin) a = zsub(a, zscal(hpin, r2));
+            a = zadd(a, zmul(zconj(sp), r1));
+        }
+    } else if (IMASS == 3) {
+        // M: spm = cmplx(0, chi3) (:2996-3030); M^dagger cmplx(0,-chi3)
+        // (:3429-3463).  Sign of the flavour-1 term: M: -,+ at s=Ls and
+        // +,- at s=1; M^dagger: +,- at s=Ls and -,+ at s=1.
+        const T spm = zmake<T>((R)0, (R)(DAG ? -c3f : c3f));
+        constexpr bool minus_first = (!DAG && SIDE == 0) || (DAG && SIDE == 1);
+        // M: spm = cmplx(chi2, chi1) (:3032-3065); M^dagger
+        // cmplx(-chi2,-chi1) (:3465-3497)
+        const T sp = DAG ? zmake<T>((R)(-c2f), (R)(-c1f)) : zmake<T>((R)c2f, (R)c1f);
+        if (f == 0) {
+            const T t1 = zmul(spm, r1), u1 = zmul(sp, r2);
+            a = minus_first ? zsub(a, t1) : zadd(a, t1);
+            a = minus_first ? zsub(a, u1) : zadd(a, u1);
+        } else {
+            const T t2 = zmul(spm, r2), u2 = zmul(zconj(sp), r1);
+            a = minus_first ? zadd(a, t2) : zsub(a, t2);
+            a = minus_first ? zadd(a, u2) : zsub(a, u2);
+        }
+    }
+}
+
 // Wall coupling of one flavour at a wall point (s = Ls for SIDE 0, s = 1 for
 // SIDE 1): Dirac pair D0, D0+1 of flavour f takes the other wall's components
 // of both flavours.  Per element the operation sequence is that of the
@@ -79,45 +121,10 @@ template <bool DAG, int IMASS, int D0, int SIDE, class T, class Ld>
 __device__ __forceinline__ void wall_terms(T acc[4], const Ld& ld, int64_t cs, int64_t other,
                                            int f, float c1f, float c2f, float c3f, bool pin,
                                            typename real_of<T>::type hpin) {
-    typedef typename real_of<T>::type R;
 #pragma unroll
-    for (int d = D0; d < D0 + 2; d++) {
-        const T r1 = ld(other + cs * d), r2 = ld(other + cs * (d + 4));
-        if (IMASS == 1) {
-            // spm = cmplx(chi3, 0) (:2912-2946 / :3345-3379), pinning
-            // (:2948-2959 / :3381-3392), spm = cmplx(chi1, -chi2)
-            // (:2962-2995 / :3395-3428)
-            const T spm = zmake<T>((R)c3f, (R)0);
-            const T sp = zmake<T>((R)c1f, (R)(-c2f));
-            if (f == 0) {
-                acc[d] = zadd(acc[d], zmul(spm, r1));
-                if (pin) acc[d] = zadd(acc[d], zscal(hpin, r1));
-                acc[d] = zadd(acc[d], zmul(sp, r2));
-            } else {
-                acc[d] = zsub(acc[d], zmul(spm, r2));
-                if (pin) acc[d] = zsub(acc[d], zscal(hpin, r2));
-                acc[d] = zadd(acc[d], zmul(zconj(sp), r1));
-            }
-        } else if (IMASS == 3) {
-            // M: spm = cmplx(0, chi3) (:2996-3030); M^dagger cmplx(0,-chi3)
-            // (:3429-3463).  Sign of the flavour-1 term: M: -,+ at s=Ls and
-            // +,- at s=1; M^dagger: +,- at s=Ls and -,+ at s=1.
-            const T spm = zmake<T>((R)0, (R)(DAG ? -c3f : c3f));
-            constexpr bool minus_first = (!DAG && SIDE == 0) || (DAG && SIDE == 1);
-            // M: spm = cmplx(chi2, chi1) (:3032-3065); M^dagger
-            // cmplx(-chi2,-chi1) (:3465-3497)
-            const T sp = DAG ? zmake<T>((R)(-c2f), (R)(-c1f)) : zmake<T>((R)c2f, (R)c1f);
-            if (f == 0) {
-                const T t1 = zmul(spm, r1), u1 = zmul(sp, r2);
-                acc[d] = minus_first ? zsub(acc[d], t1) : zadd(acc[d], t1);
-                acc[d] = minus_first ? zsub(acc[d], u1) : zadd(acc[d], u1);
-            } else {
-                const T t2 = zmul(spm, r2), u2 = zmul(zconj(sp), r1);
-                acc[d] = minus_first ? zadd(acc[d], t2) : zsub(acc[d], t2);
-                acc[d] = minus_first ? zadd(acc[d], u2) : zsub(acc[d], u2);
-            }
-        }
-    }
+    for (int d = D0; d < D0 + 2; d++)
+        wall_elem<DAG, IMASS, SIDE>(acc[d], ld(other + cs * d), ld(other + cs * (d + 4)), f, c1f,
+                                    c2f, c3f, pin, hpin);
 }
 
 // The four Dirac components of flavour f at one output point.  The flavours

@@ -415,6 +415,7 @@ struct LzRowsM {
     Real ib;
     double loc;
     T tp[4], tm[4];
+    RowWall<T> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
         const Geom& g = a.g;
         const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
@@ -425,14 +426,15 @@ struct LzRowsM {
             tp[d] = __ldg(rj + ep + g.cs * (d + 4 * f));
             tm[d] = __ldg(rj + em + g.cs * (d + 4 * f));
         }
+        row_wall_prefetch<false>(rw, rj, g, f, t, y, x, s, a.chif);
     }
     __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, int f, int t,
                                             int y, int x, int s, int i, int ixp, int ixm) {
         const Geom& g = a.g;
         const PointIdx q = row_point(g, t, y, x, s);
         T acc[4];
-        dwf_apply_rows<false, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, rj, g, q, f,
-                                     a.chif, a.diag, a.hpin, a.apbc != 0);
+        dwf_apply_rows<false, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, rw, g, q, f,
+                                     a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             acc[d] = zscal(ib, acc[d]);
@@ -480,6 +482,7 @@ struct LzRowsMd {
     Real ib, at, bj, ibm;
     double loc;
     T tp[4], tm[4], cj[4], cm[4];
+    RowWall<T> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
         const Geom& g = a.g;
         const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
@@ -494,14 +497,15 @@ struct LzRowsMd {
             cj[d] = rj[e0 + po];
             if (j > 1) cm[d] = rjm[e0 + po];
         }
+        row_wall_prefetch<true>(rw, a.vt, g, f, t, y, x, s, a.chif);
     }
     __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, int f, int t,
                                             int y, int x, int s, int i, int ixp, int ixm) {
         const Geom& g = a.g;
         const PointIdx q = row_point(g, t, y, x, s);
         T acc[4];
-        dwf_apply_rows<true, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, a.vt, g, q, f,
-                                    a.chif, a.diag, a.hpin, a.apbc != 0);
+        dwf_apply_rows<true, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, rw, g, q, f,
+                                    a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             const int64_t e = q.p + g.cs * (d + 4 * f);

@@ -230,18 +230,46 @@ template <> struct RowCvt<float2, __half2> {
     __device__ __forceinline__ static float2 get(__half2 v) { return __half22float2(v); }
 };
 
+// Operands of the wall terms that are not in the staged rows: the other
+// flavour's components on the other wall (same site, Dirac pair of the
+// wall) and chi at the site.  Loaded in Body::pre with the t neighbours, so
+// their latency overlaps the wait for the staged rows.
+template <class T>
+struct RowWall {
+    T w[2];
+    float c1, c2, c3;
+};
+
+template <bool DAG, class T, class S>
+__device__ __forceinline__ void row_wall_prefetch(RowWall<T>& rw, const S* __restrict__ gin,
+                                                  const Geom& g, int f, int t, int y, int x,
+                                                  int s, const float* __restrict__ chif) {
+    const int Ls = g.Ls;
+    const bool atL = (s == Ls - 1), at0 = (s == 0);
+    if (!(atL || at0)) return;
+    const int site = x + g.L * (y + g.L * t);
+    const int64_t other = (int64_t)Ls * site + (atL ? 0 : Ls - 1);
+    constexpr int WA = DAG ? 0 : 2;   // pair at s=Ls
+    constexpr int WB = DAG ? 2 : 0;   // pair at s=1
+    const int d0 = atL ? WA : WB;
+    const int fo = 1 - f;
+#pragma unroll
+    for (int k = 0; k < 2; k++) rw.w[k] = RowCvt<T, S>::get(__ldg(gin + other + g.cs * (d0 + k + 4 * fo)));
+    rw.c1 = __ldg(chif + site);
+    rw.c2 = __ldg(chif + g.kvol + site);
+    rw.c3 = __ldg(chif + 2 * g.kvol + site);
+}
+
 // The four Dirac components of flavour f at one output point of a staged
 // row, with the same operation sequence as dwf_apply_flavour (so the FP64
 // result is bit-identical to it).  c, yp, ym: shared rows y, y+1, y-1 (plane
 // stride Lrow, storage type S); i = x*Ls + s; ixp, ixm: the x+-1 points of
-// the row; tp, tm: the t+-1 neighbours (registers); gin, q: global field and
-// point for the wall terms.
+// the row; tp, tm: the t+-1 neighbours and rw the wall operands (registers).
 template <bool DAG, int IMASS, class T, class S>
 __device__ __forceinline__ void dwf_apply_rows(T acc[4], const S* c, const S* yp, const S* ym,
                                                int Lrow, int i, int ixp, int ixm, const T tp[4],
-                                               const T tm[4], const S* __restrict__ gin,
+                                               const T tm[4], const RowWall<T>& rw,
                                                const Geom& g, const PointIdx& q, int f,
-                                               const float* __restrict__ chif,
                                                typename real_of<T>::type diag,
                                                typename real_of<T>::type hpin, bool apbc) {
     typedef typename real_of<T>::type R;
@@ -285,22 +313,29 @@ __device__ __forceinline__ void dwf_apply_rows(T acc[4], const S* c, const S* yp
 #pragma unroll
         for (int d = DN; d < DN + 2; d++) acc[d] = zsub(acc[d], C::get(c[d * Lrow + i - 1]));
     }
-    // wall coupling (other wall, both flavours, from global memory)
+    // wall coupling: this flavour's components on the other wall come from
+    // the staged row (same site), the other flavour's and chi from rw
     constexpr int WA = DAG ? 0 : 2;
     constexpr int WB = DAG ? 2 : 0;
     const bool atL = (q.s == Ls - 1), at0 = (q.s == 0);
     if (!(atL || at0)) return;
-    const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
-                c3f = __ldg(chif + 2 * g.kvol + q.site);
-    const int64_t LsI = Ls;
-    const int64_t other = atL ? LsI * q.site : LsI * q.site + Ls - 1;
     const bool pin = (q.site == 0);
-    struct Ld {
-        const S* __restrict__ p;
-        __device__ __forceinline__ T operator()(int64_t j) const { return C::get(__ldg(p + j)); }
-    };
-    if (atL) wall_terms<DAG, IMASS, WA, 0>(acc, Ld{gin}, g.cs, other, f, c1f, c2f, c3f, pin, hpin);
-    if (at0) wall_terms<DAG, IMASS, WB, 1>(acc, Ld{gin}, g.cs, other, f, c1f, c2f, c3f, pin, hpin);
+    const int io = i - q.s + (atL ? 0 : Ls - 1);      // the other wall's point in the row
+    if (atL) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const T own = C::get(c[(WA + k) * Lrow + io]);
+            wall_elem<DAG, IMASS, 0>(acc[WA + k], f == 0 ? own : rw.w[k], f == 0 ? rw.w[k] : own,
+                                     f, rw.c1, rw.c2, rw.c3, pin, hpin);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const T own = C::get(c[(WB + k) * Lrow + io]);
+            wall_elem<DAG, IMASS, 1>(acc[WB + k], f == 0 ? own : rw.w[k], f == 0 ? rw.w[k] : own,
+                                     f, rw.c1, rw.c2, rw.c3, pin, hpin);
+        }
+    }
 }
 
 __device__ __forceinline__ PointIdx row_point(const Geom& g, int t, int y, int x, int s) {
