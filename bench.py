@@ -218,11 +218,11 @@ KERNEL_WHAT = {0: "pass-1 M q_j with |M q_j|^2",
                3: "pass-2 regeneration (solves longer than the basis store)"}
 
 
-def kernel_name(k, rows=False):
-    """Timer class k (4-7: FP32 vectors); rows: pass 1 ran the row-staged
-    kernels (the autotuner's choice for this lattice and precision)."""
-    return KERNEL_NAMES[k % 4] + ("_rows" if rows and k % 4 < 2 else "") + \
-        (" fp32" if k >= 4 else " fp64")
+def kernel_name(k, shape=""):
+    """Timer class k (4-7: FP32 vectors); shape: the stencil shape the
+    autotuner chose for pass 1 at this lattice and precision."""
+    name = KERNEL_NAMES[k % 4] + (" fp32" if k >= 4 else " fp64")
+    return name + (f" ({shape})" if shape and k % 4 < 2 else "")
 
 
 def cpu_iteration_cost(L, Ls, threads, iters, npole=20):
@@ -635,13 +635,13 @@ def instrumented(prog, chi0, state0):
 
 
 def rows_chosen(L, Ls, k):
-    """Whether the autotuner chose the row-staged kernels for class k."""
+    """The stencil shape the autotuner chose for class k's precision."""
     import chiralheisenberg_b200 as chb
     elem = 8 if k >= 4 else 16
     for t in chb.autotune_report():
         if (t["L"], t["Lt"], t["Ls"], t["elem_bytes"]) == (L, L, Ls, elem):
-            return t["choice"] == "rows"
-    return False
+            return t["choice"]
+    return ""
 
 
 def kernel_table(kt, L, Ls):

@@ -16,9 +16,10 @@ struct LdF64 {
     __device__ __forceinline__ double2 operator()(int64_t j) const { return __ldg(p + j); }
 };
 
-// Flavour-split: two threads per point (split_point / split_flavour).
-template <bool DAG, int IMASS>
-__global__ void __launch_bounds__(kSplitThreads, kSplitMinBlocks)
+// Flavour-split: two threads per point (split_point / split_flavour); OCC
+// blocks a SM (the register budget).
+template <bool DAG, int IMASS, int OCC>
+__global__ void __launch_bounds__(kSplitThreads, OCC)
     k_dslash64(double2* __restrict__ out, const double2* __restrict__ in,
                const float* __restrict__ chif, Geom g, double diag, double hpin, int apbc) {
     const int64_t p = split_point();
@@ -160,11 +161,17 @@ void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const
     const unsigned nb = split_blocks(g.npts);
     const double diag = (double)diag_of(am3), hp = (double)hpin;
     const int apbc = ibound == -1;
-    const bool rows = variant < 0 ? use_rows(g, 16, st) : variant == 1;
-    if (rows &&
+    const int shape = variant < 0 ? stencil_choice(g, 16, st) : variant;
+    if (shape == kStencilRows &&
         launch_op_rows_any<double2, double2>(dag, imass, out, in, chif, g, diag, hp, apbc, st))
         return;
-#define LAUNCH(D, I) k_dslash64<D, I><<<nb, kSplitThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc)
+#define LAUNCH(D, I)                                                                          \
+    do {                                                                                      \
+        if (shape == kStencilGather4)                                                         \
+            k_dslash64<D, I, 4><<<nb, kSplitThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc); \
+        else                                                                                  \
+            k_dslash64<D, I, 3><<<nb, kSplitThreads, 0, st>>>(out, in, chif, g, diag, hp, apbc); \
+    } while (0)
     if (!dag) {
         if (imass == 1) LAUNCH(false, 1); else if (imass == 3) LAUNCH(false, 3); else LAUNCH(false, 0);
     } else {
@@ -211,8 +218,8 @@ __global__ void __launch_bounds__(kThreads) k_dslash_lp(void* __restrict__ out,
 // FP32 storage with Ls even: a thread takes two adjacent points of one
 // flavour with 16-byte loads (dwf_apply_flavour_pair); a block covers 128
 // point pairs of both flavours.
-template <bool DAG, int IMASS>
-__global__ void __launch_bounds__(kSplitThreads, 3)
+template <bool DAG, int IMASS, int OCC>
+__global__ void __launch_bounds__(kSplitThreads, OCC)
     k_dslash_f32_pair(float2* __restrict__ out, const float2* __restrict__ in,
                       const float* __restrict__ chif, Geom g, float diag, float hpin, int apbc) {
     const int64_t p = (int64_t)blockIdx.x * (2 * kSplitPoints) +
@@ -233,7 +240,8 @@ __global__ void __launch_bounds__(kSplitThreads, 3)
 void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
                       const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
                       int variant) {
-    if (variant < 0 ? use_rows(g, half ? 4 : 8, st) : variant == 1) {
+    const int shape = variant < 0 ? stencil_choice(g, half ? 4 : 8, st) : variant;
+    if (shape == kStencilRows) {
         const float diag = diag_of(am3);
         const int apbc = ibound == -1;
         if (half ? launch_op_rows_any<__half2, float2>(dag, imass, (__half2*)out,
@@ -250,7 +258,15 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
         const int apbc = ibound == -1;
         float2* o = (float2*)out;
         const float2* i = (const float2*)in;
-#define PR(D, I) k_dslash_f32_pair<D, I><<<nb2, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
+#define PR(D, I)                                                                             \
+    do {                                                                                     \
+        if (shape == kStencilGather4)                                                        \
+            k_dslash_f32_pair<D, I, 4><<<nb2, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, \
+                                                                     apbc);                  \
+        else                                                                                 \
+            k_dslash_f32_pair<D, I, 3><<<nb2, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, \
+                                                                     apbc);                  \
+    } while (0)
         if (!dag) { if (imass == 3) PR(false, 3); else PR(false, 1); }
         else { if (imass == 3) PR(true, 3); else PR(true, 1); }
 #undef PR

@@ -326,7 +326,6 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
 // reads contiguous runs of one component plane.
 constexpr int kSplitThreads = 256;
 constexpr int kSplitPoints = kSplitThreads / 2;
-constexpr int kSplitMinBlocks = 4;   // 64 registers a thread: 32 warps per SM
 __device__ __forceinline__ int split_flavour() { return threadIdx.x >= kSplitPoints; }
 __device__ __forceinline__ int64_t split_point() {
     return (int64_t)blockIdx.x * kSplitPoints + (threadIdx.x & (kSplitPoints - 1));

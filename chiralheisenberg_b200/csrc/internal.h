@@ -53,8 +53,8 @@ struct LzHist {
 };
 
 // Operator launchers (FP64, exact evaluation order).
-// variant: -1 the tuned choice (use_rows), 0 the point-gather kernel, 1 the
-// row-staged kernel wherever its shared memory fits.
+// variant: -1 the tuned choice (stencil_choice), or one of the kStencil*
+// shapes below (the row-staged one wherever its shared memory fits).
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
                      int variant = -1);
@@ -65,12 +65,16 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
                       const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
                       int variant = -1);
 
-// Autotuner (tune.cu): whether the row-staged stencil kernels run for this
-// lattice and element size (16: FP64, 8: FP32, 4: FP16 storage).  With
-// CHDWF_STENCIL unset the first call for a (L, Lt, Ls, elem) times the
-// row-staged and the point-gather operator on scratch vectors on stream st
-// and keeps the faster; "legacy" / "rows" force a choice.
-bool use_rows(const Geom& g, int elem, cudaStream_t st);
+// Stencil kernel shapes: the point-gather kernels with 3 blocks of 256 a SM
+// (80 registers a thread) or 4 (64 registers), or the row-staged kernels.
+constexpr int kStencilGather3 = 0, kStencilRows = 1, kStencilGather4 = 2;
+
+// Autotuner (tune.cu): the stencil shape for this lattice and element size
+// (16: FP64, 8: FP32, 4: FP16 storage).  With CHDWF_STENCIL unset the first
+// call for a (L, Lt, Ls, elem) times the operator in every shape on scratch
+// vectors on stream st and keeps the fastest; "legacy" forces the
+// point-gather kernels at 3 blocks a SM, "rows" the row-staged ones.
+int stencil_choice(const Geom& g, int elem, cudaStream_t st);
 
 // Wall-slice operator for npole stacked two-slice fields (s'=0 <-> s=1,
 // s'=1 <-> s=Ls): computes M on the Ls=2 lattice of each pole.

@@ -155,8 +155,8 @@ __device__ __forceinline__ void apply_scaled(T acc[4], const T* r, typename real
 // beta_j is the sum of the previous M^dagger launch's partials (beta_1 comes
 // from the source), formed by every block.  The partial buffers: part[0..nb)
 // for this kernel, part[nb..2nb) for M^dagger.
-template <class T, int IMASS, bool PAIR>
-__global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz1_M(LzArgsT<T> a) {
+template <class T, int IMASS, bool PAIR, int OCC>
+__global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
     typedef typename real_of<T>::type Real;
     typedef LzShape<T, PAIR> S;
     constexpr int NF = S::split ? 1 : 2;
@@ -330,8 +330,8 @@ __device__ __forceinline__ void wall_put(const LzArgsT<T>& a, int j1, int s, int
 
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
 // alpha~_j is the sum of M(j)'s partials, formed by every block.
-template <class T, int IMASS, bool PAIR, bool WALLS>
-__global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks)) k_lz1_Md(LzArgsT<T> a) {
+template <class T, int IMASS, bool PAIR, bool WALLS, int OCC>
+__global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
     typedef LzShape<T, PAIR> S;
     constexpr int NF = S::split ? 1 : 2;
     LzCtl* ctl = a.ctl;
@@ -669,15 +669,17 @@ static unsigned lz_direct_blocks(int64_t npts) {
 
 // Persistent pass-1 grid: the resident blocks of both pass-1 kernels on all
 // SMs, at most one block pass per block.
-template <class T, int IMASS, bool PAIR>
+template <class T, int IMASS, bool PAIR, int OCC>
 static unsigned lz_pass1_blocks(int64_t npts) {
     int dev = 0, nsm = 0, b1 = 0, b2 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lz1_M<T, IMASS, PAIR>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_lz1_M<T, IMASS, PAIR, OCC>, kThreads, 0);
     int b3 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS, PAIR, false>, kThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_lz1_Md<T, IMASS, PAIR, true>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_lz1_Md<T, IMASS, PAIR, false, OCC>,
+                                                  kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_lz1_Md<T, IMASS, PAIR, true, OCC>,
+                                                  kThreads, 0);
     if (b3 < b2) b2 = b3;
     int64_t nb = (int64_t)nsm * (b1 < b2 ? b1 : b2);
     const int64_t direct = lz_direct_blocks<T, PAIR>(npts);
@@ -761,14 +763,14 @@ __global__ void k_lz_init(LzCtl* ctl, LzHist h, const double* part, int nb) {
     }
 }
 
-template <class T, int IMASS, bool PAIR>
-static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
-                         KernelTimer* tm) {
+template <class T, int IMASS, bool PAIR, int OCC>
+static void launch_pass1_occ(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
+                             const LzSide& side, KernelTimer* tm) {
     // algorithmic bytes: M reads q, writes vt; M^dagger reads vt, r_j, r_{j-1}
     // and writes r_{j+1}; both read chi as REAL*4
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     if (tm) tm->begin(timer_class<T>(0), st, 2 * V + chi);
-    k_lz1_M<T, IMASS, PAIR><<<nb, kThreads, 0, st>>>(a);
+    k_lz1_M<T, IMASS, PAIR, OCC><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
     // the scalar step of iteration j on the side stream, beside M^dagger(j)
     cudaEventRecord(side.fork, st);
@@ -776,10 +778,19 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
     k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
     cudaEventRecord(side.join, side.stream);
     if (tm) tm->begin(timer_class<T>(1), st, 4 * V + chi);
-    if (a.wcap > 0) k_lz1_Md<T, IMASS, PAIR, true><<<nb, kThreads, 0, st>>>(a);
-    else k_lz1_Md<T, IMASS, PAIR, false><<<nb, kThreads, 0, st>>>(a);
+    if (a.wcap > 0) k_lz1_Md<T, IMASS, PAIR, true, OCC><<<nb, kThreads, 0, st>>>(a);
+    else k_lz1_Md<T, IMASS, PAIR, false, OCC><<<nb, kThreads, 0, st>>>(a);
     if (tm) tm->end(st);
     cudaStreamWaitEvent(st, side.join, 0);
+}
+
+// The point-gather pass 1 at the register budget the autotuner chose: 3
+// blocks of 256 a SM (80 registers a thread) or 4 (64 registers).
+template <class T, int IMASS, bool PAIR>
+static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, const LzSide& side,
+                         KernelTimer* tm) {
+    if (a.occ == 4) launch_pass1_occ<T, IMASS, PAIR, 4>(a, nb, st, side, tm);
+    else launch_pass1_occ<T, IMASS, PAIR, 3>(a, nb, st, side, tm);
 }
 
 // Row-staged pass 1 (same protocol: M, the scalar step on the side stream,
@@ -807,7 +818,7 @@ static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
 // use_rows), and their plan and grid.
 template <class T>
 static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb, cudaStream_t st) {
-    if (!use_rows(g, (int)sizeof(T), st)) return false;
+    if (stencil_choice(g, (int)sizeof(T), st) != kStencilRows) return false;
     if (!row_plan(g, sizeof(T), RowMaxThreads<T>::value, rp)) return false;
     const void* kern[6] = {(const void*)k_lz1_M_rows<T, 1>, (const void*)k_lz1_M_rows<T, 3>,
                            (const void*)k_lz1_Md_rows<T, 1, false>,
@@ -1001,13 +1012,21 @@ static void launch_pass2_any(const LzArgsT<T>& a, int j, int m, int iflag, cudaS
     else launch_pass2<T, 1, false>(a, j, m, iflag, st, tm);
 }
 
+template <class T, bool PAIR>
+static unsigned lz_pass1_blocks_occ(const Geom& g, int imass, int occ) {
+    if (occ == 4)
+        return imass == 3 ? lz_pass1_blocks<T, 3, PAIR, 4>(g.npts)
+                          : lz_pass1_blocks<T, 1, PAIR, 4>(g.npts);
+    return imass == 3 ? lz_pass1_blocks<T, 3, PAIR, 3>(g.npts)
+                      : lz_pass1_blocks<T, 1, PAIR, 3>(g.npts);
+}
+
 template <class T>
-static unsigned lz_pass1_blocks_any(const Geom& g, int imass) {
+static unsigned lz_pass1_blocks_any(const Geom& g, int imass, int occ) {
     if constexpr (std::is_same<T, float2>::value) {
-        if (lz_pair<T>(g))
-            return imass == 3 ? lz_pass1_blocks<T, 3, true>(g.npts) : lz_pass1_blocks<T, 1, true>(g.npts);
+        if (lz_pair<T>(g)) return lz_pass1_blocks_occ<T, true>(g, imass, occ);
     }
-    return imass == 3 ? lz_pass1_blocks<T, 3, false>(g.npts) : lz_pass1_blocks<T, 1, false>(g.npts);
+    return lz_pass1_blocks_occ<T, false>(g, imass, occ);
 }
 
 // ---- kernel timer ----------------------------------------------------------
@@ -1396,7 +1415,8 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.npole = ndiag;
     unsigned nb = 0;
     a.rows = lz_rows_setup<T>(g, &a.rp, &nb, st) ? 1 : 0;
-    if (!a.rows) nb = lz_pass1_blocks_any<T>(g, imass);
+    a.occ = stencil_choice(g, (int)sizeof(T), st) == kStencilGather4 ? 4 : 3;
+    if (!a.rows) nb = lz_pass1_blocks_any<T>(g, imass, a.occ);
     const int nbr = reduce_blocks(g.kferm);
     // r_1 lives where ring(a, 1) looks for it: the basis store when present
     T* r1 = a.hcap > 1 ? a.basis + g.kferm : a.rb1;

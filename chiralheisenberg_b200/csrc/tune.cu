@@ -1,17 +1,18 @@
 // tune.cu -- the autotuner of the stencil kernels.
 //
-// Two kernel shapes apply the domain-wall operator: the point-gather kernels
+// The domain-wall operator has three kernel shapes: the point-gather kernels
 // (dwf_stencil.cuh: one thread per point and flavour, every neighbour read
-// through L1/L2) and the row-staged kernels (row_stage.cuh: rows y-1..y+1
-// staged in shared memory by bulk copies).  Which is faster depends on the
-// lattice: the row kernels need a row of L*Ls points to fill a block and
-// several rows per block to amortise the two extra window rows.  On the
-// first use of a (L, Lt, Ls, element size) the tuner applies M both ways to
-// scratch vectors on the caller's stream -- 2 warm-up and 5 timed
-// applications each, CUDA events, L2 not flushed (both see the same cache
-// state) -- and keeps the faster.  The choice holds for the operator and
-// for the multi-shift solver's pass 1, which use the same stencil.  The
-// table is per process; chdwf_autotune_report prints it.
+// through L1/L2) at a register budget of 80 a thread (3 blocks of 256 a
+// SM) or 64 (4 blocks, more warps in flight, some spills), and the
+// row-staged kernels (row_stage.cuh: rows y-1..y+1 staged in shared memory
+// by bulk copies).  Which is fastest depends on the lattice and the
+// precision.  On the first use of a (L, Lt, Ls, element size) the tuner
+// applies M in every shape to scratch vectors on the caller's stream -- 2
+// warm-up and 5 timed applications each, CUDA events, L2 not flushed (all
+// see the same cache state) -- and keeps the fastest.  The choice holds for
+// the operator and for the multi-shift solver's pass 1, which use the same
+// stencil at the same budgets.  The table is per process;
+// chdwf_autotune_report prints it.
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -29,9 +30,12 @@ namespace {
 
 struct TuneEntry {
     int L, Lt, Ls, elem, device;
-    bool rows;
-    float us_rows, us_gather;
+    int choice;
+    float us[3];   // per shape (kStencil*), 0 when not timed
 };
+const char* shape_name(int k) {
+    return k == kStencilRows ? "rows" : (k == kStencilGather4 ? "gather4" : "gather3");
+}
 
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune;
@@ -73,32 +77,39 @@ float time_variant(const Geom& g, int elem, int v, void* out, const void* in, co
 
 }  // namespace
 
-bool use_rows(const Geom& g, int elem, cudaStream_t st) {
+int stencil_choice(const Geom& g, int elem, cudaStream_t st) {
     const int mode = stencil_mode();
-    if (mode == 1) return false;
     RowPlan rp;
-    if (!row_plan(g, (size_t)elem, max_threads_of(elem), &rp)) return false;
-    if (mode == 2) return true;
+    const bool rows_fit = row_plan(g, (size_t)elem, max_threads_of(elem), &rp);
+    if (mode == 1) return kStencilGather3;
+    if (mode == 2) return rows_fit ? kStencilRows : kStencilGather3;
     int dev = 0;
     cudaGetDevice(&dev);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         for (const TuneEntry& t : g_tune)
             if (t.L == g.L && t.Lt == g.Lt && t.Ls == g.Ls && t.elem == elem && t.device == dev)
-                return t.rows;
+                return t.choice;
     }
     // measure on scratch vectors (zeros: the same memory traffic)
     void *in = nullptr, *out = nullptr;
     float* chif = nullptr;
     const size_t bytes = (size_t)elem * g.kferm;
-    TuneEntry t{g.L, g.Lt, g.Ls, elem, dev, false, 0.0f, 0.0f};
+    TuneEntry t{g.L, g.Lt, g.Ls, elem, dev, kStencilGather3, {0.0f, 0.0f, 0.0f}};
     if (cudaMalloc(&in, bytes) == cudaSuccess && cudaMalloc(&out, bytes) == cudaSuccess &&
         cudaMalloc(&chif, sizeof(float) * 3 * (size_t)g.kvol) == cudaSuccess) {
         cudaMemsetAsync(in, 0, bytes, st);
         cudaMemsetAsync(chif, 0, sizeof(float) * 3 * (size_t)g.kvol, st);
-        t.us_rows = time_variant(g, elem, 1, out, in, chif, st);
-        t.us_gather = time_variant(g, elem, 0, out, in, chif, st);
-        t.rows = t.us_rows < t.us_gather;
+        float best = 0.0f;
+        for (int k : {kStencilGather3, kStencilGather4, kStencilRows}) {
+            if (k == kStencilRows && !rows_fit) continue;
+            if (k == kStencilGather4 && elem == 4) continue;   // one FP16 gather kernel
+            t.us[k] = time_variant(g, elem, k, out, in, chif, st);
+            if (best == 0.0f || t.us[k] < best) {
+                best = t.us[k];
+                t.choice = k;
+            }
+        }
     }
     cudaGetLastError();
     cudaFree(in);
@@ -106,7 +117,7 @@ bool use_rows(const Geom& g, int elem, cudaStream_t st) {
     cudaFree(chif);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune.push_back(t);
-    return t.rows;
+    return t.choice;
 }
 
 }  // namespace chdwf
@@ -121,9 +132,10 @@ extern "C" int chdwf_autotune_report(char* buf, int cap) {
             char line[256];
             snprintf(line, sizeof(line),
                      "%s{\"L\": %d, \"Lt\": %d, \"Ls\": %d, \"elem_bytes\": %d, \"device\": %d, "
-                     "\"rows_us\": %.2f, \"gather_us\": %.2f, \"choice\": \"%s\"}",
-                     i ? ", " : "", t.L, t.Lt, t.Ls, t.elem, t.device, t.us_rows, t.us_gather,
-                     t.rows ? "rows" : "gather");
+                     "\"gather3_us\": %.2f, \"gather4_us\": %.2f, \"rows_us\": %.2f, "
+                     "\"choice\": \"%s\"}",
+                     i ? ", " : "", t.L, t.Lt, t.Ls, t.elem, t.device, t.us[kStencilGather3],
+                     t.us[kStencilGather4], t.us[kStencilRows], shape_name(t.choice));
             s += line;
         }
     }

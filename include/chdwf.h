@@ -258,9 +258,11 @@ int chdwf_traj_noise_solve(chdwf_ctx* ctx, const float* eta, int swall, int idir
 
 /* The stencil autotuner's choices so far in this process (no reference
  * counterpart): a JSON array with one entry per (lattice, element size) of
- * the median microseconds of the row-staged and the point-gather operator
- * and the kernel chosen.  Writes at most cap bytes (NUL-terminated) and
- * returns the length the full text needs, including the NUL. */
+ * the median microseconds of the operator in each kernel shape (the
+ * point-gather kernels at 3 or 4 blocks a SM, the row-staged kernels; 0 when
+ * a shape does not apply) and the shape chosen.  Writes at most cap bytes
+ * (NUL-terminated) and returns the length the full text needs, including
+ * the NUL. */
 int chdwf_autotune_report(char* buf, int cap);
 
 /* ---- per-shift multi-shift solutions --------------------------------------
