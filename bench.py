@@ -98,8 +98,8 @@ def parse():
     ap.add_argument("--profile-res", type=float, default=0.0,
                     help="stopping residual of both profiled solves (0: the reference's)")
     ap.add_argument("--basis-gb", type=float, default=-1.0,
-                    help="HBM budget of the stored Lanczos basis per vector precision (GB; "
-                         "<0: 60 GB in the timed runs, the library default elsewhere)")
+                    help="HBM budget of the stored FP64 Lanczos basis, FP32 half of it (GB; "
+                         "<0: 80 GB in the timed runs, the library default elsewhere)")
     ap.add_argument("--profile-operator", default="",
                     choices=["", "f64", "f32", "f16"],
                     help="bounded work for profilers: 5 applications of M at --L/--Ls in the "
@@ -660,10 +660,10 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     L, Ls = args.L, args.Ls
     prog, start = make_program(L, Ls, local_rank, rank)
-    # the basis store of each vector precision (FP32 and FP64 solves run in
-    # the same program): a fixed budget each, so the FP64 arm is not left
-    # with what the FP32 arm did not take
-    prog.set_basis_store((args.basis_gb if args.basis_gb >= 0 else 60.0) * 1e9)
+    # the basis stores (FP32 and FP64 solves run in the same program): 80 GB
+    # of FP64 vectors (1880 at 24^3x24) and as many FP32 ones, so neither arm
+    # is left with what the other did not take
+    prog.set_basis_store((args.basis_gb if args.basis_gb >= 0 else 80.0) * 1e9)
     prog.set_precision(md="f32", accept="f64")
     stream = torch.cuda.ExternalStream(prog.stream, device=local_rank)
 

@@ -1167,7 +1167,11 @@ cudaError_t LzWork::ensure(const Geom& g, int npole_max, int prec, bool walls) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         const size_t vb = (prec == kPrecF64 ? sizeof(double2) : sizeof(float2)) * (size_t)g.kferm;
-        const double budget = basis_max_bytes >= 0.0 ? basis_max_bytes : 0.4 * (double)fr;
+        // an explicit budget names the FP64 store; the FP32 store keeps the
+        // same number of vectors in half the bytes
+        const double budget = basis_max_bytes >= 0.0
+                                  ? basis_max_bytes * (prec == kPrecF64 ? 1.0 : 0.5)
+                                  : 0.4 * (double)fr;
         int64_t cap = (int64_t)(budget / (double)vb);
         if (cap > kMaxIter + 2) cap = kMaxIter + 2;
         if (cap >= 8) {

@@ -81,8 +81,9 @@ int chdwf_set_precision(chdwf_ctx* ctx, int md, int accept);
  * precision (no reference counterpart).  A solve whose iterations fit keeps
  * every Lanczos vector and forms its solution in one pass over them; longer
  * solves regenerate the vectors instead (same results, twice the operator
- * applications).  max_bytes < 0: 40% of the free HBM at the first solve
- * (default); 0: no store. */
+ * applications).  max_bytes: the FP64 store; the FP32 store keeps as many
+ * vectors in half the bytes.  max_bytes < 0: 40% of the free HBM at the
+ * first solve of each precision (default); 0: no store. */
 int chdwf_set_basis_store(chdwf_ctx* ctx, double max_bytes);
 /* the context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the library's */
