@@ -85,7 +85,7 @@ def parse():
     ap.add_argument("--no-refalg", action="store_true")
     ap.add_argument("--refalg-steps", type=int, default=3)
     ap.add_argument("--no-propagators", action="store_true")
-    ap.add_argument("--cpu-sample-iters", type=int, default=6)
+    ap.add_argument("--cpu-sample-iters", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--clock-interval-ms", type=int, default=200,
                     help="nvidia-smi sampling interval during the timed region")
@@ -236,28 +236,32 @@ def cpu_iteration_cost(L, Ls, threads, iters, npole=20):
     shape = (2, 4, L, L, L, Ls)
     Phi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
     chi = synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"])
-    # the difference of a 2k- and a k-iteration run: set-up (allocation of the
-    # pole vectors, thread start-up) cancels
+    # the difference of a 2k- and a k-iteration run gives the cost of an
+    # iteration; what is left of the k-iteration run is the set-up of a solve
+    # (allocating and touching the pole vectors, thread start-up)
     t0 = time.perf_counter()
     po.qmrherm(lat, Phi, chi, act[0], act[1], 1e-30, niterc=iters)
     t1 = time.perf_counter()
     po.qmrherm(lat, Phi, chi, act[0], act[1], 1e-30, niterc=2 * iters)
     t2 = time.perf_counter()
     t_iter = max((t2 - t1) - (t1 - t0), 1e-9) / iters
+    t_setup = max((t1 - t0) - iters * t_iter, 0.0)
     t0 = time.perf_counter()
     for _ in range(2):
         po.dslash(lat, Phi, chi)
     t_apply = (time.perf_counter() - t0) / 2
-    return t_iter, t_apply
+    return t_iter, t_apply, t_setup
 
 
-def cpu_model(profile, t_iter, t_apply, npole=20):
-    """Oracle seconds per trajectory: every solver iteration at t_iter, plus
-    the force tail of each force solve (one operator apply and derivs per
-    pole, rhmc/cheisdwf.f:733-740, counted as one apply)."""
+def cpu_model(profile, t_iter, t_apply, t_setup, npole=20):
+    """Oracle seconds per trajectory: every solver iteration at t_iter, the
+    set-up of every solve, and the force tail of each force solve (one
+    operator apply and derivs per pole, rhmc/cheisdwf.f:733-740, counted as
+    one apply)."""
     its = profile["it_pf"] + profile["it_h0"] + profile["it_h1"] + profile["it_force"]
     nsolve_force = profile["nforce"] * EXT["npf"]
-    return its * t_iter + nsolve_force * npole * t_apply, its
+    nsolve = nsolve_force + 3 * EXT["npf"]       # + heatbath and two actions per field
+    return its * t_iter + nsolve * t_setup + nsolve_force * npole * t_apply, its
 
 
 def profile_of(recs):
@@ -452,8 +456,9 @@ def run_reference(args, rank, world):
     vals, walls = [], []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        t_iter, t_apply = cpu_iteration_cost(args.L, args.Ls, threads, args.cpu_sample_iters)
-        s, its = cpu_model(profile, t_iter, t_apply)
+        t_iter, t_apply, t_setup = cpu_iteration_cost(args.L, args.Ls, threads,
+                                                      args.cpu_sample_iters)
+        s, its = cpu_model(profile, t_iter, t_apply, t_setup)
         if step >= args.warmup:
             vals.append((s, t_iter))
             walls.append(time.perf_counter() - t0)
@@ -588,16 +593,16 @@ def run_validate_cpu_model(args):
     rng = np.random.default_rng(11)
     shape = (2, 4, L, L, L, Ls)
     Phi = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * np.sqrt(0.5)
-    t_iter, t_apply = cpu_iteration_cost(L, Ls, threads, args.cpu_sample_iters)
+    t_iter, t_apply, t_setup = cpu_iteration_cost(L, Ls, threads, args.cpu_sample_iters)
     dS = np.zeros((3, L ** 3), np.float32)
     t0 = time.perf_counter()
     _, its, st, _ = po.qmrherm(lat, Phi, chi, act[0], act[1], 1e-6, iflag=1, dSdchi=dS)
     t_full = time.perf_counter() - t0
-    model = its * t_iter + 20 * t_apply
+    model = t_setup + its * t_iter + 20 * t_apply
     print(json.dumps({"validate_cpu_model": f"L=Lt={L} Ls={Ls}", "threads": threads,
                       "iterations": its, "status": st, "measured_s": t_full, "model_s": model,
                       "model_over_measured": model / t_full, "t_iter_s": t_iter,
-                      "t_apply_s": t_apply}), flush=True)
+                      "t_setup_s": t_setup, "t_apply_s": t_apply}), flush=True)
 
 
 def timed_run(prog, stream, steps, staged, barrier, world, local_rank):
@@ -772,8 +777,8 @@ def run_b200(args, rank, world, local_rank):
         line["propagators"] = bench_propagators(local_rank)
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t_iter, t_apply = cpu_iteration_cost(L, Ls, threads, args.cpu_sample_iters)
-        s_cpu, _ = cpu_model(prof64 or prof, t_iter, t_apply)
+        t_iter, t_apply, t_setup = cpu_iteration_cost(L, Ls, threads, args.cpu_sample_iters)
+        s_cpu, _ = cpu_model(prof64 or prof, t_iter, t_apply, t_setup)
         line["cpu_baseline"] = {
             "value": s_cpu, "unit": "s", "cores": threads, "kind": "port", "modelled": True,
             "ms_per_1000_iterations": t_iter * 1e6,
