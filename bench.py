@@ -746,6 +746,7 @@ def run_b200(args, rank, world, local_rank):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic_24x24.json")
     if os.path.exists(tp):
+        # ncu figures are per stencil shape; another shape's traffic is unknown
         traffic = json.load(open(tp)).get(kernel_name(dom, rows_chosen(L, Ls, dom)))
     prof = profile_of(recs)
     its_value = sum(prof[k] for k in ("it_pf", "it_h0", "it_h1", "it_force"))

@@ -66,7 +66,7 @@ EXPORTS = (
     "chdwf_format_list", "chdwf_format_edit", "chdwf_run_dir",
     "chdwf_ext_set_remez", "chdwf_ext_select_pf", "chdwf_ext_heatbath_dev", "chdwf_ext_action",
     "chdwf_ext_force", "chdwf_ext_bosonic", "chdwf_prog_set_ext", "chdwf_multishift_dev",
-    "chdwf_autotune_report", "chdwf_traj_propagators",
+    "chdwf_autotune_report", "chdwf_traj_propagators", "chdwf_stencil_launches",
 )
 
 _lib = None
@@ -216,6 +216,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_prog_set_ext.argtypes = [P, I, I, I, F]
     L.chdwf_multishift_dev.argtypes = [P, P, F, P, F, I, I, P, P, P, I, PI, PI]
     L.chdwf_autotune_report.argtypes = [C.c_char_p, I]
+    L.chdwf_stencil_launches.argtypes = [P]
     L.chdwf_traj_propagators.argtypes = [P, I, P, P, F, F, F, I, P, P]
     _lib = L
     return L
@@ -691,6 +692,16 @@ def version() -> str:
 def kernel_launches() -> int:
     """Kernels libchdwf has launched in this process."""
     return int(load_library().chdwf_kernel_launches())
+
+
+def stencil_launches() -> dict:
+    """Operator and pass-1 stencil launches in this process by kernel shape
+    (chdwf_stencil_launches): {"gather3": n, "rows": n, "gather4": n}."""
+    buf = (C.c_longlong * 3)()
+    rc = load_library().chdwf_stencil_launches(buf)
+    if rc != CHDWF_OK:
+        raise ChdwfError(rc, "stencil_launches")
+    return {"gather3": int(buf[0]), "rows": int(buf[1]), "gather4": int(buf[2])}
 
 
 DATA_DIR = os.path.join(_HERE, "data")

@@ -92,6 +92,12 @@ int chdwf_timing(chdwf_ctx* ctx, int enable) {
 
 long long chdwf_kernel_launches(void) { return launches_total(); }
 
+int chdwf_stencil_launches(long long* counts) {
+    if (!counts) return CHDWF_BAD_ARG;
+    for (int k = 0; k < 3; k++) counts[k] = stencil_launches(k);
+    return CHDWF_OK;
+}
+
 int chdwf_set_precision(chdwf_ctx* ctx, int md, int accept) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (!c || md < 0 || md > 1 || accept < 0 || accept > 1) return CHDWF_BAD_ARG;

@@ -10,6 +10,14 @@ static std::atomic<long long> g_launches{0};
 void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
+static std::atomic<long long> g_stencil[3];
+void note_stencil(int shape, long long n) {
+    if (shape >= 0 && shape < 3) g_stencil[shape].fetch_add(n, std::memory_order_relaxed);
+}
+long long stencil_launches(int shape) {
+    return shape >= 0 && shape < 3 ? g_stencil[shape].load(std::memory_order_relaxed) : 0;
+}
+
 __global__ void k_round_chi(const double* __restrict__ chi, float* __restrict__ chif, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) chif[i] = (float)chi[i];

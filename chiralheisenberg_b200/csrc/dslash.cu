@@ -52,25 +52,16 @@ struct OpRows {
     int Lrow;
     Real diag, hpin;
     int apbc;
-    T tp[4], tm[4];
     RowWall<T> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
-        const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
-        const int64_t i = (int64_t)x * g.Ls + s;
-        const int64_t ep = i + (int64_t)Lrow * (y + (int64_t)g.L * tpi);
-        const int64_t em = i + (int64_t)Lrow * (y + (int64_t)g.L * tmi);
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-            tp[d] = RowCvt<T, S>::get(__ldg(in + ep + g.cs * (d + 4 * f)));
-            tm[d] = RowCvt<T, S>::get(__ldg(in + em + g.cs * (d + 4 * f)));
-        }
         row_wall_prefetch<DAG>(rw, in, g, f, t, y, x, s, chif);
     }
-    __device__ __forceinline__ void compute(const S* c, const S* yp, const S* ym, int f, int t,
-                                            int y, int x, int s, int i, int ixp, int ixm) {
+    __device__ __forceinline__ void compute(const S* c, const S* yp, const S* ym, const S* tps,
+                                            const S* tms, int f, int t, int y, int x, int s,
+                                            int i, int ixp, int ixm) {
         const PointIdx q = row_point(g, t, y, x, s);
         T acc[4];
-        dwf_apply_rows<DAG, IMASS>(acc, c, yp, ym, Lrow, i, ixp, ixm, tp, tm, rw, g, q, f, diag,
+        dwf_apply_rows<DAG, IMASS>(acc, c, yp, ym, tps, tms, Lrow, i, ixp, ixm, rw, g, q, f, diag,
                                    hpin, apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) out[q.p + g.cs * (d + 4 * f)] = row_store(acc[d], out);
@@ -155,6 +146,14 @@ static bool launch_op_rows_any(bool dag, int imass, S* out, const S* in, const f
                       : launch_op_rows<S, T, true, 3>(out, in, chif, g, diag, hpin, apbc, st);
 }
 
+bool op_rows_launchable(const Geom& g, int elem) {
+    RowPlan rp;
+    unsigned nb = 0;
+    if (elem == 16) return op_rows_setup<double2, double2, false, 1>(g, &rp, &nb);
+    if (elem == 8) return op_rows_setup<float2, float2, false, 1>(g, &rp, &nb);
+    return op_rows_setup<__half2, float2, false, 1>(g, &rp, &nb);
+}
+
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,
                      const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
                      int variant) {
@@ -163,8 +162,11 @@ void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const
     const int apbc = ibound == -1;
     const int shape = variant < 0 ? stencil_choice(g, 16, st) : variant;
     if (shape == kStencilRows &&
-        launch_op_rows_any<double2, double2>(dag, imass, out, in, chif, g, diag, hp, apbc, st))
+        launch_op_rows_any<double2, double2>(dag, imass, out, in, chif, g, diag, hp, apbc, st)) {
+        note_stencil(kStencilRows, 1);
         return;
+    }
+    note_stencil(shape == kStencilGather4 ? kStencilGather4 : kStencilGather3, 1);
 #define LAUNCH(D, I)                                                                          \
     do {                                                                                      \
         if (shape == kStencilGather4)                                                         \
@@ -249,9 +251,12 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
                                                        apbc, st)
                  : launch_op_rows_any<float2, float2>(dag, imass, (float2*)out,
                                                       (const float2*)in, chif, g, diag, hpin,
-                                                      apbc, st))
+                                                      apbc, st)) {
+            note_stencil(kStencilRows, 1);
             return;
+        }
     }
+    note_stencil(shape == kStencilGather4 && !half ? kStencilGather4 : kStencilGather3, 1);
     if (!half && g.Ls % 2 == 0) {
         const unsigned nb2 = (unsigned)((g.npts + 2 * kSplitPoints - 1) / (2 * kSplitPoints));
         const float diag = diag_of(am3);

@@ -15,6 +15,10 @@ namespace chdwf {
 // chdwf_kernel_launches().
 void count_launches(long long n);
 long long launches_total();
+// Operator and pass-1 stencil launches by kernel shape (kStencil*), read
+// through chdwf_stencil_launches().
+void note_stencil(int shape, long long n);
+long long stencil_launches(int shape);
 
 constexpr int kMaxPoles = 32;
 constexpr int kMaxIter = 5000;     // niterc of qmrherm (rhmc/cheisdwf.f:603)
@@ -75,6 +79,10 @@ constexpr int kStencilGather3 = 0, kStencilRows = 1, kStencilGather4 = 2;
 // vectors on stream st and keeps the fastest; "legacy" forces the
 // point-gather kernels at 3 blocks a SM, "rows" the row-staged ones.
 int stencil_choice(const Geom& g, int elem, cudaStream_t st);
+// Whether the row-staged operator of this element size (16 FP64, 8 FP32,
+// 4 FP16 storage) can launch on this lattice and device: its rows fit the
+// shared memory and a block fits an SM.
+bool op_rows_launchable(const Geom& g, int elem);
 
 // Wall-slice operator for npole stacked two-slice fields (s'=0 <-> s=1,
 // s'=1 <-> s=Ls): computes M on the Ls=2 lattice of each pole.

@@ -414,27 +414,18 @@ struct LzRowsM {
     const T* rj;
     Real ib;
     double loc;
-    T tp[4], tm[4];
     RowWall<T> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
-        const Geom& g = a.g;
-        const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
-        const int64_t i = (int64_t)x * g.Ls + s, Lrow = (int64_t)g.L * g.Ls;
-        const int64_t ep = i + Lrow * (y + (int64_t)g.L * tpi), em = i + Lrow * (y + (int64_t)g.L * tmi);
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-            tp[d] = __ldg(rj + ep + g.cs * (d + 4 * f));
-            tm[d] = __ldg(rj + em + g.cs * (d + 4 * f));
-        }
-        row_wall_prefetch<false>(rw, rj, g, f, t, y, x, s, a.chif);
+        row_wall_prefetch<false>(rw, rj, a.g, f, t, y, x, s, a.chif);
     }
-    __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, int f, int t,
-                                            int y, int x, int s, int i, int ixp, int ixm) {
+    __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, const T* tps,
+                                            const T* tms, int f, int t, int y, int x, int s,
+                                            int i, int ixp, int ixm) {
         const Geom& g = a.g;
         const PointIdx q = row_point(g, t, y, x, s);
         T acc[4];
-        dwf_apply_rows<false, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, rw, g, q, f,
-                                     a.diag, a.hpin, a.apbc != 0);
+        dwf_apply_rows<false, IMASS>(acc, c, yp, ym, tps, tms, a.rp.Lrow, i, ixp, ixm, rw, g, q,
+                                     f, a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             acc[d] = zscal(ib, acc[d]);
@@ -481,30 +472,27 @@ struct LzRowsMd {
     int j;
     Real ib, at, bj, ibm;
     double loc;
-    T tp[4], tm[4], cj[4], cm[4];
+    T cj[4], cm[4];
     RowWall<T> rw;
+    // q_j and q_{j-1} at the point (streamed, not staged) and the wall operands
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
         const Geom& g = a.g;
-        const int tpi = t + 1 == g.Lt ? 0 : t + 1, tmi = t == 0 ? g.Lt - 1 : t - 1;
-        const int64_t i = (int64_t)x * g.Ls + s, Lrow = (int64_t)g.L * g.Ls;
-        const int64_t e0 = i + Lrow * (y + (int64_t)g.L * t);
-        const int64_t ep = i + Lrow * (y + (int64_t)g.L * tpi), em = i + Lrow * (y + (int64_t)g.L * tmi);
+        const int64_t e0 = (int64_t)x * g.Ls + s + (int64_t)g.L * g.Ls * (y + (int64_t)g.L * t);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             const int64_t po = g.cs * (d + 4 * f);
-            tp[d] = __ldg(a.vt + ep + po);
-            tm[d] = __ldg(a.vt + em + po);
             cj[d] = rj[e0 + po];
             if (j > 1) cm[d] = rjm[e0 + po];
         }
         row_wall_prefetch<true>(rw, a.vt, g, f, t, y, x, s, a.chif);
     }
-    __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, int f, int t,
-                                            int y, int x, int s, int i, int ixp, int ixm) {
+    __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, const T* tps,
+                                            const T* tms, int f, int t, int y, int x, int s,
+                                            int i, int ixp, int ixm) {
         const Geom& g = a.g;
         const PointIdx q = row_point(g, t, y, x, s);
         T acc[4];
-        dwf_apply_rows<true, IMASS>(acc, c, yp, ym, a.rp.Lrow, i, ixp, ixm, tp, tm, rw, g, q, f,
+        dwf_apply_rows<true, IMASS>(acc, c, yp, ym, tps, tms, a.rp.Lrow, i, ixp, ixm, rw, g, q, f,
                                     a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
@@ -971,6 +959,11 @@ static void launch_pass2(const LzArgsT<T>& a, int j, int m, int iflag, cudaStrea
         tm.end(st);
         count_launches(1);
     }
+}
+
+template <class T>
+static int pass1_shape(const LzArgsT<T>& a) {
+    return a.rows ? kStencilRows : (a.occ == 4 ? kStencilGather4 : kStencilGather3);
 }
 
 // Shape dispatch: FP32 vectors with Ls even take the two-point kernels.
@@ -1453,10 +1446,12 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
             cudaGraphLaunch(gexec, st);
             launched += chunk;
             count_launches(3 * chunk);
+            note_stencil(pass1_shape(a), 2 * chunk);
         } else {
             for (int c = 0; c < chunk && launched < kMaxIter; c++, launched++) {
                 launch_pass1_any<T>(a, nb, st, w.side, &w.timer, imass);
                 count_launches(3);
+                note_stencil(pass1_shape(a), 2);
             }
         }
         cudaEventRecord(ev[nchunk % (kAhead + 1)], st);

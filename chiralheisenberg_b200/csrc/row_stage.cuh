@@ -5,22 +5,25 @@
 // contiguous run of L*Ls elements per plane.  A block walks a contiguous
 // range of output rows rho = (f*Lt + t)*L + y of one flavour f.  For output
 // row (f, t, y) the four Dirac planes of flavour f on rows y-1, y, y+1 (same
-// t) are held in shared memory: they serve the diagonal term, the x hops,
-// the y hops and the s hops.  The t hops read rows (y, t+-1) straight from
-// global memory (L2), issued before the block waits for its shared rows, and
-// the wall terms read the other flavour at the other wall from global memory
-// as well (2 of every Ls points).
+// t) and on rows t-1, t+1 (same y) are held in shared memory: they serve the
+// diagonal term and the x, y, t and s hops.  Only the wall terms read
+// global memory (the other flavour at the other wall, 2 of every Ls points,
+// and chi), issued one output row ahead.
 //
 // Rows reach shared memory by 1-D bulk copies (cp.async.bulk, the TMA
-// engine's untiled form, this GPU's own memory only, no multicast) into a
-// ring of kRowSlots slots, one mbarrier per slot.  The window rows of a
-// block are loaded in order: for each maximal run of output rows with the
-// same (f, t), rows y_a-1, y_a, ..., y_b (mod L), i.e. run length + 2 loads.
-// Output row k of a run needs loads u, u+1, u+2 (u = run base + k); after it
-// the slot of load u is free and load u + kRowSlots is issued into it, so
-// up to kRowSlots - 3 rows are in flight ahead of the computation.  Load w
-// is the (w / kRowSlots)-th use of slot w % kRowSlots, so its wait parity is
-// (w / kRowSlots) & 1.
+// engine's untiled form, this GPU's own memory only, no multicast) into two
+// rings with one mbarrier per entry:
+//   * the window ring of kRowSlots rows along y.  The window rows of a block
+//     are loaded in order: for each maximal run of output rows with the same
+//     (f, t), rows y_a-1, y_a, ..., y_b (mod L), i.e. run length + 2 loads.
+//     Output row k of a run needs loads u, u+1, u+2 (u = run base + k);
+//     after it the slot of load u is free and load u + kRowSlots is issued
+//     into it, so up to kRowSlots - 3 rows are in flight ahead of the
+//     computation.  Load w is the (w / kRowSlots)-th use of slot
+//     w % kRowSlots, so its wait parity is (w / kRowSlots) & 1;
+//   * the t ring of kRowTEnt entries, entry k holding rows (t+1, y) and
+//     (t-1, y) of the block's k-th output row; after output row k, entry
+//     k + kRowTEnt is issued into its slot (parity (k / kRowTEnt) & 1).
 //
 // Every wait is bounded (kRowWaitNs); a block whose copy does not arrive in
 // time records an error and leaves the loop with the others at the next
@@ -35,19 +38,26 @@
 
 namespace chdwf {
 
-constexpr int kRowSlots = 5;
+constexpr int kRowSlots = 5;                      // window ring (rows along y)
+constexpr int kRowTEnt = 3;                       // t ring entries (two rows each)
 constexpr uint64_t kRowWaitNs = 1000000000ull;   // 1 s per wait
 constexpr unsigned kRowBarBytes = 128;            // mbarriers at the front of shared memory
 constexpr unsigned kRowSmemMax = 227 * 1024;
 
 // Block size limit (one thread per point of a row) and the register budget
-// that lets one such block of the largest size run on an SM.
+// that lets one such block of the largest size run on an SM: a block's warps
+// are spread over the SM's four sub-partitions, each with a quarter of the
+// register file (16384), so ceil(warps / 4) * 32 * registers <= 16384.
 template <class T> struct RowMaxThreads;
-template <> struct RowMaxThreads<double2> { static constexpr int value = 576; };
+template <> struct RowMaxThreads<double2> { static constexpr int value = 512; };
 template <> struct RowMaxThreads<float2> { static constexpr int value = 768; };
 template <class T> struct RowRegs;
 template <> struct RowRegs<double2> { static constexpr int value = 112; };
 template <> struct RowRegs<float2> { static constexpr int value = 80; };
+static_assert((RowMaxThreads<double2>::value / 32 + 3) / 4 * 32 * RowRegs<double2>::value <= 16384,
+              "FP64 row block does not fit a sub-partition's registers");
+static_assert((RowMaxThreads<float2>::value / 32 + 3) / 4 * 32 * RowRegs<float2>::value <= 16384,
+              "FP32 row block does not fit a sub-partition's registers");
 
 // Which stencil kernels run, from the environment variable CHDWF_STENCIL:
 // 0 (unset): the autotuner's choice per lattice and precision (tune.cu);
@@ -77,7 +87,8 @@ inline bool row_plan(const Geom& g, size_t elem, int max_threads, RowPlan* p) {
     if ((Lrow * (int64_t)elem) % 16 != 0) return false;
     const int64_t nthreads = (Lrow + 31) / 32 * 32;
     if (nthreads > max_threads) return false;
-    const int64_t smem = kRowBarBytes + (int64_t)kRowSlots * 4 * Lrow * (int64_t)elem;
+    const int64_t smem =
+        kRowBarBytes + (int64_t)(kRowSlots + 2 * kRowTEnt) * 4 * Lrow * (int64_t)elem;
     if (smem > kRowSmemMax) return false;
     p->Lrow = (int)Lrow;
     p->nrows = 2 * g.Lt * g.L;
@@ -170,20 +181,25 @@ __device__ __forceinline__ double sum_partials_any(const double* part, int n) {
     return total;
 }
 
-// ---- the ring of staged rows ---------------------------------------------------
+// ---- the rings of staged rows -------------------------------------------------
 template <class T>
 struct RowRing {
-    uint64_t* bar;      // kRowSlots mbarriers
+    uint64_t* bar;      // kRowSlots window mbarriers, then kRowTEnt t-ring mbarriers
     T* slots;           // kRowSlots x 4 planes x Lrow
+    T* tslots;          // kRowTEnt x 8 planes x Lrow (t+1 rows, then t-1 rows)
     int Lrow, L, Lt;
     int64_t cs;         // plane stride (elements)
     // producer cursor (thread 0): run start, run length, offset in the run
     int p_rho_a, p_len, p_o;
-    int rho1;
-    int issued;         // loads issued so far
+    int rho0, rho1;
+    int issued;         // window loads issued so far
+    int t_issued;       // t-ring entries issued so far
 
     __device__ __forceinline__ T* slot(int w) const {
         return slots + (int64_t)(w % kRowSlots) * 4 * Lrow;
+    }
+    __device__ __forceinline__ T* tslot(int k) const {
+        return tslots + (int64_t)(k % kRowTEnt) * 8 * Lrow;
     }
     __device__ __forceinline__ int run_len_from(int rho_a) const {
         const int end = (rho_a / L + 1) * L;
@@ -213,6 +229,27 @@ struct RowRing {
         }
     }
     __device__ __forceinline__ bool more() const { return p_rho_a < rho1; }
+    // thread 0: issue t-ring entry t_issued, rows (t+1, y), (t-1, y) of the
+    // block's output row rho0 + t_issued
+    __device__ __forceinline__ void issue_t(const T* src) {
+        const int k = t_issued;
+        const int rho = rho0 + k;
+        const int run = rho / L;
+        const int f = run / Lt, t = run - f * Lt, y = rho - run * L;
+        const int tp = t + 1 == Lt ? 0 : t + 1, tm = t == 0 ? Lt - 1 : t - 1;
+        uint64_t* b = bar + kRowSlots + (k % kRowTEnt);
+        const uint32_t bytes = (uint32_t)(Lrow * sizeof(T));
+        mbar_arrive_expect_tx(b, 8 * bytes);
+        T* dst = tslot(k);
+        const int64_t op = (int64_t)Lrow * (y + (int64_t)L * tp);
+        const int64_t om = (int64_t)Lrow * (y + (int64_t)L * tm);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            bulk_g2s(dst + (int64_t)d * Lrow, src + cs * (4 * f + d) + op, bytes, b);
+            bulk_g2s(dst + (int64_t)(4 + d) * Lrow, src + cs * (4 * f + d) + om, bytes, b);
+        }
+        t_issued++;
+    }
 };
 
 // The block's contiguous range of output rows.
@@ -262,13 +299,13 @@ __device__ __forceinline__ void row_wall_prefetch(RowWall<T>& rw, const S* __res
 
 // The four Dirac components of flavour f at one output point of a staged
 // row, with the same operation sequence as dwf_apply_flavour (so the FP64
-// result is bit-identical to it).  c, yp, ym: shared rows y, y+1, y-1 (plane
-// stride Lrow, storage type S); i = x*Ls + s; ixp, ixm: the x+-1 points of
-// the row; tp, tm: the t+-1 neighbours and rw the wall operands (registers).
+// result is bit-identical to it).  c, yp, ym: shared rows y, y+1, y-1; tps,
+// tms: shared rows t+1, t-1 (plane stride Lrow, storage type S); i = x*Ls + s;
+// ixp, ixm: the x+-1 points of the row; rw: the wall operands (registers).
 template <bool DAG, int IMASS, class T, class S>
 __device__ __forceinline__ void dwf_apply_rows(T acc[4], const S* c, const S* yp, const S* ym,
-                                               int Lrow, int i, int ixp, int ixm, const T tp[4],
-                                               const T tm[4], const RowWall<T>& rw,
+                                               const S* tps, const S* tms, int Lrow, int i,
+                                               int ixp, int ixm, const RowWall<T>& rw,
                                                const Geom& g, const PointIdx& q, int f,
                                                typename real_of<T>::type diag,
                                                typename real_of<T>::type hpin, bool apbc) {
@@ -292,15 +329,25 @@ __device__ __forceinline__ void dwf_apply_rows(T acc[4], const S* c, const S* yp
 #pragma unroll
     for (int d = 0; d < 4; d++) r[d] = C::get(ym[d * Lrow + i]);
     hop<1, -SF, false>(acc, r);
-    hop<2, SF, false>(acc, tp);
-    hop<2, -SF, false>(acc, tm);
+#pragma unroll
+    for (int d = 0; d < 4; d++) r[d] = C::get(tps[d * Lrow + i]);
+    hop<2, SF, false>(acc, r);
+#pragma unroll
+    for (int d = 0; d < 4; d++) r[d] = C::get(tms[d * Lrow + i]);
+    hop<2, -SF, false>(acc, r);
     // kappa = 1/2 (:2815-2829)
 #pragma unroll
     for (int d = 0; d < 4; d++) acc[d] = zscal((R)0.5, acc[d]);
     // antiperiodic boundary in t (:2831-2876): reverse the wrapped hop
-    if (apbc) {
-        if (q.it == g.Lt - 1) hop<2, SF, true>(acc, tp);
-        if (q.it == 0) hop<2, -SF, true>(acc, tm);
+    if (apbc && q.it == g.Lt - 1) {
+#pragma unroll
+        for (int d = 0; d < 4; d++) r[d] = C::get(tps[d * Lrow + i]);
+        hop<2, SF, true>(acc, r);
+    }
+    if (apbc && q.it == 0) {
+#pragma unroll
+        for (int d = 0; d < 4; d++) r[d] = C::get(tms[d * Lrow + i]);
+        hop<2, -SF, true>(acc, r);
     }
     // s hops with chiral projection (:2879-2908; M^dagger :3313-3342)
     constexpr int UP = DAG ? 0 : 2;
@@ -349,11 +396,14 @@ __device__ __forceinline__ PointIdx row_point(const Geom& g, int t, int y, int x
     return q;
 }
 
-// The loop over a block's rows.  Body::pre(f, t, y, x, s) issues the
-// point's global loads (before the block waits for its staged rows);
-// Body::compute(c, yp, ym, f, t, y, x, s, i, ixp, ixm) evaluates the point
-// from the staged rows y, y+1, y-1.  T is the storage type of the staged
-// field src.  Returns false if a copy timed out.
+// The loop over a block's rows.  Body::pre(f, t, y, x, s) issues the global
+// loads a point needs besides the staged rows (wall operands, streamed
+// vectors); it runs for the first row before the first wait and for row k+1
+// right after row k is computed, so those loads are in flight while the
+// block synchronises and waits.  Body::compute(c, yp, ym, tp, tm, f, t, y,
+// x, s, i, ixp, ixm) evaluates the point from the staged rows y, y+1, y-1
+// and t+1, t-1.  T is the storage type of the staged field src.  Returns
+// false if a copy timed out.
 template <class T, class Body>
 __device__ __forceinline__ bool row_sweep(const Geom& g, const RowPlan& rp, unsigned char* sm,
                                           const T* src, Body& body) {
@@ -365,24 +415,33 @@ __device__ __forceinline__ bool row_sweep(const Geom& g, const RowPlan& rp, unsi
     RowRing<T> rr;
     rr.bar = bar;
     rr.slots = slots;
+    rr.tslots = slots + (int64_t)kRowSlots * 4 * rp.Lrow;
     rr.Lrow = rp.Lrow;
     rr.L = g.L;
     rr.Lt = g.Lt;
     rr.cs = g.cs;
+    rr.rho0 = rho0;
     rr.rho1 = rho1;
     rr.issued = 0;
+    rr.t_issued = 0;
     rr.p_rho_a = rho0;
     rr.p_o = 0;
     rr.p_len = rho0 < rho1 ? rr.run_len_from(rho0) : 0;
     if (threadIdx.x == 0) {
         s_err = 0;
-        for (int k = 0; k < kRowSlots; k++) mbar_init(bar + k, 1);
+        for (int k = 0; k < kRowSlots + kRowTEnt; k++) mbar_init(bar + k, 1);
         fence_mbar_init();
     }
     __syncthreads();
     if (rho0 >= rho1) return true;
-    if (threadIdx.x == 0)
+    const int nk = rho1 - rho0;
+    if (threadIdx.x == 0) {
+        // the first output row's copies first, then the ones ahead
+        while (rr.issued < 3 && rr.more()) rr.issue_next(src);
+        rr.issue_t(src);
         while (rr.issued < kRowSlots && rr.more()) rr.issue_next(src);
+        while (rr.t_issued < kRowTEnt && rr.t_issued < nk) rr.issue_t(src);
+    }
     const int i = threadIdx.x;
     const bool active = i < rp.Lrow;
     const int Ls = g.Ls, L = g.L;
@@ -393,32 +452,45 @@ __device__ __forceinline__ bool row_sweep(const Geom& g, const RowPlan& rp, unsi
     int u = 0;
     int run_prev = rho0 / L;
     bool ok = true;
-    for (int rho = rho0; rho < rho1; rho++) {
+    int k = 0;
+    if (active) {
+        const int run = rho0 / L, f = run / g.Lt;
+        body.pre(f, run - f * g.Lt, rho0 - run * L, x, s);
+    }
+    for (int rho = rho0; rho < rho1; rho++, k++) {
         const int run = rho / L;
         if (run != run_prev) {
             u += 2;
             run_prev = run;
         }
         const int f = run / g.Lt, t = run - f * g.Lt, y = rho - run * L;
-        if (active) body.pre(f, t, y, x, s);
         bool got = true;
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            got &= mbar_wait_bounded(bar + (u + k) % kRowSlots, (uint32_t)(((u + k) / kRowSlots) & 1));
+        for (int w = 0; w < 3; w++)
+            got &= mbar_wait_bounded(bar + (u + w) % kRowSlots, (uint32_t)(((u + w) / kRowSlots) & 1));
+        got &= mbar_wait_bounded(bar + kRowSlots + k % kRowTEnt, (uint32_t)((k / kRowTEnt) & 1));
         if (!got) s_err = 1;
         __syncthreads();
         if (s_err) {
             ok = false;
             break;
         }
-        if (active)
-            body.compute(rr.slot(u + 1), rr.slot(u + 2), rr.slot(u), f, t, y, x, s, i, ixp, ixm);
-        __syncthreads();   // every thread is done with the slot of load u
+        if (active) {
+            const T* tr = rr.tslot(k);
+            body.compute(rr.slot(u + 1), rr.slot(u + 2), rr.slot(u), tr, tr + 4 * rp.Lrow, f, t,
+                         y, x, s, i, ixp, ixm);
+            if (rho + 1 < rho1) {
+                const int rn = (rho + 1) / L, fn = rn / g.Lt;
+                body.pre(fn, rn - fn * g.Lt, rho + 1 - rn * L, x, s);
+            }
+        }
+        __syncthreads();   // every thread is done with window load u and t entry k
         u += 1;
         const int next_u = (rho + 1 < rho1 && (rho + 1) / L != run) ? u + 2 : u;
         if (threadIdx.x == 0) {
             fence_proxy_async_smem();
             while (rr.more() && rr.issued < next_u + kRowSlots) rr.issue_next(src);
+            while (rr.t_issued < nk && rr.t_issued < k + 1 + kRowTEnt) rr.issue_t(src);
         }
     }
     if (!ok && threadIdx.x == 0) {
@@ -426,6 +498,8 @@ __device__ __forceinline__ bool row_sweep(const Geom& g, const RowPlan& rp, unsi
         // shared memory goes away
         for (int w = u; w < rr.issued; w++)
             mbar_wait_bounded(bar + w % kRowSlots, (uint32_t)((w / kRowSlots) & 1));
+        for (int e = k; e < rr.t_issued; e++)
+            mbar_wait_bounded(bar + kRowSlots + e % kRowTEnt, (uint32_t)((e / kRowTEnt) & 1));
     }
     __syncthreads();
     return ok;

@@ -4,12 +4,14 @@
 // (dwf_stencil.cuh: one thread per point and flavour, every neighbour read
 // through L1/L2) at a register budget of 80 a thread (3 blocks of 256 a
 // SM) or 64 (4 blocks, more warps in flight, some spills), and the
-// row-staged kernels (row_stage.cuh: rows y-1..y+1 staged in shared memory
-// by bulk copies).  Which is fastest depends on the lattice and the
-// precision.  On the first use of a (L, Lt, Ls, element size) the tuner
-// applies M in every shape to scratch vectors on the caller's stream -- 2
-// warm-up and 5 timed applications each, CUDA events, L2 not flushed (all
-// see the same cache state) -- and keeps the fastest.  The choice holds for
+// row-staged kernels (row_stage.cuh: rows y-1..y+1 and t-1, t+1 staged in
+// shared memory by bulk copies), where they can launch.  Which is fastest
+// depends on the lattice and the precision.  On the first use of a (L, Lt,
+// Ls, element size) the tuner applies M in every shape to scratch vectors on
+// the caller's stream -- 2 warm-up and 5 timed applications each, CUDA
+// events, L2 not flushed (all see the same cache state) -- and keeps the
+// fastest, the 3-block point-gather kernel unless another shape is faster
+// by more than kTuneMargin.  The choice holds for
 // the operator and for the multi-shift solver's pass 1, which use the same
 // stencil at the same budgets.  The table is per process;
 // chdwf_autotune_report prints it.
@@ -36,6 +38,8 @@ struct TuneEntry {
 const char* shape_name(int k) {
     return k == kStencilRows ? "rows" : (k == kStencilGather4 ? "gather4" : "gather3");
 }
+
+constexpr float kTuneMargin = 0.03f;   // 3%: above the spread of repeated timings
 
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune;
@@ -82,7 +86,7 @@ int stencil_choice(const Geom& g, int elem, cudaStream_t st) {
     RowPlan rp;
     const bool rows_fit = row_plan(g, (size_t)elem, max_threads_of(elem), &rp);
     if (mode == 1) return kStencilGather3;
-    if (mode == 2) return rows_fit ? kStencilRows : kStencilGather3;
+    if (mode == 2) return rows_fit && op_rows_launchable(g, elem) ? kStencilRows : kStencilGather3;
     int dev = 0;
     cudaGetDevice(&dev);
     {
@@ -100,12 +104,14 @@ int stencil_choice(const Geom& g, int elem, cudaStream_t st) {
         cudaMalloc(&chif, sizeof(float) * 3 * (size_t)g.kvol) == cudaSuccess) {
         cudaMemsetAsync(in, 0, bytes, st);
         cudaMemsetAsync(chif, 0, sizeof(float) * 3 * (size_t)g.kvol, st);
+        // another shape replaces the point-gather kernel at 3 blocks a SM
+        // only if it is faster by more than the timing noise (kTuneMargin)
         float best = 0.0f;
         for (int k : {kStencilGather3, kStencilGather4, kStencilRows}) {
-            if (k == kStencilRows && !rows_fit) continue;
+            if (k == kStencilRows && !(rows_fit && op_rows_launchable(g, elem))) continue;
             if (k == kStencilGather4 && elem == 4) continue;   // one FP16 gather kernel
             t.us[k] = time_variant(g, elem, k, out, in, chif, st);
-            if (best == 0.0f || t.us[k] < best) {
+            if (best == 0.0f || t.us[k] < best * (1.0f - kTuneMargin)) {
                 best = t.us[k];
                 t.choice = k;
             }

@@ -90,6 +90,11 @@ int chdwf_set_basis_store(chdwf_ctx* ctx, double max_bytes);
 void* chdwf_get_stream(chdwf_ctx* ctx);
 /* number of CUDA kernels the library has launched in this process */
 long long chdwf_kernel_launches(void);
+/* operator and multi-shift pass-1 stencil launches in this process by kernel
+ * shape: counts[0] point-gather at 3 blocks a SM, counts[1] row-staged,
+ * counts[2] point-gather at 4 blocks a SM (the shapes chdwf_autotune_report
+ * names).  No counterpart in the reference. */
+int chdwf_stencil_launches(long long* counts);
 int chdwf_timing_read(chdwf_ctx* ctx, double* ms, long long* timed, long long* launched,
                       double* bytes);
 

@@ -13,6 +13,10 @@ CHDWF_STENCIL=legacy selects the point-gather kernels for the comparison.
                                   (x to 1e-10, force to 2 REAL*4 ulps,
                                   iterations +-5); against the point-gather
                                   kernels: iterations +-2, x to 1e-12
+  large rows (24^3x24 FP32, 16^3x16 FP64: the shapes the autotuner weighs
+  for the trajectory)             bit-identical to the point-gather kernels
+Every test checks, through chdwf_stencil_launches, that the row kernels did
+run (a shape that cannot launch falls back to the point-gather kernels).
 """
 import numpy as np
 import pytest
@@ -26,6 +30,13 @@ pytestmark = pytest.mark.gpu
 
 def rel(a, b):
     return np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b))
+
+
+@pytest.fixture(autouse=True)
+def rows_ran():
+    n0 = chb.stencil_launches()["rows"]
+    yield
+    assert chb.stencil_launches()["rows"] > n0, "the row kernels did not run"
 
 
 @pytest.mark.parametrize("L,Lt,Ls", [(8, 8, 8), (6, 4, 6), (12, 12, 8), (16, 16, 16),
@@ -138,3 +149,25 @@ def test_rows_mixed_precision_trajectory(monkeypatch, remez, Ls):
     for a, b in zip(recs["f64"], recs["f32"]):
         assert a.nsteps == b.nsteps and a.accepted == b.accepted
         assert abs(a.dH - b.dH) <= 1e-8 * abs(a.H0), (a.dH, b.dH)
+
+
+@pytest.mark.parametrize("L,Ls,prec", [(24, 24, 1), (16, 16, 0)])
+def test_rows_large_bit_identical_to_gather(monkeypatch, L, Ls, prec):
+    """The row kernels at the sizes the autotuner weighs them: the same bits
+    as the point-gather kernels (both keep dwf_apply_flavour's per-element
+    operation sequence, FP32 without contraction)."""
+    from test_gpu_lowprec import _lp_apply
+    R, chi = random_fields(L, L, Ls, seed=41)
+    outs = {}
+    for mode in ("rows", "legacy"):
+        monkeypatch.setenv("CHDWF_STENCIL", mode)
+        gl = chb.Lattice(L, L, Ls, beta=0.475)
+        for dag in (False, True):
+            if prec == 0:
+                outs[(mode, dag)] = (gl.dslashd if dag else gl.dslash)(R, chi, hpin=0.3, imass=1)
+            else:
+                outs[(mode, dag)] = _lp_apply(gl, R, chi, prec, dag)
+        gl.close()
+    for dag in (False, True):
+        a, b = outs[("rows", dag)], outs[("legacy", dag)]
+        assert np.array_equal(a, b), dag

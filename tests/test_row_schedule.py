@@ -1,12 +1,15 @@
 """CPU model of the row-staged kernels' copy schedule (csrc/row_stage.cuh).
 
 The kernels' producer (thread 0 issuing bulk copies of window rows into a
-ring of slots) and consumer (every thread waiting for rows u, u+1, u+2 of
-an output row) are restated here line by line, and for many lattice shapes
-and grid sizes the model checks what the GPU code relies on:
+ring of slots, and of the t+-1 rows into a second ring) and consumer (every
+thread waiting for window rows u, u+1, u+2 and t entry k of its k-th output
+row) are restated here line by line, and for many lattice shapes and grid
+sizes the model checks what the GPU code relies on:
   * output row (f, t, y) reads window rows (f, t, y-1), (f, t, y), (f, t, y+1)
-    with y periodic;
-  * a slot is refilled only after every output row that reads it is done;
+    with y periodic, and t rows (f, t+1, y), (f, t-1, y) with t periodic;
+  * a slot of either ring is refilled only after every output row that
+    reads it is done, so each slot has at most one copy in flight (its wait
+    parity is unambiguous);
   * every wait is on a copy already issued, and every issued copy is waited
     on before the block ends (no copy in flight at exit);
   * every copy is in bounds and starts on a 16-byte boundary.
@@ -14,6 +17,7 @@ and grid sizes the model checks what the GPU code relies on:
 import pytest
 
 NS = 5   # kRowSlots
+NT = 3   # kRowTEnt
 
 
 def simulate(L, Lt, Ls, nb, elem):
@@ -54,26 +58,56 @@ def simulate(L, Lt, Ls, nb, elem):
                 if st["rho_a"] < rho1:
                     st["len"] = run_len(st["rho_a"])
 
+        nk = rho1 - rho0
+        tslots, tloads = {}, []
+
+        def issue_t():
+            k = len(tloads)
+            if k % NT in tslots:
+                assert tslots[k % NT] in tdone, ("t slot refilled before use ended", k)
+            tslots[k % NT] = k
+            rho = rho0 + k
+            run = rho // L
+            f, t, y = run // Lt, run % Lt, rho - run * L
+            for tt in ((t + 1) % Lt, (t - 1) % Lt):
+                for d in range(4):
+                    off = cs * (4 * f + d) + Lrow * (y + L * tt)
+                    assert 0 <= off and off + Lrow <= kferm
+                    assert (off * elem) % 16 == 0
+            tloads.append((f, (t + 1) % Lt, (t - 1) % Lt, y))
+
+        tdone = set()
+        while st["issued"] < 3 and st["rho_a"] < rho1:
+            issue()
+        issue_t()
         while st["issued"] < NS and st["rho_a"] < rho1:
             issue()
+        while len(tloads) < NT and len(tloads) < nk:
+            issue_t()
         u, run_prev = 0, rho0 // L
-        for rho in range(rho0, rho1):
+        for k, rho in enumerate(range(rho0, rho1)):
             run = rho // L
             if run != run_prev:
                 u += 2
                 run_prev = run
             f, t, y = run // Lt, run % Lt, rho - run * L
-            for k in range(3):
-                assert u + k < st["issued"] and slots[(u + k) % NS] == u + k
+            for w in range(3):
+                assert u + w < st["issued"] and slots[(u + w) % NS] == u + w
+            assert k < len(tloads) and tslots[k % NT] == k
             assert loads[u] == (f, t, (y - 1) % L)
             assert loads[u + 1] == (f, t, y)
             assert loads[u + 2] == (f, t, (y + 1) % L)
+            assert tloads[k] == (f, (t + 1) % Lt, (t - 1) % Lt, y)
             u += 1
             next_u = u + 2 if (rho + 1 < rho1 and (rho + 1) // L != run) else u
             done.update(range(next_u))
+            tdone.add(k)
             while st["rho_a"] < rho1 and st["issued"] < next_u + NS:
                 issue()
+            while len(tloads) < nk and len(tloads) < k + 1 + NT:
+                issue_t()
         assert st["issued"] <= u + 2   # all issued copies were waited on
+        assert len(tloads) == nk
 
 
 SHAPES = [(24, 24, 24), (16, 16, 16), (16, 16, 32), (12, 12, 8), (8, 8, 8), (4, 4, 4),
