@@ -42,7 +42,27 @@ static inline float diag_of(float am3) { return 2.0f * ((3.0f - am3) + 1.0f); } 
 template <class T> __device__ __forceinline__ T row_store(T v, T*) { return v; }
 __device__ __forceinline__ __half2 row_store(float2 v, __half2*) { return __float22half2_rn(v); }
 
-template <class S, class T, bool DAG, int IMASS>
+// Stores PPT adjacent output elements (one 16-byte or 8-byte store for a pair).
+template <class S, class T, int PPT> struct RowSt;
+template <class S, class T> struct RowSt<S, T, 1> {
+    __device__ __forceinline__ static void put(S* o, const T* v) { *o = row_store(v[0], o); }
+};
+template <> struct RowSt<float2, float2, 2> {
+    __device__ __forceinline__ static void put(float2* o, const float2* v) {
+        *reinterpret_cast<float4*>(o) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+    }
+};
+template <> struct RowSt<__half2, float2, 2> {
+    __device__ __forceinline__ static void put(__half2* o, const float2* v) {
+        const __half2 a = __float22half2_rn(v[0]), b = __float22half2_rn(v[1]);
+        uint2 q;
+        q.x = *reinterpret_cast<const uint32_t*>(&a);
+        q.y = *reinterpret_cast<const uint32_t*>(&b);
+        *reinterpret_cast<uint2*>(o) = q;
+    }
+};
+
+template <class S, class T, bool DAG, int IMASS, int PPT>
 struct OpRows {
     typedef typename real_of<T>::type Real;
     const S* __restrict__ in;
@@ -52,30 +72,36 @@ struct OpRows {
     int Lrow;
     Real diag, hpin;
     int apbc;
-    RowWall<T> rw;
+    RowWall<T, PPT> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
-        row_wall_prefetch<DAG>(rw, in, g, f, t, y, x, s, chif);
+        row_wall_prefetch<DAG, PPT>(rw, in, g, f, t, y, x, s, chif);
     }
     __device__ __forceinline__ void compute(const S* c, const S* yp, const S* ym, const S* tps,
                                             const S* tms, int f, int t, int y, int x, int s,
                                             int i, int ixp, int ixm) {
-        const PointIdx q = row_point(g, t, y, x, s);
-        T acc[4];
-        dwf_apply_rows<DAG, IMASS>(acc, c, yp, ym, tps, tms, Lrow, i, ixp, ixm, rw, g, q, f, diag,
-                                   hpin, apbc != 0);
+        const int site = x + g.L * (y + g.L * t);
+        T acc[PPT][4];
+        dwf_apply_rows<DAG, IMASS, PPT>(acc, c, yp, ym, tps, tms, Lrow, i, ixp, ixm, s, site, t,
+                                        rw, g, f, diag, hpin, apbc != 0);
+        const int64_t p0 = s + (int64_t)g.Ls * site;
 #pragma unroll
-        for (int d = 0; d < 4; d++) out[q.p + g.cs * (d + 4 * f)] = row_store(acc[d], out);
+        for (int d = 0; d < 4; d++) {
+            T v[PPT];
+#pragma unroll
+            for (int p = 0; p < PPT; p++) v[p] = acc[p][d];
+            RowSt<S, T, PPT>::put(out + p0 + g.cs * (d + 4 * f), v);
+        }
     }
 };
 
-template <class S, class T, bool DAG, int IMASS>
-__global__ void __maxnreg__(RowRegs<T>::value)
+template <class S, class T, bool DAG, int IMASS, int PPT>
+__global__ void __maxnreg__(kRowRegs)
     k_dslash_rows(S* __restrict__ out, const S* __restrict__ in, const float* __restrict__ chif,
                   Geom g, RowPlan rp, typename real_of<T>::type diag,
                   typename real_of<T>::type hpin, int apbc) {
     extern __shared__ __align__(128) unsigned char row_smem[];
-    OpRows<S, T, DAG, IMASS> body{in, out, chif, g, rp.Lrow, diag, hpin, apbc};
-    if (row_sweep<S>(g, rp, row_smem, in, body)) return;
+    OpRows<S, T, DAG, IMASS, PPT> body{in, out, chif, g, rp.Lrow, diag, hpin, apbc};
+    if (row_sweep<S, PPT>(g, rp, row_smem, in, body)) return;
     int rho0, rho1;
     row_range(rp.nrows, &rho0, &rho1);
     const T nan = zmake<T>((typename real_of<T>::type)NAN, (typename real_of<T>::type)NAN);
@@ -89,49 +115,57 @@ __global__ void __maxnreg__(RowRegs<T>::value)
 }
 
 // Plan and grid of the row-staged operator, set up once per kernel and row
-// length: the blocks that fit on all SMs at once, at most one per row.
-template <class S, class T, bool DAG, int IMASS>
-static bool op_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb) {
-    if (!row_plan(g, sizeof(S), RowMaxThreads<T>::value, rp)) return false;
+// shape: the blocks that fit on all SMs at once, at most one per row.
+template <class S, class T, bool DAG, int IMASS, int PPT>
+static bool op_rows_setup(const Geom& g, const RowPlan& rp, unsigned* nb) {
     static int cached_lrow = -1, cached_nrows = -1;
     static unsigned cached_nb = 0;
-    if (cached_lrow == rp->Lrow && cached_nrows == rp->nrows) {
+    if (cached_lrow == rp.Lrow && cached_nrows == rp.nrows) {
         *nb = cached_nb;
         return cached_nb > 0;
     }
-    const void* k = (const void*)k_dslash_rows<S, T, DAG, IMASS>;
+    const void* k = (const void*)k_dslash_rows<S, T, DAG, IMASS, PPT>;
     int dev = 0, nsm = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     unsigned n = 0;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp->smem) ==
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rp.smem) ==
             cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, rp->nthreads, rp->smem) ==
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, rp.nthreads, rp.smem) ==
             cudaSuccess &&
         per_sm >= 1) {
         int64_t m = (int64_t)nsm * per_sm;
-        if (m > rp->nrows) m = rp->nrows;
+        if (m > rp.nrows) m = rp.nrows;
         if (m >= 1) n = (unsigned)m;
     }
     cudaGetLastError();
-    cached_lrow = rp->Lrow;
-    cached_nrows = rp->nrows;
+    cached_lrow = rp.Lrow;
+    cached_nrows = rp.nrows;
     cached_nb = n;
     *nb = n;
     return n > 0;
 }
 
-template <class S, class T, bool DAG, int IMASS>
+template <class S, class T, bool DAG, int IMASS, int PPT>
 static bool launch_op_rows(S* out, const S* in, const float* chif, const Geom& g,
-                           typename real_of<T>::type diag, typename real_of<T>::type hpin,
-                           int apbc, cudaStream_t st) {
-    RowPlan rp;
+                           const RowPlan& rp, typename real_of<T>::type diag,
+                           typename real_of<T>::type hpin, int apbc, cudaStream_t st) {
     unsigned nb = 0;
-    if (!op_rows_setup<S, T, DAG, IMASS>(g, &rp, &nb)) return false;
-    k_dslash_rows<S, T, DAG, IMASS><<<nb, rp.nthreads, rp.smem, st>>>(out, in, chif, g, rp, diag,
-                                                                      hpin, apbc);
+    if (!op_rows_setup<S, T, DAG, IMASS, PPT>(g, rp, &nb)) return false;
+    k_dslash_rows<S, T, DAG, IMASS, PPT><<<nb, rp.nthreads, rp.smem, st>>>(out, in, chif, g, rp,
+                                                                           diag, hpin, apbc);
     count_launches(1);
     return true;
+}
+
+template <class S, class T, int PPT>
+static bool launch_op_rows_ppt(bool dag, int imass, S* out, const S* in, const float* chif,
+                               const Geom& g, const RowPlan& rp, typename real_of<T>::type diag,
+                               typename real_of<T>::type hpin, int apbc, cudaStream_t st) {
+#define OPR(D, I) launch_op_rows<S, T, D, I, PPT>(out, in, chif, g, rp, diag, hpin, apbc, st)
+    if (!dag) return imass == 1 ? OPR(false, 1) : OPR(false, 3);
+    return imass == 1 ? OPR(true, 1) : OPR(true, 3);
+#undef OPR
 }
 
 template <class S, class T>
@@ -139,19 +173,26 @@ static bool launch_op_rows_any(bool dag, int imass, S* out, const S* in, const f
                                const Geom& g, typename real_of<T>::type diag,
                                typename real_of<T>::type hpin, int apbc, cudaStream_t st) {
     if (imass != 1 && imass != 3) return false;
-    if (!dag)
-        return imass == 1 ? launch_op_rows<S, T, false, 1>(out, in, chif, g, diag, hpin, apbc, st)
-                          : launch_op_rows<S, T, false, 3>(out, in, chif, g, diag, hpin, apbc, st);
-    return imass == 1 ? launch_op_rows<S, T, true, 1>(out, in, chif, g, diag, hpin, apbc, st)
-                      : launch_op_rows<S, T, true, 3>(out, in, chif, g, diag, hpin, apbc, st);
+    RowPlan rp;
+    if (!row_plan(g, sizeof(S), &rp)) return false;
+    if constexpr (sizeof(S) <= 8) {
+        if (rp.ppt == 2)
+            return launch_op_rows_ppt<S, T, 2>(dag, imass, out, in, chif, g, rp, diag, hpin, apbc,
+                                               st);
+    }
+    return launch_op_rows_ppt<S, T, 1>(dag, imass, out, in, chif, g, rp, diag, hpin, apbc, st);
 }
 
 bool op_rows_launchable(const Geom& g, int elem) {
     RowPlan rp;
     unsigned nb = 0;
-    if (elem == 16) return op_rows_setup<double2, double2, false, 1>(g, &rp, &nb);
-    if (elem == 8) return op_rows_setup<float2, float2, false, 1>(g, &rp, &nb);
-    return op_rows_setup<__half2, float2, false, 1>(g, &rp, &nb);
+    if (!row_plan(g, (size_t)elem, &rp)) return false;
+    if (elem == 16) return op_rows_setup<double2, double2, false, 1, 1>(g, rp, &nb);
+    if (elem == 8)
+        return rp.ppt == 2 ? op_rows_setup<float2, float2, false, 1, 2>(g, rp, &nb)
+                           : op_rows_setup<float2, float2, false, 1, 1>(g, rp, &nb);
+    return rp.ppt == 2 ? op_rows_setup<__half2, float2, false, 1, 2>(g, rp, &nb)
+                       : op_rows_setup<__half2, float2, false, 1, 1>(g, rp, &nb);
 }
 
 void launch_dslash64(bool dag, int imass, double2* out, const double2* in, const float* chif,

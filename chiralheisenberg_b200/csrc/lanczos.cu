@@ -407,37 +407,59 @@ __device__ __forceinline__ void row_fail(LzCtl* ctl, int* hflag) {
     }
 }
 
-template <class T, int IMASS>
+// PPT adjacent elements of a global vector (one 16-byte load for an FP32 pair)
+template <class T, int PPT> struct LzLd;
+template <class T> struct LzLd<T, 1> {
+    __device__ __forceinline__ static void get(const T* p, T* v) { v[0] = *p; }
+    __device__ __forceinline__ static void put(T* p, const T* v) { *p = v[0]; }
+};
+template <> struct LzLd<float2, 2> {
+    __device__ __forceinline__ static void get(const float2* p, float2* v) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        v[0] = make_float2(q.x, q.y);
+        v[1] = make_float2(q.z, q.w);
+    }
+    __device__ __forceinline__ static void put(float2* p, const float2* v) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+    }
+};
+
+template <class T, int IMASS, int PPT>
 struct LzRowsM {
     typedef typename real_of<T>::type Real;
     const LzArgsT<T>& a;
     const T* rj;
     Real ib;
     double loc;
-    RowWall<T> rw;
+    RowWall<T, PPT> rw;
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
-        row_wall_prefetch<false>(rw, rj, a.g, f, t, y, x, s, a.chif);
+        row_wall_prefetch<false, PPT>(rw, rj, a.g, f, t, y, x, s, a.chif);
     }
     __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, const T* tps,
                                             const T* tms, int f, int t, int y, int x, int s,
                                             int i, int ixp, int ixm) {
         const Geom& g = a.g;
-        const PointIdx q = row_point(g, t, y, x, s);
-        T acc[4];
-        dwf_apply_rows<false, IMASS>(acc, c, yp, ym, tps, tms, a.rp.Lrow, i, ixp, ixm, rw, g, q,
-                                     f, a.diag, a.hpin, a.apbc != 0);
+        const int site = x + g.L * (y + g.L * t);
+        T acc[PPT][4];
+        dwf_apply_rows<false, IMASS, PPT>(acc, c, yp, ym, tps, tms, a.rp.Lrow, i, ixp, ixm, s,
+                                          site, t, rw, g, f, a.diag, a.hpin, a.apbc != 0);
+        const int64_t p0 = s + (int64_t)g.Ls * site;
 #pragma unroll
         for (int d = 0; d < 4; d++) {
-            acc[d] = zscal(ib, acc[d]);
-            a.vt[q.p + g.cs * (d + 4 * f)] = acc[d];
-            const double2 w = widen(acc[d]);
-            loc += w.x * w.x + w.y * w.y;
+            T v[PPT];
+#pragma unroll
+            for (int p = 0; p < PPT; p++) {
+                v[p] = zscal(ib, acc[p][d]);
+                const double2 w = widen(v[p]);
+                loc += w.x * w.x + w.y * w.y;
+            }
+            LzLd<T, PPT>::put(a.vt + p0 + g.cs * (d + 4 * f), v);
         }
     }
 };
 
-template <class T, int IMASS>
-__global__ void __maxnreg__(RowRegs<T>::value) k_lz1_M_rows(LzArgsT<T> a) {
+template <class T, int IMASS, int PPT>
+__global__ void __maxnreg__(kRowRegs) k_lz1_M_rows(LzArgsT<T> a) {
     extern __shared__ __align__(128) unsigned char row_smem[];
     LzCtl* ctl = a.ctl;
     if (block_stopped(ctl)) return;
@@ -452,8 +474,8 @@ __global__ void __maxnreg__(RowRegs<T>::value) k_lz1_M_rows(LzArgsT<T> a) {
             a.h.invbeta[j] = ibj;
         }
     }
-    LzRowsM<T, IMASS> body{a, ring(a, j), (typename real_of<T>::type)ibj, 0.0};
-    const bool ok = row_sweep<T>(a.g, a.rp, row_smem, body.rj, body);
+    LzRowsM<T, IMASS, PPT> body{a, ring(a, j), (typename real_of<T>::type)ibj, 0.0};
+    const bool ok = row_sweep<T, PPT>(a.g, a.rp, row_smem, body.rj, body);
     __shared__ double sh[32];
     const double loc = block_sum_any(body.loc, sh);
     if (threadIdx.x == 0) {
@@ -462,7 +484,7 @@ __global__ void __maxnreg__(RowRegs<T>::value) k_lz1_M_rows(LzArgsT<T> a) {
     }
 }
 
-template <class T, int IMASS, bool WALLS>
+template <class T, int IMASS, bool WALLS, int PPT>
 struct LzRowsMd {
     typedef typename real_of<T>::type Real;
     const LzArgsT<T>& a;
@@ -472,45 +494,50 @@ struct LzRowsMd {
     int j;
     Real ib, at, bj, ibm;
     double loc;
-    T cj[4], cm[4];
-    RowWall<T> rw;
-    // q_j and q_{j-1} at the point (streamed, not staged) and the wall operands
+    T cj[4][PPT], cm[4][PPT];
+    RowWall<T, PPT> rw;
+    // q_j and q_{j-1} at the thread's points (streamed, not staged) and the
+    // wall operands
     __device__ __forceinline__ void pre(int f, int t, int y, int x, int s) {
         const Geom& g = a.g;
         const int64_t e0 = (int64_t)x * g.Ls + s + (int64_t)g.L * g.Ls * (y + (int64_t)g.L * t);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
             const int64_t po = g.cs * (d + 4 * f);
-            cj[d] = rj[e0 + po];
-            if (j > 1) cm[d] = rjm[e0 + po];
+            LzLd<T, PPT>::get(rj + e0 + po, cj[d]);
+            if (j > 1) LzLd<T, PPT>::get(rjm + e0 + po, cm[d]);
         }
-        row_wall_prefetch<true>(rw, a.vt, g, f, t, y, x, s, a.chif);
+        row_wall_prefetch<true, PPT>(rw, a.vt, g, f, t, y, x, s, a.chif);
     }
     __device__ __forceinline__ void compute(const T* c, const T* yp, const T* ym, const T* tps,
                                             const T* tms, int f, int t, int y, int x, int s,
                                             int i, int ixp, int ixm) {
         const Geom& g = a.g;
-        const PointIdx q = row_point(g, t, y, x, s);
-        T acc[4];
-        dwf_apply_rows<true, IMASS>(acc, c, yp, ym, tps, tms, a.rp.Lrow, i, ixp, ixm, rw, g, q, f,
-                                    a.diag, a.hpin, a.apbc != 0);
+        const int site = x + g.L * (y + g.L * t);
+        T acc[PPT][4];
+        dwf_apply_rows<true, IMASS, PPT>(acc, c, yp, ym, tps, tms, a.rp.Lrow, i, ixp, ixm, s,
+                                         site, t, rw, g, f, a.diag, a.hpin, a.apbc != 0);
+        const int64_t p0 = s + (int64_t)g.Ls * site;
 #pragma unroll
         for (int d = 0; d < 4; d++) {
-            const int64_t e = q.p + g.cs * (d + 4 * f);
-            // r_{j+1} = x3 - alpha~ q_j - beta_j q_{j-1}, as three_term (:655)
-            const T qj = zscal(ib, cj[d]);
-            T v = zsub(acc[d], zscal(at, qj));
-            if (j > 1) v = zsub(v, zscal(bj, zscal(ibm, cm[d])));
-            rn[e] = v;
-            if (WALLS) wall_put(a, j + 1, q.s, q.site, d + 4 * f, v);
-            const double2 w = widen(v);
-            loc += w.x * w.x + w.y * w.y;
+            T v[PPT];
+#pragma unroll
+            for (int p = 0; p < PPT; p++) {
+                // r_{j+1} = x3 - alpha~ q_j - beta_j q_{j-1}, as three_term (:655)
+                const T qj = zscal(ib, cj[d][p]);
+                v[p] = zsub(acc[p][d], zscal(at, qj));
+                if (j > 1) v[p] = zsub(v[p], zscal(bj, zscal(ibm, cm[d][p])));
+                if (WALLS) wall_put(a, j + 1, s + p, site, d + 4 * f, v[p]);
+                const double2 w = widen(v[p]);
+                loc += w.x * w.x + w.y * w.y;
+            }
+            LzLd<T, PPT>::put(rn + p0 + g.cs * (d + 4 * f), v);
         }
     }
 };
 
-template <class T, int IMASS, bool WALLS>
-__global__ void __maxnreg__(RowRegs<T>::value) k_lz1_Md_rows(LzArgsT<T> a) {
+template <class T, int IMASS, bool WALLS, int PPT>
+__global__ void __maxnreg__(kRowRegs) k_lz1_Md_rows(LzArgsT<T> a) {
     typedef typename real_of<T>::type Real;
     extern __shared__ __align__(128) unsigned char row_smem[];
     LzCtl* ctl = a.ctl;
@@ -518,10 +545,10 @@ __global__ void __maxnreg__(RowRegs<T>::value) k_lz1_Md_rows(LzArgsT<T> a) {
     const int j = ctl->it_md;
     const int nb = gridDim.x;
     const double at = sum_partials_any(a.part, nb);
-    LzRowsMd<T, IMASS, WALLS> body{a, ring(a, j), ring(a, j - 1), ring(a, j + 1), j,
-                                   (Real)a.h.invbeta[j], (Real)at, (Real)a.h.beta[j],
-                                   (Real)(j > 1 ? a.h.invbeta[j - 1] : 0.0), 0.0};
-    const bool ok = row_sweep<T>(a.g, a.rp, row_smem, a.vt, body);
+    LzRowsMd<T, IMASS, WALLS, PPT> body{a, ring(a, j), ring(a, j - 1), ring(a, j + 1), j,
+                                        (Real)a.h.invbeta[j], (Real)at, (Real)a.h.beta[j],
+                                        (Real)(j > 1 ? a.h.invbeta[j - 1] : 0.0), 0.0};
+    const bool ok = row_sweep<T, PPT>(a.g, a.rp, row_smem, a.vt, body);
     __shared__ double sh[32];
     const double loc = block_sum_any(body.loc, sh);
     if (threadIdx.x == 0) {
@@ -783,36 +810,61 @@ static void launch_pass1(const LzArgsT<T>& a, unsigned nb, cudaStream_t st, cons
 
 // Row-staged pass 1 (same protocol: M, the scalar step on the side stream,
 // M^dagger).  Grid: the blocks that fit on all SMs at once.
-template <class T, int IMASS>
-static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
-                              const LzSide& side, KernelTimer* tm) {
+template <class T, int IMASS, int PPT>
+static void launch_pass1_rows_ppt(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
+                                  const LzSide& side, KernelTimer* tm) {
     const double V = (double)a.g.kferm * sizeof(T), chi = 12.0 * a.g.kvol;
     const unsigned nt = (unsigned)a.rp.nthreads, sm = a.rp.smem;
     if (tm) tm->begin(timer_class<T>(0), st, 2 * V + chi);
-    k_lz1_M_rows<T, IMASS><<<nb, nt, sm, st>>>(a);
+    k_lz1_M_rows<T, IMASS, PPT><<<nb, nt, sm, st>>>(a);
     if (tm) tm->end(st);
     cudaEventRecord(side.fork, st);
     cudaStreamWaitEvent(side.stream, side.fork, 0);
     k_lz_pole<T><<<1, kThreads, 0, side.stream>>>(a, (int)nb);
     cudaEventRecord(side.join, side.stream);
     if (tm) tm->begin(timer_class<T>(1), st, 4 * V + chi);
-    if (a.wcap > 0) k_lz1_Md_rows<T, IMASS, true><<<nb, nt, sm, st>>>(a);
-    else k_lz1_Md_rows<T, IMASS, false><<<nb, nt, sm, st>>>(a);
+    if (a.wcap > 0) k_lz1_Md_rows<T, IMASS, true, PPT><<<nb, nt, sm, st>>>(a);
+    else k_lz1_Md_rows<T, IMASS, false, PPT><<<nb, nt, sm, st>>>(a);
     if (tm) tm->end(st);
     cudaStreamWaitEvent(st, side.join, 0);
 }
 
-// Whether pass 1 runs on the row-staged kernels (the autotuner's choice,
-// use_rows), and their plan and grid.
+template <class T, int IMASS>
+static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
+                              const LzSide& side, KernelTimer* tm) {
+    if constexpr (std::is_same<T, float2>::value) {
+        if (a.rp.ppt == 2) {
+            launch_pass1_rows_ppt<T, IMASS, 2>(a, nb, st, side, tm);
+            return;
+        }
+    }
+    launch_pass1_rows_ppt<T, IMASS, 1>(a, nb, st, side, tm);
+}
+
+// The six pass-1 row kernels of one precision and thread shape.
+template <class T, int PPT>
+static void lz_rows_kernels(const void* kern[6]) {
+    kern[0] = (const void*)k_lz1_M_rows<T, 1, PPT>;
+    kern[1] = (const void*)k_lz1_M_rows<T, 3, PPT>;
+    kern[2] = (const void*)k_lz1_Md_rows<T, 1, false, PPT>;
+    kern[3] = (const void*)k_lz1_Md_rows<T, 1, true, PPT>;
+    kern[4] = (const void*)k_lz1_Md_rows<T, 3, false, PPT>;
+    kern[5] = (const void*)k_lz1_Md_rows<T, 3, true, PPT>;
+}
+
+// Whether pass 1 runs on the row-staged kernels (the autotuner's choice),
+// and their plan and grid.
 template <class T>
 static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb, cudaStream_t st) {
     if (stencil_choice(g, (int)sizeof(T), st) != kStencilRows) return false;
-    if (!row_plan(g, sizeof(T), RowMaxThreads<T>::value, rp)) return false;
-    const void* kern[6] = {(const void*)k_lz1_M_rows<T, 1>, (const void*)k_lz1_M_rows<T, 3>,
-                           (const void*)k_lz1_Md_rows<T, 1, false>,
-                           (const void*)k_lz1_Md_rows<T, 1, true>,
-                           (const void*)k_lz1_Md_rows<T, 3, false>,
-                           (const void*)k_lz1_Md_rows<T, 3, true>};
+    if (!row_plan(g, sizeof(T), rp)) return false;
+    const void* kern[6];
+    if constexpr (std::is_same<T, float2>::value) {
+        if (rp->ppt == 2) lz_rows_kernels<T, 2>(kern);
+        else lz_rows_kernels<T, 1>(kern);
+    } else {
+        lz_rows_kernels<T, 1>(kern);
+    }
     int dev = 0, nsm = 0, per_sm = 1 << 20;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

@@ -44,10 +44,6 @@ constexpr float kTuneMargin = 0.03f;   // 3%: above the spread of repeated timin
 std::mutex g_tune_mu;
 std::vector<TuneEntry> g_tune;
 
-int max_threads_of(int elem) {
-    return elem == 16 ? RowMaxThreads<double2>::value : RowMaxThreads<float2>::value;
-}
-
 // median microseconds of 5 applications (after 2) of variant v
 float time_variant(const Geom& g, int elem, int v, void* out, const void* in, const float* chif,
                    cudaStream_t st) {
@@ -84,7 +80,7 @@ float time_variant(const Geom& g, int elem, int v, void* out, const void* in, co
 int stencil_choice(const Geom& g, int elem, cudaStream_t st) {
     const int mode = stencil_mode();
     RowPlan rp;
-    const bool rows_fit = row_plan(g, (size_t)elem, max_threads_of(elem), &rp);
+    const bool rows_fit = row_plan(g, (size_t)elem, &rp);
     if (mode == 1) return kStencilGather3;
     if (mode == 2) return rows_fit && op_rows_launchable(g, elem) ? kStencilRows : kStencilGather3;
     int dev = 0;

@@ -1,18 +1,21 @@
 """CPU model of the row-staged kernels' copy schedule (csrc/row_stage.cuh).
 
-The kernels' producer (thread 0 issuing bulk copies of window rows into a
-ring of slots, and of the t+-1 rows into a second ring) and consumer (every
-thread waiting for window rows u, u+1, u+2 and t entry k of its k-th output
-row) are restated here line by line, and for many lattice shapes and grid
-sizes the model checks what the GPU code relies on:
+The producer (lane 0 of the block's last warp, issuing bulk copies of
+window rows into one ring of slots and of the t+-1 rows into a second ring,
+each after its slot's previous use has been released) and the consumers
+(waiting for window loads u, u+1, u+2 and t entry k of the block's k-th
+output row, then releasing what the next row does not read) are restated
+here, and for many lattice shapes and grid sizes the model checks what the
+GPU code relies on:
   * output row (f, t, y) reads window rows (f, t, y-1), (f, t, y), (f, t, y+1)
     with y periodic, and t rows (f, t+1, y), (f, t-1, y) with t periodic;
-  * a slot of either ring is refilled only after every output row that
-    reads it is done, so each slot has at most one copy in flight (its wait
-    parity is unambiguous);
-  * every wait is on a copy already issued, and every issued copy is waited
-    on before the block ends (no copy in flight at exit);
-  * every copy is in bounds and starts on a 16-byte boundary.
+  * a slot is refilled only after every consumer released its previous use,
+    so each slot has at most one copy in flight and the wait parities
+    (use count & 1) are unambiguous;
+  * the producer never waits for a release the consumers cannot give
+    (no deadlock), however far ahead it runs;
+  * every copy is in bounds and starts on a 16-byte boundary, and the
+    expect-tx byte counts stay below the mbarrier's limit (2^20 - 1).
 """
 import pytest
 
@@ -26,92 +29,100 @@ def simulate(L, Lt, Ls, nb, elem):
     cs = L * L * Lt * Ls
     kferm = 8 * cs
     assert (Lrow * elem) % 16 == 0
+    assert 8 * Lrow * elem < 2 ** 20
     for b in range(nb):
         rho0, rho1 = b * nrows // nb, (b + 1) * nrows // nb
-        if rho0 >= rho1:
+        nk = rho1 - rho0
+        if nk <= 0:
             continue
 
-        def run_len(ra):
-            return min((ra // L + 1) * L, rho1) - ra
-
-        st = {"rho_a": rho0, "o": 0, "issued": 0, "len": run_len(rho0)}
-        slots, loads, done = {}, [], set()
-
-        def issue():
-            run = st["rho_a"] // L
-            f, t = run // Lt, run % Lt
-            y = (st["rho_a"] - run * L - 1 + st["o"]) % L
-            w = st["issued"]
-            if w % NS in slots:
-                assert slots[w % NS] in done, ("slot refilled before use ended", w)
-            slots[w % NS] = w
-            for d in range(4):
-                off = cs * (4 * f + d) + Lrow * (y + L * t)
-                assert 0 <= off and off + Lrow <= kferm
-                assert (off * elem) % 16 == 0
-            loads.append((f, t, y))
-            st["issued"] += 1
-            st["o"] += 1
-            if st["o"] == st["len"] + 2:
-                st["rho_a"] += st["len"]
-                st["o"] = 0
-                if st["rho_a"] < rho1:
-                    st["len"] = run_len(st["rho_a"])
-
-        nk = rho1 - rho0
-        tslots, tloads = {}, []
-
-        def issue_t():
-            k = len(tloads)
-            if k % NT in tslots:
-                assert tslots[k % NT] in tdone, ("t slot refilled before use ended", k)
-            tslots[k % NT] = k
+        def rows_of(k):
             rho = rho0 + k
             run = rho // L
-            f, t, y = run // Lt, run % Lt, rho - run * L
+            return run // Lt, run % Lt, rho - run * L
+
+        # the window base of every step, as both sides compute it
+        u = [0] * nk
+        for k in range(1, nk):
+            u[k] = u[k - 1] + 1 + (2 if rows_of(k)[2] == 0 else 0)
+
+        # producer state
+        pr = {"ra": rho0, "o": 0, "len": min((rho0 // L + 1) * L, rho1) - rho0,
+              "issued": 0, "tissued": 0, "k": 0}
+        loads, tloads = [], []
+        released_y, released_t = set(), set()
+        slot_y, slot_t = {}, {}
+
+        def producer_step():
+            """Issue the next copy if its slot is free; False when blocked or done."""
+            k = pr["k"]
+            if k >= nk:
+                return False
+            if pr["issued"] <= u[k] + 2:
+                w = pr["issued"]
+                if w >= NS and (w - NS) not in released_y:
+                    return False
+                if w % NS in slot_y:
+                    assert slot_y[w % NS] == w - NS
+                slot_y[w % NS] = w
+                ra, o = pr["ra"], pr["o"]
+                run = ra // L
+                f, t = run // Lt, run % Lt
+                y = (ra - run * L - 1 + o) % L
+                for d in range(4):
+                    off = cs * (4 * f + d) + Lrow * (y + L * t)
+                    assert 0 <= off and off + Lrow <= kferm
+                    assert (off * elem) % 16 == 0
+                loads.append((f, t, y))
+                pr["issued"] += 1
+                pr["o"] += 1
+                if pr["o"] == pr["len"] + 2:
+                    pr["ra"] += pr["len"]
+                    pr["o"] = 0
+                    if pr["ra"] < rho1:
+                        pr["len"] = min((pr["ra"] // L + 1) * L, rho1) - pr["ra"]
+                return True
+            if k >= NT and (k - NT) not in released_t:
+                return False
+            slot_t[k % NT] = k
+            f, t, y = rows_of(k)
             for tt in ((t + 1) % Lt, (t - 1) % Lt):
                 for d in range(4):
                     off = cs * (4 * f + d) + Lrow * (y + L * tt)
                     assert 0 <= off and off + Lrow <= kferm
                     assert (off * elem) % 16 == 0
             tloads.append((f, (t + 1) % Lt, (t - 1) % Lt, y))
+            pr["tissued"] += 1
+            pr["k"] += 1
+            return True
 
-        tdone = set()
-        while st["issued"] < 3 and st["rho_a"] < rho1:
-            issue()
-        issue_t()
-        while st["issued"] < NS and st["rho_a"] < rho1:
-            issue()
-        while len(tloads) < NT and len(tloads) < nk:
-            issue_t()
-        u, run_prev = 0, rho0 // L
-        for k, rho in enumerate(range(rho0, rho1)):
-            run = rho // L
-            if run != run_prev:
-                u += 2
-                run_prev = run
-            f, t, y = run // Lt, run % Lt, rho - run * L
-            for w in range(3):
-                assert u + w < st["issued"] and slots[(u + w) % NS] == u + w
-            assert k < len(tloads) and tslots[k % NT] == k
-            assert loads[u] == (f, t, (y - 1) % L)
-            assert loads[u + 1] == (f, t, y)
-            assert loads[u + 2] == (f, t, (y + 1) % L)
+        for k in range(nk):
+            # the producer runs as far ahead as its slots allow
+            while producer_step():
+                pass
+            f, t, y = rows_of(k)
+            w0 = u[k]
+            assert w0 + 2 < pr["issued"] and k < pr["tissued"], ("consumer would wait forever", k)
+            for w in range(w0, w0 + 3):
+                assert slot_y[w % NS] == w
+            assert slot_t[k % NT] == k
+            assert loads[w0] == (f, t, (y - 1) % L)
+            assert loads[w0 + 1] == (f, t, y)
+            assert loads[w0 + 2] == (f, t, (y + 1) % L)
             assert tloads[k] == (f, (t + 1) % Lt, (t - 1) % Lt, y)
-            u += 1
-            next_u = u + 2 if (rho + 1 < rho1 and (rho + 1) // L != run) else u
-            done.update(range(next_u))
-            tdone.add(k)
-            while st["rho_a"] < rho1 and st["issued"] < next_u + NS:
-                issue()
-            while len(tloads) < nk and len(tloads) < k + 1 + NT:
-                issue_t()
-        assert st["issued"] <= u + 2   # all issued copies were waited on
-        assert len(tloads) == nk
+            if k + 1 < nk:
+                nrel = 3 if (y + 1) == L else 1
+                assert u[k + 1] == w0 + nrel
+                released_y.update(range(w0, w0 + nrel))
+            released_t.add(k)
+        while producer_step():
+            pass
+        assert pr["k"] == nk and pr["issued"] == u[nk - 1] + 3
 
 
 SHAPES = [(24, 24, 24), (16, 16, 16), (16, 16, 32), (12, 12, 8), (8, 8, 8), (4, 4, 4),
-          (3, 5, 2), (6, 4, 7), (24, 24, 16), (32, 32, 16), (2, 2, 4), (5, 3, 8), (6, 6, 5)]
+          (3, 5, 2), (6, 4, 7), (24, 24, 16), (32, 32, 16), (2, 2, 4), (5, 3, 8), (6, 6, 5),
+          (1, 3, 4), (4, 1, 4)]
 
 
 @pytest.mark.parametrize("L,Lt,Ls", SHAPES)
