@@ -127,9 +127,6 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void fence_proxy_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -400,7 +397,11 @@ __device__ __forceinline__ void dwf_apply_rows(T acc[PPT][4], const S* c, const 
 // ---- the producer: lane 0 of the block's last warp -----------------------------
 // Issues the window loads and t entries in the order the consumers need
 // them, each after its slot's previous use has been released, then waits
-// (bounded) for the copies it has in flight.
+// (bounded) for the copies it has in flight.  The consumers' reads of a slot
+// are ordered before its refill by the empty barrier alone (their arrive
+// releases, the producer's wait acquires); no proxy fence is taken between
+// copies, since one waits for the copies already in flight and would leave
+// a single copy in flight at a time.
 template <class T>
 __device__ __forceinline__ void row_produce(const Geom& g, const RowPlan& rp, uint64_t* bar,
                                             T* slots, const T* src, int rho0, int rho1,
@@ -442,7 +443,6 @@ __device__ __forceinline__ void row_produce(const Geom& g, const RowPlan& rp, ui
             const int wr = ra / L, wf = wr / Lt, wt = wr - wf * Lt;
             int wy = ra - wr * L - 1 + o;
             wy = wy < 0 ? wy + L : (wy >= L ? wy - L : wy);
-            fence_proxy_async_smem();
             mbar_arrive_expect_tx(bar + e, 4 * bytes);
             T* dst = slots + (int64_t)e * 4 * Lrow;
             const int64_t off = (int64_t)Lrow * (wy + (int64_t)L * wt);
@@ -464,7 +464,6 @@ __device__ __forceinline__ void row_produce(const Geom& g, const RowPlan& rp, ui
             break;
         }
         const int tp = t + 1 == Lt ? 0 : t + 1, tm = t == 0 ? Lt - 1 : t - 1;
-        fence_proxy_async_smem();
         mbar_arrive_expect_tx(bar + kRowFullT + e, 8 * bytes);
         T* dst = tslots + (int64_t)e * 8 * Lrow;
         const int64_t op = (int64_t)Lrow * (y + (int64_t)L * tp);
