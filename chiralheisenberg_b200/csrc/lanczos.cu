@@ -1303,34 +1303,78 @@ __global__ void __launch_bounds__(kThreads) k_lz_walls_of(LzArgsT<T> a, const T*
     a.wbasis[(int64_t)j * 8 * cs2 + t] = r[(sw ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * site + a.g.cs * c];
 }
 
-// q_j's wall slices (j = 1..m) from the wall store into every pole's two-slice
-// x_k: the same sums, in the same order, as from the full stored vectors.
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_lz_accum_walls_c(LzArgsT<T> a, int m) {
+// q_j's wall slices (j = 1..m) into every pole's two-slice x_k: the same
+// sums, in the same order, as from the full stored vectors.  One thread per
+// wall element (slice, component, site) and NC poles per pass (one pass for
+// up to 24 poles), so the store is read once or twice; the pass's y_kj and 1/beta_j
+// are staged in shared memory kYChunk iterations at a time.  STORE: the q_j
+// come from the wall store (coalesced), else from the stored basis.
+constexpr int kYChunk = 32;
+template <class T, int NC, bool STORE>
+__global__ void __launch_bounds__(kThreads, 2) k_lz_accum_walls(LzArgsT<T> a, int m, int k0) {
     typedef typename real_of<T>::type Real;
+    __shared__ double ys[NC][kYChunk];
+    __shared__ Real ibs[kYChunk];
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t cs2 = 2 * (int64_t)a.g.kvol, kf2 = 8 * cs2;
-    if (t >= kf2) return;
+    const bool act = t < kf2;
+    int64_t e = t, stride = kf2;
+    const T* src = a.wbasis;
+    if (!STORE) {
+        const int c = act ? (int)(t / cs2) : 0;             // component
+        const int64_t r = act ? t - c * cs2 : 0;           // s' + 2 site
+        e = ((r & 1) ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * (r >> 1) + a.g.cs * c;
+        stride = a.g.kferm;
+        src = a.basis;
+    }
     const int64_t H = kMaxIter + 2;
     const int n = a.npole;
-    for (int k0 = 0; k0 < n; k0 += 8) {
-        double2 acc[8];
+    double2 acc[NC];
 #pragma unroll
-        for (int k = 0; k < 8; k++) acc[k] = make_double2(0.0, 0.0);
-        for (int j = 1; j <= m; j++) {
-            const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(a.wbasis + j * kf2 + t)));
+    for (int k = 0; k < NC; k++) acc[k] = make_double2(0.0, 0.0);
+    for (int j0 = 1; j0 <= m; j0 += kYChunk) {
+        const int jn = m - j0 + 1 < kYChunk ? m - j0 + 1 : kYChunk;
+        __syncthreads();
+        for (int i = threadIdx.x; i < NC * kYChunk; i += blockDim.x) {
+            const int k = i / kYChunk, jj = i - k * kYChunk;
+            ys[k][jj] = (k0 + k < n && jj < jn) ? a.h.y[(k0 + k) * H + j0 + jj] : 0.0;
+        }
+        for (int i = threadIdx.x; i < kYChunk; i += blockDim.x)
+            ibs[i] = i < jn ? (Real)a.h.invbeta[j0 + i] : (Real)0;
+        __syncthreads();
+        if (act) {
+            // q_{j+1} is loaded while q_j is accumulated
+            const T* b = src + e + j0 * stride;
+            T qn = __ldg(b);
+#pragma unroll 1
+            for (int jj = 0; jj < jn; jj++) {
+                const T q = qn;
+                if (jj + 1 < jn) qn = __ldg(b + (jj + 1) * stride);
+                const double2 qj = widen(zscal(ibs[jj], q));
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                if (k0 + k < n) {
-                    const double y = a.h.y[(k0 + k) * H + j];
+                for (int k = 0; k < NC; k++) {
+                    const double y = ys[k][jj];
                     acc[k].x += y * qj.x;
                     acc[k].y += y * qj.y;
                 }
             }
         }
+    }
+    if (!act) return;
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-            if (k0 + k < n) a.xw[(k0 + k) * kf2 + t] = acc[k];
+    for (int k = 0; k < NC; k++)
+        if (k0 + k < n) a.xw[(k0 + k) * kf2 + t] = acc[k];
+}
+
+template <class T, bool STORE>
+static void launch_accum_walls(const LzArgsT<T>& a, int m, int n, int64_t kvol, cudaStream_t st) {
+    const unsigned nb = (unsigned)((16 * kvol + kThreads - 1) / kThreads);
+    for (int k0 = 0; k0 < n; k0 += 24) {
+        const int left = n - k0;
+        if (left <= 8) k_lz_accum_walls<T, 8, STORE><<<nb, kThreads, 0, st>>>(a, m, k0);
+        else if (left <= 16) k_lz_accum_walls<T, 16, STORE><<<nb, kThreads, 0, st>>>(a, m, k0);
+        else k_lz_accum_walls<T, 24, STORE><<<nb, kThreads, 0, st>>>(a, m, k0);
+        count_launches(1);
     }
 }
 
@@ -1386,42 +1430,6 @@ __global__ void __launch_bounds__(kThreads) k_lz_accum_poles(LzArgsT<T> a, int m
         if (k0 + k < n) xk[k0 + k][e] = acc[k];
 }
 
-// Two-slice x_k of every pole from the stored basis (force solves):
-// thread per wall element (slice, component, site), poles in chunks of 8.
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_lz_accum_walls(LzArgsT<T> a, int m) {
-    typedef typename real_of<T>::type Real;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t cs2 = 2 * (int64_t)a.g.kvol;
-    if (t >= 8 * cs2) return;
-    const int c = (int)(t / cs2);                     // component
-    const int64_t r = t - c * cs2;                    // s' + 2 site
-    const int sw = (int)(r & 1);
-    const int64_t site = r >> 1;
-    const int64_t e = (sw ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * site + a.g.cs * c;
-    const int64_t H = kMaxIter + 2, kf2 = 8 * cs2;
-    const int n = a.npole;
-    const int64_t stride = a.g.kferm;
-    for (int k0 = 0; k0 < n; k0 += 8) {
-        double2 acc[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) acc[k] = make_double2(0.0, 0.0);
-        for (int j = 1; j <= m; j++) {
-            const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(a.basis + j * stride + e)));
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                if (k0 + k < n) {
-                    const double y = a.h.y[(k0 + k) * H + j];
-                    acc[k].x += y * qj.x;
-                    acc[k].y += y * qj.y;
-                }
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++)
-            if (k0 + k < n) a.xw[(k0 + k) * kf2 + r + cs2 * c] = acc[k];
-    }
-}
 
 template <class T>
 static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, float res, int ndiag,
@@ -1585,13 +1593,9 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
                 count_launches(1);
             }
         } else if (a.wcap > 0) {
-            k_lz_accum_walls_c<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads),
-                                    kThreads, 0, st>>>(a, m);
-            count_launches(1);
+            launch_accum_walls<T, true>(a, m, ndiag, g.kvol, st);
         } else {
-            k_lz_accum_walls<T><<<(unsigned)((16 * (int64_t)g.kvol + kThreads - 1) / kThreads),
-                                  kThreads, 0, st>>>(a, m);
-            count_launches(1);
+            launch_accum_walls<T, false>(a, m, ndiag, g.kvol, st);
         }
         w.timer.end(st);
     } else {
