@@ -16,12 +16,40 @@
 
 namespace chdwf {
 
+// Unsigned division by a divisor fixed at set-up, for numerators below 2^31:
+// q = (umulhi(n, m) + n) >> l with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1 (Granlund and Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994, the round-up method
+// with an added numerator).  Three integer instructions instead of the
+// reciprocal sequence a division by a run-time value compiles to.
+struct FastDiv {
+    uint32_t d, m, l;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    f.l = 0;
+    while ((1ull << f.l) < d) f.l++;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << f.l) - d)) / d) + 1);
+    return f;
+}
+__host__ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+#ifdef __CUDA_ARCH__
+    const uint32_t t = __umulhi(n, f.m);
+#else
+    const uint32_t t = (uint32_t)(((uint64_t)n * f.m) >> 32);
+#endif
+    return (t + n) >> f.l;
+}
+
 struct Geom {
     int L, Lt, Ls;
     int kvol;         // L*L*Lt
     int64_t npts;     // kvol*Ls
     int64_t cs;       // component-plane stride = npts
     int64_t kferm;    // 8*npts complex numbers
+    FastDiv dLs, dL, dLL;   // division by Ls, L, L*L (point decoding)
+    FastDiv dPi;            // by Ls/2 - 2, the interior point pairs of a site (Ls >= 6)
 };
 
 // Lattices are limited to 2^31 - 1 points (kthird*ksize^2*ksizet), far
@@ -39,6 +67,10 @@ inline Geom make_geom(int L, int Lt, int Ls) {
     g.npts = (int64_t)g.kvol * Ls;
     g.cs = g.npts;
     g.kferm = 8 * g.npts;
+    g.dLs = make_fastdiv((uint32_t)Ls);
+    g.dL = make_fastdiv((uint32_t)L);
+    g.dLL = make_fastdiv((uint32_t)L * (uint32_t)L);
+    g.dPi = make_fastdiv(Ls >= 6 ? (uint32_t)(Ls / 2 - 2) : 1u);
     return g;
 }
 

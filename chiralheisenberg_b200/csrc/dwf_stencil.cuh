@@ -46,18 +46,18 @@ struct PointIdx {
     int64_t p;   // s + Ls*site
 };
 
-// Coordinates of point p (p < 2^31: see kMaxPoints), in 32-bit arithmetic.
+// Coordinates of point p (p < 2^31: see kMaxPoints), in 32-bit arithmetic
+// with the geometry's precomputed divisions.
 __device__ __forceinline__ PointIdx point_of(const Geom& g, int64_t p) {
     PointIdx q;
     q.p = p;
     const unsigned up = (unsigned)p, Ls = (unsigned)g.Ls, L = (unsigned)g.L;
-    const unsigned site = up / Ls;
+    const unsigned site = fdiv(up, g.dLs);
     q.s = (int)(up - site * Ls);
     q.site = (int)site;
-    const unsigned LL = L * L;
-    const unsigned it = site / LL;
-    const unsigned rem = site - it * LL;
-    const unsigned iy = rem / L;
+    const unsigned it = fdiv(site, g.dLL);
+    const unsigned rem = site - it * (L * L);
+    const unsigned iy = fdiv(rem, g.dL);
     q.it = (int)it;
     q.iy = (int)iy;
     q.ix = (int)(rem - iy * L);
@@ -219,7 +219,10 @@ struct LdF2 {
 // layout has s innermost, so an even point and its successor are adjacent),
 // which doubles the bytes per load instruction; each point's elements go
 // through the same operation sequence as dwf_apply_flavour.  Needs Ls even.
-template <bool DAG, int IMASS>
+// WALL = false is for interior pairs (2 <= s <= Ls-4): both s hops of both
+// points exist and neither point is on a wall, so the code has no branch on
+// s and no wall terms.
+template <bool DAG, int IMASS, bool WALL = true>
 __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
                                                        const float2* __restrict__ in,
                                                        const Geom& g, const PointIdx& q, int f,
@@ -287,7 +290,7 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
         float2 c0, c1;
         ld2(q.p + fo + cs * d, c0, c1);
         acc[0][d] = zsub(acc[0][d], c1);
-        if (q.s + 2 < Ls) {
+        if (!WALL || q.s + 2 < Ls) {
             float2 n0, n1;
             ld2(q.p + 2 + fo + cs * d, n0, n1);
             acc[1][d] = zsub(acc[1][d], n0);
@@ -297,13 +300,14 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
     for (int d = DN; d < DN + 2; d++) {
         float2 c0, c1;
         ld2(q.p + fo + cs * d, c0, c1);
-        if (q.s > 0) {
+        if (!WALL || q.s > 0) {
             float2 p0, p1;
             ld2(q.p - 2 + fo + cs * d, p0, p1);
             acc[0][d] = zsub(acc[0][d], p1);
         }
         acc[1][d] = zsub(acc[1][d], c0);
     }
+    if (!WALL) return;
     // wall coupling: point 1 at s=Ls (pair WA, reads s=1), point 0 at s=1
     // (pair WB, reads s=Ls)
     constexpr int WA = DAG ? 0 : 2;
