@@ -49,7 +49,6 @@ struct Geom {
     int64_t cs;       // component-plane stride = npts
     int64_t kferm;    // 8*npts complex numbers
     FastDiv dLs, dL, dLL;   // division by Ls, L, L*L (point decoding)
-    FastDiv dPi;            // by Ls/2 - 2, the interior point pairs of a site (Ls >= 6)
 };
 
 // Lattices are limited to 2^31 - 1 points (kthird*ksize^2*ksizet), far
@@ -70,7 +69,6 @@ inline Geom make_geom(int L, int Lt, int Ls) {
     g.dLs = make_fastdiv((uint32_t)Ls);
     g.dL = make_fastdiv((uint32_t)L);
     g.dLL = make_fastdiv((uint32_t)L * (uint32_t)L);
-    g.dPi = make_fastdiv(Ls >= 6 ? (uint32_t)(Ls / 2 - 2) : 1u);
     return g;
 }
 

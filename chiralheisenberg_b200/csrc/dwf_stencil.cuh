@@ -219,10 +219,7 @@ struct LdF2 {
 // layout has s innermost, so an even point and its successor are adjacent),
 // which doubles the bytes per load instruction; each point's elements go
 // through the same operation sequence as dwf_apply_flavour.  Needs Ls even.
-// WALL = false is for interior pairs (2 <= s <= Ls-4): both s hops of both
-// points exist and neither point is on a wall, so the code has no branch on
-// s and no wall terms.
-template <bool DAG, int IMASS, bool WALL = true>
+template <bool DAG, int IMASS>
 __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
                                                        const float2* __restrict__ in,
                                                        const Geom& g, const PointIdx& q, int f,
@@ -290,7 +287,7 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
         float2 c0, c1;
         ld2(q.p + fo + cs * d, c0, c1);
         acc[0][d] = zsub(acc[0][d], c1);
-        if (!WALL || q.s + 2 < Ls) {
+        if (q.s + 2 < Ls) {
             float2 n0, n1;
             ld2(q.p + 2 + fo + cs * d, n0, n1);
             acc[1][d] = zsub(acc[1][d], n0);
@@ -300,14 +297,13 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
     for (int d = DN; d < DN + 2; d++) {
         float2 c0, c1;
         ld2(q.p + fo + cs * d, c0, c1);
-        if (!WALL || q.s > 0) {
+        if (q.s > 0) {
             float2 p0, p1;
             ld2(q.p - 2 + fo + cs * d, p0, p1);
             acc[0][d] = zsub(acc[0][d], p1);
         }
         acc[1][d] = zsub(acc[1][d], c0);
     }
-    if (!WALL) return;
     // wall coupling: point 1 at s=Ls (pair WA, reads s=1), point 0 at s=1
     // (pair WB, reads s=Ls)
     constexpr int WA = DAG ? 0 : 2;

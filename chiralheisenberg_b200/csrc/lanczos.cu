@@ -113,42 +113,6 @@ __device__ __forceinline__ PtRange block_range(int64_t npts) {
     return r;
 }
 
-// Task order of the FP32 two-point pass-1 kernels.  Block b takes sites
-// [b kvol / nb, (b+1) kvol / nb).  Its wall pairs (s = 0 and s = Ls-2 of
-// every site and flavour) come first, padded to whole warps, then its
-// interior pairs, so a warp runs either the wall terms or none of them (the
-// wall branches of a warp that held both kinds took a quarter of the
-// instructions).  Body::run<WALL>(p, f) evaluates the pair at even point p
-// of flavour f.  Needs Ls even.
-template <class Body>
-__device__ __forceinline__ void pair_tasks(const Geom& g, Body& body) {
-    const int64_t nb = gridDim.x, b = blockIdx.x;
-    const int S0 = (int)(b * g.kvol / nb), S1 = (int)((b + 1) * g.kvol / nb);
-    const int ns = S1 - S0, Ls = g.Ls;
-    const int nwps = Ls == 2 ? 1 : 2;           // wall pairs per site and flavour
-    const int Pi = Ls / 2 - nwps;               // interior pairs per site (0 for Ls < 6)
-    const int nwf = ns * nwps, nw = 2 * nwf, nw32 = (nw + 31) & ~31;
-    const int nif = ns * Pi, ntask = nw32 + 2 * nif;
-#pragma unroll 1
-    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-        if (t < nw32) {
-            if (t >= nw) continue;
-            const int f = t >= nwf ? 1 : 0;
-            const int r = t - f * nwf;
-            const int site = S0 + (nwps == 2 ? (r >> 1) : r);
-            const int s = (nwps == 2 && (r & 1)) ? Ls - 2 : 0;
-            body.template run<true>((int64_t)s + (int64_t)Ls * site, f);
-        } else {
-            const int v = t - nw32;
-            const int f = v >= nif ? 1 : 0;
-            const int r = v - f * nif;
-            const int qd = (int)fdiv((uint32_t)r, g.dPi);
-            body.template run<false>((int64_t)(2 * (1 + r - qd * Pi)) + (int64_t)Ls * (S0 + qd),
-                                     f);
-        }
-    }
-}
-
 // One block pass over points [base, base + unit) of flavour(s) f0..f0+NF-1
 // (PAIR: p is the even point of the thread's pair).
 template <class T, bool PAIR = false>
@@ -187,30 +151,6 @@ __device__ __forceinline__ void apply_scaled(T acc[4], const T* r, typename real
     for (int d = 0; d < 4; d++) acc[d] = zscal(ib, acc[d]);
 }
 
-// Bodies of the FP32 two-point pass-1 kernels (pair_tasks order).
-template <int IMASS>
-struct LzPairM {
-    const LzArgsT<float2>& a;
-    const float2* rj;
-    float ib;
-    double loc;
-    template <bool WALL>
-    __device__ __forceinline__ void run(int64_t p, int f) {
-        const PointIdx q = point_of(a.g, p);
-        float2 acc[2][4];
-        dwf_apply_flavour_pair<false, IMASS, WALL>(acc, rj, a.g, q, f, a.chif, a.diag, a.hpin,
-                                                   a.apbc != 0);
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-            const float2 v0 = zscal(ib, acc[0][d]), v1 = zscal(ib, acc[1][d]);
-            st_pair(a.vt, p + a.g.cs * (d + 4 * f), v0, v1);
-            const double2 w0 = widen(v0), w1 = widen(v1);
-            loc += w0.x * w0.x + w0.y * w0.y;
-            loc += w1.x * w1.x + w1.y * w1.y;
-        }
-    }
-};
-
 // ---- pass 1, kernel 1: vt = M q_j and the block partials of |vt|^2 ---------
 // beta_j is the sum of the previous M^dagger launch's partials (beta_1 comes
 // from the source), formed by every block.  The partial buffers: part[0..nb)
@@ -235,13 +175,8 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
     }
     const T* rj = ring(a, j);
     const Real ib = (Real)ibj;
-    double loc = 0.0;
-    if constexpr (PAIR) {
-        LzPairM<IMASS> body{a, rj, ib, 0.0};
-        pair_tasks(a.g, body);
-        loc = body.loc;
-    } else {
     const PtRange R = block_range(a.g.npts);
+    double loc = 0.0;
 #pragma unroll 1
     for (int64_t base = R.begin; base < R.end; base += S::unit) {
         int64_t p;
@@ -249,7 +184,19 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
         lz_lane<T, PAIR>(base, &p, &f0);
         if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
-        {
+        if constexpr (PAIR) {
+            float2 acc[2][4];
+            dwf_apply_flavour_pair<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                 a.apbc != 0);
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const float2 v0 = zscal(ib, acc[0][d]), v1 = zscal(ib, acc[1][d]);
+                st_pair(a.vt, p + a.g.cs * (d + 4 * f0), v0, v1);
+                const double2 w0 = widen(v0), w1 = widen(v1);
+                loc += w0.x * w0.x + w0.y * w0.y;
+                loc += w1.x * w1.x + w1.y * w1.y;
+            }
+        } else {
 #pragma unroll
             for (int f = f0; f < f0 + NF; f++) {
                 T acc[4];
@@ -262,7 +209,6 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
                 }
             }
         }
-    }
     }
     __shared__ double sh[kThreads / 32];
     loc = block_sum<kThreads>(loc, sh);
@@ -382,36 +328,6 @@ __device__ __forceinline__ void wall_put(const LzArgsT<T>& a, int j1, int s, int
     a.wbasis[(int64_t)j1 * 8 * cs2 + (s == 0 ? 0 : 1) + 2 * (int64_t)site + cs2 * c] = v;
 }
 
-template <int IMASS, bool WALLS>
-struct LzPairMd {
-    const LzArgsT<float2>& a;
-    float2* rn;
-    int j;
-    double at;
-    double loc;
-    template <bool WALL>
-    __device__ __forceinline__ void run(int64_t p, int f) {
-        const PointIdx q = point_of(a.g, p);
-        float2 acc[2][4];
-        dwf_apply_flavour_pair<true, IMASS, WALL>(acc, a.vt, a.g, q, f, a.chif, a.diag, a.hpin,
-                                                  a.apbc != 0);
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-            const int64_t e = p + a.g.cs * (d + 4 * f);
-            float2 v0, v1;
-            three_term_pair(a, acc[0][d], acc[1][d], e, j, at, v0, v1);
-            st_pair(rn, e, v0, v1);
-            if (WALLS && WALL) {
-                wall_put(a, j + 1, q.s, q.site, d + 4 * f, v0);
-                wall_put(a, j + 1, q.s + 1, q.site, d + 4 * f, v1);
-            }
-            const double2 w0 = widen(v0), w1 = widen(v1);
-            loc += w0.x * w0.x + w0.y * w0.y;
-            loc += w1.x * w1.x + w1.y * w1.y;
-        }
-    }
-};
-
 // ---- pass 1, kernel 2: r_{j+1} = M^dagger vt - alpha~ q_j - beta_j q_{j-1} ---
 // alpha~_j is the sum of M(j)'s partials, formed by every block.
 template <class T, int IMASS, bool PAIR, bool WALLS, int OCC>
@@ -424,13 +340,8 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
     const int nb = gridDim.x;
     const double at = sum_partials(a.part, nb);
     T* rn = ring(a, j + 1);
-    double loc = 0.0;
-    if constexpr (PAIR) {
-        LzPairMd<IMASS, WALLS> body{a, rn, j, at, 0.0};
-        pair_tasks(a.g, body);
-        loc = body.loc;
-    } else {
     const PtRange R = block_range(a.g.npts);
+    double loc = 0.0;
 #pragma unroll 1
     for (int64_t base = R.begin; base < R.end; base += S::unit) {
         int64_t p;
@@ -438,7 +349,25 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
         lz_lane<T, PAIR>(base, &p, &f0);
         if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
-        {
+        if constexpr (PAIR) {
+            float2 acc[2][4];
+            dwf_apply_flavour_pair<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                a.apbc != 0);
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const int64_t e = p + a.g.cs * (d + 4 * f0);
+                float2 v0, v1;
+                three_term_pair(a, acc[0][d], acc[1][d], e, j, at, v0, v1);
+                st_pair(rn, e, v0, v1);
+                if (WALLS) {
+                    wall_put(a, j + 1, q.s, q.site, d + 4 * f0, v0);
+                    wall_put(a, j + 1, q.s + 1, q.site, d + 4 * f0, v1);
+                }
+                const double2 w0 = widen(v0), w1 = widen(v1);
+                loc += w0.x * w0.x + w0.y * w0.y;
+                loc += w1.x * w1.x + w1.y * w1.y;
+            }
+        } else {
 #pragma unroll
             for (int f = f0; f < f0 + NF; f++) {
                 T acc[4];
@@ -455,7 +384,6 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
                 }
             }
         }
-    }
     }
     __shared__ double sh[kThreads / 32];
     loc = block_sum<kThreads>(loc, sh);
