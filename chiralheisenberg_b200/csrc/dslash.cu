@@ -280,6 +280,133 @@ __global__ void __launch_bounds__(kSplitThreads, OCC)
     }
 }
 
+// ---- FP16 storage, four points a thread ----------------------------------------
+// Point q (s a multiple of 4) and its three successors s+1..s+3 of flavour f:
+// every load is one 16-byte access of four FP16 complex numbers (the layout
+// has s innermost), so FP16 moves as many bytes per load instruction as the
+// FP32 two-point kernel.  Each element goes through dwf_apply_flavour's
+// operation sequence in FP32.  Needs Ls a multiple of 4.
+__device__ __forceinline__ float2 h4_get(const uint4& v, int p) {
+    const uint32_t w = p == 0 ? v.x : (p == 1 ? v.y : (p == 2 ? v.z : v.w));
+    return __half22float2(*reinterpret_cast<const __half2*>(&w));
+}
+__device__ __forceinline__ uint32_t h2_bits(float2 v) {
+    const __half2 h = __float22half2_rn(v);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+template <bool DAG, int IMASS>
+__device__ __forceinline__ void dwf_apply_flavour_quad_f16(float2 acc[4][4],
+                                                           const __half2* __restrict__ in,
+                                                           const Geom& g, const PointIdx& q,
+                                                           int f, const float* __restrict__ chif,
+                                                           float diag, float hpin, bool apbc) {
+    constexpr int SF = DAG ? -1 : 1;
+    const int L = g.L, Lt = g.Lt, Ls = g.Ls;
+    const int64_t LsI = Ls, cs = g.cs, fo = g.cs * (4 * f);
+    auto ld4 = [&](int64_t n) { return __ldg(reinterpret_cast<const uint4*>(in + n)); };
+    // diagonal term (:2651-2667)
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const uint4 v = ld4(q.p + fo + cs * d);
+#pragma unroll
+        for (int p = 0; p < 4; p++) acc[p][d] = zscal(diag, h4_get(v, p));
+    }
+    const int xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
+    const int yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
+    const int tp = q.it + 1 == Lt ? 0 : q.it + 1, tm = q.it == 0 ? Lt - 1 : q.it - 1;
+    const int64_t sb = q.s + fo;
+    const int64_t rowb = (int64_t)L * (q.iy + (int64_t)L * q.it);
+    const int64_t n_xp = sb + LsI * (xp + rowb), n_xm = sb + LsI * (xm + rowb);
+    const int64_t colb = q.ix + (int64_t)L * L * q.it;
+    const int64_t n_yp = sb + LsI * (colb + (int64_t)L * yp), n_ym = sb + LsI * (colb + (int64_t)L * ym);
+    const int64_t plb = q.ix + (int64_t)L * q.iy;
+    const int64_t n_tp = sb + LsI * (plb + (int64_t)L * L * tp), n_tm = sb + LsI * (plb + (int64_t)L * L * tm);
+#define CHDWF_QUAD_HOP(N, MU, SIG, NEG)                                                   \
+    {                                                                                    \
+        uint4 v[4];                                                                      \
+        _Pragma("unroll") for (int d = 0; d < 4; d++) v[d] = ld4((N) + cs * d);          \
+        _Pragma("unroll") for (int p = 0; p < 4; p++) {                                  \
+            float2 r[4];                                                                 \
+            _Pragma("unroll") for (int d = 0; d < 4; d++) r[d] = h4_get(v[d], p);        \
+            hop<MU, SIG, NEG>(acc[p], r);                                                \
+        }                                                                                \
+    }
+    CHDWF_QUAD_HOP(n_xp, 0, SF, false)
+    CHDWF_QUAD_HOP(n_xm, 0, -SF, false)
+    CHDWF_QUAD_HOP(n_yp, 1, SF, false)
+    CHDWF_QUAD_HOP(n_ym, 1, -SF, false)
+    CHDWF_QUAD_HOP(n_tp, 2, SF, false)
+    CHDWF_QUAD_HOP(n_tm, 2, -SF, false)
+    // kappa = 1/2 (:2815-2829)
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+#pragma unroll
+        for (int d = 0; d < 4; d++) acc[p][d] = zscal(0.5f, acc[p][d]);
+    // antiperiodic boundary in t (:2831-2876)
+    if (apbc) {
+        if (q.it == Lt - 1) CHDWF_QUAD_HOP(n_tp, 2, SF, true)
+        if (q.it == 0) CHDWF_QUAD_HOP(n_tm, 2, -SF, true)
+    }
+#undef CHDWF_QUAD_HOP
+    // s hops (:2879-2908; M^dagger :3313-3342): point p takes s+p+1 (the
+    // next point of the group, or the next group's first) and s+p-1 (the
+    // previous point, or the previous group's last)
+    constexpr int UP = DAG ? 0 : 2;
+    constexpr int DN = DAG ? 2 : 0;
+#pragma unroll
+    for (int d = UP; d < UP + 2; d++) {
+        const uint4 c = ld4(q.p + fo + cs * d);
+#pragma unroll
+        for (int p = 0; p < 3; p++) acc[p][d] = zsub(acc[p][d], h4_get(c, p + 1));
+        if (q.s + 4 < Ls) acc[3][d] = zsub(acc[3][d], h4_get(ld4(q.p + 4 + fo + cs * d), 0));
+    }
+#pragma unroll
+    for (int d = DN; d < DN + 2; d++) {
+        const uint4 c = ld4(q.p + fo + cs * d);
+        if (q.s > 0) acc[0][d] = zsub(acc[0][d], h4_get(ld4(q.p - 4 + fo + cs * d), 3));
+#pragma unroll
+        for (int p = 1; p < 4; p++) acc[p][d] = zsub(acc[p][d], h4_get(c, p - 1));
+    }
+    // wall coupling: point 3 at s=Ls (pair WA, reads s=1), point 0 at s=1
+    // (pair WB, reads s=Ls)
+    constexpr int WA = DAG ? 0 : 2;
+    constexpr int WB = DAG ? 2 : 0;
+    const bool atL = (q.s + 4 == Ls), at0 = (q.s == 0);
+    if (!(atL || at0)) return;
+    const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
+                c3f = __ldg(chif + 2 * g.kvol + q.site);
+    const bool pin = (q.site == 0);
+    if (atL)
+        wall_terms<DAG, IMASS, WA, 0>(acc[3], LdF16{in}, cs, LsI * q.site, f, c1f, c2f, c3f, pin,
+                                      hpin);
+    if (at0)
+        wall_terms<DAG, IMASS, WB, 1>(acc[0], LdF16{in}, cs, LsI * q.site + Ls - 1, f, c1f, c2f,
+                                      c3f, pin, hpin);
+}
+
+template <bool DAG, int IMASS>
+__global__ void __launch_bounds__(kSplitThreads, 2)
+    k_dslash_f16_quad(__half2* __restrict__ out, const __half2* __restrict__ in,
+                      const float* __restrict__ chif, Geom g, float diag, float hpin, int apbc) {
+    const int64_t p = (int64_t)blockIdx.x * (4 * kSplitPoints) +
+                      4 * (threadIdx.x & (kSplitPoints - 1));
+    const int f = split_flavour();
+    if (p >= g.npts) return;
+    const PointIdx q = point_of(g, p);
+    float2 acc[4][4];
+    dwf_apply_flavour_quad_f16<DAG, IMASS>(acc, in, g, q, f, chif, diag, hpin, apbc != 0);
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        uint4 o;
+        o.x = h2_bits(acc[0][d]);
+        o.y = h2_bits(acc[1][d]);
+        o.z = h2_bits(acc[2][d]);
+        o.w = h2_bits(acc[3][d]);
+        *reinterpret_cast<uint4*>(out + p + g.cs * (d + 4 * f)) = o;
+    }
+}
+
 void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, const float* chif,
                       const Geom& g, float am3, float hpin, int ibound, cudaStream_t st,
                       int variant) {
@@ -298,6 +425,19 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
         }
     }
     note_stencil(shape == kStencilGather4 && !half ? kStencilGather4 : kStencilGather3, 1);
+    if (half && g.Ls % 4 == 0) {
+        const unsigned nb4 = (unsigned)((g.npts + 4 * kSplitPoints - 1) / (4 * kSplitPoints));
+        const float diag = diag_of(am3);
+        const int apbc = ibound == -1;
+        __half2* o = (__half2*)out;
+        const __half2* i = (const __half2*)in;
+#define PQ(D, I) k_dslash_f16_quad<D, I><<<nb4, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
+        if (!dag) { if (imass == 3) PQ(false, 3); else PQ(false, 1); }
+        else { if (imass == 3) PQ(true, 3); else PQ(true, 1); }
+#undef PQ
+        count_launches(1);
+        return;
+    }
     if (!half && g.Ls % 2 == 0) {
         const unsigned nb2 = (unsigned)((g.npts + 2 * kSplitPoints - 1) / (2 * kSplitPoints));
         const float diag = diag_of(am3);
