@@ -438,7 +438,7 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
         count_launches(1);
         return;
     }
-    if (!half && g.Ls % 2 == 0) {
+    if (!half && pair_ok(g)) {
         const unsigned nb2 = (unsigned)((g.npts + 2 * kSplitPoints - 1) / (2 * kSplitPoints));
         const float diag = diag_of(am3);
         const int apbc = ibound == -1;

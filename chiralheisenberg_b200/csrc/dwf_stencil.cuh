@@ -113,6 +113,58 @@ __device__ __forceinline__ void wall_elem(T& a, T r1, T r2, int f, float c1f, fl
     }
 }
 
+// wall_elem with the wall known only at run time (side1: the s = 1 wall), so
+// a thread evaluates either wall with one code path instead of a warp
+// running both branches.  a - b is formed as a + (-b), the same IEEE result.
+template <class T> __device__ __forceinline__ T zneg_if(bool n, T v) {
+    return n ? zmake<T>(-v.x, -v.y) : v;
+}
+template <bool DAG, int IMASS, class T>
+__device__ __forceinline__ void wall_elem_rt(T& a, T r1, T r2, int f, bool side1, float c1f,
+                                             float c2f, float c3f, bool pin,
+                                             typename real_of<T>::type hpin) {
+    typedef typename real_of<T>::type R;
+    if (IMASS == 1) {
+        wall_elem<DAG, 1, 0>(a, r1, r2, f, c1f, c2f, c3f, pin, hpin);   // no side dependence
+    } else if (IMASS == 3) {
+        const T spm = zmake<T>((R)0, (R)(DAG ? -c3f : c3f));
+        const bool minus_first = DAG ? side1 : !side1;
+        const T sp = DAG ? zmake<T>((R)(-c2f), (R)(-c1f)) : zmake<T>((R)c2f, (R)c1f);
+        if (f == 0) {
+            const T t1 = zmul(spm, r1), u1 = zmul(sp, r2);
+            a = zadd(a, zneg_if(minus_first, t1));
+            a = zadd(a, zneg_if(minus_first, u1));
+        } else {
+            const T t2 = zmul(spm, r2), u2 = zmul(zconj(sp), r1);
+            a = zadd(a, zneg_if(!minus_first, t2));
+            a = zadd(a, zneg_if(!minus_first, u2));
+        }
+    }
+}
+
+// The wall update of one point at either wall (atL: s = Ls, else s = 1):
+// Dirac pair WA or WB takes the other wall's components of both flavours.
+template <bool DAG, int IMASS, class T, class Ld>
+__device__ __forceinline__ void wall_terms_rt(T acc[4], const Ld& ld, int64_t cs, int64_t other,
+                                              bool atL, int f, float c1f, float c2f, float c3f,
+                                              bool pin, typename real_of<T>::type hpin) {
+    constexpr int WA = DAG ? 0 : 2;
+    constexpr int WB = DAG ? 2 : 0;
+    const int d0 = atL ? WA : WB;
+    T a0 = atL ? acc[WA] : acc[WB], a1 = atL ? acc[WA + 1] : acc[WB + 1];
+    wall_elem_rt<DAG, IMASS>(a0, ld(other + cs * d0), ld(other + cs * (d0 + 4)), f, !atL, c1f,
+                             c2f, c3f, pin, hpin);
+    wall_elem_rt<DAG, IMASS>(a1, ld(other + cs * (d0 + 1)), ld(other + cs * (d0 + 5)), f, !atL,
+                             c1f, c2f, c3f, pin, hpin);
+    if (atL) {
+        acc[WA] = a0;
+        acc[WA + 1] = a1;
+    } else {
+        acc[WB] = a0;
+        acc[WB + 1] = a1;
+    }
+}
+
 // Wall coupling of one flavour at a wall point (s = Ls for SIDE 0, s = 1 for
 // SIDE 1): Dirac pair D0, D0+1 of flavour f takes the other wall's components
 // of both flavours.  Per element the operation sequence is that of the
@@ -186,17 +238,14 @@ __device__ __forceinline__ void dwf_apply_flavour(T acc[4], const Ld& ld, const 
 #pragma unroll
         for (int d = DN; d < DN + 2; d++) acc[d] = zsub(acc[d], ld(q.p - 1 + fo + cs * d));
     }
-    // wall coupling: pair WA at s=Ls reads s=1, pair WB at s=1 reads s=Ls
-    constexpr int WA = DAG ? 0 : 2;
-    constexpr int WB = DAG ? 2 : 0;
+    // wall coupling: the pair at s=Ls reads s=1, the pair at s=1 reads s=Ls
     const bool atL = (q.s == Ls - 1), at0 = (q.s == 0);
     if (!(atL || at0)) return;
     const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
                 c3f = __ldg(chif + 2 * g.kvol + q.site);
     const int64_t other = atL ? LsI * q.site : LsI * q.site + Ls - 1;
     const bool pin = (q.site == 0);
-    if (atL) wall_terms<DAG, IMASS, WA, 0>(acc, ld, cs, other, f, c1f, c2f, c3f, pin, hpin);
-    if (at0) wall_terms<DAG, IMASS, WB, 1>(acc, ld, cs, other, f, c1f, c2f, c3f, pin, hpin);
+    wall_terms_rt<DAG, IMASS>(acc, ld, cs, other, atL, f, c1f, c2f, c3f, pin, hpin);
 }
 
 // All eight components of one output point (one thread per point).
@@ -218,7 +267,11 @@ struct LdF2 {
 // load is one 16-byte float4 holding both points' components (the spinor
 // layout has s innermost, so an even point and its successor are adjacent),
 // which doubles the bytes per load instruction; each point's elements go
-// through the same operation sequence as dwf_apply_flavour.  Needs Ls even.
+// through the same operation sequence as dwf_apply_flavour.  Needs Ls even
+// and kferm < 2^31: element indices are 32-bit (pair_ok), which halves the
+// address arithmetic of its 34 loads.
+inline bool pair_ok(const Geom& g) { return g.Ls % 2 == 0 && g.kferm < (int64_t(1) << 31); }
+
 template <bool DAG, int IMASS>
 __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
                                                        const float2* __restrict__ in,
@@ -227,8 +280,9 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
                                                        float hpin, bool apbc) {
     constexpr int SF = DAG ? -1 : 1;
     const int L = g.L, Lt = g.Lt, Ls = g.Ls;
-    const int64_t LsI = Ls, cs = g.cs, fo = g.cs * (4 * f);
-    auto ld2 = [&](int64_t n, float2& r0, float2& r1) {
+    const uint32_t LsI = (uint32_t)Ls, cs = (uint32_t)g.cs, fo = cs * (uint32_t)(4 * f);
+    const uint32_t qp = (uint32_t)q.p;
+    auto ld2 = [&](uint32_t n, float2& r0, float2& r1) {
         const float4 v = __ldg(reinterpret_cast<const float4*>(in + n));
         r0 = make_float2(v.x, v.y);
         r1 = make_float2(v.z, v.w);
@@ -237,20 +291,21 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
 #pragma unroll
     for (int d = 0; d < 4; d++) {
         float2 r0, r1;
-        ld2(q.p + fo + cs * d, r0, r1);
+        ld2(qp + fo + cs * d, r0, r1);
         acc[0][d] = zscal(diag, r0);
         acc[1][d] = zscal(diag, r1);
     }
-    const int xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
-    const int yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
-    const int tp = q.it + 1 == Lt ? 0 : q.it + 1, tm = q.it == 0 ? Lt - 1 : q.it - 1;
-    const int64_t sb = q.s + fo;
-    const int64_t rowb = (int64_t)L * (q.iy + (int64_t)L * q.it);
-    const int64_t n_xp = sb + LsI * (xp + rowb), n_xm = sb + LsI * (xm + rowb);
-    const int64_t colb = q.ix + (int64_t)L * L * q.it;
-    const int64_t n_yp = sb + LsI * (colb + (int64_t)L * yp), n_ym = sb + LsI * (colb + (int64_t)L * ym);
-    const int64_t plb = q.ix + (int64_t)L * q.iy;
-    const int64_t n_tp = sb + LsI * (plb + (int64_t)L * L * tp), n_tm = sb + LsI * (plb + (int64_t)L * L * tm);
+    const uint32_t uL = (uint32_t)L;
+    const uint32_t xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
+    const uint32_t yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
+    const uint32_t tp = q.it + 1 == Lt ? 0 : q.it + 1, tm = q.it == 0 ? Lt - 1 : q.it - 1;
+    const uint32_t sb = (uint32_t)q.s + fo;
+    const uint32_t rowb = uL * ((uint32_t)q.iy + uL * (uint32_t)q.it);
+    const uint32_t n_xp = sb + LsI * (xp + rowb), n_xm = sb + LsI * (xm + rowb);
+    const uint32_t colb = (uint32_t)q.ix + uL * uL * (uint32_t)q.it;
+    const uint32_t n_yp = sb + LsI * (colb + uL * yp), n_ym = sb + LsI * (colb + uL * ym);
+    const uint32_t plb = (uint32_t)q.ix + uL * (uint32_t)q.iy;
+    const uint32_t n_tp = sb + LsI * (plb + uL * uL * tp), n_tm = sb + LsI * (plb + uL * uL * tm);
     float2 r0[4], r1[4];
 #define CHDWF_PAIR_HOP(N, MU, SIG, NEG)                                         \
     {                                                                          \
@@ -285,21 +340,21 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
 #pragma unroll
     for (int d = UP; d < UP + 2; d++) {
         float2 c0, c1;
-        ld2(q.p + fo + cs * d, c0, c1);
+        ld2(qp + fo + cs * d, c0, c1);
         acc[0][d] = zsub(acc[0][d], c1);
         if (q.s + 2 < Ls) {
             float2 n0, n1;
-            ld2(q.p + 2 + fo + cs * d, n0, n1);
+            ld2(qp + 2 + fo + cs * d, n0, n1);
             acc[1][d] = zsub(acc[1][d], n0);
         }
     }
 #pragma unroll
     for (int d = DN; d < DN + 2; d++) {
         float2 c0, c1;
-        ld2(q.p + fo + cs * d, c0, c1);
+        ld2(qp + fo + cs * d, c0, c1);
         if (q.s > 0) {
             float2 p0, p1;
-            ld2(q.p - 2 + fo + cs * d, p0, p1);
+            ld2(qp - 2 + fo + cs * d, p0, p1);
             acc[0][d] = zsub(acc[0][d], p1);
         }
         acc[1][d] = zsub(acc[1][d], c0);
@@ -313,11 +368,24 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
     const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
                 c3f = __ldg(chif + 2 * g.kvol + q.site);
     const bool pin = (q.site == 0);
-    if (atL)
+    if (atL && at0) {   // Ls = 2: one pair holds both walls
         wall_terms<DAG, IMASS, WA, 0>(acc[1], LdF2{in}, cs, LsI * q.site, f, c1f, c2f, c3f, pin, hpin);
-    if (at0)
         wall_terms<DAG, IMASS, WB, 1>(acc[0], LdF2{in}, cs, LsI * q.site + Ls - 1, f, c1f, c2f, c3f,
                                       pin, hpin);
+        return;
+    }
+    // one wall point: point 1 at s=Ls or point 0 at s=1, through one code path
+    float2 w[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) w[d] = atL ? acc[1][d] : acc[0][d];
+    wall_terms_rt<DAG, IMASS>(w, LdF2{in}, (int64_t)cs,
+                              atL ? (int64_t)LsI * q.site : (int64_t)LsI * q.site + Ls - 1, atL, f,
+                              c1f, c2f, c3f, pin, hpin);
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        if (atL) acc[1][d] = w[d];
+        else acc[0][d] = w[d];
+    }
 }
 
 // Thread -> (point, flavour) map of the flavour-split kernels: a block of

@@ -130,12 +130,12 @@ __device__ __forceinline__ void lz_lane(int64_t base, int64_t* p, int* f0) {
 }
 
 // 16-byte access to two adjacent FP32 complex numbers (e even).
-__device__ __forceinline__ void ld_pair(const float2* b, int64_t e, float2& v0, float2& v1) {
+__device__ __forceinline__ void ld_pair(const float2* b, uint32_t e, float2& v0, float2& v1) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(b + e));
     v0 = make_float2(v.x, v.y);
     v1 = make_float2(v.z, v.w);
 }
-__device__ __forceinline__ void st_pair(float2* b, int64_t e, float2 v0, float2 v1) {
+__device__ __forceinline__ void st_pair(float2* b, uint32_t e, float2 v0, float2 v1) {
     *reinterpret_cast<float4*>(b + e) = make_float4(v0.x, v0.y, v1.x, v1.y);
 }
 
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const float2 v0 = zscal(ib, acc[0][d]), v1 = zscal(ib, acc[1][d]);
-                st_pair(a.vt, p + a.g.cs * (d + 4 * f0), v0, v1);
+                st_pair(a.vt, (uint32_t)p + (uint32_t)a.g.cs * (uint32_t)(d + 4 * f0), v0, v1);
                 const double2 w0 = widen(v0), w1 = widen(v1);
                 loc += w0.x * w0.x + w0.y * w0.y;
                 loc += w1.x * w1.x + w1.y * w1.y;
@@ -298,7 +298,7 @@ __device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, in
 
 // The same update for the two points of an FP32 pair (elements e, e+1).
 __device__ __forceinline__ void three_term_pair(const LzArgsT<float2>& a, float2 x0, float2 x1,
-                                                int64_t e, int j, double alphat, float2& v0,
+                                                uint32_t e, int j, double alphat, float2& v0,
                                                 float2& v1) {
     const float2* rj = ring(a, j);
     const float2* rjm = ring(a, j - 1);
@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
                                                 a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
-                const int64_t e = p + a.g.cs * (d + 4 * f0);
+                const uint32_t e = (uint32_t)p + (uint32_t)a.g.cs * (uint32_t)(d + 4 * f0);
                 float2 v0, v1;
                 three_term_pair(a, acc[0][d], acc[1][d], e, j, at, v0, v1);
                 st_pair(rn, e, v0, v1);
@@ -1021,7 +1021,7 @@ static int pass1_shape(const LzArgsT<T>& a) {
 // Shape dispatch: FP32 vectors with Ls even take the two-point kernels.
 template <class T>
 static bool lz_pair(const Geom& g) {
-    return std::is_same<T, float2>::value && g.Ls % 2 == 0;
+    return std::is_same<T, float2>::value && pair_ok(g);
 }
 
 template <class T>
