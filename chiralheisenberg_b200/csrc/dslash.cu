@@ -280,37 +280,71 @@ __global__ void __launch_bounds__(kSplitThreads, OCC)
     }
 }
 
-// ---- FP16 storage, four points a thread ----------------------------------------
+// ---- four points a thread (FP16 and FP32 storage) ------------------------------
 // Point q (s a multiple of 4) and its three successors s+1..s+3 of flavour f:
-// every load is one 16-byte access of four FP16 complex numbers (the layout
-// has s innermost), so FP16 moves as many bytes per load instruction as the
-// FP32 two-point kernel.  Each element goes through dwf_apply_flavour's
-// operation sequence in FP32.  Needs Ls a multiple of 4.
-__device__ __forceinline__ float2 h4_get(const uint4& v, int p) {
-    const uint32_t w = p == 0 ? v.x : (p == 1 ? v.y : (p == 2 ? v.z : v.w));
+// each neighbour is one 16-byte load of four FP16 complex numbers, or two of
+// four FP32 ones (the layout has s innermost), and the index arithmetic and
+// the wall path are shared by four points.  Each element goes through
+// dwf_apply_flavour's operation sequence in FP32.  Needs Ls a multiple of 4.
+__device__ __forceinline__ float2 h2_get(uint32_t w) {
     return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
 __device__ __forceinline__ uint32_t h2_bits(float2 v) {
     const __half2 h = __float22half2_rn(v);
     return *reinterpret_cast<const uint32_t*>(&h);
 }
+template <class S> struct Quad;
+template <> struct Quad<__half2> {
+    uint4 v;
+    __device__ __forceinline__ void load(const __half2* p, int64_t n) {
+        v = __ldg(reinterpret_cast<const uint4*>(p + n));
+    }
+    __device__ __forceinline__ float2 get(int k) const {
+        return h2_get(k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)));
+    }
+    __device__ __forceinline__ static void store(__half2* p, int64_t n, const float2* a) {
+        uint4 o;
+        o.x = h2_bits(a[0]);
+        o.y = h2_bits(a[1]);
+        o.z = h2_bits(a[2]);
+        o.w = h2_bits(a[3]);
+        *reinterpret_cast<uint4*>(p + n) = o;
+    }
+    typedef LdF16 Elem;
+};
+template <> struct Quad<float2> {
+    float4 lo, hi;
+    __device__ __forceinline__ void load(const float2* p, int64_t n) {
+        lo = __ldg(reinterpret_cast<const float4*>(p + n));
+        hi = __ldg(reinterpret_cast<const float4*>(p + n + 2));
+    }
+    __device__ __forceinline__ float2 get(int k) const {
+        return k == 0 ? make_float2(lo.x, lo.y)
+                      : (k == 1 ? make_float2(lo.z, lo.w)
+                                : (k == 2 ? make_float2(hi.x, hi.y) : make_float2(hi.z, hi.w)));
+    }
+    __device__ __forceinline__ static void store(float2* p, int64_t n, const float2* a) {
+        *reinterpret_cast<float4*>(p + n) = make_float4(a[0].x, a[0].y, a[1].x, a[1].y);
+        *reinterpret_cast<float4*>(p + n + 2) = make_float4(a[2].x, a[2].y, a[3].x, a[3].y);
+    }
+    typedef LdF32 Elem;
+};
 
-template <bool DAG, int IMASS>
-__device__ __forceinline__ void dwf_apply_flavour_quad_f16(float2 acc[4][4],
-                                                           const __half2* __restrict__ in,
-                                                           const Geom& g, const PointIdx& q,
-                                                           int f, const float* __restrict__ chif,
-                                                           float diag, float hpin, bool apbc) {
+template <bool DAG, int IMASS, class S>
+__device__ __forceinline__ void dwf_apply_flavour_quad(float2 acc[4][4], const S* __restrict__ in,
+                                                       const Geom& g, const PointIdx& q, int f,
+                                                       const float* __restrict__ chif,
+                                                       float diag, float hpin, bool apbc) {
     constexpr int SF = DAG ? -1 : 1;
     const int L = g.L, Lt = g.Lt, Ls = g.Ls;
     const int64_t LsI = Ls, cs = g.cs, fo = g.cs * (4 * f);
-    auto ld4 = [&](int64_t n) { return __ldg(reinterpret_cast<const uint4*>(in + n)); };
     // diagonal term (:2651-2667)
 #pragma unroll
     for (int d = 0; d < 4; d++) {
-        const uint4 v = ld4(q.p + fo + cs * d);
+        Quad<S> v;
+        v.load(in, q.p + fo + cs * d);
 #pragma unroll
-        for (int p = 0; p < 4; p++) acc[p][d] = zscal(diag, h4_get(v, p));
+        for (int p = 0; p < 4; p++) acc[p][d] = zscal(diag, v.get(p));
     }
     const int xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
     const int yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
@@ -324,11 +358,11 @@ __device__ __forceinline__ void dwf_apply_flavour_quad_f16(float2 acc[4][4],
     const int64_t n_tp = sb + LsI * (plb + (int64_t)L * L * tp), n_tm = sb + LsI * (plb + (int64_t)L * L * tm);
 #define CHDWF_QUAD_HOP(N, MU, SIG, NEG)                                                   \
     {                                                                                    \
-        uint4 v[4];                                                                      \
-        _Pragma("unroll") for (int d = 0; d < 4; d++) v[d] = ld4((N) + cs * d);          \
+        Quad<S> v[4];                                                                    \
+        _Pragma("unroll") for (int d = 0; d < 4; d++) v[d].load(in, (N) + cs * d);       \
         _Pragma("unroll") for (int p = 0; p < 4; p++) {                                  \
             float2 r[4];                                                                 \
-            _Pragma("unroll") for (int d = 0; d < 4; d++) r[d] = h4_get(v[d], p);        \
+            _Pragma("unroll") for (int d = 0; d < 4; d++) r[d] = v[d].get(p);            \
             hop<MU, SIG, NEG>(acc[p], r);                                                \
         }                                                                                \
     }
@@ -354,56 +388,66 @@ __device__ __forceinline__ void dwf_apply_flavour_quad_f16(float2 acc[4][4],
     // previous point, or the previous group's last)
     constexpr int UP = DAG ? 0 : 2;
     constexpr int DN = DAG ? 2 : 0;
+    typedef typename Quad<S>::Elem Ld1;
+    const Ld1 ld1{in};
 #pragma unroll
     for (int d = UP; d < UP + 2; d++) {
-        const uint4 c = ld4(q.p + fo + cs * d);
+        Quad<S> c;
+        c.load(in, q.p + fo + cs * d);
 #pragma unroll
-        for (int p = 0; p < 3; p++) acc[p][d] = zsub(acc[p][d], h4_get(c, p + 1));
-        if (q.s + 4 < Ls) acc[3][d] = zsub(acc[3][d], h4_get(ld4(q.p + 4 + fo + cs * d), 0));
+        for (int p = 0; p < 3; p++) acc[p][d] = zsub(acc[p][d], c.get(p + 1));
+        if (q.s + 4 < Ls) acc[3][d] = zsub(acc[3][d], ld1(q.p + 4 + fo + cs * d));
     }
 #pragma unroll
     for (int d = DN; d < DN + 2; d++) {
-        const uint4 c = ld4(q.p + fo + cs * d);
-        if (q.s > 0) acc[0][d] = zsub(acc[0][d], h4_get(ld4(q.p - 4 + fo + cs * d), 3));
+        Quad<S> c;
+        c.load(in, q.p + fo + cs * d);
+        if (q.s > 0) acc[0][d] = zsub(acc[0][d], ld1(q.p - 1 + fo + cs * d));
 #pragma unroll
-        for (int p = 1; p < 4; p++) acc[p][d] = zsub(acc[p][d], h4_get(c, p - 1));
+        for (int p = 1; p < 4; p++) acc[p][d] = zsub(acc[p][d], c.get(p - 1));
     }
-    // wall coupling: point 3 at s=Ls (pair WA, reads s=1), point 0 at s=1
-    // (pair WB, reads s=Ls)
-    constexpr int WA = DAG ? 0 : 2;
-    constexpr int WB = DAG ? 2 : 0;
+    // wall coupling: point 3 at s=Ls or point 0 at s=1 (one of them, Ls >= 8;
+    // both for Ls = 4)
     const bool atL = (q.s + 4 == Ls), at0 = (q.s == 0);
     if (!(atL || at0)) return;
     const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
                 c3f = __ldg(chif + 2 * g.kvol + q.site);
     const bool pin = (q.site == 0);
-    if (atL)
-        wall_terms<DAG, IMASS, WA, 0>(acc[3], LdF16{in}, cs, LsI * q.site, f, c1f, c2f, c3f, pin,
-                                      hpin);
-    if (at0)
-        wall_terms<DAG, IMASS, WB, 1>(acc[0], LdF16{in}, cs, LsI * q.site + Ls - 1, f, c1f, c2f,
-                                      c3f, pin, hpin);
+    if (atL && at0) {
+        constexpr int WA = DAG ? 0 : 2;
+        constexpr int WB = DAG ? 2 : 0;
+        wall_terms<DAG, IMASS, WA, 0>(acc[3], ld1, cs, LsI * q.site, f, c1f, c2f, c3f, pin, hpin);
+        wall_terms<DAG, IMASS, WB, 1>(acc[0], ld1, cs, LsI * q.site + Ls - 1, f, c1f, c2f, c3f,
+                                      pin, hpin);
+        return;
+    }
+    float2 w[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) w[d] = atL ? acc[3][d] : acc[0][d];
+    wall_terms_rt<DAG, IMASS>(w, ld1, cs, atL ? LsI * q.site : LsI * q.site + Ls - 1, atL, f, c1f,
+                              c2f, c3f, pin, hpin);
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        if (atL) acc[3][d] = w[d];
+        else acc[0][d] = w[d];
+    }
 }
 
-template <bool DAG, int IMASS>
+template <bool DAG, int IMASS, class S>
 __global__ void __launch_bounds__(kSplitThreads, 2)
-    k_dslash_f16_quad(__half2* __restrict__ out, const __half2* __restrict__ in,
-                      const float* __restrict__ chif, Geom g, float diag, float hpin, int apbc) {
+    k_dslash_quad(S* __restrict__ out, const S* __restrict__ in, const float* __restrict__ chif,
+                  Geom g, float diag, float hpin, int apbc) {
     const int64_t p = (int64_t)blockIdx.x * (4 * kSplitPoints) +
                       4 * (threadIdx.x & (kSplitPoints - 1));
     const int f = split_flavour();
     if (p >= g.npts) return;
     const PointIdx q = point_of(g, p);
     float2 acc[4][4];
-    dwf_apply_flavour_quad_f16<DAG, IMASS>(acc, in, g, q, f, chif, diag, hpin, apbc != 0);
+    dwf_apply_flavour_quad<DAG, IMASS, S>(acc, in, g, q, f, chif, diag, hpin, apbc != 0);
 #pragma unroll
     for (int d = 0; d < 4; d++) {
-        uint4 o;
-        o.x = h2_bits(acc[0][d]);
-        o.y = h2_bits(acc[1][d]);
-        o.z = h2_bits(acc[2][d]);
-        o.w = h2_bits(acc[3][d]);
-        *reinterpret_cast<uint4*>(out + p + g.cs * (d + 4 * f)) = o;
+        const float2 v[4] = {acc[0][d], acc[1][d], acc[2][d], acc[3][d]};
+        Quad<S>::store(out, p + g.cs * (d + 4 * f), v);
     }
 }
 
@@ -431,7 +475,20 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
         const int apbc = ibound == -1;
         __half2* o = (__half2*)out;
         const __half2* i = (const __half2*)in;
-#define PQ(D, I) k_dslash_f16_quad<D, I><<<nb4, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
+#define PQ(D, I) k_dslash_quad<D, I, __half2><<<nb4, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
+        if (!dag) { if (imass == 3) PQ(false, 3); else PQ(false, 1); }
+        else { if (imass == 3) PQ(true, 3); else PQ(true, 1); }
+#undef PQ
+        count_launches(1);
+        return;
+    }
+    if (!half && g.Ls % 4 == 0 && getenv("CHDWF_F32_QUAD")) {
+        const unsigned nb4 = (unsigned)((g.npts + 4 * kSplitPoints - 1) / (4 * kSplitPoints));
+        const float diag = diag_of(am3);
+        const int apbc = ibound == -1;
+        float2* o = (float2*)out;
+        const float2* i = (const float2*)in;
+#define PQ(D, I) k_dslash_quad<D, I, float2><<<nb4, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
         if (!dag) { if (imass == 3) PQ(false, 3); else PQ(false, 1); }
         else { if (imass == 3) PQ(true, 3); else PQ(true, 1); }
 #undef PQ
