@@ -280,12 +280,15 @@ __global__ void __launch_bounds__(kSplitThreads, OCC)
     }
 }
 
-// ---- four points a thread (FP16 and FP32 storage) ------------------------------
+// ---- FP16 storage, four points a thread ----------------------------------------
 // Point q (s a multiple of 4) and its three successors s+1..s+3 of flavour f:
-// each neighbour is one 16-byte load of four FP16 complex numbers, or two of
-// four FP32 ones (the layout has s innermost), and the index arithmetic and
-// the wall path are shared by four points.  Each element goes through
-// dwf_apply_flavour's operation sequence in FP32.  Needs Ls a multiple of 4.
+// each neighbour is one 16-byte load of four FP16 complex numbers (the layout
+// has s innermost), as many bytes per load as the FP32 two-point kernel, and
+// the index arithmetic and the wall path are shared by four points.  Each
+// element goes through dwf_apply_flavour's operation sequence in FP32.
+// Needs Ls a multiple of 4.  (Four FP32 points a thread, at the 128
+// registers they need, ran 45% slower than the two-point kernel: two blocks
+// an SM hide too little latency.)
 __device__ __forceinline__ float2 h2_get(uint32_t w) {
     return __half22float2(*reinterpret_cast<const __half2*>(&w));
 }
@@ -312,24 +315,6 @@ template <> struct Quad<__half2> {
     }
     typedef LdF16 Elem;
 };
-template <> struct Quad<float2> {
-    float4 lo, hi;
-    __device__ __forceinline__ void load(const float2* p, int64_t n) {
-        lo = __ldg(reinterpret_cast<const float4*>(p + n));
-        hi = __ldg(reinterpret_cast<const float4*>(p + n + 2));
-    }
-    __device__ __forceinline__ float2 get(int k) const {
-        return k == 0 ? make_float2(lo.x, lo.y)
-                      : (k == 1 ? make_float2(lo.z, lo.w)
-                                : (k == 2 ? make_float2(hi.x, hi.y) : make_float2(hi.z, hi.w)));
-    }
-    __device__ __forceinline__ static void store(float2* p, int64_t n, const float2* a) {
-        *reinterpret_cast<float4*>(p + n) = make_float4(a[0].x, a[0].y, a[1].x, a[1].y);
-        *reinterpret_cast<float4*>(p + n + 2) = make_float4(a[2].x, a[2].y, a[3].x, a[3].y);
-    }
-    typedef LdF32 Elem;
-};
-
 template <bool DAG, int IMASS, class S>
 __device__ __forceinline__ void dwf_apply_flavour_quad(float2 acc[4][4], const S* __restrict__ in,
                                                        const Geom& g, const PointIdx& q, int f,
@@ -476,19 +461,6 @@ void launch_dslash_lp(bool dag, int imass, int half, void* out, const void* in, 
         __half2* o = (__half2*)out;
         const __half2* i = (const __half2*)in;
 #define PQ(D, I) k_dslash_quad<D, I, __half2><<<nb4, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
-        if (!dag) { if (imass == 3) PQ(false, 3); else PQ(false, 1); }
-        else { if (imass == 3) PQ(true, 3); else PQ(true, 1); }
-#undef PQ
-        count_launches(1);
-        return;
-    }
-    if (!half && g.Ls % 4 == 0 && getenv("CHDWF_F32_QUAD")) {
-        const unsigned nb4 = (unsigned)((g.npts + 4 * kSplitPoints - 1) / (4 * kSplitPoints));
-        const float diag = diag_of(am3);
-        const int apbc = ibound == -1;
-        float2* o = (float2*)out;
-        const float2* i = (const float2*)in;
-#define PQ(D, I) k_dslash_quad<D, I, float2><<<nb4, kSplitThreads, 0, st>>>(o, i, chif, g, diag, hpin, apbc)
         if (!dag) { if (imass == 3) PQ(false, 3); else PQ(false, 1); }
         else { if (imass == 3) PQ(true, 3); else PQ(true, 1); }
 #undef PQ
