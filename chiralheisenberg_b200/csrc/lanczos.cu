@@ -188,6 +188,9 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
             float2 acc[2][4];
             dwf_apply_flavour_pair<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
                                                  a.apbc != 0);
+            // |vt|^2 is summed in FP64 from the first term: a pair's partial
+            // sum in FP32 made the FP32 force solves 7% longer (alpha~ and
+            // beta steer the recurrences)
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const float2 v0 = zscal(ib, acc[0][d]), v1 = zscal(ib, acc[1][d]);
