@@ -58,17 +58,36 @@ struct Elem {
     int64_t site;
 };
 
+// Site coordinates (site < kvol < 2^31): 32-bit divisions.
+__device__ __forceinline__ void site_xyt(const Geom& g, uint32_t site, int* x, int* y, int* t) {
+    const uint32_t L = (uint32_t)g.L, xy = site / L;
+    *x = (int)(site - xy * L);
+    const uint32_t tt = xy / L;
+    *y = (int)(xy - tt * L);
+    *t = (int)tt;
+}
+
+// Element j -> (s, site, d, f): in 32-bit arithmetic when every element
+// index fits (the 64-bit divisions it replaces are software routines).
 __device__ __forceinline__ Elem elem_of(const Geom& g, int64_t j) {
     Elem e;
-    e.s = (int)(j % g.Ls);
-    const int64_t r = j / g.Ls;
-    e.site = r % g.kvol;
-    const int c = (int)(r / g.kvol);
+    int c;
+    if (g.kferm <= (int64_t)0xffffffffLL) {
+        const uint32_t u = (uint32_t)j, Ls = (uint32_t)g.Ls, kv = (uint32_t)g.kvol;
+        const uint32_t r = u / Ls;
+        e.s = (int)(u - r * Ls);
+        const uint32_t cc = r / kv;
+        e.site = (int64_t)(r - cc * kv);
+        c = (int)cc;
+    } else {
+        e.s = (int)(j % g.Ls);
+        const int64_t r = j / g.Ls;
+        e.site = r % g.kvol;
+        c = (int)(r / g.kvol);
+    }
     e.d = c & 3;
     e.f = c >> 2;
-    e.x = (int)(e.site % g.L);
-    e.y = (int)((e.site / g.L) % g.L);
-    e.t = (int)(e.site / ((int64_t)g.L * g.L));
+    site_xyt(g, (uint32_t)e.site, &e.x, &e.y, &e.t);
     return e;
 }
 
@@ -269,7 +288,8 @@ __global__ void __launch_bounds__(kThreads) k_hmc_derivs(const float2* __restric
     if (i >= g.kvol) return;
     const int64_t kvol = g.kvol;
     const int Ls = g.Ls;
-    const int ix = (int)(i % g.L), iy = (int)((i / g.L) % g.L), it = (int)(i / ((int64_t)g.L * g.L));
+    int ix, iy, it;
+    site_xyt(g, (uint32_t)i, &ix, &iy, &it);
     float d1 = __fmul_rn(b2, chi[i]), d2 = __fmul_rn(b2, chi[kvol + i]);
     float d3 = __fmul_rn(b2, chi[2 * kvol + i]);
     for (int grp = 0; grp < 2; grp++) {

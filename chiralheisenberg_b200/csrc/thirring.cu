@@ -9,9 +9,11 @@
 // round-to-nearest intrinsics, so the result equals the sequential
 // evaluation bit for bit.  derivs gives one thread to each link (site, mu)
 // and adds its 8*kthird terms in the reference's order into a REAL*4
-// register, also bit for bit.  The multi-shift solver runs its scalar
-// recurrences on the host with the reference's implicit REAL*4 / REAL*8
-// types; its sums are FP64 block partials added in block order.
+// register, also bit for bit.  The multi-shift solver and congrad run
+// their scalar recurrences on the device, in the last block of each
+// reduction, with the reference's implicit REAL*4 / REAL*8 types; the sums
+// are FP64 block partials added in block order, and the host polls a stop
+// flag once every 16 iterations instead of reading every scalar.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -59,6 +61,15 @@ __device__ __forceinline__ void tnbr(const TGeom& g, int x, int y, int t, int mu
     }
 }
 
+// Site coordinates (site < kvol < 2^31): 32-bit divisions.
+__device__ __forceinline__ void tsite_xyt(int L, int64_t site, int* x, int* y, int* t) {
+    const uint32_t uL = (uint32_t)L, st = (uint32_t)site, xy = st / uL;
+    *x = (int)(st - xy * uL);
+    const uint32_t tt = xy / uL;
+    *y = (int)(xy - tt * uL);
+    *t = (int)tt;
+}
+
 // One element (s, site, d) of Phi = M R (DAG false, :1946-2069) or
 // Phi = M^dagger R (DAG true, :2071-2188).
 template <bool DAG, int IMASS>
@@ -69,7 +80,8 @@ __device__ double2 thr_element(const double2* __restrict__ R, const double2* __r
     auto at = [&](int ss, int64_t st, int dd) -> double2 {
         return __ldg(R + ss + (int64_t)Ls * (st + kvol * dd));
     };
-    const int x = (int)(i % L), y = (int)((i / L) % L), t = (int)(i / ((int64_t)L * L));
+    int x, y, t;
+    tsite_xyt(L, i, &x, &y, &t);
     int64_t up[3], dn[3];
 #pragma unroll
     for (int mu = 0; mu < 3; mu++) tnbr(g, x, y, t, mu, &up[mu], &dn[mu]);
@@ -115,13 +127,32 @@ __device__ double2 thr_element(const double2* __restrict__ R, const double2* __r
     return phi;
 }
 
+// Stop state of a solve whose scalar recurrences run on the device: once
+// done is set at iteration iters, the kernels queued for later iterations
+// return at once (the host polls the flag only every few iterations).
+struct ThrRun {
+    int done, iters;   // done: 0 running, 1 converged, 2 at the iteration cap
+};
+__device__ __forceinline__ bool thr_skip(const ThrRun* run, int it) {
+    return run != nullptr && run->done && it > run->iters;
+}
+
 template <bool DAG, int IMASS>
 __global__ void __launch_bounds__(kThreads) k_thr_dslash(double2* __restrict__ out,
                                                          const double2* __restrict__ in,
                                                          const double2* __restrict__ u, TGeom g,
-                                                         double diag, double2 zk) {
+                                                         double diag, double2 zk,
+                                                         const ThrRun* run, int it) {
+    if (thr_skip(run, it)) return;
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= g.kferm) return;
+    if (g.kferm <= (int64_t)0xffffffffLL) {   // 32-bit divisions when every index fits
+        const uint32_t uj = (uint32_t)j, Ls = (uint32_t)g.Ls, kv = (uint32_t)g.kvol;
+        const uint32_t r = uj / Ls, d = r / kv;
+        out[j] = thr_element<DAG, IMASS>(in, u, g, (int)(uj - r * Ls), (int64_t)(r - d * kv),
+                                         (int)d, diag, zk);
+        return;
+    }
     const int s = (int)(j % g.Ls);
     const int64_t r = j / g.Ls;
     out[j] = thr_element<DAG, IMASS>(in, u, g, s, r % g.kvol, (int)(r / g.kvol), diag, zk);
@@ -137,10 +168,11 @@ __global__ void __launch_bounds__(kThreads) k_thr_derivs(const double2* __restri
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= 3 * (int64_t)g.kvol) return;
     const int64_t kvol = g.kvol;
-    const int mu = (int)(j / kvol);
-    const int64_t i = j % kvol;
+    const int mu = (int)((uint32_t)j / (uint32_t)kvol);    // j < 3 kvol < 2^32
+    const int64_t i = j - (int64_t)mu * kvol;
     const int Ls = g.Ls;
-    const int x = (int)(i % g.L), y = (int)((i / g.L) % g.L), t = (int)(i / ((int64_t)g.L * g.L));
+    int x, y, t;
+    tsite_xyt(g.L, i, &x, &y, &t);
     int64_t up, dn;
     tnbr(g, x, y, t, mu, &up, &dn);
     const double2 tzi = make_double2(0.0, tz);
@@ -180,14 +212,61 @@ struct PoleCoef {
     double rho[kThrMaxPoles], amu[kThrMaxPoles];
 };
 
+// The solver's scalar recurrences run on the device, in thread 0 of the
+// block that finishes a reduction last, with the reference's implicit types
+// and the same operation order as a sequential host evaluation (no fused
+// multiply-adds), so the iterates do not depend on where the scalars are
+// formed.  The host only polls the stop flag every few iterations.
+struct ThrQCtl {
+    ThrRun run;
+    int niterc, ndiag;
+    float phimod, resid, alphatild, pad_;
+    double beta;                                   // REAL*8 beta of :684-704
+    double aden[kThrMaxPoles], d[kThrMaxPoles], rhom1[kThrMaxPoles];
+    double rho[kThrMaxPoles], amu[kThrMaxPoles];
+    unsigned count1, count2;
+};
+
+// Grid sum of one double per thread with the block partials added in block
+// order by one thread (the order of a host loop over the partials).  The
+// block that arrives last returns true with the total in *total (thread 0)
+// and resets the counter.  NB is the fixed grid size of the reductions.
+template <int NT, int NB>
+__device__ __forceinline__ bool last_block_seq(double v, double* part, unsigned* count,
+                                               double* total) {
+    __shared__ double sh[NT / 32];
+    __shared__ double all[NB];
+    __shared__ bool is_last;
+    v = block_sum<NT>(v, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = v;
+        __threadfence();
+        is_last = (atomicAdd(count, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    for (int i = threadIdx.x; i < NB; i += blockDim.x) all[i] = ((volatile double*)part)[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < NB; b++) s = __dadd_rn(s, all[b]);
+        *total = s;
+        *count = 0;
+    }
+    return true;
+}
+
 // q = R/beta (:684-686)
-__global__ void k_thr_q(double2* __restrict__ q, const double2* __restrict__ R, double beta,
-                        int64_t n) {
+__global__ void k_thr_q(double2* __restrict__ q, const double2* __restrict__ R,
+                        const ThrQCtl* __restrict__ c, int it, int64_t n) {
+    if (thr_skip(&c->run, it)) return;
+    const double beta = c->beta;
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j < n) q[j] = make_double2(__ddiv_rn(R[j].x, beta), __ddiv_rn(R[j].y, beta));
 }
 
-// block partials of sum Re(conjg(a)*b)
+// block partials of sum Re(conjg(a)*b); the host adds them in block order
 __global__ void __launch_bounds__(kThreads) k_thr_dot(const double2* __restrict__ a,
                                                       const double2* __restrict__ b, int64_t n,
                                                       double* __restrict__ part) {
@@ -200,14 +279,31 @@ __global__ void __launch_bounds__(kThreads) k_thr_dot(const double2* __restrict_
     if (threadIdx.x == 0) part[blockIdx.x] = loc;
 }
 
-// R = x3 - alphatild q - beta qm1 ; qm1 = q ; partials of |R|^2 (:696-703)
+// alphatild = sum Re(conjg(q)*x3), rounded once to REAL*4 (:688-694)
+__global__ void __launch_bounds__(kThreads) k_thr_alpha(const double2* __restrict__ q,
+                                                        const double2* __restrict__ x3, int64_t n,
+                                                        double* __restrict__ part,
+                                                        ThrQCtl* __restrict__ c, int it) {
+    if (thr_skip(&c->run, it)) return;
+    double loc = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        loc += zmul(zconj(q[j]), x3[j]).x;
+    double tot;
+    if (!last_block_seq<kThreads, kRedBlocks>(loc, part, &c->count1, &tot)) return;
+    if (threadIdx.x == 0) c->alphatild = (float)tot;
+}
+
+// R = x3 - alphatild q - beta qm1 ; qm1 = q ; beta = |R| (:696-704), then
+// the pole recurrences and the stopping test (:712-757) in the last block
 __global__ void __launch_bounds__(kThreads) k_thr_lanczos(double2* __restrict__ R,
                                                           double2* __restrict__ qm1,
                                                           const double2* __restrict__ q,
-                                                          const double2* __restrict__ x3,
-                                                          double alphat, double beta, int64_t n,
-                                                          double* __restrict__ part) {
-    __shared__ double sh[kThreads / 32];
+                                                          const double2* __restrict__ x3, int64_t n,
+                                                          double* __restrict__ part,
+                                                          ThrQCtl* __restrict__ c, int it) {
+    if (thr_skip(&c->run, it)) return;
+    const double alphat = (double)c->alphatild, beta = c->beta;
     double loc = 0.0;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
          j += (int64_t)gridDim.x * blockDim.x) {
@@ -217,27 +313,68 @@ __global__ void __launch_bounds__(kThreads) k_thr_lanczos(double2* __restrict__ 
         qm1[j] = qj;
         loc += zmul(zconj(r), r).x;
     }
-    loc = block_sum<kThreads>(loc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = loc;
+    double b2;
+    if (!last_block_seq<kThreads, kRedBlocks>(loc, part, &c->count2, &b2)) return;
+    if (threadIdx.x != 0) return;
+    const float beta0 = (float)beta;
+    c->beta = __dsqrt_rn(b2);
+    const int nd = c->ndiag;
+    float rhomax = 0.0f;
+    for (int k = 0; k < nd; k++) {
+        const double alpha = __dadd_rn((double)c->alphatild, c->aden[k]);
+        if (it == 1) {                                                     // :712-724
+            c->d[k] = alpha;
+            c->rho[k] = __ddiv_rn((double)beta0, alpha);
+            c->rhom1[k] = c->rho[k];
+        } else {                                                           // :725-747
+            const double amu = __ddiv_rn((double)beta0, c->d[k]);
+            const double dm1 = c->d[k];
+            const double dk = __dsub_rn(alpha, __dmul_rn((double)beta0, amu));
+            const double rho = -__ddiv_rn(__dmul_rn(__dmul_rn(amu, dm1), c->rhom1[k]), dk);
+            c->amu[k] = amu;
+            c->d[k] = dk;
+            c->rho[k] = rho;
+            const double rm = fabs(__dmul_rn((double)c->phimod, rho));
+            if (k == 0) rhomax = (float)rm;
+            else if (rm > (double)rhomax) rhomax = (float)rm;
+            c->rhom1[k] = rho;
+        }
+    }
+    const float arelax = 2.0f;                                             // :750-757
+    if (it > 1 && rhomax < __fmul_rn(arelax, c->resid)) {
+        c->run.iters = it;
+        c->run.done = 1;
+    } else if (it >= c->niterc) {
+        c->run.iters = it;
+        c->run.done = 2;
+    }
 }
 
 // all poles at once: first iteration p_k = q, x_k = rho_k q; later
-// p_k = q - amu_k p_k, x_k += rho_k p_k (:712-747; pm1 equals p)
+// p_k = q - amu_k p_k, x_k += rho_k p_k (:712-747; pm1 equals p).  Runs in
+// the iteration that stopped the solve too.
 __global__ void k_thr_poles(double2* __restrict__ p, double2* __restrict__ x1,
-                            const double2* __restrict__ q, PoleCoef c, int npole, int first,
-                            int64_t n) {
+                            const double2* __restrict__ q, const ThrQCtl* __restrict__ c,
+                            int it, int64_t n, int* hflag) {
+    if (thr_skip(&c->run, it)) return;
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j == 0 && c->run.done && hflag) {
+        *(volatile int*)hflag = c->run.done;
+        __threadfence_system();
+    }
     if (j >= n) return;
     const double2 qj = q[j];
-    for (int k = 0; k < npole; k++) {
+    const int nd = c->ndiag;
+    for (int k = 0; k < nd; k++) {
         const int64_t e = j + n * k;
-        if (first) {
+        const double rho = c->rho[k];
+        if (it == 1) {
             p[e] = qj;
-            x1[e] = zscal(c.rho[k], qj);
+            x1[e] = zscal(rho, qj);
         } else {
-            const double2 pk = zsub(qj, zscal(c.amu[k], p[e]));
+            const double2 pk = zsub(qj, zscal(c->amu[k], p[e]));
             p[e] = pk;
-            x1[e] = zadd(x1[e], zscal(c.rho[k], pk));
+            x1[e] = zadd(x1[e], zscal(rho, pk));
         }
     }
 }
@@ -289,18 +426,46 @@ __global__ void k_thr_noise(double2* __restrict__ R, const float* __restrict__ g
 }
 
 // ---- congrad (:931-1025) and measure (:1027-1285) -------------------------
-// x += alpha p
-__global__ void k_thr_axpy(double2* __restrict__ x, const double2* __restrict__ p, double a,
-                           int64_t n) {
+// The REAL*4 scalars of congrad, formed on the device like those of qmrherm.
+struct ThrCgCtl {
+    ThrRun run;
+    int64_t niterc;
+    float alpha, alphan, betad, beta, resid, pad_;
+    unsigned count1, count2;
+};
+
+// alphad = |x1|^2 ; alpha = alphan/alphad (:970-977)
+__global__ void __launch_bounds__(kThreads) k_thr_cg_alpha(const double2* __restrict__ x1,
+                                                           int64_t n, double* __restrict__ part,
+                                                           ThrCgCtl* __restrict__ c, int it) {
+    if (thr_skip(&c->run, it)) return;
+    double loc = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        loc += zmul(zconj(x1[j]), x1[j]).x;
+    double tot;
+    if (!last_block_seq<kThreads, kRedBlocks>(loc, part, &c->count1, &tot)) return;
+    if (threadIdx.x == 0) c->alpha = __fdiv_rn(c->alphan, (float)tot);
+}
+
+// x += alpha p (:979-983)
+__global__ void k_thr_axpy(double2* __restrict__ x, const double2* __restrict__ p,
+                           const ThrCgCtl* __restrict__ c, int it, int64_t n) {
+    if (thr_skip(&c->run, it)) return;
+    const double a = (double)c->alpha;
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j < n) x[j] = zadd(x[j], zscal(a, p[j]));
 }
 
-// r -= alpha x2 ; block partials of |r|^2
+// r -= alpha x2 ; betan = |r|^2, beta and the stopping test (:989-1001) in
+// the last block
 __global__ void __launch_bounds__(kThreads) k_thr_cg_r(double2* __restrict__ r,
-                                                       const double2* __restrict__ x2, double a,
-                                                       int64_t n, double* __restrict__ part) {
-    __shared__ double sh[kThreads / 32];
+                                                       const double2* __restrict__ x2, int64_t n,
+                                                       double* __restrict__ part,
+                                                       ThrCgCtl* __restrict__ c, int it,
+                                                       int* hflag) {
+    if (thr_skip(&c->run, it)) return;
+    const double a = (double)c->alpha;
     double loc = 0.0;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
          j += (int64_t)gridDim.x * blockDim.x) {
@@ -308,13 +473,33 @@ __global__ void __launch_bounds__(kThreads) k_thr_cg_r(double2* __restrict__ r,
         r[j] = v;
         loc += zmul(zconj(v), v).x;
     }
-    loc = block_sum<kThreads>(loc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = loc;
+    double bn;
+    if (!last_block_seq<kThreads, kRedBlocks>(loc, part, &c->count2, &bn)) return;
+    if (threadIdx.x != 0) return;
+    const float betan = (float)bn;
+    float beta = __fdiv_rn(betan, c->betad);
+    c->betad = betan;
+    c->alphan = betan;
+    if (it == 1) beta = 0.0f;
+    c->beta = beta;
+    if (betan < c->resid) {
+        c->run.iters = it;
+        c->run.done = 1;
+    } else if (it >= c->niterc) {
+        c->run.iters = it;
+        c->run.done = 2;
+    }
+    if (c->run.done && hflag) {
+        *(volatile int*)hflag = c->run.done;
+        __threadfence_system();
+    }
 }
 
-// p = r + beta p
-__global__ void k_thr_xpay(double2* __restrict__ p, const double2* __restrict__ r, double b,
-                           int64_t n) {
+// p = r + beta p (:1003-1005); runs in the iteration that stopped the solve
+__global__ void k_thr_xpay(double2* __restrict__ p, const double2* __restrict__ r,
+                           const ThrCgCtl* __restrict__ c, int it, int64_t n) {
+    if (thr_skip(&c->run, it)) return;
+    const double b = (double)c->beta;
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j < n) p[j] = zadd(r[j], zscal(b, p[j]));
 }
@@ -368,6 +553,10 @@ struct chdwf_thr {
     double2 *p = nullptr, *x1 = nullptr;
     double* part = nullptr;
     std::vector<double> hpart;
+    chdwf::ThrQCtl* qctl = nullptr;       // device scalars of qmrherm
+    chdwf::ThrCgCtl* cgctl = nullptr;     // device scalars of congrad
+    int* hflag_host = nullptr;            // stop flag, mapped pinned memory
+    int* hflag_dev = nullptr;
     chdwf::Rng rng;
     int isweep = 0, itot = 0, naccp = 0;
     float action = 0.0f, gaction = 0.0f, paction = 0.0f;
@@ -389,12 +578,12 @@ template <class T>
 cudaError_t talloc(T** p, size_t n) { return cudaMalloc((void**)p, sizeof(T) * n); }
 
 void thr_dslash(chdwf_thr* h, bool dag, float am, int imass, double2* out, const double2* in,
-                const double2* u) {
+                const double2* u, const chdwf::ThrRun* run = nullptr, int it = 0) {
     const unsigned nb = chdwf::tblk(h->g.kferm);
     double2 zk = imass == 1 ? make_double2((double)am, 0.0)
                             : make_double2(0.0, dag ? (double)am : (double)(-am));
     const double dg = h->diag();
-#define THR_LAUNCH(D, I) chdwf::k_thr_dslash<D, I><<<nb, chdwf::kThreads, 0, h->st>>>(out, in, u, h->g, dg, zk)
+#define THR_LAUNCH(D, I) chdwf::k_thr_dslash<D, I><<<nb, chdwf::kThreads, 0, h->st>>>(out, in, u, h->g, dg, zk, run, it)
     if (dag) {
         if (imass == 1) THR_LAUNCH(true, 1); else if (imass == 3) THR_LAUNCH(true, 3); else THR_LAUNCH(true, 5);
     } else {
@@ -422,6 +611,37 @@ cudaError_t thr_sum(chdwf_thr* h, double* out) {
     return e;
 }
 
+// Launches iterations 1, 2, ... of a solve in chunks of 16 until the
+// device raises the stop flag or cap iterations are queued.  The flag is
+// read one chunk behind, so up to two chunks are in flight; the kernels of
+// iterations past the stopping one return at once.
+template <class F>
+cudaError_t thr_run_chunks(chdwf_thr* h, int64_t cap, F&& launch_iteration) {
+    const int chunk = 16;
+    cudaEvent_t ev[2];
+    cudaError_t e = cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    if (e) return e;
+    if ((e = cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming))) {
+        cudaEventDestroy(ev[0]);
+        return e;
+    }
+    int64_t launched = 0;
+    int nchunk = 0;
+    while (launched < cap) {
+        for (int c = 0; c < chunk && launched < cap; c++) launch_iteration((int)++launched);
+        if ((e = cudaGetLastError())) break;
+        cudaEventRecord(ev[nchunk & 1], h->st);
+        if (nchunk >= 1) {
+            if ((e = cudaEventSynchronize(ev[(nchunk - 1) & 1]))) break;
+            if (*(volatile int*)h->hflag_host) break;
+        }
+        nchunk++;
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return e;
+}
+
 // qmrherm on device vectors (:630-818): Phi in, x out, Phi0 and dS of the
 // context; the scalars follow the reference's implicit typing.
 int thr_qmrherm(chdwf_thr* h, const double2* Phi, float res, int* itercg, float am, int imass,
@@ -436,59 +656,42 @@ int thr_qmrherm(chdwf_thr* h, const double2* Phi, float res, int* itercg, float 
     cudaMemsetAsync(h->qm1, 0, sizeof(double2) * n, h->st);
     chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(h->rr, h->rr, n, h->part);
     chdwf::count_launches(1);
-    double beta;
-    if ((e = thr_sum(h, &beta))) return h->fail(e, "thr_qmrherm");
-    beta = std::sqrt(beta);
-    const float phimod = (float)beta;
-    double alpha[chdwf::kThrMaxPoles], d[chdwf::kThrMaxPoles], dm1[chdwf::kThrMaxPoles];
-    double rhom1[chdwf::kThrMaxPoles];
-    chdwf::PoleCoef c;
-    memset(&c, 0, sizeof(c));
-    int capped = 1;
-    *itercg = 0;
-    for (int niter = 1; niter <= niterc; niter++) {
-        (*itercg)++;
-        chdwf::k_thr_q<<<nb, chdwf::kThreads, 0, h->st>>>(h->q, h->rr, beta, n);
-        thr_dslash(h, false, am, imass, h->vt, h->q, u);
-        thr_dslash(h, true, am, imass, h->x3, h->vt, u);
-        chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(h->q, h->x3, n, h->part);
-        chdwf::count_launches(2);
-        double at;
-        if ((e = thr_sum(h, &at))) return h->fail(e, "thr_qmrherm");
-        const float alphatild = (float)at;                               // REAL*4 (:691-694)
+    double b0;
+    if ((e = thr_sum(h, &b0))) return h->fail(e, "thr_qmrherm");
+    chdwf::ThrQCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.beta = std::sqrt(b0);
+    hc.phimod = (float)hc.beta;
+    hc.resid = resid;
+    hc.niterc = niterc;
+    hc.ndiag = ndiag;
+    for (int k = 0; k < ndiag; k++) hc.aden[k] = aden[k];
+    if ((e = cudaMemcpyAsync(h->qctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, h->st)))
+        return h->fail(e, "thr_qmrherm");
+    *h->hflag_host = 0;
+    chdwf::ThrQCtl* c = h->qctl;
+    const chdwf::ThrRun* run = &c->run;
+    e = thr_run_chunks(h, niterc, [&](int it) {
+        chdwf::k_thr_q<<<nb, chdwf::kThreads, 0, h->st>>>(h->q, h->rr, c, it, n);
+        thr_dslash(h, false, am, imass, h->vt, h->q, u, run, it);
+        thr_dslash(h, true, am, imass, h->x3, h->vt, u, run, it);
+        chdwf::k_thr_alpha<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(h->q, h->x3, n,
+                                                                            h->part, c, it);
         chdwf::k_thr_lanczos<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(
-            h->rr, h->qm1, h->q, h->x3, (double)alphatild, beta, n, h->part);
-        chdwf::count_launches(1);
-        const float beta0 = (float)beta;
-        double b2;
-        if ((e = thr_sum(h, &b2))) return h->fail(e, "thr_qmrherm");
-        beta = std::sqrt(b2);
-        for (int k = 0; k < ndiag; k++) alpha[k] = (double)alphatild + aden[k];
-        float rhomax = 0.0f;
-        if (niter == 1) {                                                  // :712-724
-            for (int k = 0; k < ndiag; k++) {
-                d[k] = alpha[k];
-                c.rho[k] = (double)beta0 / alpha[k];
-                rhom1[k] = c.rho[k];
-            }
-        } else {                                                           // :725-747
-            for (int k = 0; k < ndiag; k++) {
-                c.amu[k] = (double)beta0 / d[k];
-                dm1[k] = d[k];
-                d[k] = alpha[k] - (double)beta0 * c.amu[k];
-                c.rho[k] = -(c.amu[k] * dm1[k] * rhom1[k] / d[k]);
-                const double rm = std::fabs((double)phimod * c.rho[k]);
-                if (k == 0) rhomax = (float)rm;
-                else if (rm > (double)rhomax) rhomax = (float)rm;
-                rhom1[k] = c.rho[k];
-            }
-        }
-        chdwf::k_thr_poles<<<nb, chdwf::kThreads, 0, h->st>>>(h->p, h->x1, h->q, c, ndiag,
-                                                               niter == 1, n);
-        chdwf::count_launches(1);
-        const float arelax = 2.0f;                                         // :750-757
-        if (niter > 1 && rhomax < arelax * resid) { capped = 0; break; }
-    }
+            h->rr, h->qm1, h->q, h->x3, n, h->part, c, it);
+        chdwf::k_thr_poles<<<nb, chdwf::kThreads, 0, h->st>>>(h->p, h->x1, h->q, c, it, n,
+                                                               h->hflag_dev);
+        chdwf::count_launches(4);
+    });
+    if (e) return h->fail(e, "thr_qmrherm");
+    chdwf::ThrRun hr;
+    if ((e = cudaMemcpyAsync(&hr, run, sizeof(hr), cudaMemcpyDeviceToHost, h->st)) ||
+        (e = cudaStreamSynchronize(h->st)))
+        return h->fail(e, "thr_qmrherm");
+    *itercg = hr.iters;
+    const int capped = hr.done != 1;
+    chdwf::PoleCoef c0;
+    memset(&c0, 0, sizeof(c0));
     if (iflag < 2) {                                                       // :766-780
         chdwf::PoleCoef a;
         for (int k = 0; k < ndiag; k++) a.rho[k] = anum[k + 1];
@@ -498,7 +701,7 @@ int thr_qmrherm(chdwf_thr* h, const double2* Phi, float res, int* itercg, float 
             cudaMemcpyAsync(h->Phi0, h->x1, sizeof(double2) * n * ndiag, cudaMemcpyDeviceToDevice,
                             h->st);
     } else {                                                               // :781-806
-        chdwf::k_thr_combine<<<nb, chdwf::kThreads, 0, h->st>>>(x, Phi, h->x1, c, anum[0], 0, n);
+        chdwf::k_thr_combine<<<nb, chdwf::kThreads, 0, h->st>>>(x, Phi, h->x1, c0, anum[0], 0, n);
         chdwf::count_launches(1);
         for (int k = 0; k < ndiag; k++) {
             const double2* xk = h->x1 + n * k;
@@ -588,37 +791,40 @@ int thr_congrad(chdwf_thr* h, const double2* Phi, float res, int* itercg, float 
     double2 *p = h->q, *r = h->rr, *x1 = h->vt, *x2 = h->x3;
     cudaMemcpyAsync(p, x, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);   // :956-959
     cudaMemcpyAsync(r, Phi, sizeof(double2) * n, cudaMemcpyDeviceToDevice, h->st);
-    float betad = 1.0f, alpha = 1.0f, alphan = 0.0f;
+    chdwf::ThrCgCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.betad = 1.0f;                                                      // :951-952
+    hc.alpha = 1.0f;
+    hc.alphan = 0.0f;
+    hc.resid = resid;
+    hc.niterc = niterc;
     cudaError_t e;
-    *itercg = 0;
-    for (int64_t nx = 1; nx <= niterc; nx++) {
-        (*itercg)++;
-        thr_dslash(h, false, am, imass, x1, p, u);                        // :966
-        if (nx != 1) {                                                    // :970-983
-            chdwf::k_thr_dot<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(x1, x1, n, h->part);
-            chdwf::count_launches(1);
-            double ad;
-            if ((e = thr_sum(h, &ad))) return h->fail(e, "thr_congrad");
-            alpha = alphan / (float)ad;
-            chdwf::k_thr_axpy<<<nb, chdwf::kThreads, 0, h->st>>>(x, p, (double)alpha, n);
-            chdwf::count_launches(1);
+    if ((e = cudaMemcpyAsync(h->cgctl, &hc, sizeof(hc), cudaMemcpyHostToDevice, h->st)))
+        return h->fail(e, "thr_congrad");
+    *h->hflag_host = 0;
+    chdwf::ThrCgCtl* c = h->cgctl;
+    const chdwf::ThrRun* run = &c->run;
+    e = thr_run_chunks(h, niterc, [&](int it) {
+        thr_dslash(h, false, am, imass, x1, p, u, run, it);               // :966
+        if (it != 1) {                                                    // :970-983
+            chdwf::k_thr_cg_alpha<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(x1, n, h->part,
+                                                                                   c, it);
+            chdwf::k_thr_axpy<<<nb, chdwf::kThreads, 0, h->st>>>(x, p, c, it, n);
+            chdwf::count_launches(2);
         }
-        thr_dslash(h, true, am, imass, x2, x1, u);                        // :987
-        chdwf::k_thr_cg_r<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(r, x2, (double)alpha, n,
-                                                                          h->part);
-        chdwf::count_launches(1);
-        double bn;
-        if ((e = thr_sum(h, &bn))) return h->fail(e, "thr_congrad");
-        const float betan = (float)bn;                                    // :996-1001
-        float beta = betan / betad;
-        betad = betan;
-        alphan = betan;
-        if (nx == 1) beta = 0.0f;
-        chdwf::k_thr_xpay<<<nb, chdwf::kThreads, 0, h->st>>>(p, r, (double)beta, n);
-        chdwf::count_launches(1);
-        if (betan < resid) return CHDWF_OK;
-    }
-    return CHDWF_ITER_CAP;
+        thr_dslash(h, true, am, imass, x2, x1, u, run, it);               // :987
+        chdwf::k_thr_cg_r<<<chdwf::kRedBlocks, chdwf::kThreads, 0, h->st>>>(r, x2, n, h->part, c,
+                                                                          it, h->hflag_dev);
+        chdwf::k_thr_xpay<<<nb, chdwf::kThreads, 0, h->st>>>(p, r, c, it, n);
+        chdwf::count_launches(2);
+    });
+    if (e) return h->fail(e, "thr_congrad");
+    chdwf::ThrRun hr;
+    if ((e = cudaMemcpyAsync(&hr, run, sizeof(hr), cudaMemcpyDeviceToHost, h->st)) ||
+        (e = cudaStreamSynchronize(h->st)))
+        return h->fail(e, "thr_congrad");
+    *itercg = hr.iters;
+    return hr.done == 1 ? CHDWF_OK : CHDWF_ITER_CAP;
 }
 
 // measure (:1027-1285) with links u: psibarpsi, susclsing, aviter and the
@@ -763,6 +969,10 @@ int chdwf_thr_create(chdwf_thr** out, int ksize, int ksizet, int kthird, float d
     if (!e) e = talloc(&h->p, n * np);
     if (!e) e = talloc(&h->x1, n * np);
     if (!e) e = talloc(&h->part, chdwf::kRedBlocks);
+    if (!e) e = talloc(&h->qctl, 1);
+    if (!e) e = talloc(&h->cgctl, 1);
+    if (!e) e = cudaHostAlloc((void**)&h->hflag_host, sizeof(int), cudaHostAllocMapped);
+    if (!e) e = cudaHostGetDevicePointer((void**)&h->hflag_dev, h->hflag_host, 0);
     if (!e) e = cudaMemsetAsync(h->theta, 0, sizeof(float) * n3, h->st);
     if (!e) e = cudaMemsetAsync(h->Phi0, 0, sizeof(double2) * n * np, h->st);
     if (!e) e = cudaStreamSynchronize(h->st);
@@ -786,6 +996,9 @@ void chdwf_thr_destroy(chdwf_thr* h) {
                        h->x3, h->rr, h->p, h->x1})
         if (v) cudaFree(v);
     if (h->part) cudaFree(h->part);
+    if (h->qctl) cudaFree(h->qctl);
+    if (h->cgctl) cudaFree(h->cgctl);
+    if (h->hflag_host) cudaFreeHost(h->hflag_host);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
