@@ -114,12 +114,12 @@ int main(int argc, char** argv) {
                                 : make_double2(0.0, dag ? (double)am : (double)(-am));
         double2* o = dag ? outd.data() : out.data();
         for (g_tid = 0; g_tid < g.kferm; g_tid++) {
-            if (!dag) { if (imass == 1) k_thr_dslash<false,1>(o, R.data(), u.data(), g, diag, zk);
-                        else if (imass == 3) k_thr_dslash<false,3>(o, R.data(), u.data(), g, diag, zk);
-                        else k_thr_dslash<false,5>(o, R.data(), u.data(), g, diag, zk); }
-            else { if (imass == 1) k_thr_dslash<true,1>(o, R.data(), u.data(), g, diag, zk);
-                   else if (imass == 3) k_thr_dslash<true,3>(o, R.data(), u.data(), g, diag, zk);
-                   else k_thr_dslash<true,5>(o, R.data(), u.data(), g, diag, zk); }
+            if (!dag) { if (imass == 1) k_thr_dslash<false,1>(o, R.data(), u.data(), g, diag, zk, nullptr, 0);
+                        else if (imass == 3) k_thr_dslash<false,3>(o, R.data(), u.data(), g, diag, zk, nullptr, 0);
+                        else k_thr_dslash<false,5>(o, R.data(), u.data(), g, diag, zk, nullptr, 0); }
+            else { if (imass == 1) k_thr_dslash<true,1>(o, R.data(), u.data(), g, diag, zk, nullptr, 0);
+                   else if (imass == 3) k_thr_dslash<true,3>(o, R.data(), u.data(), g, diag, zk, nullptr, 0);
+                   else k_thr_dslash<true,5>(o, R.data(), u.data(), g, diag, zk, nullptr, 0); }
         }
     }
     const double tz = (double)(float)(2.0 * anum);
