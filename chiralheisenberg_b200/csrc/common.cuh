@@ -101,25 +101,110 @@ __device__ __forceinline__ double2 zcomb(double2 x, double2 y, bool use_i, int s
 // sequence (the pass-1 kernels and the regenerating pass 2, whatever their
 // thread shape) then produces the same bits, so regenerated Lanczos vectors
 // equal the first pass's.
-__device__ __forceinline__ float2 zadd(float2 a, float2 b) {
+//
+// On sm_100 an addition or subtraction of FP32 complex numbers is one packed
+// FP32x2 instruction (add/sub.rn.f32x2, written as PTX) instead of two scalar
+// ones; per lane it rounds exactly as __fadd_rn / __fsub_rn.  Products stay
+// scalar (__fmul_rn): measured on B200, the code generator fuses a packed
+// multiply whose only use is a packed add or subtract into a packed fused
+// multiply-add (one rounding instead of two), even with .rn, while scalar
+// products feeding packed sums are left alone.  x +- i*y mixes the lanes and
+// stays scalar.  Host builds of these helpers (the CPU tests of the element
+// functions) use the scalar forms, which give the same bits.
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
+#define CHDWF_F32X2 1
+#endif
+#ifdef CHDWF_F32X2
+#define CHDWF_F2OP(NAME, OP)                                                               \
+    __device__ __forceinline__ float2 NAME(float2 a, float2 b) {                           \
+        float2 d;                                                                          \
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t" \
+            OP " rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"                                 \
+            : "=f"(d.x), "=f"(d.y)                                                         \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                     \
+        return d;                                                                          \
+    }
+CHDWF_F2OP(f2_add, "add.rn.f32x2")
+CHDWF_F2OP(f2_sub, "sub.rn.f32x2")
+#undef CHDWF_F2OP
+#else
+__device__ __forceinline__ float2 f2_add(float2 a, float2 b) {
     return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
 }
-__device__ __forceinline__ float2 zsub(float2 a, float2 b) {
+__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
     return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
 }
-__device__ __forceinline__ float2 zmuli(float2 a) { return make_float2(-a.y, a.x); }
-__device__ __forceinline__ float2 zscal(float s, float2 a) {
-    return make_float2(__fmul_rn(s, a.x), __fmul_rn(s, a.y));
+#endif
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) {
+    return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
 }
+__device__ __forceinline__ float2 zadd(float2 a, float2 b) { return f2_add(a, b); }
+__device__ __forceinline__ float2 zsub(float2 a, float2 b) { return f2_sub(a, b); }
+__device__ __forceinline__ float2 zmuli(float2 a) { return make_float2(-a.y, a.x); }
+__device__ __forceinline__ float2 zscal(float s, float2 a) { return f2_mul(make_float2(s, s), a); }
 __device__ __forceinline__ float2 zmul(float2 a, float2 b) {
     return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
                        __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
 }
 __device__ __forceinline__ float2 zconj(float2 a) { return make_float2(a.x, -a.y); }
+// x +- y packed; x +- i*y = (x.x -+ y.y, x.y +- y.x) as two scalar operations
 __device__ __forceinline__ float2 zcomb(float2 x, float2 y, bool use_i, int sgn) {
-    float2 t = use_i ? zmuli(y) : y;
-    return sgn > 0 ? zadd(x, t) : zsub(x, t);
+    if (!use_i) return sgn > 0 ? zadd(x, y) : zsub(x, y);
+    return sgn > 0 ? make_float2(__fsub_rn(x.x, y.y), __fadd_rn(x.y, y.x))
+                   : make_float2(__fadd_rn(x.x, y.y), __fsub_rn(x.y, y.x));
 }
+
+// ---- FP32 complex numbers of two adjacent points, split by part ------------
+// The solver's FP32 Krylov vectors (Ls even) keep every aligned element pair
+// (e, e+1), e even -- two adjacent s of one component -- as the 16 bytes
+// (re_e, re_e+1, im_e, im_e+1): the "split" layout.  One 16-byte load then
+// puts both real parts in one register pair and both imaginary parts in the
+// other, so each complex operation on the two points, i*y included, is two
+// packed instructions with no lane exchange; per element the IEEE operations
+// are those of the float2 forms above.
+struct cpair {
+    float2 re, im;   // (point s, point s+1)
+};
+__device__ __forceinline__ cpair zadd(cpair a, cpair b) {
+    return cpair{f2_add(a.re, b.re), f2_add(a.im, b.im)};
+}
+__device__ __forceinline__ cpair zsub(cpair a, cpair b) {
+    return cpair{f2_sub(a.re, b.re), f2_sub(a.im, b.im)};
+}
+__device__ __forceinline__ cpair zscal(float s, cpair a) {
+    const float2 ss = make_float2(s, s);
+    return cpair{f2_mul(ss, a.re), f2_mul(ss, a.im)};
+}
+// x +- y, or x +- i*y: re = x.re -+ y.im, im = x.im +- y.re
+__device__ __forceinline__ cpair zcomb(cpair x, cpair y, bool use_i, int sgn) {
+    if (!use_i) return sgn > 0 ? zadd(x, y) : zsub(x, y);
+    return sgn > 0 ? cpair{f2_sub(x.re, y.im), f2_add(x.im, y.re)}
+                   : cpair{f2_add(x.re, y.im), f2_sub(x.im, y.re)};
+}
+__device__ __forceinline__ float2 cpair_pt(const cpair& c, int k) {   // point k as a complex
+    return k ? make_float2(c.re.y, c.im.y) : make_float2(c.re.x, c.im.x);
+}
+// Element pair at even element e of a split-layout vector
+__device__ __forceinline__ cpair ld_cpair(const float2* v, uint32_t e) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(v + e));
+    return cpair{make_float2(q.x, q.y), make_float2(q.z, q.w)};
+}
+__device__ __forceinline__ void st_cpair(float2* v, uint32_t e, const cpair& c) {
+    *reinterpret_cast<float4*>(v + e) = make_float4(c.re.x, c.re.y, c.im.x, c.im.y);
+}
+// Any element e of a split-layout vector
+__device__ __forceinline__ float2 sp_get(const float2* v, int64_t e) {
+    const float* f = reinterpret_cast<const float*>(v + (e & ~(int64_t)1));
+    const int o = (int)(e & 1);
+    return make_float2(__ldg(f + o), __ldg(f + 2 + o));
+}
+__device__ __forceinline__ void sp_put(float2* v, int64_t e, float2 x) {
+    float* f = reinterpret_cast<float*>(v + (e & ~(int64_t)1));
+    const int o = (int)(e & 1);
+    f[o] = x.x;
+    f[2 + o] = x.y;
+}
+
 
 template <class T> struct real_of;
 template <> struct real_of<double2> { typedef double type; };

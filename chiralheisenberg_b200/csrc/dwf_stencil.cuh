@@ -388,6 +388,132 @@ __device__ __forceinline__ void dwf_apply_flavour_pair(float2 acc[2][4],
     }
 }
 
+// Element loader of a split-layout FP32 vector (the wall operands).
+struct LdSp {
+    const float2* __restrict__ p;
+    __device__ __forceinline__ float2 operator()(int64_t j) const { return sp_get(p, j); }
+};
+
+// dwf_apply_flavour_pair on a split-layout vector (see cpair): the same two
+// points, loads and per-element operation sequence, with every hop, scaling
+// and three-term step done as packed FP32x2 operations on both points at
+// once.  The s hops and the wall terms act on one point of the pair and stay
+// per point.  Needs pair_ok(g).
+template <bool DAG, int IMASS>
+__device__ __forceinline__ void dwf_apply_flavour_pair_sp(cpair acc[4],
+                                                          const float2* __restrict__ in,
+                                                          const Geom& g, const PointIdx& q, int f,
+                                                          const float* __restrict__ chif,
+                                                          float diag, float hpin, bool apbc) {
+    constexpr int SF = DAG ? -1 : 1;
+    const int L = g.L, Lt = g.Lt, Ls = g.Ls;
+    const uint32_t LsI = (uint32_t)Ls, cs = (uint32_t)g.cs, fo = cs * (uint32_t)(4 * f);
+    const uint32_t qp = (uint32_t)q.p;
+    // diagonal term (:2651-2667)
+#pragma unroll
+    for (int d = 0; d < 4; d++) acc[d] = zscal(diag, ld_cpair(in, qp + fo + cs * d));
+    const uint32_t uL = (uint32_t)L;
+    const uint32_t xp = q.ix + 1 == L ? 0 : q.ix + 1, xm = q.ix == 0 ? L - 1 : q.ix - 1;
+    const uint32_t yp = q.iy + 1 == L ? 0 : q.iy + 1, ym = q.iy == 0 ? L - 1 : q.iy - 1;
+    const uint32_t tp = q.it + 1 == Lt ? 0 : q.it + 1, tm = q.it == 0 ? Lt - 1 : q.it - 1;
+    const uint32_t sb = (uint32_t)q.s + fo;
+    const uint32_t rowb = uL * ((uint32_t)q.iy + uL * (uint32_t)q.it);
+    const uint32_t n_xp = sb + LsI * (xp + rowb), n_xm = sb + LsI * (xm + rowb);
+    const uint32_t colb = (uint32_t)q.ix + uL * uL * (uint32_t)q.it;
+    const uint32_t n_yp = sb + LsI * (colb + uL * yp), n_ym = sb + LsI * (colb + uL * ym);
+    const uint32_t plb = (uint32_t)q.ix + uL * (uint32_t)q.iy;
+    const uint32_t n_tp = sb + LsI * (plb + uL * uL * tp), n_tm = sb + LsI * (plb + uL * uL * tm);
+    cpair r[4];
+#define CHDWF_SP_HOP(N, MU, SIG, NEG)                                                  \
+    {                                                                                 \
+        _Pragma("unroll") for (int d = 0; d < 4; d++) r[d] = ld_cpair(in, (N) + cs * d); \
+        hop<MU, SIG, NEG>(acc, r);                                                    \
+    }
+    CHDWF_SP_HOP(n_xp, 0, SF, false)
+    CHDWF_SP_HOP(n_xm, 0, -SF, false)
+    CHDWF_SP_HOP(n_yp, 1, SF, false)
+    CHDWF_SP_HOP(n_ym, 1, -SF, false)
+    CHDWF_SP_HOP(n_tp, 2, SF, false)
+    CHDWF_SP_HOP(n_tm, 2, -SF, false)
+    // kappa = 1/2 (:2815-2829)
+#pragma unroll
+    for (int d = 0; d < 4; d++) acc[d] = zscal(0.5f, acc[d]);
+    // antiperiodic boundary in t (:2831-2876)
+    if (apbc) {
+        if (q.it == Lt - 1) CHDWF_SP_HOP(n_tp, 2, SF, true)
+        if (q.it == 0) CHDWF_SP_HOP(n_tm, 2, -SF, true)
+    }
+#undef CHDWF_SP_HOP
+    // s hops (:2879-2908; M^dagger :3313-3342): point 0 is s, point 1 is s+1
+    constexpr int UP = DAG ? 0 : 2;
+    constexpr int DN = DAG ? 2 : 0;
+#pragma unroll
+    for (int d = UP; d < UP + 2; d++) {
+        const cpair c = ld_cpair(in, qp + fo + cs * d);
+        acc[d].re.x = __fsub_rn(acc[d].re.x, c.re.y);
+        acc[d].im.x = __fsub_rn(acc[d].im.x, c.im.y);
+        if (q.s + 2 < Ls) {
+            const cpair n = ld_cpair(in, qp + 2 + fo + cs * d);
+            acc[d].re.y = __fsub_rn(acc[d].re.y, n.re.x);
+            acc[d].im.y = __fsub_rn(acc[d].im.y, n.im.x);
+        }
+    }
+#pragma unroll
+    for (int d = DN; d < DN + 2; d++) {
+        const cpair c = ld_cpair(in, qp + fo + cs * d);
+        if (q.s > 0) {
+            const cpair pv = ld_cpair(in, qp - 2 + fo + cs * d);
+            acc[d].re.x = __fsub_rn(acc[d].re.x, pv.re.y);
+            acc[d].im.x = __fsub_rn(acc[d].im.x, pv.im.y);
+        }
+        acc[d].re.y = __fsub_rn(acc[d].re.y, c.re.x);
+        acc[d].im.y = __fsub_rn(acc[d].im.y, c.im.x);
+    }
+    // wall coupling: point 1 at s=Ls (pair WA, reads s=1), point 0 at s=1
+    // (pair WB, reads s=Ls)
+    constexpr int WA = DAG ? 0 : 2;
+    constexpr int WB = DAG ? 2 : 0;
+    const bool atL = (q.s + 2 == Ls), at0 = (q.s == 0);
+    if (!(atL || at0)) return;
+    const float c1f = __ldg(chif + q.site), c2f = __ldg(chif + g.kvol + q.site),
+                c3f = __ldg(chif + 2 * g.kvol + q.site);
+    const bool pin = (q.site == 0);
+    if (atL && at0) {   // Ls = 2: one pair holds both walls
+        float2 w0[4], w1[4];
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            w0[d] = cpair_pt(acc[d], 0);
+            w1[d] = cpair_pt(acc[d], 1);
+        }
+        wall_terms<DAG, IMASS, WA, 0>(w1, LdSp{in}, cs, LsI * q.site, f, c1f, c2f, c3f, pin, hpin);
+        wall_terms<DAG, IMASS, WB, 1>(w0, LdSp{in}, cs, LsI * q.site + Ls - 1, f, c1f, c2f, c3f,
+                                      pin, hpin);
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            acc[d].re = make_float2(w0[d].x, w1[d].x);
+            acc[d].im = make_float2(w0[d].y, w1[d].y);
+        }
+        return;
+    }
+    // one wall point: point 1 at s=Ls or point 0 at s=1, one code path
+    float2 w[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) w[d] = cpair_pt(acc[d], atL ? 1 : 0);
+    wall_terms_rt<DAG, IMASS>(w, LdSp{in}, (int64_t)cs,
+                              atL ? (int64_t)LsI * q.site : (int64_t)LsI * q.site + Ls - 1, atL,
+                              f, c1f, c2f, c3f, pin, hpin);
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        if (atL) {
+            acc[d].re.y = w[d].x;
+            acc[d].im.y = w[d].y;
+        } else {
+            acc[d].re.x = w[d].x;
+            acc[d].im.x = w[d].y;
+        }
+    }
+}
+
 // Thread -> (point, flavour) map of the flavour-split kernels: a block of
 // kSplitThreads threads covers kSplitThreads/2 consecutive points, the first
 // half of its threads flavour 0 and the second half flavour 1, so every warp

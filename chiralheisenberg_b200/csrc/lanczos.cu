@@ -46,6 +46,15 @@ __device__ __forceinline__ T* ring(const LzArgsT<T>& a, int j) {
     return r == 0 ? a.rb0 : (r == 1 ? a.rb1 : a.rb2);
 }
 
+// Element e of a Krylov vector: FP32 vectors with Ls even are in the split
+// layout (cpair), FP64 vectors and odd-Ls FP32 vectors plain.
+__device__ __forceinline__ double2 vget(const LzArgsT<double2>&, const double2* v, int64_t e) {
+    return __ldg(v + e);
+}
+__device__ __forceinline__ float2 vget(const LzArgsT<float2>& a, const float2* v, int64_t e) {
+    return a.pl ? sp_get(v, e) : __ldg(v + e);
+}
+
 static_assert(kSplitThreads == kThreads, "the reductions assume kThreads-wide blocks");
 
 // KernelTimer class of a launch: c for FP64 Krylov vectors, c + 4 for FP32.
@@ -129,16 +138,6 @@ __device__ __forceinline__ void lz_lane(int64_t base, int64_t* p, int* f0) {
     }
 }
 
-// 16-byte access to two adjacent FP32 complex numbers (e even).
-__device__ __forceinline__ void ld_pair(const float2* b, uint32_t e, float2& v0, float2& v1) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(b + e));
-    v0 = make_float2(v.x, v.y);
-    v1 = make_float2(v.z, v.w);
-}
-__device__ __forceinline__ void st_pair(float2* b, uint32_t e, float2 v0, float2 v1) {
-    *reinterpret_cast<float4*>(b + e) = make_float4(v0.x, v0.y, v1.x, v1.y);
-}
-
 // vt = M q_j with q_j = r_j / beta_j, formed as (1/beta_j) (M r_j): one
 // scaling per output element instead of one per stencil load.  The pass-1
 // kernel and the regenerating pass 2 use this same sequence.
@@ -185,17 +184,17 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
         if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
         if constexpr (PAIR) {
-            float2 acc[2][4];
-            dwf_apply_flavour_pair<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
-                                                 a.apbc != 0);
+            cpair acc[4];
+            dwf_apply_flavour_pair_sp<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                    a.apbc != 0);
             // |vt|^2 is summed in FP64 from the first term: a pair's partial
             // sum in FP32 made the FP32 force solves 7% longer (alpha~ and
             // beta steer the recurrences)
 #pragma unroll
             for (int d = 0; d < 4; d++) {
-                const float2 v0 = zscal(ib, acc[0][d]), v1 = zscal(ib, acc[1][d]);
-                st_pair(a.vt, (uint32_t)p + (uint32_t)a.g.cs * (uint32_t)(d + 4 * f0), v0, v1);
-                const double2 w0 = widen(v0), w1 = widen(v1);
+                const cpair v = zscal(ib, acc[d]);
+                st_cpair(a.vt, (uint32_t)p + (uint32_t)a.g.cs * (uint32_t)(d + 4 * f0), v);
+                const double2 w0 = widen(cpair_pt(v, 0)), w1 = widen(cpair_pt(v, 1));
                 loc += w0.x * w0.x + w0.y * w0.y;
                 loc += w1.x * w1.x + w1.y * w1.y;
             }
@@ -299,24 +298,19 @@ __device__ __forceinline__ T three_term(const LzArgsT<T>& a, T x3, int64_t e, in
     return v;
 }
 
-// The same update for the two points of an FP32 pair (elements e, e+1).
-__device__ __forceinline__ void three_term_pair(const LzArgsT<float2>& a, float2 x0, float2 x1,
-                                                uint32_t e, int j, double alphat, float2& v0,
-                                                float2& v1) {
+// The same update for the two points of an FP32 pair (elements e, e+1) of
+// split-layout vectors, both points at once.
+__device__ __forceinline__ cpair three_term_sp(const LzArgsT<float2>& a, cpair x, uint32_t e,
+                                               int j, double alphat) {
     const float2* rj = ring(a, j);
     const float2* rjm = ring(a, j - 1);
     const float ib = (float)a.h.invbeta[j], at = (float)alphat, bj = (float)a.h.beta[j];
-    float2 c0, c1;
-    ld_pair(rj, e, c0, c1);
-    v0 = zsub(x0, zscal(at, zscal(ib, c0)));
-    v1 = zsub(x1, zscal(at, zscal(ib, c1)));
+    cpair v = zsub(x, zscal(at, zscal(ib, ld_cpair(rj, e))));
     if (j > 1) {
         const float ibm = (float)a.h.invbeta[j - 1];
-        float2 m0, m1;
-        ld_pair(rjm, e, m0, m1);
-        v0 = zsub(v0, zscal(bj, zscal(ibm, m0)));
-        v1 = zsub(v1, zscal(bj, zscal(ibm, m1)));
+        v = zsub(v, zscal(bj, zscal(ibm, ld_cpair(rjm, e))));
     }
+    return v;
 }
 
 // Force solves with a wall store: element e of r_{j+1} at point (s, site),
@@ -353,15 +347,15 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
         if (p >= R.end) continue;
         const PointIdx q = point_of(a.g, p);
         if constexpr (PAIR) {
-            float2 acc[2][4];
-            dwf_apply_flavour_pair<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
-                                                a.apbc != 0);
+            cpair acc[4];
+            dwf_apply_flavour_pair_sp<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                   a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const uint32_t e = (uint32_t)p + (uint32_t)a.g.cs * (uint32_t)(d + 4 * f0);
-                float2 v0, v1;
-                three_term_pair(a, acc[0][d], acc[1][d], e, j, at, v0, v1);
-                st_pair(rn, e, v0, v1);
+                const cpair v = three_term_sp(a, acc[d], e, j, at);
+                st_cpair(rn, e, v);
+                const float2 v0 = cpair_pt(v, 0), v1 = cpair_pt(v, 1);
                 if (WALLS) {
                     wall_put(a, j + 1, q.s, q.site, d + 4 * f0, v0);
                     wall_put(a, j + 1, q.s + 1, q.site, d + 4 * f0, v1);
@@ -410,21 +404,11 @@ __device__ __forceinline__ void row_fail(LzCtl* ctl, int* hflag) {
     }
 }
 
-// PPT adjacent elements of a global vector (one 16-byte load for an FP32 pair)
+// PPT adjacent elements of a global vector
 template <class T, int PPT> struct LzLd;
 template <class T> struct LzLd<T, 1> {
     __device__ __forceinline__ static void get(const T* p, T* v) { v[0] = *p; }
     __device__ __forceinline__ static void put(T* p, const T* v) { *p = v[0]; }
-};
-template <> struct LzLd<float2, 2> {
-    __device__ __forceinline__ static void get(const float2* p, float2* v) {
-        const float4 q = *reinterpret_cast<const float4*>(p);
-        v[0] = make_float2(q.x, q.y);
-        v[1] = make_float2(q.z, q.w);
-    }
-    __device__ __forceinline__ static void put(float2* p, const float2* v) {
-        *reinterpret_cast<float4*>(p) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
-    }
 };
 
 template <class T, int IMASS, int PPT>
@@ -571,7 +555,7 @@ __device__ __forceinline__ void lz2_accumulate(const LzArgsT<T>& a, int j, const
         const double cj = a.h.c[j];
         for (int c = c0; c < c0 + nc; c++) {
             const int64_t e = p + a.g.cs * c;
-            const double2 qj = widen(zscal(ib, __ldg(rj + e)));
+            const double2 qj = widen(zscal(ib, vget(a, rj, e)));
             double2 xv = a.x[e];
             xv.x += cj * qj.x;
             xv.y += cj * qj.y;
@@ -587,7 +571,7 @@ __device__ __forceinline__ void lz2_accumulate(const LzArgsT<T>& a, int j, const
         double2 qv[8];
 #pragma unroll
         for (int c = 0; c < 8; c++)
-            if (c < nc) qv[c] = widen(zscal(ib, __ldg(rj + p + a.g.cs * (c + c0))));
+            if (c < nc) qv[c] = widen(zscal(ib, vget(a, rj, p + a.g.cs * (c + c0))));
         const int64_t base = sw + 2 * (int64_t)q.site + cs2 * c0;
         for (int k = 0; k < n; k++) {
             const double y = a.h.y[k * H + j];
@@ -619,12 +603,12 @@ __global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks))
     const T* rj = ring(a, j);
     if constexpr (PAIR) {
         if (apply) {
-            float2 acc[2][4];
-            dwf_apply_flavour_pair<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
-                                                 a.apbc != 0);
+            cpair acc[4];
+            dwf_apply_flavour_pair_sp<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                                    a.apbc != 0);
 #pragma unroll
             for (int d = 0; d < 4; d++)
-                st_pair(a.vt, p + a.g.cs * (d + 4 * f0), zscal(ib, acc[0][d]), zscal(ib, acc[1][d]));
+                st_cpair(a.vt, (uint32_t)(p + a.g.cs * (d + 4 * f0)), zscal(ib, acc[d]));
         }
         lz2_accumulate<T, IFLAG>(a, j, rj, ib, p, q, 4 * f0, 4);
         const PointIdx q1 = point_of(a.g, p + 1);
@@ -655,15 +639,13 @@ __global__ void __launch_bounds__(kThreads, (LzShape<T, PAIR>::min_blocks))
     const PointIdx q = point_of(a.g, p);
     T* rn = ring(a, j + 1);
     if constexpr (PAIR) {
-        float2 acc[2][4];
-        dwf_apply_flavour_pair<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
-                                            a.apbc != 0);
+        cpair acc[4];
+        dwf_apply_flavour_pair_sp<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
+                                               a.apbc != 0);
 #pragma unroll
         for (int d = 0; d < 4; d++) {
-            const int64_t e = p + a.g.cs * (d + 4 * f0);
-            float2 v0, v1;
-            three_term_pair(a, acc[0][d], acc[1][d], e, j, a.h.alphat[j], v0, v1);
-            st_pair(rn, e, v0, v1);
+            const uint32_t e = (uint32_t)(p + a.g.cs * (d + 4 * f0));
+            st_cpair(rn, e, three_term_sp(a, acc[d], e, j, a.h.alphat[j]));
         }
     } else {
 #pragma unroll
@@ -751,7 +733,7 @@ __global__ void __launch_bounds__(kThreads) k_lz_coeffs(LzCtl* ctl, LzHist h, in
 // r_1 = Phi in the vector precision; partial sums of |r_1|^2
 template <class T>
 __global__ void k_lz_source(T* __restrict__ r1, const double2* __restrict__ phi, int64_t n,
-                            double* __restrict__ part) {
+                            double* __restrict__ part, int pl) {
     __shared__ double sh[kThreads / 32];
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -760,7 +742,12 @@ __global__ void k_lz_source(T* __restrict__ r1, const double2* __restrict__ phi,
         T t;
         t.x = (typename real_of<T>::type)v.x;
         t.y = (typename real_of<T>::type)v.y;
-        r1[i] = t;
+        if constexpr (std::is_same<T, float2>::value) {
+            if (pl) sp_put(r1, i, t);
+            else r1[i] = t;
+        } else {
+            r1[i] = t;
+        }
         const double2 w = widen(t);
         s += w.x * w.x + w.y * w.y;
     }
@@ -832,15 +819,11 @@ static void launch_pass1_rows_ppt(const LzArgsT<T>& a, unsigned nb, cudaStream_t
     cudaStreamWaitEvent(st, side.join, 0);
 }
 
+// One point a thread: the FP64 solves and odd-Ls FP32 solves (even-Ls FP32
+// vectors are in the split layout, which only the point-gather kernels read).
 template <class T, int IMASS>
 static void launch_pass1_rows(const LzArgsT<T>& a, unsigned nb, cudaStream_t st,
                               const LzSide& side, KernelTimer* tm) {
-    if constexpr (std::is_same<T, float2>::value) {
-        if (a.rp.ppt == 2) {
-            launch_pass1_rows_ppt<T, IMASS, 2>(a, nb, st, side, tm);
-            return;
-        }
-    }
     launch_pass1_rows_ppt<T, IMASS, 1>(a, nb, st, side, tm);
 }
 
@@ -860,14 +843,9 @@ static void lz_rows_kernels(const void* kern[6]) {
 template <class T>
 static bool lz_rows_setup(const Geom& g, RowPlan* rp, unsigned* nb, cudaStream_t st) {
     if (stencil_choice(g, (int)sizeof(T), st) != kStencilRows) return false;
-    if (!row_plan(g, sizeof(T), rp)) return false;
+    if (!row_plan(g, sizeof(T), rp) || rp->ppt != 1) return false;
     const void* kern[6];
-    if constexpr (std::is_same<T, float2>::value) {
-        if (rp->ppt == 2) lz_rows_kernels<T, 2>(kern);
-        else lz_rows_kernels<T, 1>(kern);
-    } else {
-        lz_rows_kernels<T, 1>(kern);
-    }
+    lz_rows_kernels<T, 1>(kern);
     int dev = 0, nsm = 0, per_sm = 1 << 20;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1303,7 +1281,8 @@ __global__ void __launch_bounds__(kThreads) k_lz_walls_of(LzArgsT<T> a, const T*
     const int64_t rr = t - c * cs2;
     const int sw = (int)(rr & 1);
     const int64_t site = rr >> 1;
-    a.wbasis[(int64_t)j * 8 * cs2 + t] = r[(sw ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * site + a.g.cs * c];
+    a.wbasis[(int64_t)j * 8 * cs2 + t] =
+        vget(a, r, (sw ? a.g.Ls - 1 : 0) + (int64_t)a.g.Ls * site + a.g.cs * c);
 }
 
 // q_j's wall slices (j = 1..m) into every pole's two-slice x_k: the same
@@ -1347,12 +1326,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_lz_accum_walls(LzArgsT<T> a, in
         __syncthreads();
         if (act) {
             // q_{j+1} is loaded while q_j is accumulated
-            const T* b = src + e + j0 * stride;
-            T qn = __ldg(b);
+            const int64_t b = e + j0 * stride;
+            T qn = STORE ? __ldg(src + b) : vget(a, src, b);
 #pragma unroll 1
             for (int jj = 0; jj < jn; jj++) {
                 const T q = qn;
-                if (jj + 1 < jn) qn = __ldg(b + (jj + 1) * stride);
+                if (jj + 1 < jn) {
+                    const int64_t bn = b + (jj + 1) * stride;
+                    qn = STORE ? __ldg(src + bn) : vget(a, src, bn);
+                }
                 const double2 qj = widen(zscal(ibs[jj], q));
 #pragma unroll
                 for (int k = 0; k < NC; k++) {
@@ -1390,11 +1372,10 @@ __global__ void __launch_bounds__(kThreads) k_lz_accum_x(LzArgsT<T> a, int j0, i
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= a.g.kferm) return;
     double2 xv = a.x[e];
-    const T* b = a.basis + e;
     const int64_t stride = a.g.kferm;
 #pragma unroll 4
     for (int j = j0; j <= j1; j++) {
-        const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(b + j * stride)));
+        const double2 qj = widen(zscal((Real)a.h.invbeta[j], vget(a, a.basis, e + j * stride)));
         const double cj = a.h.c[j];
         xv.x += cj * qj.x;
         xv.y += cj * qj.y;
@@ -1418,7 +1399,7 @@ __global__ void __launch_bounds__(kThreads) k_lz_accum_poles(LzArgsT<T> a, int m
 #pragma unroll
     for (int k = 0; k < 8; k++) acc[k] = make_double2(0.0, 0.0);
     for (int j = 1; j <= m; j++) {
-        const double2 qj = widen(zscal((Real)a.h.invbeta[j], __ldg(a.basis + j * stride + e)));
+        const double2 qj = widen(zscal((Real)a.h.invbeta[j], vget(a, a.basis, j * stride + e)));
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             if (k0 + k < n) {
@@ -1474,7 +1455,11 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     a.xw = w.xw;
     a.npole = ndiag;
     unsigned nb = 0;
-    a.rows = lz_rows_setup<T>(g, &a.rp, &nb, st) ? 1 : 0;
+    // FP32 vectors with Ls even live in the split layout, which only the
+    // point-gather kernels read (the row-staged shape serves the FP64 solves
+    // and odd Ls)
+    a.pl = lz_pair<T>(g) ? 1 : 0;
+    a.rows = !a.pl && lz_rows_setup<T>(g, &a.rp, &nb, st) ? 1 : 0;
     a.occ = stencil_choice(g, (int)sizeof(T), st) == kStencilGather4 ? 4 : 3;
     if (!a.rows) nb = lz_pass1_blocks_any<T>(g, imass, a.occ);
     const int nbr = reduce_blocks(g.kferm);
@@ -1482,7 +1467,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     T* r1 = a.hcap > 1 ? a.basis + g.kferm : a.rb1;
 
     // r_1 = Phi, beta_1 = |r_1|
-    k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);
+    k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part, a.pl);
     k_lz_init<<<1, kThreads, 0, st>>>(w.ctl, w.hist, w.part, nbr);
     count_launches(2);
     if (a.wcap > 1) {                    // r_1's wall slices (pass 1 adds r_2, r_3, ...)
@@ -1561,7 +1546,7 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
 
     // coefficients, then pass 2 over the regenerated vectors
     k_lz_coeffs<<<1, kThreads, 0, st>>>(w.ctl, w.hist, iflag);
-    k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part);
+    k_lz_source<T><<<nbr, kThreads, 0, st>>>(r1, phi, g.kferm, w.part, a.pl);
     count_launches(2);
     if (iflag == 2) {
         // every x_k from the stored basis, poles in chunks of 8 (one pass over

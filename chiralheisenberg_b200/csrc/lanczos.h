@@ -30,6 +30,7 @@ struct LzArgsT {
     int npole;
     T* wbasis;                  // force solves: the two wall slices of each r_j,
     int wcap;                   // j < wcap, at wbasis + j*16*kvol (0: no wall store)
+    int pl;                     // FP32 vectors in the split layout (cpair; Ls even)
     int rows;                   // pass 1 on the row-staged kernels (plan rp)
     int occ;                    // else the point-gather kernels at 3 or 4 blocks a SM
     RowPlan rp;

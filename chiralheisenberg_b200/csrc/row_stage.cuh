@@ -71,13 +71,15 @@ static_assert((kRowMaxThreads / 32 + 3) / 4 * 32 * kRowRegs <= 16384,
 
 // Which stencil kernels run, from the environment variable CHDWF_STENCIL:
 // 0 (unset): the autotuner's choice per lattice and precision (tune.cu);
-// 1 ("legacy"): the point-gather kernels only; 2 ("rows"): row kernels
-// wherever they fit (tests use it to run them on small lattices).
+// 1 ("legacy"): the point-gather kernels at 3 blocks a SM; 2 ("rows"): row
+// kernels wherever they fit (tests use it to run them on small lattices);
+// 3 ("gather4"): the point-gather kernels at 4 blocks a SM.
 inline int stencil_mode() {
     const char* v = getenv("CHDWF_STENCIL");
     if (!v) return 0;
     if (strcmp(v, "legacy") == 0) return 1;
     if (strcmp(v, "rows") == 0) return 2;
+    if (strcmp(v, "gather4") == 0) return 3;
     return 0;
 }
 

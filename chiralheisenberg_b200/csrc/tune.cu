@@ -82,6 +82,7 @@ int stencil_choice(const Geom& g, int elem, cudaStream_t st) {
     RowPlan rp;
     const bool rows_fit = row_plan(g, (size_t)elem, &rp);
     if (mode == 1) return kStencilGather3;
+    if (mode == 3) return elem == 4 ? kStencilGather3 : kStencilGather4;
     if (mode == 2) return rows_fit && op_rows_launchable(g, elem) ? kStencilRows : kStencilGather3;
     int dev = 0;
     cudaGetDevice(&dev);

@@ -129,9 +129,11 @@ def test_rows_force_against_oracle(monkeypatch, remez):
 
 @pytest.mark.parametrize("Ls", [6, 5])
 def test_rows_mixed_precision_trajectory(monkeypatch, remez, Ls):
-    """FP32 force solves on the row kernels (Ls 6 and 5: rows of 36 and 30
-    points, both whole multiples of 16 bytes in FP32): the FP64 chain's
-    decisions and dH within 1e-8 of H."""
+    """Mixed precision with the row kernels forced: the FP64 heatbath and
+    action solves run on rows in both cases; the FP32 force solves run on
+    rows for Ls 5 (rows of 30 points), while for Ls 6 their vectors are in
+    the split layout, which only the point-gather kernels read.  The FP64
+    chain's decisions and dH within 1e-8 of H."""
     monkeypatch.setenv("CHDWF_STENCIL", "rows")
     L, Lt = 6, 6
     beta = 0.475

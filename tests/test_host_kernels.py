@@ -17,6 +17,11 @@ call), extracts the element functions and per-element kernels of the two
 g++ into a small program, runs every element over random inputs, and
 compares.
 
+A fourth program compares the FP32 two-point operator on the solver's
+split vector layout (dwf_apply_flavour_pair_sp, whose additions are packed
+FP32x2 instructions on the GPU) with the plain-layout one, element by
+element.
+
 It checks the arithmetic of the kernel bodies only; the device build, the
 launch shapes and the solvers are checked by the -m gpu tests.
 """
@@ -141,6 +146,7 @@ RHMC_PROGRAM = r'''
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
+#include <cstring>
 #define __forceinline__ inline
 #define __shared__
 static inline double __dadd_rn(double a, double b) { return a + b; }
@@ -194,6 +200,55 @@ int main(int argc, char** argv) {
 '''
 
 
+# The FP32 two-point operator in both vector layouts: the plain one
+# (dwf_apply_flavour_pair, the standalone FP32 operator) and the split layout
+# of the solver's Krylov vectors (dwf_apply_flavour_pair_sp).  Every element
+# must come out with the same bits.  Prints the number of differing elements.
+SPLIT_PROGRAM = RHMC_PROGRAM.split("using namespace chdwf;")[0] + r"""
+using namespace chdwf;
+int main(int argc, char** argv) {
+    int L = atoi(argv[1]), Lt = atoi(argv[2]), Ls = atoi(argv[3]);
+    Geom g = make_geom(L, Lt, Ls);
+    std::vector<float2> in(g.kferm), insp(g.kferm);
+    std::vector<float> chif(3 * g.kvol);
+    FILE* f = fopen(argv[4], "rb");
+    if (fread(in.data(), 8, g.kferm, f) != (size_t)g.kferm) return 1;
+    if (fread(chif.data(), 4, 3 * g.kvol, f) != (size_t)(3 * g.kvol)) return 1;
+    fclose(f);
+    float* sp = reinterpret_cast<float*>(insp.data());
+    for (int64_t e = 0; e < g.kferm; e += 2) {
+        sp[2 * e] = in[e].x; sp[2 * e + 1] = in[e + 1].x;
+        sp[2 * e + 2] = in[e].y; sp[2 * e + 3] = in[e + 1].y;
+    }
+    const float diag = 2.0f * ((3.0f - 1.0f) + 1.0f), hpin = 0.3f;
+    long long bad = 0, n = 0;
+    for (int dag = 0; dag < 2; dag++)
+    for (int imass = 1; imass <= 3; imass += 2)
+    for (int apbc = 0; apbc < 2; apbc++)
+    for (int64_t p = 0; p < g.npts; p += 2) {
+        const PointIdx q = point_of(g, p);
+        for (int fl = 0; fl < 2; fl++) {
+            float2 a[2][4];
+            cpair c[4];
+#define RUN(D, I) { dwf_apply_flavour_pair<D, I>(a, in.data(), g, q, fl, chif.data(), diag, hpin, apbc); \
+                    dwf_apply_flavour_pair_sp<D, I>(c, insp.data(), g, q, fl, chif.data(), diag, hpin, apbc); }
+            if (dag) { if (imass == 1) RUN(true, 1) else RUN(true, 3) }
+            else { if (imass == 1) RUN(false, 1) else RUN(false, 3) }
+#undef RUN
+            for (int d = 0; d < 4; d++)
+                for (int k = 0; k < 2; k++) {
+                    const float2 v = cpair_pt(c[d], k);
+                    n++;
+                    if (memcmp(&v, &a[k][d], sizeof(float2)) != 0) bad++;
+                }
+        }
+    }
+    printf("%lld %lld\n", bad, n);
+    return 0;
+}
+"""
+
+
 def _section(src, start, end):
     a, b = src.find(start), src.find(end)
     assert a >= 0 and b > a, f"section markers moved: {start!r} .. {end!r}"
@@ -222,6 +277,12 @@ def _build(tmp, name, code, extra=()):
 @pytest.fixture(scope="module")
 def rhmc_exe(tmp_path_factory):
     return _build(str(tmp_path_factory.mktemp("rhmc")), "rhmc", RHMC_PROGRAM,
+                  extra=["-I", CSRC])
+
+
+@pytest.fixture(scope="module")
+def split_exe(tmp_path_factory):
+    return _build(str(tmp_path_factory.mktemp("split")), "split", SPLIT_PROGRAM,
                   extra=["-I", CSRC])
 
 
@@ -264,6 +325,26 @@ def test_rhmc_fp64_operator_element_matches_oracle(rhmc_exe, tmp_path, shape, im
                     fin, fout], check=True)
     out = np.fromfile(fout, dtype=np.complex128).reshape(sh)
     assert np.array_equal(out, po.dslash(lat, R, chi, hpin=hpin, imass=imass, dag=bool(dag)))
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 6), (6, 4, 8), (4, 3, 2)])
+def test_fp32_split_layout_matches_plain_pair(split_exe, tmp_path, shape):
+    """The FP32 solver's split-layout two-point operator (packed on the GPU)
+    against the plain-layout one: same bits for M and M^dagger, both mass
+    terms, both time boundaries, the pinning term, Ls = 2 included."""
+    L, Lt, Ls = shape
+    rng = np.random.default_rng(L * 100 + Lt * 10 + Ls)
+    n = 8 * L * L * Lt * Ls
+    R = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    chi = rng.standard_normal(3 * L * L * Lt).astype(np.float32)
+    fin = str(tmp_path / "in.bin")
+    with open(fin, "wb") as f:
+        f.write(R.tobytes())
+        f.write(chi.tobytes())
+    out = subprocess.run([split_exe, str(L), str(Lt), str(Ls), fin], check=True,
+                         capture_output=True, text=True).stdout.split()
+    bad, total = int(out[0]), int(out[1])
+    assert total == 2 * 2 * 2 * n and bad == 0, (bad, total)
 
 
 @pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 5), (6, 4, 8)])
