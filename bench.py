@@ -643,8 +643,11 @@ def rows_chosen(L, Ls, k):
     """The stencil shape the autotuner chose for class k's precision."""
     import chiralheisenberg_b200 as chb
     elem = 8 if k >= 4 else 16
+    # FP32 solves with Ls even run the split-layout kernels (their own entry)
+    layout = "split" if (k >= 4 and Ls % 2 == 0) else "plain"
     for t in chb.autotune_report():
-        if (t["L"], t["Lt"], t["Ls"], t["elem_bytes"]) == (L, L, Ls, elem):
+        if (t["L"], t["Lt"], t["Ls"], t["elem_bytes"], t.get("layout", "plain")) == \
+                (L, L, Ls, elem, layout):
             return t["choice"]
     return ""
 

@@ -280,6 +280,35 @@ __global__ void __launch_bounds__(kSplitThreads, OCC)
     }
 }
 
+// The same thread shape on a split-layout vector (the FP32 solver's Krylov
+// vectors, see cpair): M only, for the autotuner, which times the shapes the
+// solver's pass 1 will run.
+template <int OCC>
+__global__ void __launch_bounds__(kSplitThreads, OCC)
+    k_dslash_f32_sp(float2* __restrict__ out, const float2* __restrict__ in,
+                    const float* __restrict__ chif, Geom g, float diag) {
+    const int64_t p = (int64_t)blockIdx.x * (2 * kSplitPoints) +
+                      2 * (threadIdx.x & (kSplitPoints - 1));
+    const int f = split_flavour();
+    if (p >= g.npts) return;
+    const PointIdx q = point_of(g, p);
+    cpair acc[4];
+    dwf_apply_flavour_pair_sp<false, 1>(acc, in, g, q, f, chif, diag, 0.0f, true);
+#pragma unroll
+    for (int d = 0; d < 4; d++) st_cpair(out, (uint32_t)(p + g.cs * (d + 4 * f)), acc[d]);
+}
+
+void launch_dslash_sp_m(float2* out, const float2* in, const float* chif, const Geom& g,
+                        cudaStream_t st, int shape) {
+    const unsigned nb2 = (unsigned)((g.npts + 2 * kSplitPoints - 1) / (2 * kSplitPoints));
+    const float diag = diag_of(1.0f);
+    if (shape == kStencilGather4)
+        k_dslash_f32_sp<4><<<nb2, kSplitThreads, 0, st>>>(out, in, chif, g, diag);
+    else
+        k_dslash_f32_sp<3><<<nb2, kSplitThreads, 0, st>>>(out, in, chif, g, diag);
+    count_launches(1);
+}
+
 // ---- FP16 storage, four points a thread ----------------------------------------
 // Point q (s a multiple of 4) and its three successors s+1..s+3 of flavour f:
 // each neighbour is one 16-byte load of four FP16 complex numbers (the layout

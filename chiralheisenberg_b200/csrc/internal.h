@@ -79,6 +79,13 @@ constexpr int kStencilGather3 = 0, kStencilRows = 1, kStencilGather4 = 2;
 // vectors on stream st and keeps the fastest; "legacy" forces the
 // point-gather kernels at 3 blocks a SM, "rows" the row-staged ones.
 int stencil_choice(const Geom& g, int elem, cudaStream_t st);
+// The same for the FP32 solver's split-layout vectors (Ls even): the
+// point-gather shapes only, timed on the split-layout operator; "rows" and
+// "legacy" give the 3-block shape, "gather4" the 4-block one.
+int stencil_choice_split(const Geom& g, cudaStream_t st);
+// M on split-layout FP32 vectors in a point-gather shape (the tuner's probe).
+void launch_dslash_sp_m(float2* out, const float2* in, const float* chif, const Geom& g,
+                        cudaStream_t st, int shape);
 // Whether the row-staged operator of this element size (16 FP64, 8 FP32,
 // 4 FP16 storage) can launch on this lattice and device: its rows fit the
 // shared memory and a block fits an SM.

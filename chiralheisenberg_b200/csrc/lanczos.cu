@@ -1460,7 +1460,10 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     // and odd Ls)
     a.pl = lz_pair<T>(g) ? 1 : 0;
     a.rows = !a.pl && lz_rows_setup<T>(g, &a.rp, &nb, st) ? 1 : 0;
-    a.occ = stencil_choice(g, (int)sizeof(T), st) == kStencilGather4 ? 4 : 3;
+    a.occ = (a.pl ? stencil_choice_split(g, st) : stencil_choice(g, (int)sizeof(T), st)) ==
+                    kStencilGather4
+                ? 4
+                : 3;
     if (!a.rows) nb = lz_pass1_blocks_any<T>(g, imass, a.occ);
     const int nbr = reduce_blocks(g.kferm);
     // r_1 lives where ring(a, 1) looks for it: the basis store when present
