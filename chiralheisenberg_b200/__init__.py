@@ -44,6 +44,7 @@ EXPORTS = (
     "chdwf_traj_get_phi", "chdwf_traj_update_momenta", "chdwf_traj_update_chi",
     "chdwf_traj_accept", "chdwf_traj_sync", "chdwf_traj_propagator",
     "chdwf_traj_set_momenta_dev", "chdwf_timing", "chdwf_timing_read", "chdwf_prog_stage",
+    "chdwf_timing_read_chunks",
     "chdwf_get_stream", "chdwf_kernel_launches", "chdwf_set_precision", "chdwf_dslash_dev_lp",
     "chdwf_prog_state_size", "chdwf_prog_get_state", "chdwf_prog_set_state",
     "chdwf_congrad_static", "chdwf_congrad_batch", "chdwf_set_basis_store",
@@ -186,6 +187,7 @@ def load_library(path: str = LIB_PATH):
     L.chdwf_traj_set_momenta_dev.argtypes = [P, P]
     L.chdwf_timing.argtypes = [P, I]
     L.chdwf_timing_read.argtypes = [P, P, P, P, P]
+    L.chdwf_timing_read_chunks.argtypes = [P, P, P]
     L.chdwf_get_stream.argtypes = [P]
     L.chdwf_get_stream.restype = P
     L.chdwf_kernel_launches.restype = C.c_longlong
@@ -468,8 +470,18 @@ class Program:
         """cudaStream_t of the program's context, as an integer handle."""
         return self.lib.chdwf_get_stream(self.context) or 0
 
-    def timing(self, enable=True):
-        self._check(self.lib.chdwf_timing(self.context, 1 if enable else 0))
+    def timing(self, enable=True, chunks=False):
+        """Solver-kernel timing: per launch (chunks=False), or per graph-replayed
+        chunk of pass-1 iterations (chunks=True, read with timing_chunks)."""
+        self._check(self.lib.chdwf_timing(self.context, (2 if chunks else 1) if enable else 0))
+
+    def timing_chunks(self):
+        """Pass-1 microseconds per iteration from graph-replayed chunks and the
+        iterations timed, per Krylov-vector precision: ([FP64, FP32], [FP64, FP32])."""
+        us = np.zeros(2, dtype=np.float64)
+        its = np.zeros(2, dtype=np.int64)
+        self._check(self.lib.chdwf_timing_read_chunks(self.context, _ptr(us), _ptr(its)))
+        return us, its
 
     def set_basis_store(self, max_bytes):
         """HBM budget of the stored Lanczos basis (bytes; 0 disables, <0 default)."""

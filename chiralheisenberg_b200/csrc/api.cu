@@ -81,13 +81,25 @@ int chdwf_timing(chdwf_ctx* ctx, int enable) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (!c) return CHDWF_BAD_ARG;
     cudaSetDevice(c->device);
+    if (enable < 0 || enable > 2) return CHDWF_BAD_ARG;
     if (enable) {
         c->lz.timer.enable();
         c->lz.timer.reset();
+        c->lz.timer.chunks = enable == 2;
     } else {
         c->lz.timer.release();
     }
     return c->status_of(cudaGetLastError(), "timing");
+}
+
+int chdwf_timing_read_chunks(chdwf_ctx* ctx, double* us_per_iter, long long* iters) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !us_per_iter || !iters) return CHDWF_BAD_ARG;
+    for (int k = 0; k < 2; k++) {
+        iters[k] = c->lz.timer.chunk_iters[k];
+        us_per_iter[k] = iters[k] > 0 ? 1e3 * c->lz.timer.chunk_ms[k] / (double)iters[k] : 0.0;
+    }
+    return CHDWF_OK;
 }
 
 long long chdwf_kernel_launches(void) { return launches_total(); }

@@ -1059,6 +1059,7 @@ static unsigned lz_pass1_blocks_any(const Geom& g, int imass, int occ) {
 void KernelTimer::enable() {
     if (enabled) return;
     for (int i = 0; i < 2 * kPool; i++) cudaEventCreate(&ev[i]);
+    for (int i = 0; i < 2 * kChunkPool; i++) cudaEventCreate(&cev[i]);
     enabled = true;
     reset();
 }
@@ -1066,7 +1067,34 @@ void KernelTimer::enable() {
 void KernelTimer::release() {
     if (!enabled) return;
     for (int i = 0; i < 2 * kPool; i++) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < 2 * kChunkPool; i++) cudaEventDestroy(cev[i]);
     enabled = false;
+    chunks = false;
+}
+
+void KernelTimer::chunk_begin(cudaStream_t st, int first) {
+    if (!enabled || cused >= kChunkPool) return;
+    cfirst[cused] = first;
+    cudaEventRecord(cev[2 * cused], st);
+}
+
+void KernelTimer::chunk_end(cudaStream_t st) {
+    if (!enabled || cused >= kChunkPool) return;
+    cudaEventRecord(cev[2 * cused + 1], st);
+    cused++;
+}
+
+void KernelTimer::collect_chunks(int m, int chunk, int prec) {
+    if (!enabled) return;
+    for (int i = 0; i < cused; i++) {
+        float ms = 0.0f;
+        if (cfirst[i] + chunk - 1 <= m &&
+            cudaEventElapsedTime(&ms, cev[2 * i], cev[2 * i + 1]) == cudaSuccess) {
+            chunk_ms[prec] += ms;
+            chunk_iters[prec] += chunk;
+        }
+    }
+    cused = 0;
 }
 
 void KernelTimer::reset() {
@@ -1077,6 +1105,9 @@ void KernelTimer::reset() {
         count[c] = 0;
         launches[c] = 0;
     }
+    cused = 0;
+    chunk_ms[0] = chunk_ms[1] = 0.0;
+    chunk_iters[0] = chunk_iters[1] = 0;
 }
 
 void KernelTimer::begin(int c, cudaStream_t st, double nbytes) {
@@ -1490,11 +1521,17 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
     // the per-launch path when kernels are being timed, else graph replays
     const cudaAccessPolicyWindow win = vt_window(a.vt, sizeof(T) * (size_t)g.kferm);
     if (win.num_bytes) set_stream_window(st, win);
-    cudaGraphExec_t gexec =
-        w.timer.enabled ? nullptr : pass1_graph<T>(w, a, nb, imass, chunk, st, win);
+    // per-launch timing issues pass 1 launch by launch; chunk timing keeps
+    // the graph replays and brackets each one
+    const bool chunked = w.timer.enabled && w.timer.chunks;
+    cudaGraphExec_t gexec = w.timer.enabled && !chunked
+                                ? nullptr
+                                : pass1_graph<T>(w, a, nb, imass, chunk, st, win);
     while (launched < kMaxIter) {
         if (gexec) {
+            if (chunked) w.timer.chunk_begin(st, launched + 1);
             cudaGraphLaunch(gexec, st);
+            if (chunked) w.timer.chunk_end(st);
             launched += chunk;
             count_launches(3 * chunk);
             note_stencil(pass1_shape(a), 2 * chunk);
@@ -1512,7 +1549,12 @@ static cudaError_t lz_solve_t(LzWork& w, const Geom& g, const double2* phi, floa
         }
         nchunk++;
     }
-    if (w.timer.enabled) {
+    if (chunked) {
+        cudaStreamSynchronize(st);
+        LzCtl hm;
+        cudaMemcpy(&hm, w.ctl, sizeof(hm), cudaMemcpyDeviceToHost);
+        w.timer.collect_chunks(hm.m, chunk, std::is_same<T, float2>::value ? 1 : 0);
+    } else if (w.timer.enabled) {
         // launches after convergence returned at once: drop them
         cudaStreamSynchronize(st);
         LzCtl hm;

@@ -65,6 +65,20 @@ struct KernelTimer {
     void end(cudaStream_t st);
     void collect();                       // after a synchronisation
     void reset();
+    // Chunk mode: pass 1 stays on its graph replays, and events bracket each
+    // replayed chunk instead of each launch, so the time per iteration
+    // carries no per-launch dispatch.  Only chunks that end at or before the
+    // solve's last iteration count.  Per vector precision (0 FP64, 1 FP32).
+    static constexpr int kChunkPool = kMaxIter / 16 + 8;
+    bool chunks = false;
+    cudaEvent_t cev[2 * kChunkPool] = {};
+    int cfirst[kChunkPool] = {};
+    int cused = 0;
+    double chunk_ms[2] = {};
+    long long chunk_iters[2] = {};
+    void chunk_begin(cudaStream_t st, int first);   // first iteration of the chunk
+    void chunk_end(cudaStream_t st);
+    void collect_chunks(int m, int chunk, int prec);   // after a synchronisation
 };
 
 struct LzGraph {

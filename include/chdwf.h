@@ -66,8 +66,15 @@ const char* chdwf_version(void);
  * M^dagger + update, 2: pass-2 accumulation from the stored basis, 3: pass-2
  * regeneration; 4-7: the same classes with FP32 Krylov vectors), the summed
  * milliseconds, the number of timed launches, the number of launches and
- * the algorithmic bytes of the timed launches (arrays of 8). */
+ * the algorithmic bytes of the timed launches (arrays of 8).  enable=2
+ * instead keeps the multi-shift pass 1 on its CUDA-graph replays (as in an
+ * untimed solve) and brackets each replayed chunk of 16 iterations with
+ * events; chdwf_timing_read_chunks then gives, per Krylov-vector precision
+ * (0: FP64, 1: FP32), the microseconds per pass-1 iteration (M, the scalar
+ * step and M^dagger) over the chunks that ended at or before their solve's
+ * last iteration, and the number of iterations timed (arrays of 2). */
 int chdwf_timing(chdwf_ctx* ctx, int enable);
+int chdwf_timing_read_chunks(chdwf_ctx* ctx, double* us_per_iter, long long* iters);
 /* Precision of the Krylov vectors in the resident trajectory solves (no
  * reference counterpart: the reference is FP64 throughout).  md: the two
  * multi-shift solves of every force evaluation; accept: the heatbath and
