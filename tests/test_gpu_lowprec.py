@@ -74,6 +74,42 @@ def test_mixed_precision_trajectory(remez):
         assert abs(a.dH - b.dH) <= 1e-8 * abs(a.H0), (a.dH, b.dH)
 
 
+def test_chunk_timing_keeps_the_trajectory(remez):
+    """Timing mode 2 (events around each graph-replayed chunk of pass 1) runs
+    the same trajectory bit for bit as an untimed sweep, times whole chunks
+    of both vector precisions, and per iteration comes out no slower than
+    the sum of the per-launch event times (mode 1) of the same trajectory."""
+    L, Lt, Ls = 8, 8, 8
+    beta = 0.475
+    chi = np.random.default_rng(4242).standard_normal((3, L * L * Lt)) / np.sqrt(beta)
+    prog = chb.Program(L, Lt, Ls, 0.1, beta, 1.0, 0.01, 0.0, 1, 10, remez["remez2"],
+                       remez["remez4"], remez["remez2g"])
+    prog.set_chi(chi)
+    prog.startup(693764523745.0)
+    prog.set_measure(5, False)
+    prog.set_precision(md="f32", accept="f64")
+    chi0, st0 = prog.get_chi(), prog.get_state()
+    plain = prog.sweep()
+    prog.set_chi(chi0)
+    prog.set_state(st0)
+    prog.timing(True, chunks=True)
+    timed = prog.sweep()
+    us, its = prog.timing_chunks()
+    prog.timing(False)
+    assert (timed.dH, timed.H0, timed.accepted) == (plain.dH, plain.H0, plain.accepted)
+    assert np.all(its > 0) and np.all(its % 16 == 0) and np.all(us > 0), (us, its)
+    prog.set_chi(chi0)
+    prog.set_state(st0)
+    prog.timing(True)
+    prog.sweep()
+    ms, timed_n, _, _ = prog.timing_read()
+    prog.timing(False)
+    prog.close()
+    for prec in (0, 1):
+        per_launch = 1e3 * sum(ms[4 * prec + c] / max(timed_n[4 * prec + c], 1) for c in (0, 1))
+        assert us[prec] <= 1.05 * per_launch, (prec, us[prec], per_launch)
+
+
 @pytest.mark.parametrize("Ls", [5, 6])
 @pytest.mark.parametrize("store", [-1.0, 0.0])
 def test_mixed_force_thread_shapes(remez, Ls, store):
