@@ -277,7 +277,9 @@ def bench_propagators(local_rank, seed=2024, nens=24, nsrc=4, res=1e-8):
     (L=Lt in {8,12,16}, Ls in {8,16,24}, seeded), chi ~ N(0,1), 4 point
     sources each (flavour 1,2 x Dirac 3,4 at a seeded site on s=1),
     Phi = M^dag xi, x0 = Phi as in fermion(); CGNE to residual 1e-8.
-    Returns solves/s one at a time and batched (one set of launches)."""
+    Returns solves/s one at a time and batched (one set of launches), each
+    the median of three timed runs after an untimed one; the batched time
+    includes resetting the initial guesses."""
     import ctypes as C
     import torch
     import chiralheisenberg_b200 as chb
@@ -302,22 +304,40 @@ def bench_propagators(local_rank, seed=2024, nens=24, nsrc=4, res=1e-8):
                                              x.data_ptr(), chi.data_ptr()), Phi, x, chi))
         lats.append(gl)
     torch.cuda.synchronize()
-    # one at a time (the reference's sequence of congrad calls)
-    t0 = time.perf_counter()
-    its1 = []
-    for gl, s, Phi, x, chi in systems:
-        xx = Phi.clone()
-        it = C.c_int()
-        gl.lib.chdwf_congrad_dev(gl.h, C.c_void_p(Phi.data_ptr()), res, C.byref(it), 0.0, 1,
-                                 C.c_void_p(chi.data_ptr()), C.c_void_p(xx.data_ptr()))
-        its1.append(it.value)
-    torch.cuda.synchronize()
-    t_one = time.perf_counter() - t0
-    # batched
-    t0 = time.perf_counter()
-    its2, sts = chb.congrad_batch(lats[0], [s for _, s, _, _, _ in systems], res)
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
+
+    def one_at_a_time():
+        # the reference's sequence of congrad calls
+        its = []
+        for gl, s, Phi, x, chi in systems:
+            xx = Phi.clone()
+            it = C.c_int()
+            gl.lib.chdwf_congrad_dev(gl.h, C.c_void_p(Phi.data_ptr()), res, C.byref(it), 0.0, 1,
+                                     C.c_void_p(chi.data_ptr()), C.c_void_p(xx.data_ptr()))
+            its.append(it.value)
+        torch.cuda.synchronize()
+        return its
+
+    def batched():
+        for _, _, Phi, x, _ in systems:
+            x.copy_(Phi)                      # the same initial guess every run
+        torch.cuda.synchronize()
+        out = chb.congrad_batch(lats[0], [s for _, s, _, _, _ in systems], res)
+        torch.cuda.synchronize()
+        return out
+
+    # one untimed run of each (first-call set-up, graph capture), then the
+    # median of three timed runs
+    one_at_a_time()
+    batched()
+    t_ones, t_batches = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        its1 = one_at_a_time()
+        t_ones.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        its2, sts = batched()
+        t_batches.append(time.perf_counter() - t0)
+    t_one, t_batch = float(np.median(t_ones)), float(np.median(t_batches))
     for gl in lats:
         gl.close()
     n = len(systems)
