@@ -159,21 +159,20 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
     typedef typename real_of<T>::type Real;
     typedef LzShape<T, PAIR> S;
     constexpr int NF = S::split ? 1 : 2;
+    // One flavour a thread: beta_j is first needed to scale the block's
+    // first outputs, so its sum over the previous launch's partials (an L2
+    // round trip and two block barriers) is formed after the first pass's
+    // stencil loads are issued.  Every thread of the block reaches it (the
+    // loop's trip count is the same for the whole block).
+    constexpr bool LATE = NF == 1;
     LzCtl* ctl = a.ctl;
     if (block_stopped(ctl)) return;
     const int j = ctl->it_m;
     const int nb = gridDim.x;
-    const double bj = j == 1 ? a.h.beta[1] : sqrt(sum_partials(a.part + nb, nb));
-    const double ibj = j == 1 ? a.h.invbeta[1] : 1.0 / bj;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->it_md = j;
-        if (j > 1) {
-            a.h.beta[j] = bj;
-            a.h.invbeta[j] = ibj;
-        }
-    }
+    bool have = j == 1 || !LATE;
+    double bj = j == 1 ? a.h.beta[1] : (LATE ? 0.0 : sqrt(sum_partials(a.part + nb, nb)));
+    double ibj = j == 1 ? a.h.invbeta[1] : (LATE ? 0.0 : 1.0 / bj);
     const T* rj = ring(a, j);
-    const Real ib = (Real)ibj;
     const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
 #pragma unroll 1
@@ -181,12 +180,20 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
         int64_t p;
         int f0;
         lz_lane<T, PAIR>(base, &p, &f0);
-        if (p >= R.end) continue;
-        const PointIdx q = point_of(a.g, p);
+        const bool act = p < R.end;
+        const PointIdx q = point_of(a.g, act ? p : R.begin);
         if constexpr (PAIR) {
             cpair acc[4];
-            dwf_apply_flavour_pair_sp<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag, a.hpin,
-                                                    a.apbc != 0);
+            if (act)
+                dwf_apply_flavour_pair_sp<false, IMASS>(acc, rj, a.g, q, f0, a.chif, a.diag,
+                                                        a.hpin, a.apbc != 0);
+            if (!have) {
+                bj = sqrt(sum_partials(a.part + nb, nb));
+                ibj = 1.0 / bj;
+                have = true;
+            }
+            if (!act) continue;
+            const Real ib = (Real)ibj;
             // |vt|^2 is summed in FP64 from the first term: a pair's partial
             // sum in FP32 made the FP32 force solves 7% longer (alpha~ and
             // beta steer the recurrences)
@@ -198,7 +205,28 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
                 loc += w0.x * w0.x + w0.y * w0.y;
                 loc += w1.x * w1.x + w1.y * w1.y;
             }
+        } else if constexpr (LATE) {
+            T acc[4];
+            if (act)
+                dwf_apply_flavour<false, IMASS>(acc, LdPlainT<T>{rj}, a.g, q, f0, a.chif, a.diag,
+                                                a.hpin, a.apbc != 0);
+            if (!have) {
+                bj = sqrt(sum_partials(a.part + nb, nb));
+                ibj = 1.0 / bj;
+                have = true;
+            }
+            if (!act) continue;
+            const Real ib = (Real)ibj;
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                const T v = zscal(ib, acc[d]);   // apply_scaled's scaling
+                a.vt[p + a.g.cs * (d + 4 * f0)] = v;
+                const double2 w = widen(v);
+                loc += w.x * w.x + w.y * w.y;
+            }
         } else {
+            if (!act) continue;
+            const Real ib = (Real)ibj;
 #pragma unroll
             for (int f = f0; f < f0 + NF; f++) {
                 T acc[4];
@@ -210,6 +238,17 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_M(LzArgsT<T> a) {
                     loc += w.x * w.x + w.y * w.y;
                 }
             }
+        }
+    }
+    if (!have) {   // a block whose range is empty
+        bj = sqrt(sum_partials(a.part + nb, nb));
+        ibj = 1.0 / bj;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->it_md = j;
+        if (j > 1) {
+            a.h.beta[j] = bj;
+            a.h.invbeta[j] = ibj;
         }
     }
     __shared__ double sh[kThreads / 32];
@@ -331,11 +370,15 @@ template <class T, int IMASS, bool PAIR, bool WALLS, int OCC>
 __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
     typedef LzShape<T, PAIR> S;
     constexpr int NF = S::split ? 1 : 2;
+    // alpha~_j, as beta_j in k_lz1_M, is summed after the first pass's
+    // stencil (one flavour a thread)
+    constexpr bool LATE = NF == 1;
     LzCtl* ctl = a.ctl;
     if (block_stopped(ctl)) return;
     const int j = ctl->it_md;
     const int nb = gridDim.x;
-    const double at = sum_partials(a.part, nb);
+    bool have = !LATE;
+    double at = LATE ? 0.0 : sum_partials(a.part, nb);
     T* rn = ring(a, j + 1);
     const PtRange R = block_range(a.g.npts);
     double loc = 0.0;
@@ -344,12 +387,18 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
         int64_t p;
         int f0;
         lz_lane<T, PAIR>(base, &p, &f0);
-        if (p >= R.end) continue;
-        const PointIdx q = point_of(a.g, p);
+        const bool act = p < R.end;
+        const PointIdx q = point_of(a.g, act ? p : R.begin);
         if constexpr (PAIR) {
             cpair acc[4];
-            dwf_apply_flavour_pair_sp<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag, a.hpin,
-                                                   a.apbc != 0);
+            if (act)
+                dwf_apply_flavour_pair_sp<true, IMASS>(acc, a.vt, a.g, q, f0, a.chif, a.diag,
+                                                       a.hpin, a.apbc != 0);
+            if (!have) {
+                at = sum_partials(a.part, nb);
+                have = true;
+            }
+            if (!act) continue;
 #pragma unroll
             for (int d = 0; d < 4; d++) {
                 const uint32_t e = (uint32_t)p + (uint32_t)a.g.cs * (uint32_t)(d + 4 * f0);
@@ -365,15 +414,24 @@ __global__ void __launch_bounds__(kThreads, OCC) k_lz1_Md(LzArgsT<T> a) {
                 loc += w1.x * w1.x + w1.y * w1.y;
             }
         } else {
+            T acc[NF][4];
+            if (LATE && act)
+                dwf_apply_flavour<true, IMASS>(acc[0], LdPlainT<T>{a.vt}, a.g, q, f0, a.chif,
+                                               a.diag, a.hpin, a.apbc != 0);
+            if (!have) {
+                at = sum_partials(a.part, nb);
+                have = true;
+            }
+            if (!act) continue;
 #pragma unroll
             for (int f = f0; f < f0 + NF; f++) {
-                T acc[4];
-                dwf_apply_flavour<true, IMASS>(acc, LdPlainT<T>{a.vt}, a.g, q, f, a.chif, a.diag,
-                                               a.hpin, a.apbc != 0);
+                if (!LATE)
+                    dwf_apply_flavour<true, IMASS>(acc[f - f0], LdPlainT<T>{a.vt}, a.g, q, f,
+                                                   a.chif, a.diag, a.hpin, a.apbc != 0);
 #pragma unroll
                 for (int d = 0; d < 4; d++) {
                     const int64_t e = p + a.g.cs * (d + 4 * f);
-                    const T v = three_term(a, acc[d], e, j, at);
+                    const T v = three_term(a, acc[f - f0][d], e, j, at);
                     rn[e] = v;
                     if (WALLS) wall_put(a, j + 1, q.s, q.site, d + 4 * f, v);
                     const double2 w = widen(v);
