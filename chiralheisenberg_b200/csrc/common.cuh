@@ -9,7 +9,10 @@
 // point-fastest with the fifth dimension s innermost.  One thread owns one
 // lattice point (s, site) and all eight components, so every plane access of
 // a warp is a contiguous, coalesced run of 16-byte (FP64) elements and the
-// host<->device copies at the drop-in boundary are plain memcpys.
+// host<->device copies at the drop-in boundary are plain memcpys.  The
+// solver's FP32 Krylov vectors (Ls even, never copied across the boundary)
+// keep the same planes with each pair of adjacent s split by part: see
+// cpair below.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
