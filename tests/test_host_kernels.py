@@ -20,7 +20,7 @@ compares.
 A fourth program compares the FP32 two-point operator on the solver's
 split vector layout (dwf_apply_flavour_pair_sp, whose additions are packed
 FP32x2 instructions on the GPU) with the plain-layout one, element by
-element.
+element, and a fifth checks that layout's element accessors.
 
 It checks the arithmetic of the kernel bodies only; the device build, the
 launch shapes and the solvers are checked by the -m gpu tests.
@@ -249,6 +249,39 @@ int main(int argc, char** argv) {
 """
 
 
+# Element accessors of the split layout (common.cuh): sp_put of a plain
+# vector, read back with sp_get and as element pairs with ld_cpair /
+# cpair_pt, then a st_cpair round trip.  Prints the number of mismatches.
+ACCESS_PROGRAM = RHMC_PROGRAM.split("using namespace chdwf;")[0] + r"""
+using namespace chdwf;
+int main(int argc, char** argv) {
+    const int64_t n = atoll(argv[1]);
+    std::vector<float2> plain(n), sp(n), back(n);
+    for (int64_t e = 0; e < n; e++) plain[e] = make_float2(0.5f * e + 0.25f, -1.0f * e - 0.75f);
+    for (int64_t e = n - 1; e >= 0; e--) sp_put(sp.data(), e, plain[e]);   // any order
+    long long bad = 0;
+    for (int64_t e = 0; e < n; e++) {
+        const float2 v = sp_get(sp.data(), e);
+        if (v.x != plain[e].x || v.y != plain[e].y) bad++;
+    }
+    const float* f = reinterpret_cast<const float*>(sp.data());
+    for (int64_t e = 0; e < n; e += 2) {
+        if (f[2 * e] != plain[e].x || f[2 * e + 1] != plain[e + 1].x ||
+            f[2 * e + 2] != plain[e].y || f[2 * e + 3] != plain[e + 1].y) bad++;
+        const cpair c = ld_cpair(sp.data(), (uint32_t)e);
+        for (int k = 0; k < 2; k++) {
+            const float2 v = cpair_pt(c, k);
+            if (v.x != plain[e + k].x || v.y != plain[e + k].y) bad++;
+        }
+        st_cpair(back.data(), (uint32_t)e, c);
+    }
+    if (memcmp(back.data(), sp.data(), sizeof(float2) * n) != 0) bad++;
+    printf("%lld\n", bad);
+    return 0;
+}
+"""
+
+
 def _section(src, start, end):
     a, b = src.find(start), src.find(end)
     assert a >= 0 and b > a, f"section markers moved: {start!r} .. {end!r}"
@@ -283,6 +316,12 @@ def rhmc_exe(tmp_path_factory):
 @pytest.fixture(scope="module")
 def split_exe(tmp_path_factory):
     return _build(str(tmp_path_factory.mktemp("split")), "split", SPLIT_PROGRAM,
+                  extra=["-I", CSRC])
+
+
+@pytest.fixture(scope="module")
+def access_exe(tmp_path_factory):
+    return _build(str(tmp_path_factory.mktemp("access")), "access", ACCESS_PROGRAM,
                   extra=["-I", CSRC])
 
 
@@ -345,6 +384,15 @@ def test_fp32_split_layout_matches_plain_pair(split_exe, tmp_path, shape):
                          capture_output=True, text=True).stdout.split()
     bad, total = int(out[0]), int(out[1])
     assert total == 2 * 2 * 2 * n and bad == 0, (bad, total)
+
+
+def test_split_layout_accessors(access_exe):
+    """sp_put / sp_get / ld_cpair / st_cpair agree with the split layout's
+    definition: element pair (e, e+1), e even, stored as (re_e, re_e+1,
+    im_e, im_e+1)."""
+    out = subprocess.run([access_exe, "4096"], check=True, capture_output=True,
+                         text=True).stdout.split()
+    assert int(out[0]) == 0
 
 
 @pytest.mark.parametrize("shape", [(4, 4, 4), (3, 2, 5), (6, 4, 8)])
