@@ -69,6 +69,27 @@ EXT = dict(npf=2, nsteps=10, integrator="omelyan", poles=20, rescga=1e-9, rescgg
 PROFILE_EXT = os.path.join(ROOT, "profiles", "iteration_profile_ext_24x24.json")
 
 
+# ---- replicas (one independent Markov chain per rank) -----------------------
+def replica_seed(seed, rank):
+    """The reference generator's seed of rank's chain: rank 0 runs the
+    single-GPU chain, every other rank an independent one."""
+    return seed + 1000.0 * rank
+
+
+def max_over_ranks(ms, world, device):
+    """The slowest rank's elapsed milliseconds (every rank gets it)."""
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def seconds_per_trajectory(ms_max, steps, world):
+    """Whole-job figure: world chains of steps trajectories each in ms_max."""
+    return (ms_max / 1e3) / (steps * world)
+
+
 def con_path(L, Ls):
     return os.path.join(DATA, f"con_{L}x{L}x{Ls}_b{CFG['beta']}")
 
@@ -202,7 +223,7 @@ def make_program(L, Ls, local_rank, rank=0, ext=True):
         chi, seed = synthetic_chi(L, L, CFG["beta"], CFG["chi_seed"]), CFG["seed"]
         start = "raw N(0,1/beta) seeded"
     prog.set_chi(chi)
-    prog.startup(seed + 1000.0 * rank)
+    prog.startup(replica_seed(seed, rank))
     prog.set_measure(5, False)
     if ext:
         hb, act = ext_sets()
@@ -641,10 +662,7 @@ def timed_run(prog, stream, steps, staged, barrier, world, local_rank):
     barrier()
     ms = ev[0].elapsed_time(ev[-1])
     per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
-    t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item()), recs, per_step
+    return max_over_ranks(ms, world, f"cuda:{local_rank}"), recs, per_step
 
 
 def instrumented(prog, chi0, state0):
@@ -745,7 +763,7 @@ def run_b200(args, rank, world, local_rank):
         dh = [abs(a.dH - b.dH) for a, b in zip(recs, recs64)]
         dh_rel = [abs(a.dH - b.dH) / abs(b.H0) for a, b in zip(recs, recs64)]
         prof64 = profile_of(recs64)
-        fp64 = {"value": (ms64 / 1e3) / (args.steps * world), "unit": "s",
+        fp64 = {"value": seconds_per_trajectory(ms64, args.steps, world), "unit": "s",
                 "speedup_of_value": ms64 / ms_value,
                 "dH_max_abs_diff": max(dh), "dH_max_diff_rel_H0": max(dh_rel),
                 "dH_rms_fp64": float(np.sqrt(np.mean([b.dH ** 2 for b in recs64]))),
@@ -762,16 +780,15 @@ def run_b200(args, rank, world, local_rank):
         ms_r, recs_r, _ = timed_run(rprog, stream_of(rprog, local_rank), args.refalg_steps, True,
                                     barrier, world, local_rank)
         its = sum(r.it_pf + r.it_h0 + r.it_h1 + r.it_guid + r.it_force for r in recs_r)
-        refalg = {"value": (ms_r / 1e3) / (args.refalg_steps * world), "unit": "s",
+        refalg = {"value": seconds_per_trajectory(ms_r, args.refalg_steps, world), "unit": "s",
                   "precision": "fp64 (the drop-in)", "trajectories": args.refalg_steps,
                   "ms_per_1000_iterations": ms_r / its * 1e3,
                   "nforce": [r.nforce for r in recs_r],
                   "algorithm": "1 pseudofermion, shipped remez2/remez4/remez2g, leapfrog dt=0.1 "
                                "with random length (iterl=10), as rhmc/cheisdwf.f"}
         rprog.close()
-    ntraj = args.steps * world
-    value = (ms_value / 1e3) / ntraj
-    e2e = (ms_e2e / 1e3) / ntraj
+    value = seconds_per_trajectory(ms_value, args.steps, world)
+    e2e = seconds_per_trajectory(ms_e2e, args.steps, world)
     kvol = L * L * L
     h2d = EXT["npf"] * 64 * kvol * Ls + 12 * kvol      # heatbath Gaussians + momenta
     d2h = 12 * kvol + 64                               # momenta for vel2 + scalars
